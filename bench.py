@@ -1,0 +1,424 @@
+#!/usr/bin/env python
+"""Census+SGM throughput on B200: batched pairs vs one pair per call.
+
+Workload (default ``batch64``): 64 rectified pairs of uneven size (width
+log-uniform in 1024..6048, aspect 3:2 or 4:3), 8-bit synthetic images lifted
+to 16 bit, label ranges drawn from {64, 128, 192, 256, 384}; half of the pairs
+use the 4-level hierarchy with +-8 labels around the upsampled coarse
+disparity (range_radius 0, range_margin 8), half a single full-range level.
+A step matches the whole batch with one call of the batch C ABI. The metric
+counts W*H*D cells of the full label range at level 0 per pair (the
+reference's convention), in Gcells/s over the whole job.
+
+  value  device-resident inputs and outputs, CUDA events on the launching stream
+  e2e    same call with pinned host buffers: the step's host->device copies of
+         all images and the device->host read of all disparity maps inside the
+         timed region
+  per_pair  the same pairs matched one call per pair (the plain GPU matcher)
+
+`python bench.py --impl reference` times the CPU oracle (a restatement of the
+reference matcher, all host threads) on a bounded sample of the same pairs.
+Under torchrun every rank matches its own batch (weak scaling); the time is
+the maximum over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Census+SGM Gcells/s (W·H·D) batched vs per-pair, bit-exact; p50/p99 latency"
+ND_CHOICES = (64, 128, 192, 256, 384)
+# Algorithmic HBM bytes of the SGM tile kernel: the forward partial sum S
+# (u16) written once and read once per aggregated cell, plus per tile pixel
+# the two Census codes read (2 x 8 B) and disparity + confidence written (8 B).
+ALG_BYTES_PER_CELL = 4
+ALG_BYTES_PER_PIXEL = 24
+# Integer operations per aggregated cell (8 paths x ~7 ops, 8 sum adds, cost).
+INT_OPS_PER_CELL = 66
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640"), default="batch64")
+    ap.add_argument("--pairs", type=int, default=64)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-per-pair", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_pairs(name: str, npairs: int, seed: int):
+    """(width, height, nd, options dict) per pair, deterministic."""
+    rng = np.random.default_rng(seed)
+    out = []
+    if name == "pair640":
+        return [dict(w=640, h=480, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
+    if name == "pair3072":
+        return [dict(w=3072, h=2048, nd=256, levels=3, radius=0, margin=8, textureless=0.15, occluded=0.10,
+                     seed=seed)]
+    for i in range(npairs):
+        w = int(round(math.exp(rng.uniform(math.log(1024), math.log(6048)))))
+        aspect = 1.5 if rng.random() < 0.5 else 4.0 / 3.0
+        h = int(round(w / aspect))
+        nd = int(ND_CHOICES[rng.integers(0, len(ND_CHOICES))])
+        hier = i % 2 == 1
+        out.append(dict(w=w, h=h, nd=nd, levels=3 if hier else 0, radius=0 if hier else 3, margin=8 if hier else 4,
+                        textureless=0.0, occluded=0.0, seed=seed * 1000 + i))
+    return out
+
+
+def make_images(lib, spec):
+    from regard3d_mvs_b200.types import CSynthParams
+
+    p = CSynthParams(spec["w"], spec["h"], spec["nd"], spec["seed"] & 0xFFFFFFFF, 1.5, 2.0, 8,
+                     spec["textureless"], spec["occluded"])
+    L = np.empty((spec["h"], spec["w"]), np.uint8)
+    R = np.empty_like(L)
+    st = lib.r3dgpu_synth_pair(ctypes.byref(p), L.ctypes.data, R.ctypes.data, None)
+    if st != 0:
+        raise RuntimeError(f"synth failed: {st}")
+    return L.astype(np.uint16) * np.uint16(257), R.astype(np.uint16) * np.uint16(257)
+
+
+def options_for(spec):
+    from regard3d_mvs_b200.types import StereoOptions
+
+    return StereoOptions(levels=spec["levels"], range_radius=spec["radius"], range_margin=spec["margin"])
+
+
+def full_range_cells(specs) -> int:
+    return sum(s["w"] * s["h"] * ((s["nd"] + 15) // 16 * 16) for s in specs)
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.samples = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def summary(self):
+        if not getattr(self, "samples", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(p[0]) for p in self.samples if p[0].replace(".", "").isdigit()]
+        mx = [float(p[1]) for p in self.samples if p[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for p in self.samples for k in range(4) if p[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def sgm_traffic_per_cell():
+    """DRAM bytes per aggregated cell of the SGM kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "sgm_tile_kernel_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_cell"]), float(d.get("dram_bytes_per_pixel", 0.0))
+    return None, None
+
+
+def cpu_baseline(specs, seconds_target=15.0):
+    """The oracle on a bounded sample: the smallest pair of the workload,
+    full matcher, all host threads."""
+    from oracle import oracle
+    from regard3d_mvs_b200 import _native
+
+    lib = _native.load()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    spec = min(specs, key=lambda s: s["w"] * s["h"] * s["nd"])
+    L, R = make_images(lib, spec)
+    t0 = time.perf_counter()
+    r = oracle.match_stereo(L, R, None, None, 0, spec["nd"], options_for(spec))
+    dt = time.perf_counter() - t0
+    cells = spec["w"] * spec["h"] * ((spec["nd"] + 15) // 16 * 16)
+    return {"value": cells / dt / 1e9, "unit": "Gcells/s", "cores": threads, "kind": "port",
+            "sample": f"one {spec['w']}x{spec['h']} pair, {spec['nd']} labels, levels {spec['levels']}, "
+                      f"{dt:.2f} s, {r.cells} aggregated cells"}
+
+
+def run_reference(args, rank, world):
+    """The CPU oracle (restatement of the reference matcher) on a bounded
+    sample of the workload: each step matches one pair, cropped to at most
+    1536 px wide, with all host threads."""
+    if rank != 0:
+        return
+    from oracle import oracle
+    from regard3d_mvs_b200 import _native
+
+    lib = _native.load()
+    threads = os.cpu_count() or 1
+    oracle.set_threads(threads)
+    specs = workload_pairs(args.workload, args.pairs, args.seed)
+    sample = []
+    for s in specs:
+        c = dict(s)
+        if c["w"] > 1536:
+            c["h"] = int(round(c["h"] * 1536 / c["w"]))
+            c["w"] = 1536
+        sample.append(c)
+    imgs = [make_images(lib, s) for s in sample[: args.warmup + args.steps]] if len(sample) >= args.warmup + args.steps \
+        else [make_images(lib, sample[i % len(sample)]) for i in range(args.warmup + args.steps)]
+    cells = 0
+    elapsed = 0.0
+    for i in range(args.warmup + args.steps):
+        s = sample[i % len(sample)]
+        L, R = imgs[i]
+        t0 = time.perf_counter()
+        oracle.match_stereo(L, R, None, None, 0, s["nd"], options_for(s))
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            elapsed += dt
+            cells += s["w"] * s["h"] * ((s["nd"] + 15) // 16 * 16)
+    value = cells / elapsed / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "Gcells/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": args.workload, "sample": "one pair per step, cropped to <= 1536 px wide"},
+            "cpu_baseline": {"value": value, "unit": "Gcells/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} pairs of the {args.workload} list, one per step, <= 1536 px wide"},
+            "e2e": {"value": value, "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = dist_mod
+
+    from regard3d_mvs_b200 import Matcher
+    from regard3d_mvs_b200.types import CDisparityMap, CPair, CProfile, CViewU8, CViewU16, to_c_options
+
+    m = Matcher(device=local)
+    lib = m.lib
+    specs = workload_pairs(args.workload, args.pairs, args.seed + 7919 * rank)
+    host = [make_images(lib, s) for s in specs]
+    dev = torch.device(f"cuda:{local}")
+    stream = torch.cuda.current_stream(dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    # Device-resident inputs and outputs.
+    dL = [torch.from_numpy(L.view(np.int16)).to(dev) for L, _ in host]
+    dR = [torch.from_numpy(R.view(np.int16)).to(dev) for _, R in host]
+    dD = [torch.empty((s["h"], s["w"]), dtype=torch.float32, device=dev) for s in specs]
+    dC = [torch.empty((s["h"], s["w"]), dtype=torch.float32, device=dev) for s in specs]
+    n = len(specs)
+    pairs = (CPair * n)()
+    for i, s in enumerate(specs):
+        p = pairs[i]
+        p.left = CViewU16(dL[i].data_ptr(), s["w"], s["h"], s["w"])
+        p.right = CViewU16(dR[i].data_ptr(), s["w"], s["h"], s["w"])
+        p.left_valid = CViewU8()
+        p.right_valid = CViewU8()
+        p.disparity_min = 0
+        p.num_disparities = s["nd"]
+        p.options = to_c_options(options_for(s))
+        p.out = CDisparityMap(dD[i].data_ptr(), dC[i].data_ptr(), s["w"], 0, 0, 0, 0, 0)
+
+    def step():
+        st = lib.r3dgpu_match_stereo_batch(pairs, n, sptr)
+        if st != 0:
+            raise RuntimeError(lib.r3dgpu_last_error().decode())
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cells_full = full_range_cells(specs)
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    lib.r3dgpu_profile_enable(1)
+    prof = CProfile()
+    lib.r3dgpu_profile_take(ctypes.byref(prof))
+    launches0 = lib.r3dgpu_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        barrier()
+    launches = lib.r3dgpu_launch_count() - launches0
+    lib.r3dgpu_profile_take(ctypes.byref(prof))
+    lib.r3dgpu_profile_enable(0)
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = world * cells_full * args.steps / (ms * 1e-3) / 1e9
+    total_cells = sum(int(pairs[i].out.cells) for i in range(n))
+
+    # End to end: pinned host buffers, copies inside the timed region.
+    hL = [torch.from_numpy(L.view(np.int16)).pin_memory() for L, _ in host]
+    hR = [torch.from_numpy(R.view(np.int16)).pin_memory() for _, R in host]
+    hD = [torch.empty((s["h"], s["w"]), dtype=torch.float32).pin_memory() for s in specs]
+    h2d = sum(t.numel() * 2 for t in hL) + sum(t.numel() * 2 for t in hR)
+    d2h = sum(t.numel() * 4 for t in hD)
+
+    def e2e_step():
+        for i in range(n):
+            dL[i].copy_(hL[i], non_blocking=True)
+            dR[i].copy_(hR[i], non_blocking=True)
+        step()
+        for i in range(n):
+            hD[i].copy_(dD[i], non_blocking=True)
+
+    e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * cells_full * args.steps / (e2e_ms * 1e-3) / 1e9
+
+    # Plain GPU matcher: one call per pair (same kernels, no batching).
+    per_pair = None
+    if not args.no_per_pair:
+        lat = []
+        barrier()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for i in range(n):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            st = lib.r3dgpu_match_stereo(ctypes.byref(pairs[i].left), ctypes.byref(pairs[i].right),
+                                         ctypes.byref(pairs[i].left_valid), ctypes.byref(pairs[i].right_valid),
+                                         pairs[i].disparity_min, pairs[i].num_disparities,
+                                         ctypes.byref(pairs[i].options), ctypes.byref(pairs[i].out), sptr)
+            if st != 0:
+                raise RuntimeError(lib.r3dgpu_last_error().decode())
+            b.record(stream)
+            lat.append((a, b))
+        p1.record(stream)
+        barrier()
+        pp_ms = max_over_ranks(p0.elapsed_time(p1))
+        lats = sorted(a.elapsed_time(b) for a, b in lat)
+        per_pair = {"value": world * cells_full / (pp_ms * 1e-3) / 1e9, "unit": "Gcells/s", "ms_per_batch": pp_ms,
+                    "latency_ms": {"p50": float(np.percentile(lats, 50)), "p99": float(np.percentile(lats, 99)),
+                                   "max": lats[-1]}}
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        sgm_ms = prof.sgm_ms / max(prof.sgm_launches, 1)
+        alg_bytes = (ALG_BYTES_PER_CELL * prof.sgm_cells + ALG_BYTES_PER_PIXEL * prof.sgm_pixels) / max(prof.sgm_launches, 1)
+        achieved = alg_bytes / (sgm_ms * 1e-3) / 1e9 if sgm_ms > 0 else 0.0
+        tpc, tpp = sgm_traffic_per_cell()
+        traffic = None
+        if tpc is not None:
+            traffic = (tpc * prof.sgm_cells + tpp * prof.sgm_pixels) / max(prof.sgm_launches, 1)
+        sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+        clocks = clk.summary()
+        int_peak = sm_count * 128 * (clocks.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
+        int_achieved = INT_OPS_PER_CELL * prof.sgm_cells / max(prof.sgm_ms * 1e-3, 1e-12) / 1e12
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": args.workload, "pairs": n, "full_range_cells_per_step": cells_full,
+                       "aggregated_cells_per_step": total_cells, "l2": "inputs larger than L2 (126 MB)",
+                       "parallelism": f"weak: {world} rank(s), each its own batch"},
+            "e2e": {"value": e2e_value, "unit": "Gcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_ms / args.steps},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "sgm_tile_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "avg_launch_ms": sgm_ms, "launches": int(prof.sgm_launches),
+                         "alg_bytes_per_launch": alg_bytes,
+                         "sgm_share_of_step": prof.sgm_ms / max(ms, 1e-9)},
+            "int_roofline": {"ops_per_cell": INT_OPS_PER_CELL, "achieved_tops": int_achieved,
+                             "nominal_int32_tops": int_peak, "frac": int_achieved / int_peak},
+            "clocks": clocks,
+        }
+        if per_pair is not None:
+            line["per_pair"] = per_pair
+            line["batched_vs_per_pair"] = value / per_pair["value"]
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(specs)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

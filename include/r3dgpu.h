@@ -1,0 +1,211 @@
+/*
+ * r3dgpu — B200-native Census+SGM stereo matcher, C ABI.
+ *
+ * Drop-in replacement for the matcher of R3DMVS (rhiestan/Regard3D_MVS):
+ * every entry point below names the reference interface it replaces
+ * (path within the reference project, file:line). The library computes on
+ * the GPU only; there is no CPU fallback. Every call returns an r3dgpu_status
+ * and leaves a thread-local message for r3dgpu_last_error().
+ *
+ * Images are non-owning strided views (the reference's ImageView,
+ * src/r3d/core/image.hpp:15-60): `stride` is in elements. Entry points whose
+ * name ends in _host take host pointers and copy inside the call; the others
+ * take device pointers.
+ */
+#ifndef R3DGPU_H
+#define R3DGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the reference throws r3d::Error / r3d::Cancelled /
+ * std::bad_alloc at the same points, src/r3d/core/error.hpp:10-30,
+ * src/r3d/core/cancel.hpp:9-13). */
+typedef enum r3dgpu_status {
+  R3DGPU_OK = 0,
+  R3DGPU_EINVAL = 1,     /* invalid options, sizes or ranges (r3d::Error) */
+  R3DGPU_ECANCELLED = 2, /* cancellation requested (r3d::Cancelled) */
+  R3DGPU_ENOMEM = 3,     /* device or host allocation failed (std::bad_alloc) */
+  R3DGPU_EDEVICE = 4,    /* CUDA error, or no usable sm_100 device */
+  R3DGPU_ETIMEOUT = 5,   /* a bounded device-side wait gave up */
+  R3DGPU_EUNSUPPORTED = 6 /* valid input beyond this build's limits (e.g. labels per pixel) */
+} r3dgpu_status;
+
+/* SubpixelMethod, src/r3d/stereo/stereo_matcher.hpp:23-27 (same order). */
+enum { R3DGPU_SUBPIXEL_NONE = 0, R3DGPU_SUBPIXEL_PARABOLA = 1, R3DGPU_SUBPIXEL_EQUIANGULAR = 2 };
+
+/* StereoOptions, src/r3d/stereo/stereo_matcher.hpp:30-57: same fields, same
+ * meaning, same defaults (r3dgpu_default_options). `scalar_kernels` is kept
+ * for layout parity and ignored. */
+typedef struct r3dgpu_stereo_options {
+  int32_t p1;
+  int32_t p2;
+  int32_t p2_adapt;
+  int32_t invalid_cost;
+  int32_t subpixel;
+  float uniqueness;
+  int32_t lr_max_diff;
+  int32_t lr_full_match;
+  int32_t speckle_size;
+  float speckle_diff;
+  int32_t median;
+  int32_t levels;
+  int32_t range_radius;
+  int32_t range_margin;
+  int32_t range_fill;
+  int32_t tile_size;
+  int32_t tile_margin;
+  int32_t tile_blend;
+  uint64_t memory_budget;
+  int32_t scalar_kernels;
+  int32_t reserved;
+} r3dgpu_stereo_options;
+
+/* ImageView<const T> (src/r3d/core/image.hpp:15-60), single channel. A view
+ * with data == NULL or a zero size is "empty" (masks: all pixels valid). */
+typedef struct r3dgpu_view_u16 {
+  const uint16_t* data;
+  int32_t width;
+  int32_t height;
+  int64_t stride;
+} r3dgpu_view_u16;
+
+typedef struct r3dgpu_view_u8 {
+  const uint8_t* data;
+  int32_t width;
+  int32_t height;
+  int64_t stride;
+} r3dgpu_view_u8;
+
+/* DisparityMap, src/r3d/stereo/stereo_matcher.hpp:61-68. The caller owns
+ * `disparity` and `confidence` (width x height floats, row stride `stride`
+ * elements, host memory for _host calls, device memory otherwise);
+ * confidence may be NULL. Invalid disparities are +inf. */
+typedef struct r3dgpu_disparity_map {
+  float* disparity;
+  float* confidence;
+  int64_t stride;
+  int32_t disparity_min;   /* out */
+  int32_t num_disparities; /* out: rounded up to 16 */
+  int32_t levels;          /* out: coarser pyramid levels used */
+  int32_t reserved;
+  uint64_t cells;          /* out: aggregated (pixel, label) cells, all levels, both directions */
+} r3dgpu_disparity_map;
+
+/* Message of the last failed call on this thread ("" after success). */
+const char* r3dgpu_last_error(void);
+
+/* Reference defaults (StereoOptions{}). */
+void r3dgpu_default_options(r3dgpu_stereo_options* out);
+
+/* Number of coarser levels chosen by levels = -1.
+ * Replaces r3d::detail::automatic_levels, src/r3d/stereo/stereo_matcher.cpp:1105-1122. */
+int32_t r3dgpu_automatic_levels(int32_t width, int32_t height, int32_t num_disparities);
+
+/* Selects the CUDA device used by this thread's later calls (default 0). */
+r3dgpu_status r3dgpu_set_device(int32_t device);
+
+/* Matches a rectified pair (host images, host outputs; copies inside).
+ * Replaces r3d::match_stereo, src/r3d/stereo/stereo_matcher.hpp:82-85
+ * (implementation src/r3d/stereo/stereo_matcher.cpp:1023-1095). */
+r3dgpu_status r3dgpu_match_stereo_host(const r3dgpu_view_u16* left, const r3dgpu_view_u16* right,
+                                       const r3dgpu_view_u8* left_valid, const r3dgpu_view_u8* right_valid,
+                                       int32_t disparity_min, int32_t num_disparities,
+                                       const r3dgpu_stereo_options* options, r3dgpu_disparity_map* out);
+
+/* Same with device-resident images and outputs; runs on `stream`
+ * (cudaStream_t, NULL = legacy default stream) and synchronises it. */
+r3dgpu_status r3dgpu_match_stereo(const r3dgpu_view_u16* left, const r3dgpu_view_u16* right,
+                                  const r3dgpu_view_u8* left_valid, const r3dgpu_view_u8* right_valid,
+                                  int32_t disparity_min, int32_t num_disparities,
+                                  const r3dgpu_stereo_options* options, r3dgpu_disparity_map* out, void* stream);
+
+/* One pair of a batch (device pointers). */
+typedef struct r3dgpu_pair {
+  r3dgpu_view_u16 left;
+  r3dgpu_view_u16 right;
+  r3dgpu_view_u8 left_valid;
+  r3dgpu_view_u8 right_valid;
+  int32_t disparity_min;
+  int32_t num_disparities;
+  r3dgpu_stereo_options options;
+  r3dgpu_disparity_map out;
+} r3dgpu_pair;
+
+/* Matches many pairs of uneven size, range and hierarchy depth together:
+ * every stage runs once for all pairs (one launch per stage, tiles of all
+ * pairs in one persistent work queue). Results equal r3dgpu_match_stereo per
+ * pair. No reference counterpart: the reference matches pairs one at a time
+ * (src/r3d/mvs/multi_stereo.cpp:264-293). */
+r3dgpu_status r3dgpu_match_stereo_batch(r3dgpu_pair* pairs, int32_t count, void* stream);
+
+/* Census image, 62 bits per pixel (device pointers; out stride in elements).
+ * Replaces r3d::census_transform, src/r3d/stereo/census.hpp:20. */
+r3dgpu_status r3dgpu_census_transform(const r3dgpu_view_u16* image, uint64_t* out, int64_t out_stride,
+                                      void* stream);
+
+/* One 2x binomial pyramid reduction of a 16-bit image (device pointers).
+ * Replaces r3d::pyramid_down<uint16_t>, src/r3d/core/pyramid.hpp:21-22. */
+r3dgpu_status r3dgpu_pyramid_down_u16(const r3dgpu_view_u16* image, uint16_t* out, int64_t out_stride,
+                                      void* stream);
+
+/* Aggregated volume of the whole image as one tile (host images; out holds
+ * the labels of every pixel in row-major pixel order; `out_capacity` is its
+ * length in elements; `out_count` receives the cell count). ranges_lo /
+ * ranges_num: per-pixel label ranges (width x height, contiguous) or NULL.
+ * Replaces r3d::detail::sgm_cost_volume, src/r3d/stereo/stereo_matcher.hpp:98-101. */
+r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3dgpu_view_u16* right,
+                                          int32_t disparity_min, int32_t num_disparities,
+                                          const r3dgpu_stereo_options* options, const uint16_t* ranges_lo,
+                                          const uint16_t* ranges_num, uint16_t* out, uint64_t out_capacity,
+                                          uint64_t* out_count);
+
+/* Label ranges from the next coarser level (host arrays, contiguous).
+ * Replaces r3d::detail::ranges_from_coarse, src/r3d/stereo/stereo_matcher.hpp:121-125. */
+r3dgpu_status r3dgpu_ranges_from_coarse_host(const float* coarse, int32_t coarse_width, int32_t coarse_height,
+                                             int32_t width, int32_t height, const uint8_t* fine_valid,
+                                             const uint8_t* partner_valid, int32_t partner_width,
+                                             int32_t partner_sign, int32_t disparity_min,
+                                             int32_t num_disparities, const r3dgpu_stereo_options* options,
+                                             int32_t mirrored, uint16_t* lo_out, uint16_t* num_out);
+
+/* Speckle filter in place (host array, contiguous).
+ * Replaces r3d::remove_speckles, src/r3d/stereo/stereo_matcher.hpp:89. */
+r3dgpu_status r3dgpu_remove_speckles_host(float* disparity, int32_t width, int32_t height, int32_t min_size,
+                                          float max_diff);
+
+/* 3x3 median of the valid disparities (host arrays, contiguous).
+ * Replaces r3d::median_filter_3x3, src/r3d/stereo/stereo_matcher.hpp:91. */
+r3dgpu_status r3dgpu_median_filter_3x3_host(const float* disparity, int32_t width, int32_t height, float* out);
+
+/* Kernel launches issued by this process so far (the library counts its own
+ * launches; bench.py reads the difference around a timed region). */
+uint64_t r3dgpu_launch_count(void);
+
+/* Device time of the SGM tile kernel, measured with CUDA events on the
+ * launching stream around every launch and read after each call's final
+ * synchronisation (profiling adds no synchronisation of its own). No
+ * reference counterpart (the reference logs wall-clock stage times,
+ * src/r3d/stereo/stereo_matcher.cpp:663-677). */
+typedef struct r3dgpu_profile {
+  double sgm_ms;         /* summed device time of the SGM launches */
+  uint64_t sgm_launches; /* SGM launches */
+  uint64_t sgm_cells;    /* aggregated (pixel, label) cells of their tiles */
+  uint64_t sgm_tiles;    /* tiles processed */
+  uint64_t sgm_pixels;   /* tile pixels processed */
+} r3dgpu_profile;
+
+/* Enables (1) or disables (0) the accounting on this thread. */
+void r3dgpu_profile_enable(int32_t on);
+/* Returns the totals accumulated on this thread since the last call and resets them. */
+void r3dgpu_profile_take(r3dgpu_profile* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* R3DGPU_H */

@@ -1,0 +1,204 @@
+"""ctypes access to the CPU oracle (oracle/r3d_oracle.cpp) — TEST INFRASTRUCTURE.
+
+Only the tests, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg
+import this module: it is the checker of the GPU library, never part of the
+product. Each function mirrors the reference function it restates
+(rhiestan/Regard3D_MVS, src/r3d/stereo/stereo_matcher.hpp and census.hpp).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle_r3d.so")
+_lib = None
+
+
+def build() -> str:
+    """Compiles the oracle with its Makefile (g++, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        i32 = ctypes.c_int
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_set_threads.argtypes = [i32]
+        L.orc_max_threads.restype = i32
+        L.orc_census.argtypes = [P, i32, i32, P]
+        L.orc_pyramid_down_u16.argtypes = [P, i32, i32, P]
+        L.orc_pyramid_down_u8.argtypes = [P, i32, i32, P]
+        L.orc_automatic_levels.argtypes = [i32, i32, i32]
+        L.orc_automatic_levels.restype = i32
+        L.orc_sgm_cost_volume.argtypes = [P, i32, i32, P, i32, i32, i32, P, P, P, P, ctypes.c_uint64, P]
+        L.orc_ranges_from_coarse.argtypes = [P, i32, i32, i32, i32, P, P, i32, i32, i32, i32, P, i32, P, P]
+        L.orc_remove_speckles.argtypes = [P, i32, i32, i32, ctypes.c_float]
+        L.orc_median_filter_3x3.argtypes = [P, i32, i32, P]
+        L.orc_match_stereo.argtypes = [P, i32, i32, P, i32, P, P, i32, i32, P, P, P, P]
+        L.orc_match_tiles.argtypes = [P, i32, i32, P, i32, P, P, i32, i32, P, P, P, i32, P, P, P]
+        _lib = L
+    return _lib
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise OracleError(lib().orc_last_error().decode())
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _c(a, dtype):
+    return None if a is None else np.ascontiguousarray(a, dtype=dtype)
+
+
+def options_struct(opts):
+    """r3dgpu_stereo_options from a StereoOptions-like object (duck typed)."""
+    from regard3d_mvs_b200.types import StereoOptions, to_c_options  # layout shared with the product header
+
+    return to_c_options(opts if opts is not None else StereoOptions())
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())
+
+
+def census_transform(img: np.ndarray) -> np.ndarray:
+    img = _c(img, np.uint16)
+    out = np.empty(img.shape, np.uint64)
+    _check(lib().orc_census(_ptr(img), img.shape[1], img.shape[0], _ptr(out)))
+    return out
+
+
+def pyramid_down(img: np.ndarray) -> np.ndarray:
+    h, w = img.shape
+    if img.dtype == np.uint8:
+        img = _c(img, np.uint8)
+        out = np.empty(((h + 1) // 2, (w + 1) // 2), np.uint8)
+        _check(lib().orc_pyramid_down_u8(_ptr(img), w, h, _ptr(out)))
+    else:
+        img = _c(img, np.uint16)
+        out = np.empty(((h + 1) // 2, (w + 1) // 2), np.uint16)
+        _check(lib().orc_pyramid_down_u16(_ptr(img), w, h, _ptr(out)))
+    return out
+
+
+def automatic_levels(w: int, h: int, nd: int) -> int:
+    return int(lib().orc_automatic_levels(w, h, nd))
+
+
+def sgm_cost_volume(left, right, dmin, nd, options=None, ranges=None) -> np.ndarray:
+    left = _c(left, np.uint16)
+    right = _c(right, np.uint16)
+    o = options_struct(options)
+    lo = num = None
+    if ranges is not None:
+        lo = _c(ranges[0], np.uint16)
+        num = _c(ranges[1], np.uint16)
+    count = ctypes.c_uint64(0)
+    h, wl = left.shape
+    wr = right.shape[1]
+    _check(lib().orc_sgm_cost_volume(_ptr(left), wl, h, _ptr(right), wr, dmin, nd, ctypes.byref(o), _ptr(lo),
+                                     _ptr(num), None, 0, ctypes.byref(count)))
+    out = np.empty(count.value, np.uint16)
+    _check(lib().orc_sgm_cost_volume(_ptr(left), wl, h, _ptr(right), wr, dmin, nd, ctypes.byref(o), _ptr(lo),
+                                     _ptr(num), _ptr(out), count.value, ctypes.byref(count)))
+    return out
+
+
+def ranges_from_coarse(coarse, width, height, fine_valid, partner_valid, partner_width, partner_sign, dmin, nd,
+                       options=None, mirrored=False):
+    coarse = _c(coarse, np.float32)
+    fv = _c(fine_valid, np.uint8)
+    pv = _c(partner_valid, np.uint8)
+    o = options_struct(options)
+    lo = np.empty((height, width), np.uint16)
+    num = np.empty((height, width), np.uint16)
+    _check(lib().orc_ranges_from_coarse(_ptr(coarse), coarse.shape[1], coarse.shape[0], width, height, _ptr(fv),
+                                        _ptr(pv), partner_width, partner_sign, dmin, nd, ctypes.byref(o),
+                                        int(bool(mirrored)), _ptr(lo), _ptr(num)))
+    return lo, num
+
+
+def remove_speckles(disp: np.ndarray, min_size: int, max_diff: float) -> np.ndarray:
+    d = np.array(disp, dtype=np.float32, order="C", copy=True)
+    _check(lib().orc_remove_speckles(_ptr(d), d.shape[1], d.shape[0], int(min_size), float(max_diff)))
+    return d
+
+
+def median_filter_3x3(disp: np.ndarray) -> np.ndarray:
+    d = _c(disp, np.float32)
+    out = np.empty_like(d)
+    _check(lib().orc_median_filter_3x3(_ptr(d), d.shape[1], d.shape[0], _ptr(out)))
+    return out
+
+
+@dataclass
+class OracleMap:
+    disparity: np.ndarray
+    confidence: np.ndarray
+    disparity_min: int
+    num_disparities: int
+    levels: int
+    cells: int
+
+
+def match_stereo(left, right, left_valid=None, right_valid=None, disparity_min=0, num_disparities=64,
+                 options=None) -> OracleMap:
+    left = _c(left, np.uint16)
+    right = _c(right, np.uint16)
+    lv = _c(left_valid, np.uint8)
+    rv = _c(right_valid, np.uint8)
+    o = options_struct(options)
+    h, wl = left.shape
+    if right.shape[0] != h or left.size == 0 or right.size == 0:
+        raise OracleError("stereo: rectified images must be non-empty with equal height")
+    disp = np.empty((h, wl), np.float32)
+    conf = np.empty((h, wl), np.float32)
+    meta = np.zeros(3, np.int64)
+    _check(lib().orc_match_stereo(_ptr(left), wl, h, _ptr(right), right.shape[1], _ptr(lv), _ptr(rv),
+                                  int(disparity_min), int(num_disparities), ctypes.byref(o), _ptr(disp), _ptr(conf),
+                                  _ptr(meta)))
+    return OracleMap(disp, conf, int(disparity_min), int(meta[1]), int(meta[0]), int(meta[2]))
+
+
+def match_tiles(left, right, left_valid=None, right_valid=None, disparity_min=0, num_disparities=64, options=None,
+                ranges=None, diagonal_lr=False):
+    left = _c(left, np.uint16)
+    right = _c(right, np.uint16)
+    lv = _c(left_valid, np.uint8)
+    rv = _c(right_valid, np.uint8)
+    o = options_struct(options)
+    lo = num = None
+    if ranges is not None:
+        lo = _c(ranges[0], np.uint16)
+        num = _c(ranges[1], np.uint16)
+    h, wl = left.shape
+    disp = np.empty((h, wl), np.float32)
+    conf = np.empty((h, wl), np.float32)
+    cells = ctypes.c_uint64(0)
+    _check(lib().orc_match_tiles(_ptr(left), wl, h, _ptr(right), right.shape[1], _ptr(lv), _ptr(rv),
+                                 int(disparity_min), int(num_disparities), ctypes.byref(o), _ptr(lo), _ptr(num),
+                                 int(bool(diagonal_lr)), _ptr(disp), _ptr(conf), ctypes.byref(cells)))
+    return disp, conf, int(cells.value)

@@ -1,0 +1,126 @@
+"""Loads the r3dgpu C-ABI library (include/r3dgpu.h) with ctypes.
+
+The product library is ``regard3d_mvs_b200/_lib/libr3dgpu.so``, built for
+sm_100a by ``regard3d_mvs_b200/build.py``. There is no CPU fallback: if the
+library is missing or no B200 is present, calls fail with an error.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+from .types import CDisparityMap, COptions, CPair, CProfile, CSynthParams, CViewU8, CViewU16
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libr3dgpu.so")
+
+STATUS = {
+    0: "R3DGPU_OK",
+    1: "R3DGPU_EINVAL",
+    2: "R3DGPU_ECANCELLED",
+    3: "R3DGPU_ENOMEM",
+    4: "R3DGPU_EDEVICE",
+    5: "R3DGPU_ETIMEOUT",
+    6: "R3DGPU_EUNSUPPORTED",
+}
+
+# Every symbol include/r3dgpu.h declares.
+EXPORTS = (
+    "r3dgpu_last_error",
+    "r3dgpu_default_options",
+    "r3dgpu_automatic_levels",
+    "r3dgpu_set_device",
+    "r3dgpu_match_stereo_host",
+    "r3dgpu_match_stereo",
+    "r3dgpu_match_stereo_batch",
+    "r3dgpu_census_transform",
+    "r3dgpu_pyramid_down_u16",
+    "r3dgpu_sgm_cost_volume_host",
+    "r3dgpu_ranges_from_coarse_host",
+    "r3dgpu_remove_speckles_host",
+    "r3dgpu_median_filter_3x3_host",
+    "r3dgpu_launch_count",
+    "r3dgpu_profile_enable",
+    "r3dgpu_profile_take",
+)
+
+
+class StereoError(RuntimeError):
+    """r3d::Error counterpart: carries the library's status name."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class NativeLibraryMissing(RuntimeError):
+    pass
+
+
+def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
+    P = ctypes.c_void_p
+    i32 = ctypes.c_int32
+    st = ctypes.c_int
+    L.r3dgpu_last_error.restype = ctypes.c_char_p
+    L.r3dgpu_default_options.argtypes = [ctypes.POINTER(COptions)]
+    L.r3dgpu_default_options.restype = None
+    L.r3dgpu_automatic_levels.argtypes = [i32, i32, i32]
+    L.r3dgpu_automatic_levels.restype = i32
+    L.r3dgpu_set_device.argtypes = [i32]
+    L.r3dgpu_set_device.restype = st
+    L.r3dgpu_match_stereo_host.argtypes = [ctypes.POINTER(CViewU16), ctypes.POINTER(CViewU16),
+                                           ctypes.POINTER(CViewU8), ctypes.POINTER(CViewU8), i32, i32,
+                                           ctypes.POINTER(COptions), ctypes.POINTER(CDisparityMap)]
+    L.r3dgpu_match_stereo_host.restype = st
+    L.r3dgpu_match_stereo.argtypes = [ctypes.POINTER(CViewU16), ctypes.POINTER(CViewU16), ctypes.POINTER(CViewU8),
+                                      ctypes.POINTER(CViewU8), i32, i32, ctypes.POINTER(COptions),
+                                      ctypes.POINTER(CDisparityMap), P]
+    L.r3dgpu_match_stereo.restype = st
+    L.r3dgpu_match_stereo_batch.argtypes = [ctypes.POINTER(CPair), i32, P]
+    L.r3dgpu_match_stereo_batch.restype = st
+    L.r3dgpu_census_transform.argtypes = [ctypes.POINTER(CViewU16), P, ctypes.c_int64, P]
+    L.r3dgpu_census_transform.restype = st
+    L.r3dgpu_pyramid_down_u16.argtypes = [ctypes.POINTER(CViewU16), P, ctypes.c_int64, P]
+    L.r3dgpu_pyramid_down_u16.restype = st
+    L.r3dgpu_sgm_cost_volume_host.argtypes = [ctypes.POINTER(CViewU16), ctypes.POINTER(CViewU16), i32, i32,
+                                              ctypes.POINTER(COptions), P, P, P, ctypes.c_uint64,
+                                              ctypes.POINTER(ctypes.c_uint64)]
+    L.r3dgpu_sgm_cost_volume_host.restype = st
+    L.r3dgpu_ranges_from_coarse_host.argtypes = [P, i32, i32, i32, i32, P, P, i32, i32, i32, i32,
+                                                 ctypes.POINTER(COptions), i32, P, P]
+    L.r3dgpu_ranges_from_coarse_host.restype = st
+    L.r3dgpu_remove_speckles_host.argtypes = [P, i32, i32, i32, ctypes.c_float]
+    L.r3dgpu_remove_speckles_host.restype = st
+    L.r3dgpu_median_filter_3x3_host.argtypes = [P, i32, i32, P]
+    L.r3dgpu_median_filter_3x3_host.restype = st
+    L.r3dgpu_launch_count.argtypes = []
+    L.r3dgpu_launch_count.restype = ctypes.c_uint64
+    L.r3dgpu_profile_enable.argtypes = [i32]
+    L.r3dgpu_profile_enable.restype = None
+    L.r3dgpu_profile_take.argtypes = [ctypes.POINTER(CProfile)]
+    L.r3dgpu_profile_take.restype = None
+    if hasattr(L, "r3dgpu_synth_pair"):
+        L.r3dgpu_synth_pair.argtypes = [ctypes.POINTER(CSynthParams), P, P, P]
+        L.r3dgpu_synth_pair.restype = st
+    return L
+
+
+_cache: dict[str, ctypes.CDLL] = {}
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """The library at `path` (default: the in-tree CUDA build)."""
+    path = os.path.abspath(path or LIB_PATH)
+    if path not in _cache:
+        if not os.path.exists(path):
+            raise NativeLibraryMissing(
+                f"r3dgpu CUDA library not found at {path}; build it with "
+                "`python -m regard3d_mvs_b200.build` (nvcc, sm_100a)")
+        _cache[path] = _declare(ctypes.CDLL(path))
+    return _cache[path]
+
+
+def check(lib: ctypes.CDLL, status: int) -> None:
+    if status != 0:
+        raise StereoError(status, lib.r3dgpu_last_error().decode())

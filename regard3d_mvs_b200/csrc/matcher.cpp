@@ -1,0 +1,1178 @@
+// Host side of r3dgpu: option checks, level pyramid, tile layout, the stage
+// sequence of every level, batching of many pairs, and the C ABI.
+//
+// The control flow restates r3d::match_stereo (rhiestan/Regard3D_MVS,
+// src/r3d/stereo/stereo_matcher.cpp:1023-1095) and match_level (:831-886):
+// levels L..0, full label range at the coarsest level, per-pixel ranges from
+// the coarser disparities below it, a left and (with lr_full_match) a
+// mirrored right-to-left match per level, the left-right check(s), speckle
+// and median filters. Every stage runs on the GPU; the host only plans
+// (tile layout, job tables, buffer sizes) and launches.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "sgm.h"
+
+namespace r3dgpu {
+namespace {
+
+thread_local std::string t_error;
+thread_local int t_device = 0;
+
+// Profiling of the SGM launches (r3dgpu_profile_*).
+struct ProfileState {
+  bool on = false;
+  r3dgpu_profile acc{};
+  struct Pending {
+    cudaEvent_t a, b;
+    uint64_t cells, tiles, pixels;
+  };
+  std::vector<Pending> pending;
+};
+thread_local ProfileState t_prof;
+
+void profile_collect() {
+  for (auto& p : t_prof.pending) {
+    float ms = 0.0F;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) t_prof.acc.sgm_ms += ms;
+    (void)cudaGetLastError();
+    cudaEventDestroy(p.a);
+    cudaEventDestroy(p.b);
+    t_prof.acc.sgm_launches += 1;
+    t_prof.acc.sgm_cells += p.cells;
+    t_prof.acc.sgm_tiles += p.tiles;
+    t_prof.acc.sgm_pixels += p.pixels;
+  }
+  t_prof.pending.clear();
+}
+
+int align16(int n) { return (n + 15) / 16 * 16; }
+// stereo_matcher.cpp:889-890
+int floor_shift(int v, int k) { return v >= 0 ? v >> k : -((-v + (1 << k) - 1) >> k); }
+int ceil_shift(int v, int k) { return -floor_shift(-v, k); }
+
+// stereo_matcher.cpp:81-95 (same conditions and messages).
+void check_options(const r3dgpu_stereo_options& o) {
+  if (o.p1 < 0 || o.p2 < o.p1 || o.p2 > 8000)
+    fail(R3DGPU_EINVAL, "stereo: invalid penalties P1 = " + std::to_string(o.p1) + ", P2 = " + std::to_string(o.p2) +
+                            " (0 <= P1 <= P2 <= 8000)");
+  if (o.invalid_cost < 0 || o.invalid_cost > 255)
+    fail(R3DGPU_EINVAL, "stereo: invalid_cost " + std::to_string(o.invalid_cost) + " outside [0, 255]");
+  if (o.tile_size < 16 || o.tile_margin < 0 || o.tile_blend < 0)
+    fail(R3DGPU_EINVAL, "stereo: invalid tiling " + std::to_string(o.tile_size) + " / " + std::to_string(o.tile_margin) +
+                            " / " + std::to_string(o.tile_blend));
+  if (o.levels < -1 || o.levels > 12 || o.range_radius < 0 || o.range_margin < 0 || o.range_fill < 0)
+    fail(R3DGPU_EINVAL, "stereo: invalid hierarchy levels " + std::to_string(o.levels) + " / radius " +
+                            std::to_string(o.range_radius) + " / margin " + std::to_string(o.range_margin) + " / fill " +
+                            std::to_string(o.range_fill));
+  if (o.subpixel < 0 || o.subpixel > 2) fail(R3DGPU_EINVAL, "stereo: invalid subpixel method");
+}
+
+// stereo_matcher.cpp:1105-1122
+int automatic_levels(int width, int height, int nd) {
+  int levels = 0, w = width, h = height, n = nd;
+  while (levels < 8) {
+    const int nw = (w + 1) / 2, nh = (h + 1) / 2;
+    if (std::min(nw, nh) < 96 || n <= 48) break;
+    w = nw;
+    h = nh;
+    n = (n + 1) / 2;
+    ++levels;
+  }
+  return levels;
+}
+
+// stereo_matcher.cpp:69-79
+void p2_lut(const r3dgpu_stereo_options& o, uint16_t* lut) {
+  for (int di = 0; di < 256; ++di) {
+    int p2 = o.p2;
+    if (o.p2_adapt > 0) p2 = std::max(o.p1 + 1, o.p2 * o.p2_adapt / (o.p2_adapt + di));
+    lut[di] = static_cast<uint16_t>(p2);
+  }
+}
+
+// ------------------------------------------------------------------ memory
+// Bump allocator over grow-only device chunks; reset() rewinds it so that the
+// next call reuses the same memory without cudaMalloc.
+class Arena {
+ public:
+  void reset() {
+    for (auto& c : chunks_) c.used = 0;
+    cur_ = 0;
+  }
+  template <class T>
+  T* alloc(size_t n) {
+    size_t bytes = (n * sizeof(T) + 255) & ~static_cast<size_t>(255);
+    if (bytes == 0) bytes = 256;
+    while (cur_ < chunks_.size()) {
+      Chunk& c = chunks_[cur_];
+      if (c.used + bytes <= c.buf.size()) {
+        T* p = reinterpret_cast<T*>(c.buf.get() + c.used);
+        c.used += bytes;
+        return p;
+      }
+      ++cur_;
+    }
+    chunks_.emplace_back();
+    chunks_.back().buf.reset(std::max(bytes, kChunk));
+    chunks_.back().used = bytes;
+    cur_ = chunks_.size() - 1;
+    return reinterpret_cast<T*>(chunks_.back().buf.get());
+  }
+
+ private:
+  static constexpr size_t kChunk = size_t{256} << 20;
+  struct Chunk {
+    DeviceBuffer<unsigned char> buf;
+    size_t used = 0;
+  };
+  std::vector<Chunk> chunks_;
+  size_t cur_ = 0;
+};
+
+// Grow-only pinned host staging.
+class Pinned {
+ public:
+  ~Pinned() {
+    if (p_) cudaFreeHost(p_);
+  }
+  void reset() { used_ = 0; }
+  template <class T>
+  T* alloc(size_t n) {
+    const size_t bytes = (n * sizeof(T) + 255) & ~static_cast<size_t>(255);
+    if (used_ + bytes > cap_) {
+      // Earlier allocations of this call stay valid: keep them in retired blocks.
+      if (p_) retired_.push_back(p_);
+      cap_ = std::max(bytes, std::max(cap_ * 2, size_t{1} << 20));
+      R3D_CUDA(cudaMallocHost(reinterpret_cast<void**>(&p_), cap_));
+      used_ = 0;
+    }
+    T* r = reinterpret_cast<T*>(p_ + used_);
+    used_ += bytes;
+    return r;
+  }
+  // Frees the blocks replaced during the last call (after the stream synced).
+  void release_retired() {
+    for (unsigned char* p : retired_) cudaFreeHost(p);
+    retired_.clear();
+  }
+
+ private:
+  unsigned char* p_ = nullptr;
+  size_t cap_ = 0, used_ = 0;
+  std::vector<unsigned char*> retired_;
+};
+
+struct Workspace {
+  int device = -1;
+  int sms = 0;
+  int smem_optin = 0;
+  Arena arena;
+  Pinned pinned;
+  DeviceBuffer<unsigned char> scratch;
+  DeviceBuffer<int> counter;
+};
+
+Workspace& workspace() {
+  thread_local std::vector<std::unique_ptr<Workspace>> per_device;
+  int dev = t_device;
+  if (static_cast<int>(per_device.size()) <= dev) per_device.resize(dev + 1);
+  if (!per_device[dev]) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= dev) {
+      (void)cudaGetLastError();
+      fail(R3DGPU_EDEVICE, "r3dgpu: no CUDA device " + std::to_string(dev));
+    }
+    R3D_CUDA(cudaSetDevice(dev));
+    cudaDeviceProp prop{};
+    R3D_CUDA(cudaGetDeviceProperties(&prop, dev));
+#ifndef R3DGPU_SIMT_EMULATION
+    if (prop.major != 10)
+      fail(R3DGPU_EDEVICE, std::string("r3dgpu: built for sm_100a, device is ") + prop.name + " (sm_" +
+                               std::to_string(prop.major) + std::to_string(prop.minor) + ")");
+#endif
+    auto ws = std::make_unique<Workspace>();
+    ws->device = dev;
+    ws->sms = prop.multiProcessorCount;
+    ws->smem_optin = static_cast<int>(prop.sharedMemPerBlockOptin);
+    ws->counter.reset(64);
+    per_device[dev] = std::move(ws);
+  }
+  R3D_CUDA(cudaSetDevice(dev));
+  return *per_device[dev];
+}
+
+// ------------------------------------------------------------------ views
+template <class T>
+struct DView {
+  const T* p = nullptr;
+  int w = 0, h = 0;
+  int64_t stride = 0;
+  bool empty() const { return p == nullptr || w == 0 || h == 0; }
+};
+
+// ------------------------------------------------------------------ tiles
+struct Tile {
+  int x0, y0, w, h;
+  int c0x, c1x, c0y, c1y;
+};
+
+// stereo_matcher.cpp:545-552
+std::vector<int> split(int size, int tile) {
+  const int n = std::max(1, (size + tile - 1) / tile);
+  std::vector<int> b(n + 1);
+  for (int i = 0; i <= n; ++i) b[i] = static_cast<int>(static_cast<long long>(size) * i / n);
+  return b;
+}
+
+struct Layout {
+  std::vector<Tile> tiles;
+  int tiles_x = 0;
+};
+
+Layout make_layout(int W, int H, int ts, const r3dgpu_stereo_options& o) {
+  const int ext = o.tile_margin + (o.tile_blend + 1) / 2;
+  Layout L;
+  const auto bx = split(W, ts), by = split(H, ts);
+  L.tiles_x = static_cast<int>(bx.size()) - 1;
+  for (size_t j = 0; j + 1 < by.size(); ++j)
+    for (size_t i = 0; i + 1 < bx.size(); ++i) {
+      Tile t;
+      t.x0 = std::max(0, bx[i] - ext);
+      const int x1 = std::min(W, bx[i + 1] + ext);
+      t.y0 = std::max(0, by[j] - ext);
+      const int y1 = std::min(H, by[j + 1] + ext);
+      t.w = x1 - t.x0;
+      t.h = y1 - t.y0;
+      t.c0x = bx[i];
+      t.c1x = bx[i + 1];
+      t.c0y = by[j];
+      t.c1y = by[j + 1];
+      L.tiles.push_back(t);
+    }
+  return L;
+}
+
+// stereo_matcher.cpp:571-578
+size_t estimated_tile_bytes(uint64_t cells_u, const Tile& t, size_t right_width) {
+  const size_t cells = static_cast<size_t>(cells_u);
+  const size_t w = static_cast<size_t>(t.w), h = static_cast<size_t>(t.h);
+  const size_t row_cells = cells / std::max<size_t>(h, 1);
+  return cells * 2 + row_cells * 2 + 6 * (row_cells + w * 2 * 8) * 2 + w * h * 32 + (w + right_width + 16) * (h + 6) * 8;
+}
+
+// ------------------------------------------------------------------ pair state
+struct Match {
+  SgmMatch m{};
+  Layout layout;
+  int tile_size = 0;
+  std::vector<uint64_t> tile_cells;  // host copy (ranged: counted on the device)
+  std::vector<int> tile_maxnum;
+  bool ranged = false;
+  // device outputs of the SGM stage
+  float* tile_disp = nullptr;
+  float* tile_conf = nullptr;
+  std::vector<size_t> tile_off;  // per tile, offset into tile_disp / tile_conf
+  unsigned long long* d_cells = nullptr;
+  int first_job = 0;
+  // counting buffers (ranged)
+  unsigned long long* d_count = nullptr;
+  int* d_maxnum = nullptr;
+  unsigned long long* h_count = nullptr;
+  int* h_maxnum = nullptr;
+};
+
+struct LevelIn {
+  DView<uint16_t> left, right;
+  DView<uint8_t> lmask, rmask;
+  int dmin = 0, nd = 0;
+};
+
+struct PairRun {
+  const r3dgpu_pair* req = nullptr;
+  r3dgpu_stereo_options o{};
+  int levels = 0;
+  bool check_lr = false, lr_full = false;
+  std::vector<LevelIn> lv;
+  int cur = -1;  // level being processed
+  // coarser-level results
+  float* coarse_left = nullptr;
+  float* coarse_right = nullptr;
+  int coarse_wl = 0, coarse_wr = 0, coarse_h = 0;
+  // this level
+  Match left, right;
+  bool has_right = false;
+  RowInterval *int_l = nullptr, *int_r = nullptr;
+  float *disp_l = nullptr, *conf_l = nullptr, *disp_r = nullptr;
+  uint64_t cells = 0;
+  std::vector<unsigned long long*> cell_arrays;  // device, summed at the end
+  std::vector<int> cell_counts;
+  std::vector<unsigned long long*> h_cell_arrays;
+};
+
+DView<uint16_t> view_of(const r3dgpu_view_u16& v) { return {v.data, v.width, v.height, v.stride}; }
+DView<uint8_t> view_of(const r3dgpu_view_u8& v) {
+  DView<uint8_t> d{v.data, v.width, v.height, v.stride};
+  if (d.empty()) return {};
+  return d;
+}
+
+void validate_pair(const r3dgpu_pair& p) {
+  check_options(p.options);
+  if (p.num_disparities <= 0) fail(R3DGPU_EINVAL, "stereo: no disparities to search");
+  const auto& L = p.left;
+  const auto& R = p.right;
+  if (L.data == nullptr || R.data == nullptr || L.width <= 0 || L.height <= 0 || R.width <= 0 || R.height <= 0 ||
+      L.height != R.height)
+    fail(R3DGPU_EINVAL, "stereo: rectified images must be non-empty with equal height (" + std::to_string(L.width) +
+                            "x" + std::to_string(L.height) + ", " + std::to_string(R.width) + "x" +
+                            std::to_string(R.height) + ")");
+  if (L.stride < L.width || R.stride < R.width) fail(R3DGPU_EINVAL, "stereo: image stride smaller than width");
+  const auto lv = view_of(p.left_valid), rv = view_of(p.right_valid);
+  if (!lv.empty() && (lv.w != L.width || lv.h != L.height))
+    fail(R3DGPU_EINVAL, "stereo: left mask size differs from the image");
+  if (!rv.empty() && (rv.w != R.width || rv.h != R.height))
+    fail(R3DGPU_EINVAL, "stereo: right mask size differs from the image");
+  if (p.out.disparity == nullptr || p.out.stride < L.width) fail(R3DGPU_EINVAL, "stereo: missing output buffer");
+  if (L.width > 65535 || R.width > 65535) fail(R3DGPU_EUNSUPPORTED, "stereo: images wider than 65535 pixels");
+}
+
+// Level pyramid (stereo_matcher.cpp:1036-1058): u16 images, reduced masks.
+void build_levels(PairRun& P, Arena& A, cudaStream_t s) {
+  const r3dgpu_pair& q = *P.req;
+  P.lv.assign(P.levels + 1, LevelIn{});
+  P.lv[0].left = view_of(q.left);
+  P.lv[0].right = view_of(q.right);
+  P.lv[0].lmask = view_of(q.left_valid);
+  P.lv[0].rmask = view_of(q.right_valid);
+  for (int l = 1; l <= P.levels; ++l) {
+    const LevelIn& a = P.lv[l - 1];
+    LevelIn& b = P.lv[l];
+    auto down16 = [&](const DView<uint16_t>& v) {
+      DView<uint16_t> o;
+      o.w = (v.w + 1) / 2;
+      o.h = (v.h + 1) / 2;
+      o.stride = o.w;
+      uint16_t* p = A.alloc<uint16_t>(static_cast<size_t>(o.w) * o.h);
+      launch_pyramid_u16(v.p, v.stride, v.w, v.h, p, o.stride, s);
+      o.p = p;
+      return o;
+    };
+    auto down8 = [&](const DView<uint8_t>& v) {
+      if (v.empty()) return DView<uint8_t>{};
+      DView<uint8_t> o;
+      o.w = (v.w + 1) / 2;
+      o.h = (v.h + 1) / 2;
+      o.stride = o.w;
+      uint8_t* p = A.alloc<uint8_t>(static_cast<size_t>(o.w) * o.h);
+      launch_reduce_mask(v.p, v.stride, v.w, v.h, p, o.stride, s);
+      o.p = p;
+      return o;
+    };
+    b.left = down16(a.left);
+    b.right = down16(a.right);
+    b.lmask = down8(a.lmask);
+    b.rmask = down8(a.rmask);
+  }
+  const int dmin = q.disparity_min, dmax = q.disparity_min + q.num_disparities - 1;
+  for (int l = 0; l <= P.levels; ++l) {
+    P.lv[l].dmin = floor_shift(dmin, l);
+    P.lv[l].nd = align16(ceil_shift(dmax, l) - P.lv[l].dmin + 1);
+  }
+}
+
+void fill_match(SgmMatch& m, const r3dgpu_stereo_options& o, const DView<uint16_t>& base, const uint64_t* cb,
+                const uint64_t* cp, int wp, const RowInterval* bv, const RowInterval* pv, const uint16_t* rlo,
+                const uint16_t* rnum, int dmin, int nd, bool diagonal, bool confidence) {
+  m = SgmMatch{};
+  m.base = base.p;
+  m.base_stride = base.stride;
+  m.cbase = cb;
+  m.cb_stride = base.w;
+  m.cpart = cp;
+  m.cp_stride = wp;
+  m.bv = bv;
+  m.pv = pv;
+  m.rlo = rlo;
+  m.rnum = rnum;
+  m.r_stride = base.w;
+  m.wb = base.w;
+  m.wp = wp;
+  m.h = base.h;
+  m.dmin = dmin;
+  m.nd = nd;
+  m.p1 = o.p1;
+  m.invalid_cost = o.invalid_cost;
+  m.subpixel = o.subpixel;
+  m.uniqueness = o.uniqueness;
+  m.lr_max_diff = o.lr_max_diff;
+  m.diagonal_lr = diagonal ? 1 : 0;
+  m.confidence = confidence ? 1 : 0;
+  p2_lut(o, m.lut);
+}
+
+// Stage 1 of a level: mirrored inputs, Census images, row intervals, label
+// ranges from the coarser level, candidate tile layouts (and their device
+// cell counts for ranged matches).
+void prepare_level(PairRun& P, Arena& A, Pinned& H, cudaStream_t s) {
+  const int l = P.cur;
+  const LevelIn& in = P.lv[l];
+  const r3dgpu_stereo_options& o = P.o;
+  const int wl = in.left.w, wr = in.right.w, h = in.left.h;
+  auto census = [&](const DView<uint16_t>& v) {
+    uint64_t* c = A.alloc<uint64_t>(static_cast<size_t>(v.w) * v.h);
+    launch_census(v.p, v.stride, v.w, v.h, c, v.w, s);
+    return c;
+  };
+  auto intervals = [&](const DView<uint8_t>& m, int w) {
+    RowInterval* r = A.alloc<RowInterval>(h);
+    launch_intervals(m.empty() ? nullptr : m.p, m.stride, w, h, r, s);
+    return r;
+  };
+  const uint64_t* cl = census(in.left);
+  const uint64_t* cr = census(in.right);
+  P.int_l = intervals(in.lmask, wl);
+  P.int_r = intervals(in.rmask, wr);
+  const bool ranged = l < P.levels;
+  const uint16_t *llo = nullptr, *lnum = nullptr, *rlo = nullptr, *rnum = nullptr;
+  if (ranged) {
+    if (P.coarse_left == nullptr) fail(R3DGPU_EDEVICE, "stereo: internal error, no coarser level");
+    uint16_t* lo = A.alloc<uint16_t>(static_cast<size_t>(wl) * h);
+    uint16_t* nu = A.alloc<uint16_t>(static_cast<size_t>(wl) * h);
+    float* scr = A.alloc<float>(static_cast<size_t>(ranges_scratch_floats(P.coarse_wl, P.coarse_h, o.range_fill)));
+    RangeParams rp{o.range_radius, o.range_margin, o.range_fill, in.dmin, in.nd, -1, 0};
+    launch_ranges_from_coarse(P.coarse_left, P.coarse_wl, P.coarse_h, wl, h, in.lmask.empty() ? nullptr : in.lmask.p,
+                              in.lmask.stride, P.int_r, rp, scr, lo, nu, s);
+    llo = lo;
+    lnum = nu;
+  }
+  fill_match(P.left.m, o, in.left, cl, cr, wr, P.int_l, P.int_r, llo, lnum, in.dmin, in.nd,
+             P.check_lr && !P.lr_full, true);
+  P.has_right = P.check_lr && P.lr_full;
+  if (P.has_right) {
+    uint16_t* ml = A.alloc<uint16_t>(static_cast<size_t>(wl) * h);
+    uint16_t* mr = A.alloc<uint16_t>(static_cast<size_t>(wr) * h);
+    launch_mirror_u16(in.left.p, in.left.stride, wl, h, ml, s);
+    launch_mirror_u16(in.right.p, in.right.stride, wr, h, mr, s);
+    const DView<uint16_t> vml{ml, wl, h, wl}, vmr{mr, wr, h, wr};
+    DView<uint8_t> mlm, mrm;
+    if (!in.lmask.empty()) {
+      uint8_t* p = A.alloc<uint8_t>(static_cast<size_t>(wl) * h);
+      launch_mirror_u8(in.lmask.p, in.lmask.stride, wl, h, p, s);
+      mlm = {p, wl, h, wl};
+    }
+    if (!in.rmask.empty()) {
+      uint8_t* p = A.alloc<uint8_t>(static_cast<size_t>(wr) * h);
+      launch_mirror_u8(in.rmask.p, in.rmask.stride, wr, h, p, s);
+      mrm = {p, wr, h, wr};
+    }
+    const uint64_t* cml = census(vml);
+    const uint64_t* cmr = census(vmr);
+    RowInterval* iml = intervals(mlm, wl);
+    RowInterval* imr = intervals(mrm, wr);
+    if (ranged) {
+      if (P.coarse_right == nullptr) fail(R3DGPU_EDEVICE, "stereo: internal error, no coarser right map");
+      uint16_t* lo = A.alloc<uint16_t>(static_cast<size_t>(wr) * h);
+      uint16_t* nu = A.alloc<uint16_t>(static_cast<size_t>(wr) * h);
+      float* scr = A.alloc<float>(static_cast<size_t>(ranges_scratch_floats(P.coarse_wr, P.coarse_h, o.range_fill)));
+      RangeParams rp{o.range_radius, o.range_margin, o.range_fill, in.dmin, in.nd, +1, 1};
+      launch_ranges_from_coarse(P.coarse_right, P.coarse_wr, P.coarse_h, wr, h,
+                                in.rmask.empty() ? nullptr : in.rmask.p, in.rmask.stride, P.int_l, rp, scr, lo, nu, s);
+      rlo = lo;
+      rnum = nu;
+    }
+    fill_match(P.right.m, o, vmr, cmr, cml, wl, imr, iml, rlo, rnum, in.dmin + wr - wl, in.nd, false, false);
+  }
+  // Candidate layouts; ranged matches count their tiles' labels on the device.
+  auto plan = [&](Match& M, int W) {
+    M.ranged = M.m.rlo != nullptr;
+    M.tile_size = o.tile_size;
+    M.layout = make_layout(W, h, M.tile_size, o);
+    if (M.ranged) {
+      const int n = static_cast<int>(M.layout.tiles.size());
+      int4* ht = H.alloc<int4>(n);
+      for (int i = 0; i < n; ++i) {
+        const Tile& t = M.layout.tiles[i];
+        ht[i] = make_int4(t.x0, t.y0, t.w, t.h);
+      }
+      int4* dt = A.alloc<int4>(n);
+      R3D_CUDA(cudaMemcpyAsync(dt, ht, sizeof(int4) * n, cudaMemcpyHostToDevice, s));
+      M.d_count = A.alloc<unsigned long long>(n);
+      M.d_maxnum = A.alloc<int>(n);
+      launch_tile_cells(M.m.rnum, M.m.r_stride, dt, n, M.d_count, M.d_maxnum, s);
+      M.h_count = H.alloc<unsigned long long>(n);
+      M.h_maxnum = H.alloc<int>(n);
+      R3D_CUDA(cudaMemcpyAsync(M.h_count, M.d_count, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, s));
+      R3D_CUDA(cudaMemcpyAsync(M.h_maxnum, M.d_maxnum, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    }
+  };
+  plan(P.left, wl);
+  if (P.has_right) plan(P.right, wr);
+}
+
+// After the counts arrived: apply the reference's tile-size halving rule
+// (stereo_matcher.cpp:643-648) and fix every tile's cell count and max label
+// count. Returns false when a ranged match must be recounted.
+bool finalize_layout(Match& M, int W, int H_, int partner_w, const r3dgpu_stereo_options& o, Arena& A, Pinned& HP,
+                     cudaStream_t s) {
+  const size_t n = M.layout.tiles.size();
+  M.tile_cells.resize(n);
+  M.tile_maxnum.resize(n);
+  for (size_t i = 0; i < n; ++i) {
+    const Tile& t = M.layout.tiles[i];
+    if (M.ranged) {
+      M.tile_cells[i] = M.h_count[i];
+      M.tile_maxnum[i] = M.h_maxnum[i];
+    } else {
+      M.tile_cells[i] = static_cast<uint64_t>(t.w) * static_cast<uint64_t>(t.h) * static_cast<uint64_t>(M.m.nd);
+      M.tile_maxnum[i] = M.m.nd;
+    }
+  }
+  size_t maxb = 0;
+  for (size_t i = 0; i < n; ++i)
+    maxb = std::max(maxb, estimated_tile_bytes(M.tile_cells[i], M.layout.tiles[i], static_cast<size_t>(partner_w)));
+  if (M.tile_size > 64 && maxb > o.memory_budget) {
+    M.tile_size /= 2;
+    M.layout = make_layout(W, H_, M.tile_size, o);
+    if (M.ranged) {
+      const int nn = static_cast<int>(M.layout.tiles.size());
+      int4* ht = HP.alloc<int4>(nn);
+      for (int i = 0; i < nn; ++i) {
+        const Tile& t = M.layout.tiles[i];
+        ht[i] = make_int4(t.x0, t.y0, t.w, t.h);
+      }
+      int4* dt = A.alloc<int4>(nn);
+      R3D_CUDA(cudaMemcpyAsync(dt, ht, sizeof(int4) * nn, cudaMemcpyHostToDevice, s));
+      M.d_count = A.alloc<unsigned long long>(nn);
+      M.d_maxnum = A.alloc<int>(nn);
+      launch_tile_cells(M.m.rnum, M.m.r_stride, dt, nn, M.d_count, M.d_maxnum, s);
+      M.h_count = HP.alloc<unsigned long long>(nn);
+      M.h_maxnum = HP.alloc<int>(nn);
+      R3D_CUDA(cudaMemcpyAsync(M.h_count, M.d_count, sizeof(unsigned long long) * nn, cudaMemcpyDeviceToHost, s));
+      R3D_CUDA(cudaMemcpyAsync(M.h_maxnum, M.d_maxnum, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
+      return false;
+    }
+    return finalize_layout(M, W, H_, partner_w, o, A, HP, s);
+  }
+  for (size_t i = 0; i < n; ++i)
+    if (M.tile_cells[i] >= (uint64_t{1} << 31))
+      fail(R3DGPU_EUNSUPPORTED, "stereo: a tile has 2^31 or more labels; use a smaller tile_size");
+  return true;
+}
+
+// Stage 3 of a level: blending, left-right check(s), filters.
+void finish_level(PairRun& P, Arena& A, Pinned& H, cudaStream_t s) {
+  const int l = P.cur;
+  const LevelIn& in = P.lv[l];
+  const r3dgpu_stereo_options& o = P.o;
+  const int wl = in.left.w, wr = in.right.w, h = in.left.h;
+  auto blend = [&](Match& M, int W, bool mirror_out, float offset, float* disp, float* conf) {
+    const int n = static_cast<int>(M.layout.tiles.size());
+    BlendTile* bt = H.alloc<BlendTile>(n);
+    for (int i = 0; i < n; ++i) {
+      const Tile& t = M.layout.tiles[i];
+      bt[i] = BlendTile{t.x0, t.y0, t.w, t.h, t.c0x, t.c1x, t.c0y, t.c1y, M.tile_disp + M.tile_off[i],
+                        M.tile_conf ? M.tile_conf + M.tile_off[i] : nullptr};
+    }
+    BlendTile* d = A.alloc<BlendTile>(n);
+    R3D_CUDA(cudaMemcpyAsync(d, bt, sizeof(BlendTile) * n, cudaMemcpyHostToDevice, s));
+    launch_blend(d, n, M.layout.tiles_x, nullptr, nullptr, W, h, o.tile_blend, mirror_out ? 1 : 0, offset, disp, conf,
+                 W, s);
+  };
+  P.disp_l = A.alloc<float>(static_cast<size_t>(wl) * h);
+  P.conf_l = A.alloc<float>(static_cast<size_t>(wl) * h);
+  blend(P.left, wl, false, 0.0F, P.disp_l, P.conf_l);
+  const bool need_right = P.lr_full && l > 0;
+  const int speckle = o.speckle_size >> (2 * l);
+  int* uf = nullptr;
+  auto post_filter = [&](float*& d, int W) {
+    if (speckle > 1) {
+      if (!uf) uf = A.alloc<int>(2 * static_cast<size_t>(std::max(wl, wr)) * h);
+      launch_remove_speckles(d, W, h, speckle, o.speckle_diff, uf, s);
+    }
+    if (o.median) {
+      float* m = A.alloc<float>(static_cast<size_t>(W) * h);
+      launch_median3x3(d, W, h, m, s);
+      d = m;
+    }
+  };
+  if (P.has_right) {
+    P.disp_r = A.alloc<float>(static_cast<size_t>(wr) * h);
+    blend(P.right, wr, true, static_cast<float>(wr - wl), P.disp_r, nullptr);
+    uint8_t* bad_l = A.alloc<uint8_t>(static_cast<size_t>(wl) * h);
+    if (need_right) {
+      uint8_t* bad_r = A.alloc<uint8_t>(static_cast<size_t>(wr) * h);
+      launch_lr_check(P.disp_r, P.disp_l, wr, h, wl, +1, o.lr_max_diff, bad_r, s);
+      launch_lr_check(P.disp_l, P.disp_r, wl, h, wr, -1, o.lr_max_diff, bad_l, s);
+      launch_apply_bad(P.disp_l, bad_l, static_cast<int64_t>(wl) * h, s);
+      launch_apply_bad(P.disp_r, bad_r, static_cast<int64_t>(wr) * h, s);
+      post_filter(P.disp_r, wr);
+    } else {
+      launch_lr_check(P.disp_l, P.disp_r, wl, h, wr, -1, o.lr_max_diff, bad_l, s);
+      launch_apply_bad(P.disp_l, bad_l, static_cast<int64_t>(wl) * h, s);
+    }
+  }
+  post_filter(P.disp_l, wl);
+  P.coarse_left = P.disp_l;
+  P.coarse_wl = wl;
+  P.coarse_h = h;
+  if (need_right) {
+    P.coarse_right = P.disp_r;
+    P.coarse_wr = wr;
+  } else {
+    P.coarse_right = nullptr;
+  }
+}
+
+// Runs a batch of pairs to completion on stream s.
+void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
+  Workspace& W = workspace();
+  W.arena.reset();
+  W.pinned.reset();
+  Arena& A = W.arena;
+  Pinned& H = W.pinned;
+  std::vector<PairRun> runs(count);
+  int max_levels = 0;
+  for (int i = 0; i < count; ++i) {
+    validate_pair(pairs[i]);
+    PairRun& P = runs[i];
+    P.req = &pairs[i];
+    P.o = pairs[i].options;
+    P.levels = P.o.levels >= 0 ? P.o.levels
+                               : automatic_levels(pairs[i].left.width, pairs[i].left.height, pairs[i].num_disparities);
+    P.check_lr = P.o.lr_max_diff >= 0;
+    P.lr_full = P.check_lr && P.o.lr_full_match != 0;
+    max_levels = std::max(max_levels, P.levels);
+  }
+  for (auto& P : runs) build_levels(P, A, s);
+
+  for (int round = 0; round <= max_levels; ++round) {
+    std::vector<PairRun*> active;
+    // Round r runs level max_levels - r of every pair that has it, so that
+    // all pairs reach level 0 (the largest) in the last round.
+    for (auto& P : runs) {
+      const int l = max_levels - round;
+      if (l <= P.levels) {
+        P.cur = l;
+        active.push_back(&P);
+      }
+    }
+    // Stage 1.
+    bool any_ranged = false;
+    for (PairRun* P : active) {
+      prepare_level(*P, A, H, s);
+      any_ranged = any_ranged || P->left.ranged || (P->has_right && P->right.ranged);
+    }
+    if (any_ranged) R3D_CUDA(cudaStreamSynchronize(s));
+    // Tile sizes and counts.
+    while (true) {
+      bool again = false;
+      for (PairRun* P : active) {
+        const LevelIn& in = P->lv[P->cur];
+        if (!finalize_layout(P->left, in.left.w, in.left.h, in.right.w, P->o, A, H, s)) again = true;
+        if (P->has_right && !finalize_layout(P->right, in.right.w, in.right.h, in.left.w, P->o, A, H, s)) again = true;
+      }
+      if (!again) break;
+      R3D_CUDA(cudaStreamSynchronize(s));
+    }
+    // Stage 2: one SGM launch for every tile of every active match.
+    std::vector<Match*> matches;
+    for (PairRun* P : active) {
+      matches.push_back(&P->left);
+      if (P->has_right) matches.push_back(&P->right);
+    }
+    const int nm = static_cast<int>(matches.size());
+    SgmMatch* hm = H.alloc<SgmMatch>(nm);
+    int njobs = 0, max_num = 16;
+    for (int i = 0; i < nm; ++i) {
+      hm[i] = matches[i]->m;
+      njobs += static_cast<int>(matches[i]->layout.tiles.size());
+      for (int v : matches[i]->tile_maxnum) max_num = std::max(max_num, v);
+    }
+    const int maxc = sgm_maxc_for(max_num);
+    const int rows = sgm_rows_for(maxc, W.smem_optin);
+    SgmJob* hj = H.alloc<SgmJob>(njobs);
+    size_t slot_bytes = 0;
+    int jb = 0;
+    for (int i = 0; i < nm; ++i) {
+      Match& M = *matches[i];
+      const int n = static_cast<int>(M.layout.tiles.size());
+      size_t px_total = 0;
+      M.tile_off.resize(n);
+      for (int t = 0; t < n; ++t) {
+        M.tile_off[t] = px_total;
+        px_total += static_cast<size_t>(M.layout.tiles[t].w) * M.layout.tiles[t].h;
+      }
+      M.tile_disp = A.alloc<float>(px_total);
+      M.tile_conf = M.m.confidence ? A.alloc<float>(px_total) : nullptr;
+      M.d_cells = A.alloc<unsigned long long>(n);
+      M.first_job = jb;
+      for (int t = 0; t < n; ++t) {
+        const Tile& T = M.layout.tiles[t];
+        SgmJob& J = hj[jb++];
+        J = SgmJob{};
+        J.match = i;
+        J.x0 = T.x0;
+        J.y0 = T.y0;
+        J.w = T.w;
+        J.h = T.h;
+        J.disp = M.tile_disp + M.tile_off[t];
+        J.conf = M.tile_conf ? M.tile_conf + M.tile_off[t] : nullptr;
+        J.cells = M.d_cells + t;
+        slot_bytes = std::max(slot_bytes, sgm_slot_layout(T.w, T.h, M.tile_cells[t], maxc, M.m.nd).total);
+      }
+    }
+    // Largest tiles first (longest processing time first).
+    {
+      std::vector<int> order(njobs);
+      for (int i = 0; i < njobs; ++i) order[i] = i;
+      std::vector<uint64_t> work(njobs);
+      for (int i = 0, k = 0; i < nm; ++i)
+        for (size_t t = 0; t < matches[i]->layout.tiles.size(); ++t) work[k++] = matches[i]->tile_cells[t];
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+      std::vector<SgmJob> tmp(hj, hj + njobs);
+      for (int i = 0; i < njobs; ++i) hj[i] = tmp[order[i]];
+    }
+    SgmMatch* dm = A.alloc<SgmMatch>(nm);
+    SgmJob* dj = A.alloc<SgmJob>(njobs);
+    R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch) * nm, cudaMemcpyHostToDevice, s));
+    R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmJob) * njobs, cudaMemcpyHostToDevice, s));
+    // Persistent grid: one CTA per resident slot, bounded by the jobs and by
+    // a scratch budget.
+    int per_sm = 1;
+    {
+      const int smem = sgm_smem_layout(maxc, rows).total;
+      per_sm = std::max(1, std::min(4, (W.smem_optin + 1024) / (smem + 1024)));
+    }
+    const size_t budget = size_t{48} << 30;
+    int grid = std::min(njobs, W.sms * per_sm);
+    grid = std::max(1, std::min<int>(grid, static_cast<int>(std::max<size_t>(1, budget / std::max<size_t>(slot_bytes, 1)))));
+    W.scratch.reserve(static_cast<size_t>(grid) * slot_bytes);
+    R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int), s));
+    ProfileState::Pending ev{};
+    if (t_prof.on) {
+      R3D_CUDA(cudaEventCreate(&ev.a));
+      R3D_CUDA(cudaEventCreate(&ev.b));
+      R3D_CUDA(cudaEventRecord(ev.a, s));
+    }
+    launch_sgm(dm, dj, njobs, maxc, rows, grid, W.scratch.get(), slot_bytes, W.counter.get(), s);
+    if (t_prof.on) {
+      R3D_CUDA(cudaEventRecord(ev.b, s));
+      for (int i = 0; i < nm; ++i)
+        for (size_t t = 0; t < matches[i]->layout.tiles.size(); ++t) {
+          ev.cells += matches[i]->tile_cells[t];
+          ev.pixels += static_cast<uint64_t>(matches[i]->layout.tiles[t].w) * matches[i]->layout.tiles[t].h;
+        }
+      ev.tiles = static_cast<uint64_t>(njobs);
+      t_prof.pending.push_back(ev);
+    }
+    // Stage 3.
+    for (PairRun* P : active) {
+      P->cell_arrays.push_back(P->left.d_cells);
+      P->cell_counts.push_back(static_cast<int>(P->left.layout.tiles.size()));
+      if (P->has_right) {
+        P->cell_arrays.push_back(P->right.d_cells);
+        P->cell_counts.push_back(static_cast<int>(P->right.layout.tiles.size()));
+      }
+      finish_level(*P, A, H, s);
+    }
+  }
+  // Outputs and cell counts.
+  for (auto& P : runs) {
+    r3dgpu_disparity_map& out = const_cast<r3dgpu_pair*>(P.req)->out;
+    const int wl = P.lv[0].left.w, h = P.lv[0].left.h;
+    launch_copy2d_f32(P.coarse_left, wl, wl, h, out.disparity, out.stride, s);
+    if (out.confidence) launch_copy2d_f32(P.conf_l, wl, wl, h, out.confidence, out.stride, s);
+    for (size_t k = 0; k < P.cell_arrays.size(); ++k) {
+      unsigned long long* hc = H.alloc<unsigned long long>(P.cell_counts[k]);
+      R3D_CUDA(cudaMemcpyAsync(hc, P.cell_arrays[k], sizeof(unsigned long long) * P.cell_counts[k],
+                               cudaMemcpyDeviceToHost, s));
+      P.h_cell_arrays.push_back(hc);
+    }
+  }
+  R3D_CUDA(cudaStreamSynchronize(s));
+  H.release_retired();
+  profile_collect();
+  for (auto& P : runs) {
+    uint64_t cells = 0;
+    for (size_t k = 0; k < P.h_cell_arrays.size(); ++k)
+      for (int t = 0; t < P.cell_counts[k]; ++t) cells += P.h_cell_arrays[k][t];
+    r3dgpu_disparity_map& out = const_cast<r3dgpu_pair*>(P.req)->out;
+    out.disparity_min = P.req->disparity_min;
+    out.num_disparities = align16(P.req->num_disparities);
+    out.levels = P.levels;
+    out.cells = cells;
+  }
+}
+
+template <class F>
+r3dgpu_status guarded(F&& f) {
+  try {
+    t_error.clear();
+    f();
+    return R3DGPU_OK;
+  } catch (const Error& e) {
+    t_error = e.what();
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    t_error = "r3dgpu: out of host memory";
+    return R3DGPU_ENOMEM;
+  } catch (const std::exception& e) {
+    t_error = e.what();
+    return R3DGPU_EDEVICE;
+  }
+}
+
+// Host image -> device copy in the arena.
+template <class T>
+T* upload(Arena& A, const T* p, int w, int h, int64_t stride, cudaStream_t s) {
+  T* d = A.alloc<T>(static_cast<size_t>(w) * h);
+  R3D_CUDA(cudaMemcpy2DAsync(d, sizeof(T) * w, p, sizeof(T) * stride, sizeof(T) * w, h, cudaMemcpyHostToDevice, s));
+  return d;
+}
+
+}  // namespace
+}  // namespace r3dgpu
+
+using namespace r3dgpu;
+
+extern "C" {
+
+const char* r3dgpu_last_error(void) { return t_error.c_str(); }
+
+void r3dgpu_default_options(r3dgpu_stereo_options* o) {
+  *o = r3dgpu_stereo_options{};
+  o->p1 = 28;
+  o->p2 = 200;
+  o->p2_adapt = 4;
+  o->invalid_cost = 31;
+  o->subpixel = R3DGPU_SUBPIXEL_EQUIANGULAR;
+  o->uniqueness = 0.0F;
+  o->lr_max_diff = 1;
+  o->lr_full_match = 1;
+  o->speckle_size = 100;
+  o->speckle_diff = 1.0F;
+  o->median = 1;
+  o->levels = -1;
+  o->range_radius = 3;
+  o->range_margin = 4;
+  o->range_fill = 64;
+  o->tile_size = 512;
+  o->tile_margin = 32;
+  o->tile_blend = 32;
+  o->memory_budget = uint64_t{2} << 30;
+  o->scalar_kernels = 0;
+}
+
+int32_t r3dgpu_automatic_levels(int32_t width, int32_t height, int32_t nd) { return automatic_levels(width, height, nd); }
+
+r3dgpu_status r3dgpu_set_device(int32_t device) {
+  return guarded([&] {
+    if (device < 0) fail(R3DGPU_EINVAL, "r3dgpu: negative device index");
+    t_device = device;
+    (void)workspace();
+  });
+}
+
+uint64_t r3dgpu_launch_count(void) { return launch_counter().load(); }
+
+void r3dgpu_profile_enable(int32_t on) { t_prof.on = on != 0; }
+
+void r3dgpu_profile_take(r3dgpu_profile* out) {
+  if (out) *out = t_prof.acc;
+  t_prof.acc = r3dgpu_profile{};
+}
+
+r3dgpu_status r3dgpu_match_stereo_batch(r3dgpu_pair* pairs, int32_t count, void* stream) {
+  return guarded([&] {
+    if (count < 0 || (count > 0 && pairs == nullptr)) fail(R3DGPU_EINVAL, "stereo: bad batch");
+    if (count == 0) return;
+    run_batch(pairs, count, static_cast<cudaStream_t>(stream));
+  });
+}
+
+r3dgpu_status r3dgpu_match_stereo(const r3dgpu_view_u16* left, const r3dgpu_view_u16* right,
+                                  const r3dgpu_view_u8* left_valid, const r3dgpu_view_u8* right_valid,
+                                  int32_t disparity_min, int32_t num_disparities, const r3dgpu_stereo_options* options,
+                                  r3dgpu_disparity_map* out, void* stream) {
+  return guarded([&] {
+    if (!left || !right || !out) fail(R3DGPU_EINVAL, "stereo: null argument");
+    r3dgpu_pair p{};
+    p.left = *left;
+    p.right = *right;
+    if (left_valid) p.left_valid = *left_valid;
+    if (right_valid) p.right_valid = *right_valid;
+    p.disparity_min = disparity_min;
+    p.num_disparities = num_disparities;
+    if (options) {
+      p.options = *options;
+    } else {
+      r3dgpu_default_options(&p.options);
+    }
+    p.out = *out;
+    run_batch(&p, 1, static_cast<cudaStream_t>(stream));
+    *out = p.out;
+  });
+}
+
+r3dgpu_status r3dgpu_match_stereo_host(const r3dgpu_view_u16* left, const r3dgpu_view_u16* right,
+                                       const r3dgpu_view_u8* left_valid, const r3dgpu_view_u8* right_valid,
+                                       int32_t disparity_min, int32_t num_disparities,
+                                       const r3dgpu_stereo_options* options, r3dgpu_disparity_map* out) {
+  return guarded([&] {
+    if (!left || !right || !out || !left->data || !right->data) fail(R3DGPU_EINVAL, "stereo: null argument");
+    if (!out->disparity) fail(R3DGPU_EINVAL, "stereo: missing output buffer");
+    Workspace& W = workspace();
+    cudaStream_t s = nullptr;
+    // Inputs go into a dedicated allocation: run_batch rewinds the arena.
+    const int wl = left->width, wr = right->width, h = left->height;
+    if (wl <= 0 || wr <= 0 || h <= 0 || right->height != h)
+      fail(R3DGPU_EINVAL, "stereo: rectified images must be non-empty with equal height");
+    const bool lm = left_valid && left_valid->data && left_valid->width > 0;
+    const bool rm = right_valid && right_valid->data && right_valid->width > 0;
+    const size_t bytes = sizeof(uint16_t) * (static_cast<size_t>(wl) + wr) * h + (lm ? static_cast<size_t>(wl) * h : 0) +
+                         (rm ? static_cast<size_t>(wr) * h : 0) + 2 * sizeof(float) * static_cast<size_t>(wl) * h + 1024;
+    static thread_local DeviceBuffer<unsigned char> io;
+    io.reserve(bytes);
+    unsigned char* p = io.get();
+    auto take = [&](size_t n) {
+      unsigned char* r = p;
+      p += (n + 255) & ~static_cast<size_t>(255);
+      return r;
+    };
+    uint16_t* dl = reinterpret_cast<uint16_t*>(take(sizeof(uint16_t) * static_cast<size_t>(wl) * h));
+    uint16_t* dr = reinterpret_cast<uint16_t*>(take(sizeof(uint16_t) * static_cast<size_t>(wr) * h));
+    R3D_CUDA(cudaMemcpy2DAsync(dl, 2 * wl, left->data, 2 * left->stride, 2 * wl, h, cudaMemcpyHostToDevice, s));
+    R3D_CUDA(cudaMemcpy2DAsync(dr, 2 * wr, right->data, 2 * right->stride, 2 * wr, h, cudaMemcpyHostToDevice, s));
+    r3dgpu_pair q{};
+    q.left = r3dgpu_view_u16{dl, wl, h, wl};
+    q.right = r3dgpu_view_u16{dr, wr, h, wr};
+    if (lm) {
+      if (left_valid->width != wl || left_valid->height != h)
+        fail(R3DGPU_EINVAL, "stereo: left mask size differs from the image");
+      uint8_t* d = take(static_cast<size_t>(wl) * h);
+      R3D_CUDA(cudaMemcpy2DAsync(d, wl, left_valid->data, left_valid->stride, wl, h, cudaMemcpyHostToDevice, s));
+      q.left_valid = r3dgpu_view_u8{d, wl, h, wl};
+    }
+    if (rm) {
+      if (right_valid->width != wr || right_valid->height != h)
+        fail(R3DGPU_EINVAL, "stereo: right mask size differs from the image");
+      uint8_t* d = take(static_cast<size_t>(wr) * h);
+      R3D_CUDA(cudaMemcpy2DAsync(d, wr, right_valid->data, right_valid->stride, wr, h, cudaMemcpyHostToDevice, s));
+      q.right_valid = r3dgpu_view_u8{d, wr, h, wr};
+    }
+    float* dd = reinterpret_cast<float*>(take(sizeof(float) * static_cast<size_t>(wl) * h));
+    float* dc = reinterpret_cast<float*>(take(sizeof(float) * static_cast<size_t>(wl) * h));
+    q.disparity_min = disparity_min;
+    q.num_disparities = num_disparities;
+    if (options) {
+      q.options = *options;
+    } else {
+      r3dgpu_default_options(&q.options);
+    }
+    q.out.disparity = dd;
+    q.out.confidence = dc;
+    q.out.stride = wl;
+    (void)W;
+    run_batch(&q, 1, s);
+    R3D_CUDA(cudaMemcpy2DAsync(out->disparity, sizeof(float) * out->stride, dd, sizeof(float) * wl, sizeof(float) * wl,
+                               h, cudaMemcpyDeviceToHost, s));
+    if (out->confidence)
+      R3D_CUDA(cudaMemcpy2DAsync(out->confidence, sizeof(float) * out->stride, dc, sizeof(float) * wl,
+                                 sizeof(float) * wl, h, cudaMemcpyDeviceToHost, s));
+    R3D_CUDA(cudaStreamSynchronize(s));
+    out->disparity_min = q.out.disparity_min;
+    out->num_disparities = q.out.num_disparities;
+    out->levels = q.out.levels;
+    out->cells = q.out.cells;
+  });
+}
+
+r3dgpu_status r3dgpu_census_transform(const r3dgpu_view_u16* image, uint64_t* out, int64_t out_stride, void* stream) {
+  return guarded([&] {
+    if (!image || !out) fail(R3DGPU_EINVAL, "census_transform: null argument");
+    (void)workspace();
+    if (image->width <= 0 || image->height <= 0) return;
+    launch_census(image->data, image->stride, image->width, image->height, out, out_stride,
+                  static_cast<cudaStream_t>(stream));
+    R3D_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  });
+}
+
+r3dgpu_status r3dgpu_pyramid_down_u16(const r3dgpu_view_u16* image, uint16_t* out, int64_t out_stride, void* stream) {
+  return guarded([&] {
+    if (!image || !out) fail(R3DGPU_EINVAL, "pyramid_down: null argument");
+    if (image->width <= 0 || image->height <= 0) fail(R3DGPU_EINVAL, "pyramid_down: empty image");
+    (void)workspace();
+    launch_pyramid_u16(image->data, image->stride, image->width, image->height, out, out_stride,
+                       static_cast<cudaStream_t>(stream));
+    R3D_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+  });
+}
+
+r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3dgpu_view_u16* right,
+                                          int32_t disparity_min, int32_t num_disparities,
+                                          const r3dgpu_stereo_options* options, const uint16_t* ranges_lo,
+                                          const uint16_t* ranges_num, uint16_t* out, uint64_t out_capacity,
+                                          uint64_t* out_count) {
+  return guarded([&] {
+    if (!left || !right || !out_count) fail(R3DGPU_EINVAL, "sgm_cost_volume: null argument");
+    r3dgpu_stereo_options o;
+    if (options) {
+      o = *options;
+    } else {
+      r3dgpu_default_options(&o);
+    }
+    check_options(o);
+    const int wl = left->width, wr = right->width, h = left->height;
+    if (wl <= 0 || wr <= 0 || h <= 0 || right->height != h)
+      fail(R3DGPU_EINVAL, "stereo: rectified images must be non-empty with equal height");
+    if (num_disparities <= 0) fail(R3DGPU_EINVAL, "stereo: no disparities to search");
+    const int nd = align16(num_disparities);
+    uint64_t cells = 0;
+    int max_num = nd;
+    if (ranges_lo && ranges_num) {
+      max_num = 0;
+      for (int64_t i = 0; i < static_cast<int64_t>(wl) * h; ++i) {
+        const int lo = ranges_lo[i], n = ranges_num[i];
+        if (n <= 0 || n % 16 != 0 || lo + n > nd)
+          fail(R3DGPU_EINVAL, "stereo: invalid label range " + std::to_string(lo) + " + " + std::to_string(n) +
+                                  " at (" + std::to_string(i % wl) + ", " + std::to_string(i / wl) + ") for " +
+                                  std::to_string(nd) + " labels");
+        cells += static_cast<uint64_t>(n);
+        max_num = std::max(max_num, n);
+      }
+    } else {
+      cells = static_cast<uint64_t>(wl) * h * nd;
+    }
+    *out_count = cells;
+    if (out == nullptr) return;
+    if (out_capacity < cells) fail(R3DGPU_EINVAL, "sgm_cost_volume: output too small");
+    if (cells >= (uint64_t{1} << 31)) fail(R3DGPU_EUNSUPPORTED, "sgm_cost_volume: 2^31 or more labels");
+    Workspace& W = workspace();
+    W.arena.reset();
+    W.pinned.reset();
+    Arena& A = W.arena;
+    cudaStream_t s = nullptr;
+    const uint16_t* dl = upload(A, left->data, wl, h, left->stride, s);
+    const uint16_t* dr = upload(A, right->data, wr, h, right->stride, s);
+    uint64_t* cl = A.alloc<uint64_t>(static_cast<size_t>(wl) * h);
+    uint64_t* cr = A.alloc<uint64_t>(static_cast<size_t>(wr) * h);
+    launch_census(dl, wl, wl, h, cl, wl, s);
+    launch_census(dr, wr, wr, h, cr, wr, s);
+    RowInterval* il = A.alloc<RowInterval>(h);
+    RowInterval* ir = A.alloc<RowInterval>(h);
+    launch_intervals(nullptr, 0, wl, h, il, s);
+    launch_intervals(nullptr, 0, wr, h, ir, s);
+    uint16_t *rlo = nullptr, *rnum = nullptr;
+    if (ranges_lo && ranges_num) {
+      rlo = upload(A, ranges_lo, wl, h, wl, s);
+      rnum = upload(A, ranges_num, wl, h, wl, s);
+    }
+    SgmMatch* hm = W.pinned.alloc<SgmMatch>(1);
+    fill_match(*hm, o, DView<uint16_t>{dl, wl, h, wl}, cl, cr, wr, il, ir, rlo, rnum, disparity_min, nd, false, false);
+    const int maxc = sgm_maxc_for(max_num);
+    const int rows = sgm_rows_for(maxc, W.smem_optin);
+    float* disp = A.alloc<float>(static_cast<size_t>(wl) * h);
+    unsigned long long* dcells = A.alloc<unsigned long long>(1);
+    uint16_t* vol = A.alloc<uint16_t>(cells);
+    SgmJob* hj = W.pinned.alloc<SgmJob>(1);
+    *hj = SgmJob{};
+    hj->match = 0;
+    hj->w = wl;
+    hj->h = h;
+    hj->disp = disp;
+    hj->cells = dcells;
+    hj->volume = vol;
+    SgmMatch* dm = A.alloc<SgmMatch>(1);
+    SgmJob* dj = A.alloc<SgmJob>(1);
+    R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch), cudaMemcpyHostToDevice, s));
+    R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmJob), cudaMemcpyHostToDevice, s));
+    const size_t slot = sgm_slot_layout(wl, h, cells, maxc, nd).total;
+    W.scratch.reserve(slot);
+    R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int), s));
+    launch_sgm(dm, dj, 1, maxc, rows, 1, W.scratch.get(), slot, W.counter.get(), s);
+    R3D_CUDA(cudaMemcpyAsync(out, vol, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s));
+    R3D_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+r3dgpu_status r3dgpu_ranges_from_coarse_host(const float* coarse, int32_t wc, int32_t hc, int32_t width,
+                                             int32_t height, const uint8_t* fine_valid, const uint8_t* partner_valid,
+                                             int32_t partner_width, int32_t partner_sign, int32_t disparity_min,
+                                             int32_t num_disparities, const r3dgpu_stereo_options* options,
+                                             int32_t mirrored, uint16_t* lo_out, uint16_t* num_out) {
+  return guarded([&] {
+    if (!coarse || !lo_out || !num_out) fail(R3DGPU_EINVAL, "ranges_from_coarse: null argument");
+    if (wc != (width + 1) / 2 || hc != (height + 1) / 2)
+      fail(R3DGPU_EINVAL, "stereo: coarse map of " + std::to_string(wc) + "x" + std::to_string(hc) + " for a level of " +
+                              std::to_string(width) + "x" + std::to_string(height));
+    r3dgpu_stereo_options o;
+    if (options) {
+      o = *options;
+    } else {
+      r3dgpu_default_options(&o);
+    }
+    Workspace& W = workspace();
+    W.arena.reset();
+    Arena& A = W.arena;
+    cudaStream_t s = nullptr;
+    const float* dc = upload(A, coarse, wc, hc, wc, s);
+    const uint8_t* dfv = fine_valid ? upload(A, fine_valid, width, height, width, s) : nullptr;
+    const uint8_t* dpv = partner_valid ? upload(A, partner_valid, partner_width, height, partner_width, s) : nullptr;
+    RowInterval* pr = A.alloc<RowInterval>(height);
+    launch_intervals(dpv, partner_width, partner_width, height, pr, s);
+    float* scr = A.alloc<float>(static_cast<size_t>(ranges_scratch_floats(wc, hc, o.range_fill)));
+    uint16_t* lo = A.alloc<uint16_t>(static_cast<size_t>(width) * height);
+    uint16_t* nu = A.alloc<uint16_t>(static_cast<size_t>(width) * height);
+    RangeParams rp{o.range_radius, o.range_margin, o.range_fill, disparity_min, align16(num_disparities), partner_sign,
+                   mirrored ? 1 : 0};
+    launch_ranges_from_coarse(dc, wc, hc, width, height, dfv, width, pr, rp, scr, lo, nu, s);
+    R3D_CUDA(cudaMemcpyAsync(lo_out, lo, sizeof(uint16_t) * width * height, cudaMemcpyDeviceToHost, s));
+    R3D_CUDA(cudaMemcpyAsync(num_out, nu, sizeof(uint16_t) * width * height, cudaMemcpyDeviceToHost, s));
+    R3D_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+r3dgpu_status r3dgpu_remove_speckles_host(float* disparity, int32_t width, int32_t height, int32_t min_size,
+                                          float max_diff) {
+  return guarded([&] {
+    if (!disparity && width > 0 && height > 0) fail(R3DGPU_EINVAL, "remove_speckles: null argument");
+    if (min_size <= 1 || width <= 0 || height <= 0) return;
+    Workspace& W = workspace();
+    W.arena.reset();
+    Arena& A = W.arena;
+    cudaStream_t s = nullptr;
+    float* d = upload(A, static_cast<const float*>(disparity), width, height, width, s);
+    int* uf = A.alloc<int>(2 * static_cast<size_t>(width) * height);
+    launch_remove_speckles(d, width, height, min_size, max_diff, uf, s);
+    R3D_CUDA(cudaMemcpyAsync(disparity, d, sizeof(float) * width * height, cudaMemcpyDeviceToHost, s));
+    R3D_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+r3dgpu_status r3dgpu_median_filter_3x3_host(const float* disparity, int32_t width, int32_t height, float* out) {
+  return guarded([&] {
+    if ((!disparity || !out) && width > 0 && height > 0) fail(R3DGPU_EINVAL, "median_filter_3x3: null argument");
+    if (width <= 0 || height <= 0) return;
+    Workspace& W = workspace();
+    W.arena.reset();
+    Arena& A = W.arena;
+    cudaStream_t s = nullptr;
+    const float* d = upload(A, disparity, width, height, width, s);
+    float* m = A.alloc<float>(static_cast<size_t>(width) * height);
+    launch_median3x3(d, width, height, m, s);
+    R3D_CUDA(cudaMemcpyAsync(out, m, sizeof(float) * width * height, cudaMemcpyDeviceToHost, s));
+    R3D_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,161 @@
+// Portability layer of the r3dgpu kernels.
+//
+// Under nvcc (the product build) every macro below is the plain CUDA
+// construct. Under a host compiler with R3DGPU_SIMT_EMULATION defined (the
+// test-only emulator build, tests/simt/) the same kernel sources run on the
+// CPU: each CUDA thread is a fiber, barriers and warp shuffles switch fibers,
+// cp.async copies are deferred until their wait, and buffers are plain heap
+// allocations so that AddressSanitizer checks every index. The emulator is
+// never part of the product library.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+
+#ifndef R3DGPU_SIMT_EMULATION
+// ============================================================ CUDA build
+#include <cuda_runtime.h>
+
+#define R3D_GLOBAL __global__
+#define R3D_DEVICE __device__ __forceinline__
+#define R3D_DEVICE_NOINLINE __device__
+#define R3D_HOSTDEV __host__ __device__ __forceinline__
+#define R3D_RESTRICT __restrict__
+#define R3D_LAUNCH_BOUNDS(n) __launch_bounds__(n)
+#define R3D_DYNAMIC_SMEM(name) extern __shared__ __align__(16) unsigned char name[]
+#define R3D_LAUNCH(kernel, grid, block, smem, stream, ...) kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__)
+
+namespace r3dsimt {
+
+R3D_DEVICE bool finitef(float v) { return isfinite(v); }
+R3D_DEVICE int imin(int a, int b) { return min(a, b); }
+R3D_DEVICE int imax(int a, int b) { return max(a, b); }
+R3D_DEVICE uint32_t umin(uint32_t a, uint32_t b) { return min(a, b); }
+R3D_DEVICE uint32_t umax(uint32_t a, uint32_t b) { return max(a, b); }
+R3D_DEVICE uint32_t lane_id() { return threadIdx.x & 31u; }
+R3D_DEVICE uint32_t shfl(uint32_t v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+R3D_DEVICE uint32_t shfl_xor(uint32_t v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+R3D_DEVICE void syncwarp() { __syncwarp(); }
+R3D_DEVICE void syncthreads() { __syncthreads(); }
+R3D_DEVICE void fence() { __threadfence(); }
+R3D_DEVICE uint32_t vmin2(uint32_t a, uint32_t b) { return __vminu2(a, b); }
+R3D_DEVICE uint32_t vadd2(uint32_t a, uint32_t b) { return __vadd2(a, b); }
+R3D_DEVICE uint32_t perm(uint32_t a, uint32_t b, uint32_t s) { return __byte_perm(a, b, s); }
+R3D_DEVICE int popc64(uint64_t v) { return __popcll(v); }
+
+// 16-byte asynchronous global -> shared copy (L2 only). Both addresses must
+// be 16-byte aligned.
+R3D_DEVICE void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+R3D_DEVICE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+R3D_DEVICE void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+}  // namespace r3dsimt
+
+#else
+// ============================================================ emulator build
+#include <algorithm>
+#include <cmath>
+#include <functional>
+#include <vector>
+
+#define R3D_GLOBAL
+#define R3D_DEVICE inline
+#define R3D_DEVICE_NOINLINE inline
+#define R3D_HOSTDEV inline
+#define R3D_RESTRICT
+#define R3D_LAUNCH_BOUNDS(n)
+#define R3D_DYNAMIC_SMEM(name) unsigned char* name = ::r3dsimt::dynamic_smem()
+#define R3D_LAUNCH(kernel, grid, block, smem, stream, ...) \
+  ::r3dsimt::launch((grid), (block), (smem), [=]() { kernel(__VA_ARGS__); })
+
+struct dim3 {
+  unsigned x = 1, y = 1, z = 1;
+  dim3(unsigned a = 1, unsigned b = 1, unsigned c = 1) : x(a), y(b), z(c) {}
+};
+struct uint3 {
+  unsigned x, y, z;
+};
+struct alignas(16) int4 {
+  int x, y, z, w;
+};
+inline int4 make_int4(int x, int y, int z, int w) { return int4{x, y, z, w}; }
+
+namespace r3dsimt {
+
+// Per-fiber CUDA coordinates (set by the scheduler).
+struct Coords {
+  uint3 tid, bid;
+  dim3 bdim, gdim;
+};
+const Coords& coords();
+unsigned char* dynamic_smem();
+void launch(dim3 grid, dim3 block, size_t smem, const std::function<void()>& body);
+
+inline bool finitef(float v) { return std::isfinite(v); }
+inline int imin(int a, int b) { return a < b ? a : b; }
+inline int imax(int a, int b) { return a > b ? a : b; }
+inline uint32_t umin(uint32_t a, uint32_t b) { return a < b ? a : b; }
+inline uint32_t umax(uint32_t a, uint32_t b) { return a > b ? a : b; }
+uint32_t lane_id();
+uint32_t shfl(uint32_t v, int src);
+uint32_t shfl_xor(uint32_t v, int m);
+void syncwarp();
+void syncthreads();
+inline void fence() {}
+inline uint32_t vmin2(uint32_t a, uint32_t b) {
+  const uint32_t lo = std::min(a & 0xFFFFu, b & 0xFFFFu), hi = std::min(a >> 16, b >> 16);
+  return lo | (hi << 16);
+}
+inline uint32_t vadd2(uint32_t a, uint32_t b) {
+  return ((a + b) & 0xFFFFu) | (((a >> 16) + (b >> 16)) << 16);
+}
+inline uint32_t perm(uint32_t a, uint32_t b, uint32_t s) {
+  const uint64_t v = (static_cast<uint64_t>(b) << 32) | a;
+  uint32_t r = 0;
+  for (int i = 0; i < 4; ++i) {
+    const unsigned sel = (s >> (4 * i)) & 7u;
+    r |= static_cast<uint32_t>((v >> (8 * sel)) & 0xFFu) << (8 * i);
+  }
+  return r;
+}
+inline int popc64(uint64_t v) { return __builtin_popcountll(v); }
+void cp_async16(void* smem_dst, const void* gmem_src);
+void cp_async_commit();
+void cp_async_wait_n(int n);
+template <int N>
+inline void cp_async_wait() {
+  cp_async_wait_n(N);
+}
+
+}  // namespace r3dsimt
+
+#define threadIdx (::r3dsimt::coords().tid)
+#define blockIdx (::r3dsimt::coords().bid)
+#define blockDim (::r3dsimt::coords().bdim)
+#define gridDim (::r3dsimt::coords().gdim)
+
+// Device intrinsics used by the kernels, with their CUDA semantics.
+inline float __fadd_rn(float a, float b) { return a + b; }
+inline float __fsub_rn(float a, float b) { return a - b; }
+inline float __fmul_rn(float a, float b) { return a * b; }
+inline float __fdiv_rn(float a, float b) { return a / b; }
+inline int atomicAdd(int* p, int v) { const int o = *p; *p = o + v; return o; }
+inline unsigned atomicAdd(unsigned* p, unsigned v) { const unsigned o = *p; *p = o + v; return o; }
+inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v) {
+  const unsigned long long o = *p;
+  *p = o + v;
+  return o;
+}
+inline unsigned atomicMin(unsigned* p, unsigned v) { const unsigned o = *p; if (v < o) *p = v; return o; }
+inline int atomicCAS(int* p, int cmp, int v) { const int o = *p; if (o == cmp) *p = v; return o; }
+template <class T>
+inline T __ldcg(const T* p) { return *p; }
+template <class T>
+inline T __ldg(const T* p) { return *p; }
+#endif

@@ -1,0 +1,316 @@
+"""Python mirror of the reference matcher interface over the r3dgpu C ABI.
+
+Function names, arguments and error behaviour follow r3d::match_stereo and
+its companions (rhiestan/Regard3D_MVS, src/r3d/stereo/stereo_matcher.hpp:82-128,
+census.hpp:20, core/pyramid.hpp:21): invalid options or sizes raise
+``StereoError`` (r3d::Error). Images are 2-D numpy arrays (uint16 grey, uint8
+masks with 255 = valid); 8-bit images must be lifted with ``lift_u8`` (x257,
+as the reference's image reader does, src/r3d/io/image_io.hpp:25-26).
+
+All computation runs in the CUDA library; ``Matcher(lib_path=...)`` can bind a
+different build of the same C ABI (the tests use that for the CPU emulator of
+the kernels).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _native
+from .types import (CDisparityMap, COptions, CPair, CViewU8, CViewU16, DisparityMap, LabelRanges, StereoOptions,
+                    to_c_options)
+
+
+def lift_u8(img: np.ndarray) -> np.ndarray:
+    """8-bit grey -> 16-bit (v * 257), the reference's rule for 8-bit files."""
+    return img.astype(np.uint16) * np.uint16(257)
+
+
+def _u16(a: np.ndarray) -> np.ndarray:
+    a = np.asarray(a)
+    if a.ndim != 2:
+        raise _native.StereoError(1, "stereo: expected a single-channel image")
+    return np.ascontiguousarray(a, dtype=np.uint16)
+
+
+def _view16(a: np.ndarray | None) -> CViewU16:
+    v = CViewU16()
+    if a is not None and a.size:
+        v.data = a.ctypes.data
+        v.height, v.width = a.shape
+        v.stride = a.strides[0] // a.itemsize
+    return v
+
+
+def _view8(a: np.ndarray | None) -> CViewU8:
+    v = CViewU8()
+    if a is not None and a.size:
+        v.data = a.ctypes.data
+        v.height, v.width = a.shape
+        v.stride = a.strides[0] // a.itemsize
+    return v
+
+
+def _opts(options: StereoOptions | None) -> COptions:
+    return to_c_options(options if options is not None else StereoOptions())
+
+
+class Matcher:
+    """Binds the matcher functions to one build of the C ABI and one device."""
+
+    def __init__(self, lib_path: str | None = None, device: int = 0, host_is_device: bool = False):
+        self.lib = _native.load(lib_path)
+        self.device = device
+        # True for builds whose "device" memory is host memory (the emulator).
+        self.host_is_device = host_is_device
+        _native.check(self.lib, self.lib.r3dgpu_set_device(device))
+
+    def _check(self, status: int) -> None:
+        _native.check(self.lib, status)
+
+    # ---------------------------------------------------------------- r3d::match_stereo
+    def match_stereo(self, left, right, left_valid=None, right_valid=None, disparity_min: int = 0,
+                     num_disparities: int = 64, options: StereoOptions | None = None) -> DisparityMap:
+        L, R = _u16(left), _u16(right)
+        lv = None if left_valid is None else np.ascontiguousarray(left_valid, dtype=np.uint8)
+        rv = None if right_valid is None else np.ascontiguousarray(right_valid, dtype=np.uint8)
+        h, w = L.shape
+        disp = np.empty((h, w), np.float32)
+        conf = np.empty((h, w), np.float32)
+        out = CDisparityMap()
+        out.disparity = disp.ctypes.data
+        out.confidence = conf.ctypes.data
+        out.stride = w
+        o = _opts(options)
+        self._check(self.lib.r3dgpu_match_stereo_host(ctypes.byref(_view16(L)), ctypes.byref(_view16(R)),
+                                                      ctypes.byref(_view8(lv)), ctypes.byref(_view8(rv)),
+                                                      int(disparity_min), int(num_disparities), ctypes.byref(o),
+                                                      ctypes.byref(out)))
+        return DisparityMap(disp, conf, out.disparity_min, out.num_disparities, out.levels, int(out.cells))
+
+    # ---------------------------------------------------------------- batched matching
+    def match_stereo_batch(self, pairs: Sequence[dict], stream: int | None = None) -> list[DisparityMap]:
+        """Matches many pairs in one pass of every stage.
+
+        Each pair is a dict with keys left, right, (left_valid, right_valid,)
+        disparity_min, num_disparities, (options). Host arrays are copied to the
+        device (through torch on a GPU build) and results copied back.
+        """
+        keep = []
+        cp = (CPair * len(pairs))()
+        outs = []
+        for i, p in enumerate(pairs):
+            L, R = _u16(p["left"]), _u16(p["right"])
+            lv = p.get("left_valid")
+            rv = p.get("right_valid")
+            lv = None if lv is None else np.ascontiguousarray(lv, dtype=np.uint8)
+            rv = None if rv is None else np.ascontiguousarray(rv, dtype=np.uint8)
+            h, w = L.shape
+            dL, dR, dlv, drv = (self._to_device(a, keep) for a in (L, R, lv, rv))
+            disp, conf = self._empty_device((h, w), keep), self._empty_device((h, w), keep)
+            c = cp[i]
+            c.left = CViewU16(dL, w, h, w)
+            c.right = CViewU16(dR, R.shape[1], h, R.shape[1])
+            c.left_valid = CViewU8(dlv, w, h, w) if lv is not None else CViewU8()
+            c.right_valid = CViewU8(drv, R.shape[1], h, R.shape[1]) if rv is not None else CViewU8()
+            c.disparity_min = int(p.get("disparity_min", 0))
+            c.num_disparities = int(p["num_disparities"])
+            c.options = _opts(p.get("options"))
+            c.out.disparity = disp[0]
+            c.out.confidence = conf[0]
+            c.out.stride = w
+            outs.append((disp, conf, (h, w)))
+        self._check(self.lib.r3dgpu_match_stereo_batch(cp, len(pairs), stream))
+        res = []
+        for i, (disp, conf, shape) in enumerate(outs):
+            res.append(DisparityMap(self._to_host(disp, shape), self._to_host(conf, shape), cp[i].out.disparity_min,
+                                    cp[i].out.num_disparities, cp[i].out.levels, int(cp[i].out.cells)))
+        return res
+
+    def _to_device(self, a: np.ndarray | None, keep: list):
+        if a is None:
+            return None
+        if self.host_is_device:
+            keep.append(a)
+            return a.ctypes.data
+        import torch
+
+        t = torch.from_numpy(a.view(np.int16) if a.dtype == np.uint16 else a).to(f"cuda:{self.device}")
+        keep.append(t)
+        return t.data_ptr()
+
+    def _empty_device(self, shape, keep: list):
+        if self.host_is_device:
+            a = np.empty(shape, np.float32)
+            keep.append(a)
+            return (a.ctypes.data, a)
+        import torch
+
+        t = torch.empty(shape, dtype=torch.float32, device=f"cuda:{self.device}")
+        keep.append(t)
+        return (t.data_ptr(), t)
+
+    def _to_host(self, d, shape) -> np.ndarray:
+        obj = d[1]
+        if self.host_is_device:
+            return obj
+        return obj.cpu().numpy()
+
+    # ---------------------------------------------------------------- companions
+    def census_transform(self, img) -> np.ndarray:
+        """census.hpp:20: u64 Census code per pixel."""
+        I = _u16(img)
+        h, w = I.shape
+        keep: list = []
+        dI = self._to_device(I, keep)
+        out = self._empty_u64((h, w), keep)
+        v = CViewU16(dI, w, h, w)
+        self._check(self.lib.r3dgpu_census_transform(ctypes.byref(v), out[0], w, None))
+        return self._u64_to_host(out)
+
+    def pyramid_down(self, img) -> np.ndarray:
+        """pyramid.hpp:21: one 2x binomial reduction of a 16-bit image."""
+        I = _u16(img)
+        h, w = I.shape
+        keep: list = []
+        dI = self._to_device(I, keep)
+        dh, dw = (h + 1) // 2, (w + 1) // 2
+        if self.host_is_device:
+            out = np.empty((dh, dw), np.uint16)
+            ptr = out.ctypes.data
+        else:
+            import torch
+
+            t = torch.empty((dh, dw), dtype=torch.int16, device=f"cuda:{self.device}")
+            ptr = t.data_ptr()
+        v = CViewU16(dI, w, h, w)
+        self._check(self.lib.r3dgpu_pyramid_down_u16(ctypes.byref(v), ptr, dw, None))
+        if self.host_is_device:
+            return out
+        return t.cpu().numpy().view(np.uint16)
+
+    def _empty_u64(self, shape, keep):
+        if self.host_is_device:
+            a = np.empty(shape, np.uint64)
+            keep.append(a)
+            return (a.ctypes.data, a)
+        import torch
+
+        t = torch.empty(shape, dtype=torch.int64, device=f"cuda:{self.device}")
+        keep.append(t)
+        return (t.data_ptr(), t)
+
+    def _u64_to_host(self, d) -> np.ndarray:
+        if self.host_is_device:
+            return d[1]
+        return d[1].cpu().numpy().view(np.uint64)
+
+    def sgm_cost_volume(self, left, right, disparity_min: int, num_disparities: int,
+                        options: StereoOptions | None = None, ranges: LabelRanges | None = None) -> np.ndarray:
+        """detail::sgm_cost_volume (stereo_matcher.hpp:98-101): the aggregated
+        volume of the whole image as one tile, labels of every pixel in
+        row-major pixel order."""
+        L, R = _u16(left), _u16(right)
+        o = _opts(options)
+        lo = num = None
+        if ranges is not None:
+            lo = np.ascontiguousarray(ranges.lo, dtype=np.uint16)
+            num = np.ascontiguousarray(ranges.num, dtype=np.uint16)
+        count = ctypes.c_uint64(0)
+        args = (ctypes.byref(_view16(L)), ctypes.byref(_view16(R)), int(disparity_min), int(num_disparities),
+                ctypes.byref(o), None if lo is None else lo.ctypes.data, None if num is None else num.ctypes.data)
+        self._check(self.lib.r3dgpu_sgm_cost_volume_host(*args, None, 0, ctypes.byref(count)))
+        out = np.empty(count.value, np.uint16)
+        self._check(self.lib.r3dgpu_sgm_cost_volume_host(*args, out.ctypes.data, count.value, ctypes.byref(count)))
+        return out
+
+    def ranges_from_coarse(self, coarse, width: int, height: int, fine_valid, partner_valid, partner_width: int,
+                           partner_sign: int, disparity_min: int, num_disparities: int,
+                           options: StereoOptions | None = None, mirrored: bool = False) -> LabelRanges:
+        """detail::ranges_from_coarse (stereo_matcher.hpp:121-125)."""
+        C = np.ascontiguousarray(coarse, dtype=np.float32)
+        fv = None if fine_valid is None else np.ascontiguousarray(fine_valid, dtype=np.uint8)
+        pv = None if partner_valid is None else np.ascontiguousarray(partner_valid, dtype=np.uint8)
+        lo = np.empty((height, width), np.uint16)
+        num = np.empty((height, width), np.uint16)
+        o = _opts(options)
+        self._check(self.lib.r3dgpu_ranges_from_coarse_host(
+            C.ctypes.data, C.shape[1], C.shape[0], width, height, None if fv is None else fv.ctypes.data,
+            None if pv is None else pv.ctypes.data, partner_width, partner_sign, disparity_min, num_disparities,
+            ctypes.byref(o), int(bool(mirrored)), lo.ctypes.data, num.ctypes.data))
+        return LabelRanges(lo, num)
+
+    def remove_speckles(self, disparity: np.ndarray, min_size: int, max_diff: float) -> np.ndarray:
+        """stereo_matcher.hpp:89 (in place on a C-contiguous float32 array; returned as well)."""
+        d = disparity if (disparity.dtype == np.float32 and disparity.flags.c_contiguous) else \
+            np.ascontiguousarray(disparity, dtype=np.float32)
+        self._check(self.lib.r3dgpu_remove_speckles_host(d.ctypes.data, d.shape[1], d.shape[0], int(min_size),
+                                                         float(max_diff)))
+        return d
+
+    def median_filter_3x3(self, disparity: np.ndarray) -> np.ndarray:
+        """stereo_matcher.hpp:91"""
+        d = np.ascontiguousarray(disparity, dtype=np.float32)
+        out = np.empty_like(d)
+        self._check(self.lib.r3dgpu_median_filter_3x3_host(d.ctypes.data, d.shape[1], d.shape[0], out.ctypes.data))
+        return out
+
+    def automatic_levels(self, width: int, height: int, num_disparities: int) -> int:
+        return int(self.lib.r3dgpu_automatic_levels(width, height, num_disparities))
+
+    def launch_count(self) -> int:
+        return int(self.lib.r3dgpu_launch_count())
+
+
+_default: Matcher | None = None
+
+
+def default_matcher() -> Matcher:
+    global _default
+    if _default is None:
+        _default = Matcher()
+    return _default
+
+
+def match_stereo(left, right, left_valid=None, right_valid=None, disparity_min: int = 0, num_disparities: int = 64,
+                 options: StereoOptions | None = None) -> DisparityMap:
+    return default_matcher().match_stereo(left, right, left_valid, right_valid, disparity_min, num_disparities, options)
+
+
+def match_stereo_batch(pairs: Sequence[dict]) -> list[DisparityMap]:
+    return default_matcher().match_stereo_batch(pairs)
+
+
+def census_transform(img) -> np.ndarray:
+    return default_matcher().census_transform(img)
+
+
+def pyramid_down(img) -> np.ndarray:
+    return default_matcher().pyramid_down(img)
+
+
+def remove_speckles(disparity: np.ndarray, min_size: int, max_diff: float) -> np.ndarray:
+    return default_matcher().remove_speckles(disparity, min_size, max_diff)
+
+
+def median_filter_3x3(disparity: np.ndarray) -> np.ndarray:
+    return default_matcher().median_filter_3x3(disparity)
+
+
+class detail:  # noqa: N801 — mirrors the reference's r3d::detail namespace
+    @staticmethod
+    def sgm_cost_volume(left, right, disparity_min, num_disparities, options=None, ranges=None):
+        return default_matcher().sgm_cost_volume(left, right, disparity_min, num_disparities, options, ranges)
+
+    @staticmethod
+    def ranges_from_coarse(coarse, width, height, fine_valid, partner_valid, partner_width, partner_sign,
+                           disparity_min, num_disparities, options=None, mirrored=False):
+        return default_matcher().ranges_from_coarse(coarse, width, height, fine_valid, partner_valid, partner_width,
+                                                    partner_sign, disparity_min, num_disparities, options, mirrored)
+
+    @staticmethod
+    def automatic_levels(width, height, num_disparities):
+        return default_matcher().automatic_levels(width, height, num_disparities)

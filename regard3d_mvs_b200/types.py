@@ -1,0 +1,184 @@
+"""Option and result types of the matcher, mirroring the reference's C++ types.
+
+``StereoOptions`` and ``DisparityMap`` follow r3d::StereoOptions and
+r3d::DisparityMap (rhiestan/Regard3D_MVS, src/r3d/stereo/stereo_matcher.hpp:23-68):
+same field names, meanings and defaults. The ctypes structures mirror
+include/r3dgpu.h field for field.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import enum
+from dataclasses import dataclass, field
+
+import numpy as np
+
+INVALID_DISPARITY = float("inf")  # kInvalidDisparity, stereo_matcher.hpp:59
+
+
+class SubpixelMethod(enum.IntEnum):
+    """stereo_matcher.hpp:23-27"""
+
+    none = 0
+    parabola = 1
+    equiangular = 2
+
+
+@dataclass
+class StereoOptions:
+    """stereo_matcher.hpp:30-57 (defaults tuned by the reference on Middlebury 2014)."""
+
+    p1: int = 28
+    p2: int = 200
+    p2_adapt: int = 4
+    invalid_cost: int = 31
+    subpixel: SubpixelMethod = SubpixelMethod.equiangular
+    uniqueness: float = 0.0
+    lr_max_diff: int = 1
+    lr_full_match: bool = True
+    speckle_size: int = 100
+    speckle_diff: float = 1.0
+    median: bool = True
+    levels: int = -1
+    range_radius: int = 3
+    range_margin: int = 4
+    range_fill: int = 64
+    tile_size: int = 512
+    tile_margin: int = 32
+    tile_blend: int = 32
+    memory_budget: int = 2 << 30
+    scalar_kernels: bool = False  # accepted for interface parity; the GPU build has one kernel path
+
+
+@dataclass
+class DisparityMap:
+    """stereo_matcher.hpp:61-68: disparity is x_left - x_right (+inf where unknown)."""
+
+    disparity: np.ndarray
+    confidence: np.ndarray
+    disparity_min: int = 0
+    num_disparities: int = 0
+    levels: int = 0
+    cells: int = 0
+
+
+@dataclass
+class LabelRanges:
+    """stereo_matcher.hpp:73-76: pixel (x, y) searches labels lo .. lo + num - 1."""
+
+    lo: np.ndarray
+    num: np.ndarray
+
+
+class COptions(ctypes.Structure):
+    _fields_ = [
+        ("p1", ctypes.c_int32),
+        ("p2", ctypes.c_int32),
+        ("p2_adapt", ctypes.c_int32),
+        ("invalid_cost", ctypes.c_int32),
+        ("subpixel", ctypes.c_int32),
+        ("uniqueness", ctypes.c_float),
+        ("lr_max_diff", ctypes.c_int32),
+        ("lr_full_match", ctypes.c_int32),
+        ("speckle_size", ctypes.c_int32),
+        ("speckle_diff", ctypes.c_float),
+        ("median", ctypes.c_int32),
+        ("levels", ctypes.c_int32),
+        ("range_radius", ctypes.c_int32),
+        ("range_margin", ctypes.c_int32),
+        ("range_fill", ctypes.c_int32),
+        ("tile_size", ctypes.c_int32),
+        ("tile_margin", ctypes.c_int32),
+        ("tile_blend", ctypes.c_int32),
+        ("memory_budget", ctypes.c_uint64),
+        ("scalar_kernels", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+class CViewU16(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("stride", ctypes.c_int64)]
+
+
+class CViewU8(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+                ("stride", ctypes.c_int64)]
+
+
+class CDisparityMap(ctypes.Structure):
+    _fields_ = [
+        ("disparity", ctypes.c_void_p),
+        ("confidence", ctypes.c_void_p),
+        ("stride", ctypes.c_int64),
+        ("disparity_min", ctypes.c_int32),
+        ("num_disparities", ctypes.c_int32),
+        ("levels", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("cells", ctypes.c_uint64),
+    ]
+
+
+class CPair(ctypes.Structure):
+    _fields_ = [
+        ("left", CViewU16),
+        ("right", CViewU16),
+        ("left_valid", CViewU8),
+        ("right_valid", CViewU8),
+        ("disparity_min", ctypes.c_int32),
+        ("num_disparities", ctypes.c_int32),
+        ("options", COptions),
+        ("out", CDisparityMap),
+    ]
+
+
+class CProfile(ctypes.Structure):
+    _fields_ = [
+        ("sgm_ms", ctypes.c_double),
+        ("sgm_launches", ctypes.c_uint64),
+        ("sgm_cells", ctypes.c_uint64),
+        ("sgm_tiles", ctypes.c_uint64),
+        ("sgm_pixels", ctypes.c_uint64),
+    ]
+
+
+class CSynthParams(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("num_disparities", ctypes.c_int32),
+        ("seed", ctypes.c_uint32),
+        ("blur_sigma", ctypes.c_float),
+        ("noise_sigma", ctypes.c_float),
+        ("planes", ctypes.c_int32),
+        ("textureless_fraction", ctypes.c_float),
+        ("occluded_fraction", ctypes.c_float),
+    ]
+
+
+def to_c_options(o) -> COptions:
+    """Fills the C struct from a StereoOptions (or any object with its fields)."""
+    c = COptions()
+    c.p1 = int(o.p1)
+    c.p2 = int(o.p2)
+    c.p2_adapt = int(o.p2_adapt)
+    c.invalid_cost = int(o.invalid_cost)
+    c.subpixel = int(o.subpixel)
+    c.uniqueness = float(o.uniqueness)
+    c.lr_max_diff = int(o.lr_max_diff)
+    c.lr_full_match = int(bool(o.lr_full_match))
+    c.speckle_size = int(o.speckle_size)
+    c.speckle_diff = float(o.speckle_diff)
+    c.median = int(bool(o.median))
+    c.levels = int(o.levels)
+    c.range_radius = int(o.range_radius)
+    c.range_margin = int(o.range_margin)
+    c.range_fill = int(o.range_fill)
+    c.tile_size = int(o.tile_size)
+    c.tile_margin = int(o.tile_margin)
+    c.tile_blend = int(o.tile_blend)
+    c.memory_budget = int(o.memory_budget)
+    c.scalar_kernels = int(bool(o.scalar_kernels))
+    c.reserved = 0
+    return c

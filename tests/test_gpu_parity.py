@@ -1,0 +1,251 @@
+"""GPU parity: the CUDA library (through its C ABI) against the CPU oracle.
+
+Integer outputs (Census codes, aggregated volumes, label ranges, cell
+counts) must be bit-exact; disparity maps too, since the library reproduces
+the reference's float operations one by one (tolerance 0 here; the contract
+bound for subpixel values is 1e-4 px). Cases follow the reference's stereo
+tests (tests/test_stereo.cpp) plus the 640x480 / 128-label single-level pair
+and a smaller hierarchical pair.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from images import Rng, Texture, mismatch_report, random_image, render_pair, same_disparities, to_u16
+from regard3d_mvs_b200.types import LabelRanges, StereoOptions, SubpixelMethod
+
+pytestmark = pytest.mark.gpu
+
+SUBPIXEL_TOL = 1e-4  # px; disparities are compared exactly, the bound is stated for the record
+
+
+def _assert_same_map(a, b):
+    assert same_disparities(a.disparity, b.disparity), mismatch_report(a.disparity, b.disparity)
+    assert a.cells == b.cells
+    assert a.levels == b.levels
+    assert a.num_disparities == b.num_disparities
+
+
+def test_census(gpu_matcher, oracle):
+    for w in (1, 5, 16, 31, 64, 77, 640):
+        img = random_image(w, 13, w)
+        if w % 2 == 0:
+            img = (img >> 13).astype(np.uint16)  # 8 levels: many ties
+        assert np.array_equal(gpu_matcher.census_transform(img), oracle.census_transform(img))
+
+
+def test_pyramid(gpu_matcher, oracle):
+    for w, h in ((77, 41), (640, 480), (1, 1), (3, 2)):
+        img = random_image(w, h, w + h)
+        assert np.array_equal(gpu_matcher.pyramid_down(img), oracle.pyramid_down(img))
+
+
+@pytest.mark.parametrize("p2_adapt", [0, 12])
+@pytest.mark.parametrize("dmin,nd", [(-3, 16), (2, 48)])
+def test_volume_equals_textbook(gpu_matcher, oracle, p2_adapt, dmin, nd):
+    # tests/test_stereo.cpp:87-117
+    tex = Texture(3)
+    left, right, _ = render_pair(tex, 41, 23, lambda x, y: 5.0 + 0.1 * x)
+    noise = random_image(41, 23, 9)
+    right = right ^ (noise & 0x0F00)
+    o = StereoOptions(p2_adapt=p2_adapt, p2=120)
+    assert np.array_equal(gpu_matcher.sgm_cost_volume(left, right, dmin, nd, o),
+                          oracle.sgm_cost_volume(left, right, dmin, nd, o))
+
+
+def test_volume_with_ranges(gpu_matcher, oracle):
+    # tests/test_stereo.cpp:119-151
+    tex = Texture(13)
+    w, h, nd = 37, 19, 96
+    left, right, _ = render_pair(tex, w, h, lambda x, y: 20.0 + 0.5 * x - 0.3 * y)
+    r = Rng(31)
+    num = np.zeros((h, w), np.uint16)
+    lo = np.zeros((h, w), np.uint16)
+    for y in range(h):
+        for x in range(w):
+            n = 16 * r.uniform_int(1, 3)
+            num[y, x] = n
+            lo[y, x] = r.uniform_int(0, nd - n)
+    o = StereoOptions(p2=150, p2_adapt=8)
+    got = gpu_matcher.sgm_cost_volume(left, right, -2, nd, o, LabelRanges(lo, num))
+    assert np.array_equal(got, oracle.sgm_cost_volume(left, right, -2, nd, o, (lo, num)))
+    full = LabelRanges(np.zeros((h, w), np.uint16), np.full((h, w), nd, np.uint16))
+    assert np.array_equal(gpu_matcher.sgm_cost_volume(left, right, -2, nd, o, full),
+                          gpu_matcher.sgm_cost_volume(left, right, -2, nd, o))
+
+
+def test_volume_large_labels(gpu_matcher, oracle):
+    # Several 64-label chunks per pixel and sums that wrap modulo 2^16.
+    tex = Texture(17)
+    left, right, _ = render_pair(tex, 48, 20, lambda x, y: 30.0 + 0.2 * x)
+    o = StereoOptions(p1=300, p2=8000, p2_adapt=0, invalid_cost=255)
+    for nd in (208, 400):
+        assert np.array_equal(gpu_matcher.sgm_cost_volume(left, right, -5, nd, o),
+                              oracle.sgm_cost_volume(left, right, -5, nd, o))
+
+
+@pytest.mark.parametrize("method", [SubpixelMethod.parabola, SubpixelMethod.equiangular])
+def test_slanted_plane(gpu_matcher, oracle, method):
+    tex = Texture(11)
+    left, right, _ = render_pair(tex, 200, 120, lambda x, y: 12.3 + 0.04 * x + 0.02 * y)
+    o = StereoOptions(subpixel=method)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, 0, 32, o),
+                     oracle.match_stereo(left, right, None, None, 0, 32, o))
+
+
+@pytest.mark.parametrize("opts", [
+    StereoOptions(tile_size=48, tile_margin=8, tile_blend=8),
+    StereoOptions(tile_size=48, tile_margin=8, tile_blend=8, lr_full_match=False),
+    StereoOptions(tile_size=1024),
+    StereoOptions(tile_size=48, tile_margin=8, tile_blend=0, uniqueness=0.15, subpixel=SubpixelMethod.none),
+    StereoOptions(lr_max_diff=-1, speckle_size=0, median=False, levels=1),
+])
+def test_tiles_and_options(gpu_matcher, oracle, opts):
+    tex = Texture(5)
+    left, right, _ = render_pair(tex, 150, 90, lambda x, y: np.where(x < 70, 6.0, 14.5))
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, 0, 32, opts),
+                     oracle.match_stereo(left, right, None, None, 0, 32, opts))
+
+
+@pytest.mark.parametrize("levels", [0, 1])
+def test_masks(gpu_matcher, oracle, levels):
+    tex = Texture(8)
+    left, right, _ = render_pair(tex, 120, 60, lambda x, y: 10.0 + 0 * x)
+    lm = np.full((60, 120), 255, np.uint8)
+    rm = np.full((60, 120), 255, np.uint8)
+    lm[:, 100:] = 0
+    rm[:, :40] = 0
+    lm[7, :] = 0  # a fully masked row
+    o = StereoOptions(levels=levels)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, lm, rm, 0, 32, o),
+                     oracle.match_stereo(left, right, lm, rm, 0, 32, o))
+
+
+@pytest.mark.parametrize("full", [False, True])
+def test_masked_wedge_lr(gpu_matcher, oracle, full):
+    tex = Texture(21)
+    left, right, _ = render_pair(tex, 160, 60, lambda x, y: 10.0 + 0 * x)
+    r = Rng(4)
+    nl = np.array([r.normal(0.0, 3000.0) for _ in range(2 * 160 * 60)])
+    left = to_u16(left + nl[0::2].reshape(60, 160))
+    right = to_u16(right + nl[1::2].reshape(60, 160))
+    y, x = np.mgrid[0:60, 0:160]
+    lmask = np.where(x < 70 + 2 * y, 255, 0).astype(np.uint8)
+    o = StereoOptions(lr_full_match=full, tile_size=64)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, lmask, None, 0, 256, o),
+                     oracle.match_stereo(left, right, lmask, None, 0, 256, o))
+
+
+@pytest.mark.parametrize("levels", [0, 1])
+@pytest.mark.parametrize("full", [False, True])
+def test_different_widths_negative_disparities(gpu_matcher, oracle, levels, full):
+    tex = Texture(23)
+    wl, wr, h, d = 150, 190, 60, -7.0
+    yy, xl = np.mgrid[0:h, 0:wl].astype(np.float64)
+    yr, xr = np.mgrid[0:h, 0:wr].astype(np.float64)
+    left = to_u16(tex(xl, yy))
+    right = to_u16(tex(xr + d, yr))
+    o = StereoOptions(lr_full_match=full, levels=levels)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, -20, 32, o),
+                     oracle.match_stereo(left, right, None, None, -20, 32, o))
+
+
+def test_ranges_from_coarse(gpu_matcher, oracle):
+    wc, hc = 40, 20
+    coarse = np.where(np.arange(wc)[None, :] < wc // 2, 10.0, 30.0).astype(np.float32).repeat(hc, 0)
+    coarse[5, 5] = np.inf
+    coarse[:, 30:] = np.inf
+    w, h, dmin, nd = 2 * wc, 2 * hc, 4, 96
+    valid = np.full((h, w), 255, np.uint8)
+    valid[1, 1] = 0
+    o = StereoOptions(range_radius=1, range_margin=3, range_fill=4)
+    for fv, pv, pw, sign, mir in ((valid, None, 1000, 1, False), (valid, None, w, -1, False), (None, valid, w, 1, True)):
+        a = gpu_matcher.ranges_from_coarse(coarse, w, h, fv, pv, pw, sign, dmin, nd, o, mir)
+        b = oracle.ranges_from_coarse(coarse, w, h, fv, pv, pw, sign, dmin, nd, o, mir)
+        assert np.array_equal(a.lo, b[0]) and np.array_equal(a.num, b[1])
+
+
+def test_speckle_and_median(gpu_matcher, oracle):
+    rng = np.random.default_rng(3)
+    d = np.round(rng.normal(20, 3, (90, 130))).astype(np.float32)
+    d[rng.random(d.shape) < 0.1] = np.inf
+    for size in (2, 6, 40):
+        assert same_disparities(gpu_matcher.remove_speckles(d.copy(), size, 1.0), oracle.remove_speckles(d, size, 1.0))
+    assert same_disparities(gpu_matcher.median_filter_3x3(d), oracle.median_filter_3x3(d))
+
+
+def _synthetic_pair(w, h, nd, seed):
+    """Blurred uniform noise, piecewise-planar disparity, bilinear warp, noise."""
+    rng = np.random.default_rng(seed)
+    base = rng.uniform(0, 255, (h, w + nd + 8))
+    k = np.exp(-0.5 * (np.arange(-5, 6) / 1.5) ** 2)
+    k /= k.sum()
+    base = np.apply_along_axis(lambda r: np.convolve(r, k, mode="same"), 1, base)
+    base = np.apply_along_axis(lambda c: np.convolve(c, k, mode="same"), 0, base)
+    base = (base - base.min()) / (base.max() - base.min()) * 255.0
+    ys, xs = np.mgrid[0:h, 0:w].astype(np.float64)
+    seeds = rng.uniform(0, 1, (8, 2)) * [w, h]
+    planes = np.stack([rng.uniform(-0.02, 0.02, 8), rng.uniform(-0.02, 0.02, 8), rng.uniform(5, nd - 8, 8)], 1)
+    lab = np.argmin((xs[..., None] - seeds[:, 0]) ** 2 + (ys[..., None] - seeds[:, 1]) ** 2, axis=-1)
+    disp = np.clip(planes[lab, 0] * xs + planes[lab, 1] * ys + planes[lab, 2], 5, nd - 8)
+    left = base[:, :w]
+    xsrc = xs + disp
+    x0 = np.floor(xsrc).astype(int)
+    f = xsrc - x0
+    right = base[np.arange(h)[:, None], x0] * (1 - f) + base[np.arange(h)[:, None], x0 + 1] * f
+    right = right + rng.normal(0, 2, right.shape)
+    L = np.clip(np.round(left), 0, 255).astype(np.uint8)
+    R = np.clip(np.round(right), 0, 255).astype(np.uint8)
+    return L.astype(np.uint16) * 257, R.astype(np.uint16) * 257
+
+
+def test_single_level_640x480_128(gpu_matcher, oracle):
+    """The reference's CPU-runnable configuration: 640x480, labels 0..127, one level."""
+    left, right = _synthetic_pair(640, 480, 128, 1)
+    o = StereoOptions(levels=0)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, 0, 128, o),
+                     oracle.match_stereo(left, right, None, None, 0, 128, o))
+
+
+def test_hierarchical_pair(gpu_matcher, oracle):
+    """Hierarchy with per-pixel ranges (+-8 around the upsampled coarse disparity)."""
+    left, right = _synthetic_pair(768, 512, 256, 2)
+    o = StereoOptions(levels=3, range_radius=0, range_margin=8)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, 0, 256, o),
+                     oracle.match_stereo(left, right, None, None, 0, 256, o))
+    o = StereoOptions(levels=-1)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, 0, 256, o),
+                     oracle.match_stereo(left, right, None, None, 0, 256, o))
+
+
+def test_batch_equals_single(gpu_matcher):
+    """Pairs of uneven size, range and depth matched together give the same
+    maps as matched one by one."""
+    pairs = []
+    for i, (w, h, nd, lv) in enumerate(((320, 240, 64, 0), (256, 200, 128, 2), (400, 300, 96, -1), (96, 64, 32, 0))):
+        left, right = _synthetic_pair(w, h, nd, 10 + i)
+        pairs.append(dict(left=left, right=right, disparity_min=0, num_disparities=nd, options=StereoOptions(levels=lv)))
+    batch = gpu_matcher.match_stereo_batch(pairs)
+    for p, b in zip(pairs, batch):
+        s = gpu_matcher.match_stereo(p["left"], p["right"], None, None, 0, p["num_disparities"], p["options"])
+        _assert_same_map(b, s)
+        assert np.array_equal(b.confidence, s.confidence)
+
+
+def test_errors(gpu_matcher):
+    from regard3d_mvs_b200 import StereoError
+
+    img = random_image(32, 16, 1)
+    with pytest.raises(StereoError):
+        gpu_matcher.match_stereo(img, img, None, None, 0, 16, StereoOptions(p1=300, p2=200))
+    with pytest.raises(StereoError):
+        gpu_matcher.match_stereo(img, img, None, None, 0, 0)
+    with pytest.raises(StereoError):
+        gpu_matcher.match_stereo(img, img[:8], None, None, 0, 16)
+    with pytest.raises(StereoError):
+        gpu_matcher.match_stereo(img, img, np.zeros((3, 3), np.uint8), None, 0, 16)
+    # The context stays usable after errors.
+    r = gpu_matcher.match_stereo(img, img, None, None, 0, 16, StereoOptions(levels=0))
+    assert r.disparity.shape == (16, 32)
