@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "sgm.h"
+#include "sgm_full.h"
 
 namespace r3dgpu {
 namespace {
@@ -417,6 +418,11 @@ void fill_match(SgmMatch& m, const r3dgpu_stereo_options& o, const DView<uint16_
   m.diagonal_lr = diagonal ? 1 : 0;
   m.confidence = confidence ? 1 : 0;
   p2_lut(o, m.lut);
+  // A path value is at most max(P2) + max(cost) (min_q + P2 bounds the best
+  // predecessor term); 8 of them fit 16 bits unless the penalties are extreme.
+  int max_p2 = 0;
+  for (int i = 0; i < 256; ++i) max_p2 = std::max(max_p2, static_cast<int>(m.lut[i]));
+  m.sum_no_carry = 8 * (max_p2 + std::max(o.invalid_cost, 62)) <= 65535 ? 1 : 0;
 }
 
 // Stage 1 of a level: mirrored inputs, Census images, row intervals, label
@@ -683,7 +689,8 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
       if (!again) break;
       R3D_CUDA(cudaStreamSynchronize(s));
     }
-    // Stage 2: one SGM launch for every tile of every active match.
+    // Stage 2: SGM launches. Full-range matches go to the full-range kernel,
+    // one launch per label-count shape; ranged matches to the general kernel.
     std::vector<Match*> matches;
     for (PairRun* P : active) {
       matches.push_back(&P->left);
@@ -691,18 +698,8 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     }
     const int nm = static_cast<int>(matches.size());
     SgmMatch* hm = H.alloc<SgmMatch>(nm);
-    int njobs = 0, max_num = 16;
     for (int i = 0; i < nm; ++i) {
       hm[i] = matches[i]->m;
-      njobs += static_cast<int>(matches[i]->layout.tiles.size());
-      for (int v : matches[i]->tile_maxnum) max_num = std::max(max_num, v);
-    }
-    const int maxc = sgm_maxc_for(max_num);
-    const int rows = sgm_rows_for(maxc, W.smem_optin);
-    SgmJob* hj = H.alloc<SgmJob>(njobs);
-    size_t slot_bytes = 0;
-    int jb = 0;
-    for (int i = 0; i < nm; ++i) {
       Match& M = *matches[i];
       const int n = static_cast<int>(M.layout.tiles.size());
       size_t px_total = 0;
@@ -714,65 +711,100 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
       M.tile_disp = A.alloc<float>(px_total);
       M.tile_conf = M.m.confidence ? A.alloc<float>(px_total) : nullptr;
       M.d_cells = A.alloc<unsigned long long>(n);
-      M.first_job = jb;
-      for (int t = 0; t < n; ++t) {
-        const Tile& T = M.layout.tiles[t];
-        SgmJob& J = hj[jb++];
-        J = SgmJob{};
-        J.match = i;
-        J.x0 = T.x0;
-        J.y0 = T.y0;
-        J.w = T.w;
-        J.h = T.h;
-        J.disp = M.tile_disp + M.tile_off[t];
-        J.conf = M.tile_conf ? M.tile_conf + M.tile_off[t] : nullptr;
-        J.cells = M.d_cells + t;
-        slot_bytes = std::max(slot_bytes, sgm_slot_layout(T.w, T.h, M.tile_cells[t], maxc, M.m.nd).total);
-      }
-    }
-    // Largest tiles first (longest processing time first).
-    {
-      std::vector<int> order(njobs);
-      for (int i = 0; i < njobs; ++i) order[i] = i;
-      std::vector<uint64_t> work(njobs);
-      for (int i = 0, k = 0; i < nm; ++i)
-        for (size_t t = 0; t < matches[i]->layout.tiles.size(); ++t) work[k++] = matches[i]->tile_cells[t];
-      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
-      std::vector<SgmJob> tmp(hj, hj + njobs);
-      for (int i = 0; i < njobs; ++i) hj[i] = tmp[order[i]];
     }
     SgmMatch* dm = A.alloc<SgmMatch>(nm);
-    SgmJob* dj = A.alloc<SgmJob>(njobs);
     R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch) * nm, cudaMemcpyHostToDevice, s));
-    R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmJob) * njobs, cudaMemcpyHostToDevice, s));
-    // Persistent grid: one CTA per resident slot, bounded by the jobs and by
-    // a scratch budget.
-    int per_sm = 1;
-    {
-      const int smem = sgm_smem_layout(maxc, rows).total;
-      per_sm = std::max(1, std::min(4, (W.smem_optin + 1024) / (smem + 1024)));
+    struct Group {
+      bool full;
+      SgmFullPlan plan;
+      int nd;
+      std::vector<int> ids;
+    };
+    std::vector<Group> groups;
+    for (int i = 0; i < nm; ++i) {
+      const Match& M = *matches[i];
+      SgmFullPlan plan{{0, 0}, 0};
+      if (!M.ranged) plan = sgm_full_plan(M.m.nd, W.smem_optin);
+      const bool full = plan.shape.g_ != 0;
+      Group* g = nullptr;
+      for (auto& q : groups)
+        if (q.full == full && (!full || q.nd == M.m.nd)) g = &q;
+      if (!g) {
+        groups.push_back(Group{full, plan, full ? M.m.nd : 0, {}});
+        g = &groups.back();
+      }
+      g->ids.push_back(i);
     }
-    const size_t budget = size_t{48} << 30;
-    int grid = std::min(njobs, W.sms * per_sm);
-    grid = std::max(1, std::min<int>(grid, static_cast<int>(std::max<size_t>(1, budget / std::max<size_t>(slot_bytes, 1)))));
-    W.scratch.reserve(static_cast<size_t>(grid) * slot_bytes);
-    R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int), s));
-    ProfileState::Pending ev{};
-    if (t_prof.on) {
-      R3D_CUDA(cudaEventCreate(&ev.a));
-      R3D_CUDA(cudaEventCreate(&ev.b));
-      R3D_CUDA(cudaEventRecord(ev.a, s));
-    }
-    launch_sgm(dm, dj, njobs, maxc, rows, grid, W.scratch.get(), slot_bytes, W.counter.get(), s);
-    if (t_prof.on) {
-      R3D_CUDA(cudaEventRecord(ev.b, s));
-      for (int i = 0; i < nm; ++i)
-        for (size_t t = 0; t < matches[i]->layout.tiles.size(); ++t) {
-          ev.cells += matches[i]->tile_cells[t];
-          ev.pixels += static_cast<uint64_t>(matches[i]->layout.tiles[t].w) * matches[i]->layout.tiles[t].h;
+    for (const Group& g : groups) {
+      int njobs = 0, max_num = 16;
+      for (int i : g.ids) {
+        njobs += static_cast<int>(matches[i]->layout.tiles.size());
+        for (int v : matches[i]->tile_maxnum) max_num = std::max(max_num, v);
+      }
+      const int maxc = g.full ? 0 : sgm_maxc_for(max_num);
+      const int rows = g.full ? g.plan.rows : sgm_rows_for(maxc, W.smem_optin);
+      SgmJob* hj = H.alloc<SgmJob>(njobs);
+      std::vector<uint64_t> work(njobs);
+      size_t slot_bytes = 0;
+      uint64_t cells_sum = 0, px_sum = 0;
+      int jb = 0;
+      for (int i : g.ids) {
+        Match& M = *matches[i];
+        for (size_t t = 0; t < M.layout.tiles.size(); ++t) {
+          const Tile& T = M.layout.tiles[t];
+          SgmJob& J = hj[jb];
+          J = SgmJob{};
+          J.match = i;
+          J.x0 = T.x0;
+          J.y0 = T.y0;
+          J.w = T.w;
+          J.h = T.h;
+          J.disp = M.tile_disp + M.tile_off[t];
+          J.conf = M.tile_conf ? M.tile_conf + M.tile_off[t] : nullptr;
+          J.cells = M.d_cells + t;
+          work[jb] = M.tile_cells[t];
+          cells_sum += M.tile_cells[t];
+          px_sum += static_cast<uint64_t>(T.w) * T.h;
+          slot_bytes = std::max(slot_bytes, g.full ? sgm_full_slot_layout(T.w, T.h, M.m.nd, 2 * g.plan.shape.g_ * g.plan.shape.k_).total
+                                                   : sgm_slot_layout(T.w, T.h, M.tile_cells[t], maxc, M.m.nd).total);
+          ++jb;
         }
-      ev.tiles = static_cast<uint64_t>(njobs);
-      t_prof.pending.push_back(ev);
+      }
+      // Largest tiles first (longest processing time first).
+      {
+        std::vector<int> order(njobs);
+        for (int i = 0; i < njobs; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
+        std::vector<SgmJob> tmp(hj, hj + njobs);
+        for (int i = 0; i < njobs; ++i) hj[i] = tmp[order[i]];
+      }
+      SgmJob* dj = A.alloc<SgmJob>(njobs);
+      R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmJob) * njobs, cudaMemcpyHostToDevice, s));
+      const int smem = g.full ? sgm_full_smem(g.plan.shape, rows) : sgm_smem_layout(maxc, rows).total;
+      const int per_sm = std::max(1, std::min(4, (W.smem_optin + 1024) / (smem + 1024)));
+      const size_t budget = size_t{48} << 30;
+      int grid = std::min(njobs, W.sms * per_sm);
+      grid = std::max(1, std::min<int>(grid, static_cast<int>(std::max<size_t>(1, budget / std::max<size_t>(slot_bytes, 1)))));
+      W.scratch.reserve(static_cast<size_t>(grid) * slot_bytes);
+      R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int), s));
+      ProfileState::Pending ev{};
+      if (t_prof.on) {
+        R3D_CUDA(cudaEventCreate(&ev.a));
+        R3D_CUDA(cudaEventCreate(&ev.b));
+        R3D_CUDA(cudaEventRecord(ev.a, s));
+      }
+      if (g.full) {
+        launch_sgm_full(g.plan.shape, g.nd, dm, dj, njobs, rows, grid, W.scratch.get(), slot_bytes, W.counter.get(), s);
+      } else {
+        launch_sgm(dm, dj, njobs, maxc, rows, grid, W.scratch.get(), slot_bytes, W.counter.get(), s);
+      }
+      if (t_prof.on) {
+        R3D_CUDA(cudaEventRecord(ev.b, s));
+        ev.cells = cells_sum;
+        ev.pixels = px_sum;
+        ev.tiles = static_cast<uint64_t>(njobs);
+        t_prof.pending.push_back(ev);
+      }
     }
     // Stage 3.
     for (PairRun* P : active) {
@@ -1079,8 +1111,10 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
     }
     SgmMatch* hm = W.pinned.alloc<SgmMatch>(1);
     fill_match(*hm, o, DView<uint16_t>{dl, wl, h, wl}, cl, cr, wr, il, ir, rlo, rnum, disparity_min, nd, false, false);
-    const int maxc = sgm_maxc_for(max_num);
-    const int rows = sgm_rows_for(maxc, W.smem_optin);
+    const SgmFullPlan plan = (ranges_lo && ranges_num) ? SgmFullPlan{{0, 0}, 0} : sgm_full_plan(nd, W.smem_optin);
+    const SgmFullShape sh = plan.shape;
+    const int maxc = sh.g_ ? 0 : sgm_maxc_for(max_num);
+    const int rows = sh.g_ ? plan.rows : sgm_rows_for(maxc, W.smem_optin);
     float* disp = A.alloc<float>(static_cast<size_t>(wl) * h);
     unsigned long long* dcells = A.alloc<unsigned long long>(1);
     uint16_t* vol = A.alloc<uint16_t>(cells);
@@ -1096,10 +1130,15 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
     SgmJob* dj = A.alloc<SgmJob>(1);
     R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch), cudaMemcpyHostToDevice, s));
     R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmJob), cudaMemcpyHostToDevice, s));
-    const size_t slot = sgm_slot_layout(wl, h, cells, maxc, nd).total;
+    const size_t slot = sh.g_ ? sgm_full_slot_layout(wl, h, nd, 2 * sh.g_ * sh.k_).total
+                              : sgm_slot_layout(wl, h, cells, maxc, nd).total;
     W.scratch.reserve(slot);
     R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int), s));
-    launch_sgm(dm, dj, 1, maxc, rows, 1, W.scratch.get(), slot, W.counter.get(), s);
+    if (sh.g_) {
+      launch_sgm_full(sh, nd, dm, dj, 1, rows, 1, W.scratch.get(), slot, W.counter.get(), s);
+    } else {
+      launch_sgm(dm, dj, 1, maxc, rows, 1, W.scratch.get(), slot, W.counter.get(), s);
+    }
     R3D_CUDA(cudaMemcpyAsync(out, vol, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s));
     R3D_CUDA(cudaStreamSynchronize(s));
   });

@@ -35,7 +35,7 @@ struct SgmMatch {
   int p1, invalid_cost, subpixel;
   float uniqueness;
   int lr_max_diff, diagonal_lr, confidence;
-  int pad_;
+  int sum_no_carry;   // 1 if 8 paths can never exceed 65535 (plain 32-bit adds of packed sums are exact)
   uint16_t lut[256];  // P2 by 8-bit intensity step
 };
 

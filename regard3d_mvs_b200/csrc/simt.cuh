@@ -39,6 +39,9 @@ R3D_DEVICE void syncwarp() { __syncwarp(); }
 R3D_DEVICE void syncthreads() { __syncthreads(); }
 R3D_DEVICE void fence() { __threadfence(); }
 R3D_DEVICE uint32_t vmin2(uint32_t a, uint32_t b) { return __vminu2(a, b); }
+// Per-halfword min(a, b, c) and min(a + b, c) (DPX instructions on sm_90+).
+R3D_DEVICE uint32_t vmin3(uint32_t a, uint32_t b, uint32_t c) { return __vimin3_u16x2(a, b, c); }
+R3D_DEVICE uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) { return __viaddmin_u16x2(a, b, c); }
 R3D_DEVICE uint32_t vadd2(uint32_t a, uint32_t b) { return __vadd2(a, b); }
 R3D_DEVICE uint32_t perm(uint32_t a, uint32_t b, uint32_t s) { return __byte_perm(a, b, s); }
 R3D_DEVICE int popc64(uint64_t v) { return __popcll(v); }
@@ -84,7 +87,19 @@ struct uint3 {
 struct alignas(16) int4 {
   int x, y, z, w;
 };
+struct alignas(8) int2 {
+  int x, y;
+};
+struct alignas(16) uint4 {
+  unsigned x, y, z, w;
+};
+struct alignas(8) uint2 {
+  unsigned x, y;
+};
 inline int4 make_int4(int x, int y, int z, int w) { return int4{x, y, z, w}; }
+inline int2 make_int2(int x, int y) { return int2{x, y}; }
+inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return uint4{x, y, z, w}; }
+inline uint2 make_uint2(unsigned x, unsigned y) { return uint2{x, y}; }
 
 namespace r3dsimt {
 
@@ -110,6 +125,12 @@ void syncthreads();
 inline void fence() {}
 inline uint32_t vmin2(uint32_t a, uint32_t b) {
   const uint32_t lo = std::min(a & 0xFFFFu, b & 0xFFFFu), hi = std::min(a >> 16, b >> 16);
+  return lo | (hi << 16);
+}
+inline uint32_t vmin3(uint32_t a, uint32_t b, uint32_t c) { return vmin2(vmin2(a, b), c); }
+inline uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) {
+  const uint32_t lo = std::min((a + b) & 0xFFFFu, c & 0xFFFFu);
+  const uint32_t hi = std::min(((a >> 16) + (b >> 16)) & 0xFFFFu, c >> 16);
   return lo | (hi << 16);
 }
 inline uint32_t vadd2(uint32_t a, uint32_t b) {
