@@ -321,6 +321,10 @@ def main():
     launches = lib.r3dgpu_launch_count() - launches0
     lib.r3dgpu_profile_take(ctypes.byref(prof))
     lib.r3dgpu_profile_enable(0)
+    nbytes = lib.r3dgpu_profile_launches(None, 0)
+    buf = ctypes.create_string_buffer(int(nbytes) + 1)
+    lib.r3dgpu_profile_launches(buf, nbytes + 1)
+    launch_log = json.loads(buf.value.decode() or "[]")
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     value = world * cells_full * args.steps / (ms * 1e-3) / 1e9
     total_cells = sum(int(pairs[i].out.cells) for i in range(n))
@@ -409,6 +413,17 @@ def main():
                              "nominal_int32_tops": int_peak, "frac": int_achieved / int_peak},
             "clocks": clocks,
         }
+        breakdown = {}
+        for e in launch_log:
+            k = f"{e['kernel']}:{e['shape']}"
+            b = breakdown.setdefault(k, {"launches": 0, "ms": 0.0, "cells": 0, "tiles": 0})
+            b["launches"] += 1
+            b["ms"] += e["ms"]
+            b["cells"] += e["cells"]
+            b["tiles"] += e["tiles"]
+        for b in breakdown.values():
+            b["gcells_per_s"] = b["cells"] / max(b["ms"], 1e-9) / 1e6
+        line["sgm_breakdown"] = breakdown
         if per_pair is not None:
             line["per_pair"] = per_pair
             line["batched_vs_per_pair"] = value / per_pair["value"]

@@ -204,6 +204,12 @@ void r3dgpu_profile_enable(int32_t on);
 /* Returns the totals accumulated on this thread since the last call and resets them. */
 void r3dgpu_profile_take(r3dgpu_profile* out);
 
+/* The launches behind the last r3dgpu_profile_take, one JSON object per
+ * launch ({"kernel", "shape", "tiles", "cells", "pixels", "ms", "grid", "rows"}),
+ * as a JSON array written into buf (truncated to len - 1 bytes). Returns the
+ * full length. */
+uint64_t r3dgpu_profile_launches(char* buf, uint64_t len);
+
 #ifdef __cplusplus
 }
 #endif

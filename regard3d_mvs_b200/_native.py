@@ -43,6 +43,7 @@ EXPORTS = (
     "r3dgpu_launch_count",
     "r3dgpu_profile_enable",
     "r3dgpu_profile_take",
+    "r3dgpu_profile_launches",
 )
 
 
@@ -100,6 +101,8 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_profile_enable.restype = None
     L.r3dgpu_profile_take.argtypes = [ctypes.POINTER(CProfile)]
     L.r3dgpu_profile_take.restype = None
+    L.r3dgpu_profile_launches.argtypes = [ctypes.c_char_p, ctypes.c_uint64]
+    L.r3dgpu_profile_launches.restype = ctypes.c_uint64
     if hasattr(L, "r3dgpu_synth_pair"):
         L.r3dgpu_synth_pair.argtypes = [ctypes.POINTER(CSynthParams), P, P, P]
         L.r3dgpu_synth_pair.restype = st

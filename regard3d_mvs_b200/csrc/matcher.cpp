@@ -35,8 +35,12 @@ struct ProfileState {
   struct Pending {
     cudaEvent_t a, b;
     uint64_t cells, tiles, pixels;
+    std::string kernel, shape;
+    int grid, rows;
   };
   std::vector<Pending> pending;
+  std::string launches;       // JSON objects of the launches since the last take
+  std::string last_launches;  // those of the last take
 };
 thread_local ProfileState t_prof;
 
@@ -51,6 +55,15 @@ void profile_collect() {
     t_prof.acc.sgm_cells += p.cells;
     t_prof.acc.sgm_tiles += p.tiles;
     t_prof.acc.sgm_pixels += p.pixels;
+    char line[256];
+    std::snprintf(line, sizeof(line),
+                  "{\"kernel\": \"%s\", \"shape\": \"%s\", \"tiles\": %llu, \"cells\": %llu, \"pixels\": %llu, "
+                  "\"ms\": %.4f, \"grid\": %d, \"rows\": %d}",
+                  p.kernel.c_str(), p.shape.c_str(), static_cast<unsigned long long>(p.tiles),
+                  static_cast<unsigned long long>(p.cells), static_cast<unsigned long long>(p.pixels),
+                  static_cast<double>(ms), p.grid, p.rows);
+    if (!t_prof.launches.empty()) t_prof.launches += ", ";
+    t_prof.launches += line;
   }
   t_prof.pending.clear();
 }
@@ -803,6 +816,12 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
         ev.cells = cells_sum;
         ev.pixels = px_sum;
         ev.tiles = static_cast<uint64_t>(njobs);
+        ev.kernel = g.full ? "sgm_full_kernel" : "sgm_tile_kernel";
+        ev.shape = g.full ? std::to_string(g.plan.shape.g_) + "x" + std::to_string(g.plan.shape.k_) + "/nd" +
+                                std::to_string(g.nd)
+                          : "maxc" + std::to_string(maxc);
+        ev.grid = grid;
+        ev.rows = rows;
         t_prof.pending.push_back(ev);
       }
     }
@@ -921,6 +940,18 @@ void r3dgpu_profile_enable(int32_t on) { t_prof.on = on != 0; }
 void r3dgpu_profile_take(r3dgpu_profile* out) {
   if (out) *out = t_prof.acc;
   t_prof.acc = r3dgpu_profile{};
+  t_prof.last_launches = "[" + t_prof.launches + "]";
+  t_prof.launches.clear();
+}
+
+uint64_t r3dgpu_profile_launches(char* buf, uint64_t len) {
+  const std::string& s = t_prof.last_launches;
+  if (buf && len > 0) {
+    const size_t n = std::min<size_t>(s.size(), static_cast<size_t>(len - 1));
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return s.size();
 }
 
 r3dgpu_status r3dgpu_match_stereo_batch(r3dgpu_pair* pairs, int32_t count, void* stream) {
