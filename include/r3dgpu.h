@@ -178,6 +178,25 @@ r3dgpu_status r3dgpu_ranges_from_coarse_host(const float* coarse, int32_t coarse
 r3dgpu_status r3dgpu_remove_speckles_host(float* disparity, int32_t width, int32_t height, int32_t min_size,
                                           float max_diff);
 
+/* Speckle filter in place on a DEVICE map (contiguous, width * height floats)
+ * that allocates no GPU memory: no reference counterpart. It is for callers
+ * that cannot let the library call cudaMalloc -- an application whose own
+ * pool allocator owns the device's memory, or a pipeline that cannot take the
+ * device-wide synchronisation of cudaFree. The union-find scratch is a static
+ * device array of 32 MiB that every GPU loading this library holds until the
+ * process exits; maps above 4,194,304 pixels (2048 x 2048) are rejected with
+ * R3DGPU_EINVAL. The work is enqueued on `stream` (cudaStream_t, NULL = legacy
+ * default stream) without synchronising it; launch errors are returned, errors
+ * during execution surface at the caller's next synchronisation. The first
+ * call on a device looks up the array's device address for that device (the
+ * current one); make that first call before any stream capture on the device.
+ * All calls share the one array, so calls whose work overlaps on the GPU
+ * (different streams or host threads without ordering between them) race:
+ * order them on one stream or synchronise between them. Results equal
+ * r3dgpu_remove_speckles_host's. */
+r3dgpu_status r3dgpu_remove_speckles_no_alloc(float* disparity, int32_t width, int32_t height, int32_t min_size,
+                                              float max_diff, void* stream);
+
 /* 3x3 median of the valid disparities (host arrays, contiguous).
  * Replaces r3d::median_filter_3x3, src/r3d/stereo/stereo_matcher.hpp:91. */
 r3dgpu_status r3dgpu_median_filter_3x3_host(const float* disparity, int32_t width, int32_t height, float* out);

@@ -39,6 +39,7 @@ EXPORTS = (
     "r3dgpu_sgm_cost_volume_host",
     "r3dgpu_ranges_from_coarse_host",
     "r3dgpu_remove_speckles_host",
+    "r3dgpu_remove_speckles_no_alloc",
     "r3dgpu_median_filter_3x3_host",
     "r3dgpu_launch_count",
     "r3dgpu_profile_enable",
@@ -93,6 +94,8 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_ranges_from_coarse_host.restype = st
     L.r3dgpu_remove_speckles_host.argtypes = [P, i32, i32, i32, ctypes.c_float]
     L.r3dgpu_remove_speckles_host.restype = st
+    L.r3dgpu_remove_speckles_no_alloc.argtypes = [P, i32, i32, i32, ctypes.c_float, P]
+    L.r3dgpu_remove_speckles_no_alloc.restype = st
     L.r3dgpu_median_filter_3x3_host.argtypes = [P, i32, i32, P]
     L.r3dgpu_median_filter_3x3_host.restype = st
     L.r3dgpu_launch_count.argtypes = []

@@ -1229,6 +1229,13 @@ r3dgpu_status r3dgpu_remove_speckles_host(float* disparity, int32_t width, int32
   });
 }
 
+r3dgpu_status r3dgpu_remove_speckles_no_alloc(float* disparity, int32_t width, int32_t height, int32_t min_size,
+                                              float max_diff, void* stream) {
+  return guarded([&] {
+    remove_speckles_static_scratch(disparity, width, height, min_size, max_diff, static_cast<cudaStream_t>(stream));
+  });
+}
+
 r3dgpu_status r3dgpu_median_filter_3x3_host(const float* disparity, int32_t width, int32_t height, float* out) {
   return guarded([&] {
     if ((!disparity || !out) && width > 0 && height > 0) fail(R3DGPU_EINVAL, "median_filter_3x3: null argument");

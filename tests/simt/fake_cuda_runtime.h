@@ -61,6 +61,12 @@ cudaError_t cudaEventSynchronize(cudaEvent_t e);
 cudaError_t cudaEventElapsedTime(float* ms, cudaEvent_t a, cudaEvent_t b);
 cudaError_t cudaStreamWaitEvent(cudaStream_t st, cudaEvent_t e, unsigned flags = 0);
 
+// Emulated device memory is host memory: a symbol's address is its own.
+template <class T>
+cudaError_t cudaGetSymbolAddress(void** p, const T& symbol) {
+  *p = const_cast<void*>(static_cast<const void*>(&symbol));
+  return cudaSuccess;
+}
 template <class F>
 cudaError_t cudaFuncSetAttribute(F, cudaFuncAttribute, int) {
   return cudaSuccess;
