@@ -383,13 +383,17 @@ def main():
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
-        sgm_ms = prof.sgm_ms / max(prof.sgm_launches, 1)
-        alg_bytes = (ALG_BYTES_PER_CELL * prof.sgm_cells + ALG_BYTES_PER_PIXEL * prof.sgm_pixels) / max(prof.sgm_launches, 1)
+        # The SGM launches of a round run concurrently (one stream per kernel
+        # shape); the unit of the roofline is a round's SGM stage, timed from
+        # its fork to its join on the launching stream.
+        rounds = max(sum(1 for e in launch_log if e["kernel"] == "sgm_round"), 1)
+        sgm_ms = prof.sgm_ms / rounds
+        alg_bytes = (ALG_BYTES_PER_CELL * prof.sgm_cells + ALG_BYTES_PER_PIXEL * prof.sgm_pixels) / rounds
         achieved = alg_bytes / (sgm_ms * 1e-3) / 1e9 if sgm_ms > 0 else 0.0
         tpc, tpp = sgm_traffic_per_cell()
         traffic = None
         if tpc is not None:
-            traffic = (tpc * prof.sgm_cells + tpp * prof.sgm_pixels) / max(prof.sgm_launches, 1)
+            traffic = (tpc * prof.sgm_cells + tpp * prof.sgm_pixels) / rounds
         sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
         clocks = clk.summary()
         int_peak = sm_count * 128 * (clocks.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
@@ -404,10 +408,11 @@ def main():
             "e2e": {"value": e2e_value, "unit": "Gcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "sgm_tile_kernel", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": "SGM stage: sgm_full_kernel + sgm_ranged_kernel launches of a round",
+                         "achieved": achieved, "peak": peak,
                          "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "avg_launch_ms": sgm_ms, "launches": int(prof.sgm_launches),
-                         "alg_bytes_per_launch": alg_bytes,
+                         "traffic": traffic, "avg_stage_ms": sgm_ms, "stages": rounds,
+                         "launches": int(prof.sgm_launches), "alg_bytes_per_stage": alg_bytes,
                          "sgm_share_of_step": prof.sgm_ms / max(ms, 1e-9)},
             "int_roofline": {"ops_per_cell": INT_OPS_PER_CELL, "achieved_tops": int_achieved,
                              "nominal_int32_tops": int_peak, "frac": int_achieved / int_peak},
@@ -415,6 +420,8 @@ def main():
         }
         breakdown = {}
         for e in launch_log:
+            if e["kernel"] == "sgm_round":
+                continue
             k = f"{e['kernel']}:{e['shape']}"
             b = breakdown.setdefault(k, {"launches": 0, "ms": 0.0, "cells": 0, "tiles": 0})
             b["launches"] += 1

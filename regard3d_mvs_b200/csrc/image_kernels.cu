@@ -437,19 +437,21 @@ R3D_GLOBAL void blend_kernel(const BlendTile* __restrict__ tiles, int ntiles, in
 
 // ------------------------------------------------------------------ tile cells
 R3D_GLOBAL void tile_cells_kernel(const uint16_t* R3D_RESTRICT rnum, int64_t stride, const int4* R3D_RESTRICT tiles,
-                                  unsigned long long* R3D_RESTRICT cells, int* R3D_RESTRICT maxnum) {
+                                  unsigned long long* R3D_RESTRICT cells, int* R3D_RESTRICT stats) {
   R3D_DYNAMIC_SMEM(smem_raw);
   unsigned long long* ssum = reinterpret_cast<unsigned long long*>(smem_raw);
-  int* smax = reinterpret_cast<int*>(smem_raw + 8 * 32);
+  int* sst = reinterpret_cast<int*>(smem_raw + 8 * 32);  // [warp][kTileStats]
   const int4 t = tiles[blockIdx.x];
   unsigned long long s = 0;
-  int mx = 0;
+  int st[kTileStats] = {};
   const int64_t n = static_cast<int64_t>(t.z) * t.w;
   for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
     const int y = static_cast<int>(i / t.z), x = static_cast<int>(i % t.z);
     const int v = rnum[static_cast<int64_t>(t.y + y) * stride + t.x + x];
     s += static_cast<unsigned long long>(v);
-    mx = r3dsimt::imax(mx, v);
+    st[0] = r3dsimt::imax(st[0], v);
+#pragma unroll
+    for (int k = 1; k < kTileStats; ++k) st[k] += v > tile_stat_width(k - 1) ? 1 : 0;
   }
   // Warp reduction (64-bit sum as two 32-bit halves), then across warps.
 #pragma unroll
@@ -457,23 +459,27 @@ R3D_GLOBAL void tile_cells_kernel(const uint16_t* R3D_RESTRICT rnum, int64_t str
     const uint32_t lo = r3dsimt::shfl_xor(static_cast<uint32_t>(s), o);
     const uint32_t hi = r3dsimt::shfl_xor(static_cast<uint32_t>(s >> 32), o);
     s += (static_cast<unsigned long long>(hi) << 32) | lo;
-    mx = r3dsimt::imax(mx, static_cast<int>(r3dsimt::shfl_xor(static_cast<uint32_t>(mx), o)));
+    st[0] = r3dsimt::imax(st[0], static_cast<int>(r3dsimt::shfl_xor(static_cast<uint32_t>(st[0]), o)));
+#pragma unroll
+    for (int k = 1; k < kTileStats; ++k) st[k] += static_cast<int>(r3dsimt::shfl_xor(static_cast<uint32_t>(st[k]), o));
   }
   const int warp = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31u);
   if (lane == 0) {
     ssum[warp] = s;
-    smax[warp] = mx;
+#pragma unroll
+    for (int k = 0; k < kTileStats; ++k) sst[warp * kTileStats + k] = st[k];
   }
   r3dsimt::syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long tot = 0;
-    int m = 0;
+    int out[kTileStats] = {};
     for (int i = 0; i < static_cast<int>(blockDim.x >> 5); ++i) {
       tot += ssum[i];
-      m = r3dsimt::imax(m, smax[i]);
+      out[0] = r3dsimt::imax(out[0], sst[i * kTileStats]);
+      for (int k = 1; k < kTileStats; ++k) out[k] += sst[i * kTileStats + k];
     }
     cells[blockIdx.x] = tot;
-    maxnum[blockIdx.x] = m;
+    for (int k = 0; k < kTileStats; ++k) stats[static_cast<int64_t>(blockIdx.x) * kTileStats + k] = out[k];
   }
 }
 
@@ -642,9 +648,10 @@ void launch_blend(const BlendTile* tiles, int ntiles, int tiles_x, const int* /*
 }
 
 void launch_tile_cells(const uint16_t* rnum, int64_t stride, const int4* tiles, int ntiles, unsigned long long* cells,
-                       int* maxnum, cudaStream_t s) {
+                       int* stats, cudaStream_t s) {
   if (ntiles <= 0) return;
-  R3D_LAUNCH(tile_cells_kernel, dim3(ntiles), dim3(256), 8 * 32 + 4 * 32, s, rnum, stride, tiles, cells, maxnum);
+  R3D_LAUNCH(tile_cells_kernel, dim3(ntiles), dim3(256), 8 * 32 + 4 * kTileStats * 8, s, rnum, stride, tiles, cells,
+             stats);
   launched("tile_cells_kernel");
 }
 

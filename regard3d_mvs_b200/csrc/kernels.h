@@ -68,9 +68,16 @@ void launch_blend(const BlendTile* tiles, int ntiles, int tiles_x, const int* bx
                   int blend, int mirror_out, float offset, float* out_disp, float* out_conf, int64_t ostride,
                   cudaStream_t s);
 
-// Per tile: number of labels (sum of num over its pixels) and the largest
-// num. tiles: (x0, y0, w, h) per tile; one block per tile.
+// Per-tile label statistics: stats[0] = largest num, stats[1 + i] = pixels
+// with num above tile_stat_width(i) (32, 64, 128, 192, 256, 384, 512).
+constexpr int kTileStats = 8;
+R3D_HOSTDEV constexpr int tile_stat_width(int i) {
+  return i < 3 ? 32 << i : (i < 5 ? 192 + 64 * (i - 3) : (i == 5 ? 384 : 512));
+}
+
+// Per tile: number of labels (sum of num over its pixels) and the label
+// statistics (kTileStats ints). tiles: (x0, y0, w, h) per tile; one block per tile.
 void launch_tile_cells(const uint16_t* rnum, int64_t stride, const int4* tiles, int ntiles,
-                       unsigned long long* cells, int* maxnum, cudaStream_t s);
+                       unsigned long long* cells, int* stats, cudaStream_t s);
 
 }  // namespace r3dgpu

@@ -9,6 +9,7 @@
 // and median filters. Every stage runs on the GPU; the host only plans
 // (tile layout, job tables, buffer sizes) and launches.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -21,9 +22,18 @@
 #include "kernels.h"
 #include "sgm.h"
 #include "sgm_full.h"
+#include "sgm_ranged.h"
 
 namespace r3dgpu {
 namespace {
+
+// Ranged tiles go to the ranged kernel unless R3DGPU_RANGED_KERNEL=general
+// selects the general per-chunk kernel (both compute the same results).
+bool general_ranged_kernel() {
+  const char* e = std::getenv("R3DGPU_RANGED_KERNEL");
+  return e != nullptr && std::string(e) == "general";
+}
+
 
 thread_local std::string t_error;
 thread_local int t_device = 0;
@@ -37,6 +47,7 @@ struct ProfileState {
     uint64_t cells, tiles, pixels;
     std::string kernel, shape;
     int grid, rows;
+    bool span;  // the SGM stage of a round (fork to join), not one launch
   };
   std::vector<Pending> pending;
   std::string launches;       // JSON objects of the launches since the last take
@@ -47,10 +58,19 @@ thread_local ProfileState t_prof;
 void profile_collect() {
   for (auto& p : t_prof.pending) {
     float ms = 0.0F;
-    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) t_prof.acc.sgm_ms += ms;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) != cudaSuccess) ms = 0.0F;
     (void)cudaGetLastError();
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
+    if (p.span) {
+      // Launches of a round overlap: the stage time is the round's span.
+      t_prof.acc.sgm_ms += ms;
+      char line[96];
+      std::snprintf(line, sizeof(line), "{\"kernel\": \"sgm_round\", \"ms\": %.4f}", static_cast<double>(ms));
+      if (!t_prof.launches.empty()) t_prof.launches += ", ";
+      t_prof.launches += line;
+      continue;
+    }
     t_prof.acc.sgm_launches += 1;
     t_prof.acc.sgm_cells += p.cells;
     t_prof.acc.sgm_tiles += p.tiles;
@@ -193,6 +213,23 @@ struct Workspace {
   Pinned pinned;
   DeviceBuffer<unsigned char> scratch;
   DeviceBuffer<int> counter;
+  // Side streams for the concurrent SGM launches of a round, and the events
+  // that fork them from and join them into the call's stream (created on
+  // first use, kept for the workspace's life).
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> side_done;
+  cudaEvent_t fork = nullptr;
+  void ensure_side(int n) {
+    if (fork == nullptr) R3D_CUDA(cudaEventCreate(&fork));
+    while (static_cast<int>(side.size()) < n) {
+      cudaStream_t st = nullptr;
+      cudaEvent_t ev = nullptr;
+      R3D_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      R3D_CUDA(cudaEventCreate(&ev));
+      side.push_back(st);
+      side_done.push_back(ev);
+    }
+  }
 };
 
 Workspace& workspace() {
@@ -290,6 +327,7 @@ struct Match {
   int tile_size = 0;
   std::vector<uint64_t> tile_cells;  // host copy (ranged: counted on the device)
   std::vector<int> tile_maxnum;
+  std::vector<int> tile_width;  // ranged: label width of the kernel shape chosen for the tile
   bool ranged = false;
   // device outputs of the SGM stage
   float* tile_disp = nullptr;
@@ -299,9 +337,9 @@ struct Match {
   int first_job = 0;
   // counting buffers (ranged)
   unsigned long long* d_count = nullptr;
-  int* d_maxnum = nullptr;
+  int* d_stats = nullptr;  // kTileStats per tile
   unsigned long long* h_count = nullptr;
-  int* h_maxnum = nullptr;
+  int* h_stats = nullptr;
 };
 
 struct LevelIn {
@@ -525,12 +563,12 @@ void prepare_level(PairRun& P, Arena& A, Pinned& H, cudaStream_t s) {
       int4* dt = A.alloc<int4>(n);
       R3D_CUDA(cudaMemcpyAsync(dt, ht, sizeof(int4) * n, cudaMemcpyHostToDevice, s));
       M.d_count = A.alloc<unsigned long long>(n);
-      M.d_maxnum = A.alloc<int>(n);
-      launch_tile_cells(M.m.rnum, M.m.r_stride, dt, n, M.d_count, M.d_maxnum, s);
+      M.d_stats = A.alloc<int>(static_cast<size_t>(n) * kTileStats);
+      launch_tile_cells(M.m.rnum, M.m.r_stride, dt, n, M.d_count, M.d_stats, s);
       M.h_count = H.alloc<unsigned long long>(n);
-      M.h_maxnum = H.alloc<int>(n);
+      M.h_stats = H.alloc<int>(static_cast<size_t>(n) * kTileStats);
       R3D_CUDA(cudaMemcpyAsync(M.h_count, M.d_count, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost, s));
-      R3D_CUDA(cudaMemcpyAsync(M.h_maxnum, M.d_maxnum, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+      R3D_CUDA(cudaMemcpyAsync(M.h_stats, M.d_stats, sizeof(int) * n * kTileStats, cudaMemcpyDeviceToHost, s));
     }
   };
   plan(P.left, wl);
@@ -545,11 +583,14 @@ bool finalize_layout(Match& M, int W, int H_, int partner_w, const r3dgpu_stereo
   const size_t n = M.layout.tiles.size();
   M.tile_cells.resize(n);
   M.tile_maxnum.resize(n);
+  M.tile_width.assign(n, 0);
   for (size_t i = 0; i < n; ++i) {
     const Tile& t = M.layout.tiles[i];
     if (M.ranged) {
+      const int* st = M.h_stats + i * kTileStats;
       M.tile_cells[i] = M.h_count[i];
-      M.tile_maxnum[i] = M.h_maxnum[i];
+      M.tile_maxnum[i] = st[0];
+      M.tile_width[i] = sgm_ranged_width_for(st, static_cast<int64_t>(t.w) * t.h);
     } else {
       M.tile_cells[i] = static_cast<uint64_t>(t.w) * static_cast<uint64_t>(t.h) * static_cast<uint64_t>(M.m.nd);
       M.tile_maxnum[i] = M.m.nd;
@@ -571,12 +612,12 @@ bool finalize_layout(Match& M, int W, int H_, int partner_w, const r3dgpu_stereo
       int4* dt = A.alloc<int4>(nn);
       R3D_CUDA(cudaMemcpyAsync(dt, ht, sizeof(int4) * nn, cudaMemcpyHostToDevice, s));
       M.d_count = A.alloc<unsigned long long>(nn);
-      M.d_maxnum = A.alloc<int>(nn);
-      launch_tile_cells(M.m.rnum, M.m.r_stride, dt, nn, M.d_count, M.d_maxnum, s);
+      M.d_stats = A.alloc<int>(static_cast<size_t>(nn) * kTileStats);
+      launch_tile_cells(M.m.rnum, M.m.r_stride, dt, nn, M.d_count, M.d_stats, s);
       M.h_count = HP.alloc<unsigned long long>(nn);
-      M.h_maxnum = HP.alloc<int>(nn);
+      M.h_stats = HP.alloc<int>(static_cast<size_t>(nn) * kTileStats);
       R3D_CUDA(cudaMemcpyAsync(M.h_count, M.d_count, sizeof(unsigned long long) * nn, cudaMemcpyDeviceToHost, s));
-      R3D_CUDA(cudaMemcpyAsync(M.h_maxnum, M.d_maxnum, sizeof(int) * nn, cudaMemcpyDeviceToHost, s));
+      R3D_CUDA(cudaMemcpyAsync(M.h_stats, M.d_stats, sizeof(int) * nn * kTileStats, cudaMemcpyDeviceToHost, s));
       return false;
     }
     return finalize_layout(M, W, H_, partner_w, o, A, HP, s);
@@ -727,103 +768,195 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     }
     SgmMatch* dm = A.alloc<SgmMatch>(nm);
     R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch) * nm, cudaMemcpyHostToDevice, s));
+    // Launch groups: full-range matches by label count; ranged tiles by the
+    // kernel shape chosen for each tile (or all into the general kernel).
+    enum Kind { kFull, kRanged, kGeneral };
     struct Group {
-      bool full;
+      Kind kind;
       SgmFullPlan plan;
-      int nd;
-      std::vector<int> ids;
+      int nd;     // full: label count; ranged: shape width
+      std::vector<std::pair<int, int>> tiles;  // (match, tile)
     };
     std::vector<Group> groups;
+    auto group_for = [&](Kind kind, int key, SgmFullPlan plan) -> Group& {
+      for (auto& q : groups)
+        if (q.kind == kind && q.nd == key) return q;
+      groups.push_back(Group{kind, plan, key, {}});
+      return groups.back();
+    };
     for (int i = 0; i < nm; ++i) {
       const Match& M = *matches[i];
-      SgmFullPlan plan{{0, 0}, 0};
-      if (!M.ranged) plan = sgm_full_plan(M.m.nd, W.smem_optin);
-      const bool full = plan.shape.g_ != 0;
-      Group* g = nullptr;
-      for (auto& q : groups)
-        if (q.full == full && (!full || q.nd == M.m.nd)) g = &q;
-      if (!g) {
-        groups.push_back(Group{full, plan, full ? M.m.nd : 0, {}});
-        g = &groups.back();
-      }
-      g->ids.push_back(i);
-    }
-    for (const Group& g : groups) {
-      int njobs = 0, max_num = 16;
-      for (int i : g.ids) {
-        njobs += static_cast<int>(matches[i]->layout.tiles.size());
-        for (int v : matches[i]->tile_maxnum) max_num = std::max(max_num, v);
-      }
-      const int maxc = g.full ? 0 : sgm_maxc_for(max_num);
-      const int rows = g.full ? g.plan.rows : sgm_rows_for(maxc, W.smem_optin);
-      SgmJob* hj = H.alloc<SgmJob>(njobs);
-      std::vector<uint64_t> work(njobs);
-      size_t slot_bytes = 0;
-      uint64_t cells_sum = 0, px_sum = 0;
-      int jb = 0;
-      for (int i : g.ids) {
-        Match& M = *matches[i];
-        for (size_t t = 0; t < M.layout.tiles.size(); ++t) {
-          const Tile& T = M.layout.tiles[t];
-          SgmJob& J = hj[jb];
-          J = SgmJob{};
-          J.match = i;
-          J.x0 = T.x0;
-          J.y0 = T.y0;
-          J.w = T.w;
-          J.h = T.h;
-          J.disp = M.tile_disp + M.tile_off[t];
-          J.conf = M.tile_conf ? M.tile_conf + M.tile_off[t] : nullptr;
-          J.cells = M.d_cells + t;
-          work[jb] = M.tile_cells[t];
-          cells_sum += M.tile_cells[t];
-          px_sum += static_cast<uint64_t>(T.w) * T.h;
-          slot_bytes = std::max(slot_bytes, g.full ? sgm_full_slot_layout(T.w, T.h, M.m.nd, 2 * g.plan.shape.g_ * g.plan.shape.k_).total
-                                                   : sgm_slot_layout(T.w, T.h, M.tile_cells[t], maxc, M.m.nd).total);
-          ++jb;
+      const int nt = static_cast<int>(M.layout.tiles.size());
+      if (!M.ranged) {
+        const SgmFullPlan plan = sgm_full_plan(M.m.nd, W.smem_optin);
+        if (plan.shape.g_ != 0) {
+          Group& g = group_for(kFull, M.m.nd, plan);
+          for (int t = 0; t < nt; ++t) g.tiles.emplace_back(i, t);
+          continue;
         }
       }
-      // Largest tiles first (longest processing time first).
-      {
-        std::vector<int> order(njobs);
-        for (int i = 0; i < njobs; ++i) order[i] = i;
-        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work[a] > work[b]; });
-        std::vector<SgmJob> tmp(hj, hj + njobs);
-        for (int i = 0; i < njobs; ++i) hj[i] = tmp[order[i]];
+      for (int t = 0; t < nt; ++t) {
+        if (M.ranged && !general_ranged_kernel())
+          group_for(kRanged, M.tile_width[t], SgmFullPlan{{0, 0}, 0}).tiles.emplace_back(i, t);
+        else
+          group_for(kGeneral, 0, SgmFullPlan{{0, 0}, 0}).tiles.emplace_back(i, t);
       }
-      SgmJob* dj = A.alloc<SgmJob>(njobs);
-      R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmJob) * njobs, cudaMemcpyHostToDevice, s));
-      const int smem = g.full ? sgm_full_smem(g.plan.shape, rows) : sgm_smem_layout(maxc, rows).total;
-      const int per_sm = std::max(1, std::min(4, (W.smem_optin + 1024) / (smem + 1024)));
-      const size_t budget = size_t{48} << 30;
-      int grid = std::min(njobs, W.sms * per_sm);
-      grid = std::max(1, std::min<int>(grid, static_cast<int>(std::max<size_t>(1, budget / std::max<size_t>(slot_bytes, 1)))));
-      W.scratch.reserve(static_cast<size_t>(grid) * slot_bytes);
-      R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int), s));
+    }
+    // Plan every group's launch: jobs (largest tiles first), scratch slot,
+    // CTAs per SM, and an estimate of its slowest tile (a CTA runs a tile
+    // alone: band steps x per-step cost).
+    struct Launch {
+      const Group* g;
+      int njobs, rows, ndw, maxc, per_sm, grid, smem;
+      SgmRangedPlan rplan;
+      SgmJob* dj;
+      size_t slot_bytes, scratch_off;
+      uint64_t cells_sum, px_sum;
+      double longest;
+    };
+    std::vector<Launch> launches;
+    for (const Group& g : groups) {
+      Launch L{};
+      L.g = &g;
+      L.njobs = static_cast<int>(g.tiles.size());
+      int max_num = 16;
+      for (const auto& mt : g.tiles) max_num = std::max(max_num, matches[mt.first]->tile_maxnum[mt.second]);
+      const bool full = g.kind == kFull, ranged = g.kind == kRanged;
+      L.rplan = ranged ? sgm_ranged_plan(sgm_ranged_shape_for_width(g.nd), W.smem_optin) : SgmRangedPlan{{0, 0}, 0};
+      L.ndw = ranged ? sgm_ranged_ndw(L.rplan.shape, max_num) : 0;
+      L.maxc = g.kind == kGeneral ? sgm_maxc_for(max_num) : 0;
+      L.rows = full ? g.plan.rows : (ranged ? L.rplan.rows : sgm_rows_for(L.maxc, W.smem_optin));
+      const int kk = full ? g.plan.shape.k_ : (ranged ? L.rplan.shape.k_ : 2 * L.maxc);
+      SgmJob* hj = H.alloc<SgmJob>(L.njobs);
+      std::vector<double> work(L.njobs);
+      int jb = 0;
+      for (const auto& mt : g.tiles) {
+        const int i = mt.first, t = mt.second;
+        Match& M = *matches[i];
+        const Tile& T = M.layout.tiles[t];
+        SgmJob& J = hj[jb];
+        J = SgmJob{};
+        J.match = i;
+        J.x0 = T.x0;
+        J.y0 = T.y0;
+        J.w = T.w;
+        J.h = T.h;
+        J.disp = M.tile_disp + M.tile_off[t];
+        J.conf = M.tile_conf ? M.tile_conf + M.tile_off[t] : nullptr;
+        J.cells = M.d_cells + t;
+        const double steps = 2.0 * ((T.h + L.rows - 1) / L.rows) * (T.w + 2.0 * (L.rows - 1));
+        work[jb] = steps * (1.0 + kk / 4.0) + static_cast<double>(M.tile_cells[t]) / 256.0;
+        L.longest = std::max(L.longest, work[jb]);
+        L.cells_sum += M.tile_cells[t];
+        L.px_sum += static_cast<uint64_t>(T.w) * T.h;
+        L.slot_bytes = std::max(
+            L.slot_bytes, full ? sgm_full_slot_layout(T.w, T.h, M.m.nd, 2 * g.plan.shape.g_ * g.plan.shape.k_).total
+                          : ranged ? sgm_ranged_slot_layout(T.w, T.h, M.tile_cells[t], M.m.nd, L.ndw, L.rows).total
+                                   : sgm_slot_layout(T.w, T.h, M.tile_cells[t], L.maxc, M.m.nd).total);
+        ++jb;
+      }
+      {
+        std::vector<int> order(L.njobs);
+        for (int i = 0; i < L.njobs; ++i) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
+        std::vector<SgmJob> tmp(hj, hj + L.njobs);
+        for (int i = 0; i < L.njobs; ++i) hj[i] = tmp[order[i]];
+      }
+      L.dj = A.alloc<SgmJob>(L.njobs);
+      R3D_CUDA(cudaMemcpyAsync(L.dj, hj, sizeof(SgmJob) * L.njobs, cudaMemcpyHostToDevice, s));
+      L.smem = full ? sgm_full_smem(g.plan.shape, L.rows)
+               : ranged ? sgm_ranged_smem(L.rplan.shape, L.rows)
+                        : sgm_smem_layout(L.maxc, L.rows).total;
+      L.per_sm = std::max(1, std::min(4, (W.smem_optin + 1024) / (L.smem + 1024)));
+      L.grid = std::max(1, std::min(L.njobs, W.sms * L.per_sm));
+      L.slot_bytes = sgm_align16(L.slot_bytes);
+      launches.push_back(L);
+    }
+    // Scratch for all groups at once, within the budget: grids shrink in
+    // proportion when the slots would not fit.
+    {
+      const size_t budget = size_t{64} << 30;
+      size_t total = 0;
+      for (const Launch& L : launches) total += static_cast<size_t>(L.grid) * L.slot_bytes;
+      if (total > budget) {
+        const double f = static_cast<double>(budget) / static_cast<double>(total);
+        total = 0;
+        for (Launch& L : launches) {
+          L.grid = std::max(1, static_cast<int>(L.grid * f));
+          total += static_cast<size_t>(L.grid) * L.slot_bytes;
+        }
+      }
+      size_t off = 0;
+      for (Launch& L : launches) {
+        L.scratch_off = off;
+        off += static_cast<size_t>(L.grid) * L.slot_bytes;
+      }
+      W.scratch.reserve(off);
+      if (static_cast<int>(W.counter.size()) < static_cast<int>(launches.size())) W.counter.reset(launches.size());
+      R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int) * launches.size(), s));
+    }
+    // Slowest tiles first: each group on its own stream, forked from and
+    // joined into the call's stream, so that one group's last tiles overlap
+    // the other groups' work.
+    std::vector<int> lorder(launches.size());
+    for (size_t i = 0; i < launches.size(); ++i) lorder[i] = static_cast<int>(i);
+    std::stable_sort(lorder.begin(), lorder.end(),
+                     [&](int x, int y) { return launches[x].longest > launches[y].longest; });
+    const int nside = std::min<int>(static_cast<int>(launches.size()), 16);
+    W.ensure_side(nside);
+    ProfileState::Pending span{};
+    if (t_prof.on) {
+      R3D_CUDA(cudaEventCreate(&span.a));
+      R3D_CUDA(cudaEventCreate(&span.b));
+      R3D_CUDA(cudaEventRecord(span.a, s));
+      span.span = true;
+    }
+    R3D_CUDA(cudaEventRecord(W.fork, s));
+    for (int j = 0; j < nside; ++j) R3D_CUDA(cudaStreamWaitEvent(W.side[j], W.fork, 0));
+    for (size_t q = 0; q < lorder.size(); ++q) {
+      const int li = lorder[q];
+      const Launch& L = launches[li];
+      const Group& g = *L.g;
+      cudaStream_t gs = W.side[q % nside];
+      unsigned char* scratch = W.scratch.get() + L.scratch_off;
+      int* counter = W.counter.get() + li;
       ProfileState::Pending ev{};
       if (t_prof.on) {
         R3D_CUDA(cudaEventCreate(&ev.a));
         R3D_CUDA(cudaEventCreate(&ev.b));
-        R3D_CUDA(cudaEventRecord(ev.a, s));
+        R3D_CUDA(cudaEventRecord(ev.a, gs));
       }
-      if (g.full) {
-        launch_sgm_full(g.plan.shape, g.nd, dm, dj, njobs, rows, grid, W.scratch.get(), slot_bytes, W.counter.get(), s);
+      if (g.kind == kFull) {
+        launch_sgm_full(g.plan.shape, g.nd, dm, L.dj, L.njobs, L.rows, L.grid, scratch, L.slot_bytes, counter, gs);
+      } else if (g.kind == kRanged) {
+        launch_sgm_ranged(L.rplan.shape, dm, L.dj, L.njobs, L.rows, L.ndw, L.grid, scratch, L.slot_bytes, counter, gs);
       } else {
-        launch_sgm(dm, dj, njobs, maxc, rows, grid, W.scratch.get(), slot_bytes, W.counter.get(), s);
+        launch_sgm(dm, L.dj, L.njobs, L.maxc, L.rows, L.grid, scratch, L.slot_bytes, counter, gs);
       }
       if (t_prof.on) {
-        R3D_CUDA(cudaEventRecord(ev.b, s));
-        ev.cells = cells_sum;
-        ev.pixels = px_sum;
-        ev.tiles = static_cast<uint64_t>(njobs);
-        ev.kernel = g.full ? "sgm_full_kernel" : "sgm_tile_kernel";
-        ev.shape = g.full ? std::to_string(g.plan.shape.g_) + "x" + std::to_string(g.plan.shape.k_) + "/nd" +
-                                std::to_string(g.nd)
-                          : "maxc" + std::to_string(maxc);
-        ev.grid = grid;
-        ev.rows = rows;
+        R3D_CUDA(cudaEventRecord(ev.b, gs));
+        ev.cells = L.cells_sum;
+        ev.pixels = L.px_sum;
+        ev.tiles = static_cast<uint64_t>(L.njobs);
+        ev.kernel = g.kind == kFull ? "sgm_full_kernel" : (g.kind == kRanged ? "sgm_ranged_kernel" : "sgm_tile_kernel");
+        ev.shape = g.kind == kFull ? std::to_string(g.plan.shape.g_) + "x" + std::to_string(g.plan.shape.k_) + "/nd" +
+                                         std::to_string(g.nd)
+                   : g.kind == kRanged ? std::to_string(L.rplan.shape.g_) + "x" + std::to_string(L.rplan.shape.k_) +
+                                             "/ndw" + std::to_string(L.ndw)
+                                       : "maxc" + std::to_string(L.maxc);
+        ev.grid = L.grid;
+        ev.rows = L.rows;
         t_prof.pending.push_back(ev);
       }
+    }
+    for (int j = 0; j < nside; ++j) {
+      R3D_CUDA(cudaEventRecord(W.side_done[j], W.side[j]));
+      R3D_CUDA(cudaStreamWaitEvent(s, W.side_done[j], 0));
+    }
+    if (t_prof.on) {
+      R3D_CUDA(cudaEventRecord(span.b, s));
+      span.kernel = "sgm_round";
+      t_prof.pending.push_back(span);
     }
     // Stage 3.
     for (PairRun* P : active) {
@@ -1144,8 +1277,22 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
     fill_match(*hm, o, DView<uint16_t>{dl, wl, h, wl}, cl, cr, wr, il, ir, rlo, rnum, disparity_min, nd, false, false);
     const SgmFullPlan plan = (ranges_lo && ranges_num) ? SgmFullPlan{{0, 0}, 0} : sgm_full_plan(nd, W.smem_optin);
     const SgmFullShape sh = plan.shape;
-    const int maxc = sh.g_ ? 0 : sgm_maxc_for(max_num);
-    const int rows = sh.g_ ? plan.rows : sgm_rows_for(maxc, W.smem_optin);
+    const bool ranged = !sh.g_ && !general_ranged_kernel();
+    SgmRangedPlan rplan{{0, 0}, 0};
+    if (ranged) {
+      // The whole image is one tile: its label statistics from the host ranges.
+      int st[kTileStats] = {};
+      for (int64_t i = 0; i < static_cast<int64_t>(wl) * h; ++i) {
+        const int n = ranges_num[i];
+        st[0] = std::max(st[0], n);
+        for (int k = 1; k < kTileStats; ++k) st[k] += n > tile_stat_width(k - 1) ? 1 : 0;
+      }
+      rplan = sgm_ranged_plan(sgm_ranged_shape_for_width(sgm_ranged_width_for(st, static_cast<int64_t>(wl) * h)),
+                              W.smem_optin);
+    }
+    const int ndw = ranged ? sgm_ranged_ndw(rplan.shape, max_num) : 0;
+    const int maxc = (sh.g_ || ranged) ? 0 : sgm_maxc_for(max_num);
+    const int rows = sh.g_ ? plan.rows : (ranged ? rplan.rows : sgm_rows_for(maxc, W.smem_optin));
     float* disp = A.alloc<float>(static_cast<size_t>(wl) * h);
     unsigned long long* dcells = A.alloc<unsigned long long>(1);
     uint16_t* vol = A.alloc<uint16_t>(cells);
@@ -1161,12 +1308,15 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
     SgmJob* dj = A.alloc<SgmJob>(1);
     R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch), cudaMemcpyHostToDevice, s));
     R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmJob), cudaMemcpyHostToDevice, s));
-    const size_t slot = sh.g_ ? sgm_full_slot_layout(wl, h, nd, 2 * sh.g_ * sh.k_).total
-                              : sgm_slot_layout(wl, h, cells, maxc, nd).total;
+    const size_t slot = sh.g_    ? sgm_full_slot_layout(wl, h, nd, 2 * sh.g_ * sh.k_).total
+                        : ranged ? sgm_ranged_slot_layout(wl, h, cells, nd, ndw, rows).total
+                                 : sgm_slot_layout(wl, h, cells, maxc, nd).total;
     W.scratch.reserve(slot);
     R3D_CUDA(cudaMemsetAsync(W.counter.get(), 0, sizeof(int), s));
     if (sh.g_) {
       launch_sgm_full(sh, nd, dm, dj, 1, rows, 1, W.scratch.get(), slot, W.counter.get(), s);
+    } else if (ranged) {
+      launch_sgm_ranged(rplan.shape, dm, dj, 1, rows, ndw, 1, W.scratch.get(), slot, W.counter.get(), s);
     } else {
       launch_sgm(dm, dj, 1, maxc, rows, 1, W.scratch.get(), slot, W.counter.get(), s);
     }

@@ -24,12 +24,17 @@
 #include "common.cuh"
 #include "sgm.h"
 #include "sgm_full.h"
+#include "sgm_simd.cuh"
 
 namespace r3dgpu {
 
 namespace {
 
-constexpr uint32_t kSent2 = 0x7FFF7FFFu;
+using sgm_simd::group_umin;
+using sgm_simd::group_vmin2;
+using sgm_simd::kSent2;
+using sgm_simd::load_words;
+using sgm_simd::store_words;
 constexpr float kInfF = __builtin_huge_valf();
 
 template <int G, int K>
@@ -42,61 +47,6 @@ struct FullCfg {
 
 // Ring vectors of a row: V slots 0..2, DB slots 3..6, DA slots 7..8 (minima likewise).
 constexpr int kVec = 9;
-
-template <int G>
-R3D_DEVICE uint32_t group_vmin2(uint32_t v) {
-#pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1) v = r3dsimt::vmin2(v, r3dsimt::shfl_xor(v, o));
-  return v;
-}
-template <int G>
-R3D_DEVICE uint32_t group_umin(uint32_t v) {
-#pragma unroll
-  for (int o = G / 2; o > 0; o >>= 1) v = r3dsimt::umin(v, r3dsimt::shfl_xor(v, o));
-  return v;
-}
-
-// Words base[-1 .. K] of a vector (base 16-byte aligned when K % 4 == 0,
-// 8-byte aligned when K is even).
-template <int K>
-R3D_DEVICE void load_words(const uint32_t* base, uint32_t (&w)[K + 2]) {
-  w[0] = base[-1];
-  if constexpr (K % 4 == 0) {
-#pragma unroll
-    for (int i = 0; i < K; i += 4) {
-      const uint4 v = *reinterpret_cast<const uint4*>(base + i);
-      w[1 + i] = v.x;
-      w[2 + i] = v.y;
-      w[3 + i] = v.z;
-      w[4 + i] = v.w;
-    }
-  } else if constexpr (K % 2 == 0) {
-#pragma unroll
-    for (int i = 0; i < K; i += 2) {
-      const uint2 v = *reinterpret_cast<const uint2*>(base + i);
-      w[1 + i] = v.x;
-      w[2 + i] = v.y;
-    }
-  } else {
-#pragma unroll
-    for (int i = 0; i < K; ++i) w[1 + i] = base[i];
-  }
-  w[K + 1] = base[K];
-}
-
-template <int K>
-R3D_DEVICE void store_words(uint32_t* base, const uint32_t (&o)[K]) {
-  if constexpr (K % 4 == 0) {
-#pragma unroll
-    for (int i = 0; i < K; i += 4) *reinterpret_cast<uint4*>(base + i) = make_uint4(o[i], o[i + 1], o[i + 2], o[i + 3]);
-  } else if constexpr (K % 2 == 0) {
-#pragma unroll
-    for (int i = 0; i < K; i += 2) *reinterpret_cast<uint2*>(base + i) = make_uint2(o[i], o[i + 1]);
-  } else {
-#pragma unroll
-    for (int i = 0; i < K; ++i) base[i] = o[i];
-  }
-}
 
 // Shared-memory layout (bytes).
 template <int G, int K>
@@ -477,19 +427,6 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
   }
 }
 
-R3D_DEVICE float subpixel_full(int method, float sm, float s0, float sp) {
-  float delta = 0.0F;
-  if (method == R3DGPU_SUBPIXEL_PARABOLA) {
-    const float denom = __fadd_rn(__fsub_rn(sm, __fmul_rn(2.0F, s0)), sp);
-    delta = denom > 0.0F ? __fdiv_rn(__fsub_rn(sm, sp), __fmul_rn(2.0F, denom)) : 0.0F;
-  } else if (method == R3DGPU_SUBPIXEL_EQUIANGULAR) {
-    const float a = __fsub_rn(sm, s0), b = __fsub_rn(sp, s0);
-    const float slope = a < b ? b : a;
-    delta = slope > 0.0F ? __fdiv_rn(__fsub_rn(sm, sp), __fmul_rn(2.0F, slope)) : 0.0F;
-  }
-  return delta < -0.5F ? -0.5F : (delta > 0.5F ? 0.5F : delta);
-}
-
 template <int G, int K, bool MASKED>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kSgmFullThreads)
     sgm_full_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmJob* R3D_RESTRICT jobs, int njobs, int rows,
@@ -657,7 +594,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kSgmFullThreads)
         if (ok) {
           float delta = 0.0F;
           if (best > 0 && best < nd - 1)
-            delta = subpixel_full(m.subpixel, static_cast<float>(sm), best_cost, static_cast<float>(sp));
+            delta = sgm_simd::subpixel_delta(m.subpixel, static_cast<float>(sm), best_cost, static_cast<float>(sp));
           d = __fadd_rn(static_cast<float>(m.dmin + best), delta);
           if (m.confidence)
             cf = (sec != 0xFFFFu && sec > 0u) ? __fsub_rn(1.0F, __fdiv_rn(best_cost, static_cast<float>(sec))) : 0.0F;

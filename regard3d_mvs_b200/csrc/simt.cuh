@@ -35,6 +35,8 @@ R3D_DEVICE uint32_t umax(uint32_t a, uint32_t b) { return max(a, b); }
 R3D_DEVICE uint32_t lane_id() { return threadIdx.x & 31u; }
 R3D_DEVICE uint32_t shfl(uint32_t v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 R3D_DEVICE uint32_t shfl_xor(uint32_t v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+R3D_DEVICE uint32_t ballot(bool p) { return __ballot_sync(0xffffffffu, p); }
+R3D_DEVICE int ffs(uint32_t v) { return __ffs(static_cast<int>(v)); }  // 1 + index of the lowest set bit, 0 if none
 R3D_DEVICE void syncwarp() { __syncwarp(); }
 R3D_DEVICE void syncthreads() { __syncthreads(); }
 R3D_DEVICE void fence() { __threadfence(); }
@@ -44,6 +46,8 @@ R3D_DEVICE uint32_t vmin3(uint32_t a, uint32_t b, uint32_t c) { return __vimin3_
 R3D_DEVICE uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) { return __viaddmin_u16x2(a, b, c); }
 R3D_DEVICE uint32_t vadd2(uint32_t a, uint32_t b) { return __vadd2(a, b); }
 R3D_DEVICE uint32_t perm(uint32_t a, uint32_t b, uint32_t s) { return __byte_perm(a, b, s); }
+// Low word of (hi:lo) >> s, s in [0, 31].
+R3D_DEVICE uint32_t funnel_r(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_r(lo, hi, s); }
 R3D_DEVICE int popc64(uint64_t v) { return __popcll(v); }
 
 // 16-byte asynchronous global -> shared copy (L2 only). Both addresses must
@@ -120,6 +124,8 @@ inline uint32_t umax(uint32_t a, uint32_t b) { return a > b ? a : b; }
 uint32_t lane_id();
 uint32_t shfl(uint32_t v, int src);
 uint32_t shfl_xor(uint32_t v, int m);
+uint32_t ballot(bool p);
+inline int ffs(uint32_t v) { return __builtin_ffs(static_cast<int>(v)); }
 void syncwarp();
 void syncthreads();
 inline void fence() {}
@@ -144,6 +150,9 @@ inline uint32_t perm(uint32_t a, uint32_t b, uint32_t s) {
     r |= static_cast<uint32_t>((v >> (8 * sel)) & 0xFFu) << (8 * i);
   }
   return r;
+}
+inline uint32_t funnel_r(uint32_t lo, uint32_t hi, uint32_t s) {
+  return static_cast<uint32_t>(((static_cast<uint64_t>(hi) << 32) | lo) >> (s & 31u));
 }
 inline int popc64(uint64_t v) { return __builtin_popcountll(v); }
 void cp_async16(void* smem_dst, const void* gmem_src);

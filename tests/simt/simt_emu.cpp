@@ -147,6 +147,17 @@ uint32_t shfl(uint32_t v, int src) {
 
 uint32_t shfl_xor(uint32_t v, int m) { return shfl(v, static_cast<int>(lane_id() ^ static_cast<uint32_t>(m))); }
 
+uint32_t ballot(bool p) {
+  WarpState& ws = (*t_warps)[warp_of(t_cur)];
+  ws.buf[lane_id()] = p ? 1u : 0u;
+  warp_barrier();
+  uint32_t r = 0;
+  for (int i = 0; i < 32; ++i)
+    if (ws.buf[i]) r |= 1u << i;
+  warp_barrier();
+  return r;
+}
+
 void syncwarp() { warp_barrier(); }
 
 void syncthreads() {

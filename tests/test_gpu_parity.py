@@ -220,6 +220,49 @@ def test_hierarchical_pair(gpu_matcher, oracle):
                      oracle.match_stereo(left, right, None, None, 0, 256, o))
 
 
+def _smooth_ranges(w, h, nd, seed, wide_frac=0.05):
+    """Ranges shaped like a hierarchical level's: lo drifting slowly, a few
+    jumps, num mostly 16 or 32, some wide pixels."""
+    rng = np.random.default_rng(seed)
+    base = np.cumsum(rng.integers(-1, 2, (h, w)) * (rng.random((h, w)) < 0.3), axis=1)
+    base = base + np.cumsum(rng.integers(-2, 3, (h, 1)), axis=0)
+    base = base + np.where(rng.random((h, w)) < 0.03, rng.integers(-40, 40, (h, w)), 0)
+    num = np.where(rng.random((h, w)) < 0.2, 16, 32)
+    num = np.where(rng.random((h, w)) < wide_frac, rng.choice([48, 64, 96, nd], (h, w)), num)
+    num = np.minimum(num, nd)
+    lo = np.clip(nd // 3 + base, 0, nd - num)
+    return lo.astype(np.uint16), num.astype(np.uint16)
+
+
+@pytest.mark.parametrize("kernel,shape,rows", [("ranged", "4,4", 32), ("ranged", "8,4", 16), ("ranged", "4,4", 8),
+                                               ("ranged", "8,4", 64), ("ranged", "8,8", 12), ("ranged", "16,12", 6),
+                                               ("ranged", "32,8", 5), ("ranged", "", 0), ("general", "", 0)])
+def test_ranged_volume_kernels(gpu_matcher, oracle, monkeypatch, kernel, shape, rows):
+    """Per-pixel ranges through the ranged kernel (both shapes, several band
+    heights: aligned, shifted and bounds-checked predecessor reads, wide
+    pixels, seams) and through the general kernel, against the textbook volume."""
+    monkeypatch.setenv("R3DGPU_RANGED_KERNEL", kernel)
+    if shape:
+        monkeypatch.setenv("R3DGPU_RANGED_SHAPE", shape)
+        monkeypatch.setenv("R3DGPU_RANGED_ROWS", str(rows))
+    left, right = _synthetic_pair(211, 157, 256, 7)
+    lo, num = _smooth_ranges(211, 157, 256, 3)
+    for o in (StereoOptions(), StereoOptions(p1=300, p2=8000, p2_adapt=0, invalid_cost=255)):
+        assert np.array_equal(gpu_matcher.sgm_cost_volume(left, right, -4, 256, o, LabelRanges(lo, num)),
+                              oracle.sgm_cost_volume(left, right, -4, 256, o, (lo, num)))
+
+
+@pytest.mark.parametrize("lr_full", [True, False])
+def test_ranged_kernel_hierarchy_shapes(gpu_matcher, oracle, monkeypatch, lr_full):
+    """The hierarchy with the wide-range shape and short bands."""
+    monkeypatch.setenv("R3DGPU_RANGED_SHAPE", "8,4")
+    monkeypatch.setenv("R3DGPU_RANGED_ROWS", "12")
+    left, right = _synthetic_pair(500, 380, 192, 4)
+    o = StereoOptions(levels=2, range_radius=0, range_margin=8, lr_full_match=lr_full, tile_size=256)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, 0, 192, o),
+                     oracle.match_stereo(left, right, None, None, 0, 192, o))
+
+
 def test_batch_equals_single(gpu_matcher):
     """Pairs of uneven size, range and depth matched together give the same
     maps as matched one by one."""

@@ -124,3 +124,62 @@ def test_invalid_input_is_rejected(simt_matcher):
     with pytest.raises(StereoError):
         simt_matcher.sgm_cost_volume(img, img, 0, 32, None,
                                      LabelRanges(np.zeros((8, 16), np.uint16), np.full((8, 16), 48, np.uint16)))
+
+
+def _smooth_ranges(w, h, nd, seed, wide_frac=0.08):
+    """Per-pixel ranges shaped like a hierarchical level's: lo drifts slowly
+    (small shifts between neighbours, now and then a jump), num mostly 16 or
+    32, a few wide pixels."""
+    rng = np.random.default_rng(seed)
+    base = np.cumsum(rng.integers(-1, 2, (h, w)) * (rng.random((h, w)) < 0.3), axis=1)
+    base = base + np.cumsum(rng.integers(-2, 3, (h, 1)), axis=0)
+    jumps = rng.random((h, w)) < 0.03
+    base = base + np.where(jumps, rng.integers(-40, 40, (h, w)), 0)
+    num = np.where(rng.random((h, w)) < 0.2, 16, 32)
+    wide = rng.random((h, w)) < wide_frac
+    num = np.minimum(np.where(wide, rng.choice([48, 64, 96, nd], (h, w)), num), nd).astype(np.int64)
+    lo = np.clip(nd // 3 + base, 0, nd - num)
+    return lo.astype(np.uint16), num.astype(np.uint16)
+
+
+@pytest.mark.parametrize("shape,rows", [("4,4", 8), ("8,4", 4), ("4,4", 32), ("8,8", 4), ("16,12", 2), ("32,8", 3)])
+def test_ranged_kernel_volume(simt_matcher, oracle, monkeypatch, shape, rows):
+    """Ranged kernel: aligned, shifted and bounds-checked predecessor reads,
+    wide pixels, band seams (few rows per band), against the textbook volume."""
+    monkeypatch.setenv("R3DGPU_RANGED_SHAPE", shape)
+    monkeypatch.setenv("R3DGPU_RANGED_ROWS", str(rows))
+    tex = Texture(29)
+    w, h, nd = 37, 29, 128
+    left, right, _ = render_pair(tex, w, h, lambda x, y: 40.0 + 0.3 * x - 0.2 * y)
+    lo, num = _smooth_ranges(w, h, nd, 5)
+    for o in (StereoOptions(p2=150, p2_adapt=8), StereoOptions(p1=300, p2=8000, p2_adapt=0, invalid_cost=255)):
+        assert np.array_equal(simt_matcher.sgm_cost_volume(left, right, -3, nd, o, LabelRanges(lo, num)),
+                              oracle.sgm_cost_volume(left, right, -3, nd, o, (lo, num)))
+
+
+@pytest.mark.parametrize("lr_full", [True, False])
+def test_ranged_kernel_hierarchy(simt_matcher, oracle, monkeypatch, lr_full):
+    """The hierarchy through the ranged kernel with many bands per tile."""
+    monkeypatch.setenv("R3DGPU_RANGED_ROWS", "8")
+    tex = Texture(31)
+    left, right, _ = render_pair(tex, 72, 52, lambda x, y: np.where(x < 35, 6.0 + 0.05 * y, 17.5))
+    o = StereoOptions(levels=2, tile_size=48, tile_margin=8, tile_blend=8, lr_full_match=lr_full, range_radius=1,
+                      range_margin=4)
+    _same_map(simt_matcher.match_stereo(left, right, None, None, 0, 32, o),
+              oracle.match_stereo(left, right, None, None, 0, 32, o))
+
+
+@pytest.mark.parametrize("opts", [
+    StereoOptions(levels=1, range_margin=20, tile_size=32, tile_margin=4, tile_blend=4, uniqueness=0.05),
+    StereoOptions(levels=1, range_margin=20, tile_size=32, tile_margin=4, tile_blend=4, lr_full_match=False,
+                  subpixel=SubpixelMethod.parabola),
+])
+def test_ranged_kernel_wide_pixels_wta(simt_matcher, oracle, monkeypatch, opts):
+    """Large range margins make most pixels wider than a row's narrow width:
+    the warp-cooperative wide path decides the winners, second bests,
+    subpixel neighbours and diagonal LR keys."""
+    monkeypatch.setenv("R3DGPU_RANGED_ROWS", "8")
+    tex = Texture(37)
+    left, right, _ = render_pair(tex, 60, 34, lambda x, y: np.where(y < 15, 9.0 + 0.1 * x, 21.0))
+    _same_map(simt_matcher.match_stereo(left, right, None, None, 0, 48, opts),
+              oracle.match_stereo(left, right, None, None, 0, 48, opts))
