@@ -49,6 +49,11 @@ ALG_BYTES_PER_PIXEL = 24
 INT_OPS_PER_CELL = 66
 
 
+def _native_check(lib, status):
+    if status != 0:
+        raise RuntimeError(lib.r3dgpu_last_error().decode())
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -60,6 +65,11 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-per-pair", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="also run the serving sweep (config 3) in a fresh process and add its results")
+    ap.add_argument("--serve-only", type=float, default=0.0, metavar="PAIRS_PER_S",
+                    help="run only the serving sweep against this saturated rate; print its JSON")
+    ap.add_argument("--serve-seconds", type=float, default=15.0, help="arrival window per load point")
     return ap.parse_args()
 
 
@@ -234,6 +244,87 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
+SERVE_REQUEST_BUDGET = 118 << 30  # config 3's 150 GB: 118 GB for admitted requests + 2 x 16 GB worker scratch
+SERVE_WORKERS = 2
+
+
+def run_serving(args, sat_pairs_per_s: float) -> dict:
+    """Config 3: Poisson arrivals of the workload's pairs at fractions of the
+    saturated batch rate, through the serving loop (continuous batching,
+    admission by device-memory budget). Per load point: latency percentiles
+    of submit -> result on the host, achieved throughput, mean batch size."""
+    import torch
+
+    from regard3d_mvs_b200 import Server
+    from regard3d_mvs_b200._native import load
+
+    lib = load()
+    specs = workload_pairs("batch64", args.pairs, args.seed)
+
+    def pinned(a):
+        t = torch.from_numpy(a.view(np.int16) if a.dtype == np.uint16 else a).pin_memory()
+        return t.numpy().view(a.dtype)
+
+    # Page-locked inputs, and page-locked output maps from a pool per pair
+    # (a request takes a free map, its completion returns it).
+    host = [tuple(pinned(x) for x in make_images(lib, s)) for s in specs]
+    pool: list[list[np.ndarray]] = [[] for _ in specs]
+
+    def take(i):
+        return pool[i].pop() if pool[i] else pinned(np.empty((specs[i]["h"], specs[i]["w"]), np.float32))
+    cells = [s["w"] * s["h"] * ((s["nd"] + 15) // 16 * 16) for s in specs]
+    rng = np.random.default_rng(args.seed + 1)
+    points = []
+    free0, total = torch.cuda.mem_get_info(0)
+    peak_used = total - free0
+    with Server(device=0, workers=SERVE_WORKERS, max_batch=16, hbm_budget=SERVE_REQUEST_BUDGET,
+                scratch_budget=16 << 30) as srv:
+        # Warm-up: every worker compiles nothing, but allocates its buffers.
+        warm = [(i, srv.submit(host[i][0], host[i][1], None, None, 0, specs[i]["nd"], options_for(specs[i]),
+                               out=(take(i), None))) for i in range(min(4, len(specs)))]
+        for i, t in warm:
+            m, _ = srv.wait(t)
+            pool[i].append(m.disparity)
+        for frac in SERVE_FRACTIONS:
+            lam = frac * sat_pairs_per_s
+            nreq = int(min(max(16, round(lam * args.serve_seconds)), 192))
+            order = rng.integers(0, len(specs), nreq)
+            gaps = rng.exponential(1.0 / lam, nreq)
+            tickets = []
+            t0 = time.perf_counter()
+            arrival = t0
+            for k in range(nreq):
+                arrival += gaps[k]
+                delay = arrival - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                i = int(order[k])
+                tickets.append((i, srv.submit(host[i][0], host[i][1], None, None, 0, specs[i]["nd"],
+                                              options_for(specs[i]), out=(take(i), None))))
+                free, _ = torch.cuda.mem_get_info(0)
+                peak_used = max(peak_used, total - free)
+            lat, batch = [], []
+            for i, t in tickets:
+                m, tm = srv.wait(t)
+                pool[i].append(m.disparity)
+                lat.append(tm["total_ms"])
+                batch.append(tm["batch_size"])
+            t1 = time.perf_counter()
+            lat = np.array(lat)
+            done_cells = sum(cells[i] for i, _ in tickets)
+            points.append({"load": frac, "offered_pairs_per_s": lam, "requests": nreq,
+                           "gcells_per_s": done_cells / (t1 - t0) / 1e9,
+                           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                                          "p999": float(np.percentile(lat, 99.9)), "max": float(lat.max())},
+                           "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
+                           "mean_batch": float(np.mean(batch))})
+    return {"saturated_pairs_per_s": sat_pairs_per_s, "workers": SERVE_WORKERS, "max_batch": 16,
+            "host_buffers": "page-locked inputs and disparity maps; no confidence maps",
+            "request_budget_bytes": SERVE_REQUEST_BUDGET, "worker_scratch_bytes": 16 << 30,
+            "device_used_peak_gb": peak_used / 1e9, "arrivals": "Poisson", "points": points}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -241,6 +332,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.serve_only > 0:
+        print(json.dumps(run_serving(args, args.serve_only)), flush=True)
         return
 
     import torch
@@ -436,6 +530,16 @@ def main():
             line["batched_vs_per_pair"] = value / per_pair["value"]
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(specs)
+        if args.serve and world == 1:
+            # In a fresh process, with this one's device memory given back.
+            del dL, dR, dD, dC
+            _native_check(lib, lib.r3dgpu_release_workspace())
+            torch.cuda.empty_cache()
+            out = subprocess.run([sys.executable, os.path.abspath(__file__), "--serve-only",
+                                  str(n * args.steps / (ms * 1e-3)), "--pairs", str(args.pairs), "--seed",
+                                  str(args.seed), "--serve-seconds", str(args.serve_seconds)],
+                                 capture_output=True, text=True, check=True)
+            line["serving"] = json.loads(out.stdout.strip().splitlines()[-1])
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

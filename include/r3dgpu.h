@@ -201,6 +201,11 @@ r3dgpu_status r3dgpu_remove_speckles_no_alloc(float* disparity, int32_t width, i
  * Replaces r3d::median_filter_3x3, src/r3d/stereo/stereo_matcher.hpp:91. */
 r3dgpu_status r3dgpu_median_filter_3x3_host(const float* disparity, int32_t width, int32_t height, float* out);
 
+/* Frees the device and pinned host buffers that this thread's calls keep on
+ * its current device for reuse (they grow to the largest call made so far);
+ * the next call allocates them again. No reference counterpart. */
+r3dgpu_status r3dgpu_release_workspace(void);
+
 /* Kernel launches issued by this process so far (the library counts its own
  * launches; bench.py reads the difference around a timed region). */
 uint64_t r3dgpu_launch_count(void);

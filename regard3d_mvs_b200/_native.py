@@ -10,7 +10,8 @@ from __future__ import annotations
 import ctypes
 import os
 
-from .types import CDisparityMap, COptions, CPair, CProfile, CSynthParams, CViewU8, CViewU16
+from .types import (CDisparityMap, COptions, CPair, CProfile, CRequestTimes, CServerConfig, CSynthParams, CViewU8,
+                    CViewU16)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libr3dgpu.so")
@@ -25,7 +26,7 @@ STATUS = {
     6: "R3DGPU_EUNSUPPORTED",
 }
 
-# Every symbol include/r3dgpu.h declares.
+# Every symbol include/r3dgpu.h and include/r3dgpu_server.h declare.
 EXPORTS = (
     "r3dgpu_last_error",
     "r3dgpu_default_options",
@@ -41,10 +42,17 @@ EXPORTS = (
     "r3dgpu_remove_speckles_host",
     "r3dgpu_remove_speckles_no_alloc",
     "r3dgpu_median_filter_3x3_host",
+    "r3dgpu_release_workspace",
     "r3dgpu_launch_count",
     "r3dgpu_profile_enable",
     "r3dgpu_profile_take",
     "r3dgpu_profile_launches",
+    # include/r3dgpu_server.h
+    "r3dgpu_server_create",
+    "r3dgpu_server_submit",
+    "r3dgpu_server_wait",
+    "r3dgpu_server_pending",
+    "r3dgpu_server_destroy",
 )
 
 
@@ -98,6 +106,8 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_remove_speckles_no_alloc.restype = st
     L.r3dgpu_median_filter_3x3_host.argtypes = [P, i32, i32, P]
     L.r3dgpu_median_filter_3x3_host.restype = st
+    L.r3dgpu_release_workspace.argtypes = []
+    L.r3dgpu_release_workspace.restype = st
     L.r3dgpu_launch_count.argtypes = []
     L.r3dgpu_launch_count.restype = ctypes.c_uint64
     L.r3dgpu_profile_enable.argtypes = [i32]
@@ -106,6 +116,18 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_profile_take.restype = None
     L.r3dgpu_profile_launches.argtypes = [ctypes.c_char_p, ctypes.c_uint64]
     L.r3dgpu_profile_launches.restype = ctypes.c_uint64
+    # The request struct has the layout of r3dgpu_pair.
+    L.r3dgpu_server_create.argtypes = [ctypes.POINTER(CServerConfig), ctypes.POINTER(P)]
+    L.r3dgpu_server_create.restype = st
+    L.r3dgpu_server_submit.argtypes = [P, ctypes.POINTER(CPair), ctypes.POINTER(ctypes.c_uint64)]
+    L.r3dgpu_server_submit.restype = st
+    L.r3dgpu_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(CPair),
+                                     ctypes.POINTER(CRequestTimes)]
+    L.r3dgpu_server_wait.restype = st
+    L.r3dgpu_server_pending.argtypes = [P]
+    L.r3dgpu_server_pending.restype = i32
+    L.r3dgpu_server_destroy.argtypes = [P]
+    L.r3dgpu_server_destroy.restype = st
     if hasattr(L, "r3dgpu_synth_pair"):
         L.r3dgpu_synth_pair.argtypes = [ctypes.POINTER(CSynthParams), P, P, P]
         L.r3dgpu_synth_pair.restype = st

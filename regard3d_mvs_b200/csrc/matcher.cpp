@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "matcher_internal.h"
 #include "sgm.h"
 #include "sgm_full.h"
 #include "sgm_ranged.h"
@@ -37,6 +38,7 @@ bool general_ranged_kernel() {
 
 thread_local std::string t_error;
 thread_local int t_device = 0;
+thread_local size_t t_scratch_budget = 0;  // 0: the default SGM scratch budget
 
 // Profiling of the SGM launches (r3dgpu_profile_*).
 struct ProfileState {
@@ -219,6 +221,11 @@ struct Workspace {
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> side_done;
   cudaEvent_t fork = nullptr;
+  ~Workspace() {
+    for (cudaStream_t st : side) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : side_done) cudaEventDestroy(ev);
+    if (fork != nullptr) cudaEventDestroy(fork);
+  }
   void ensure_side(int n) {
     if (fork == nullptr) R3D_CUDA(cudaEventCreate(&fork));
     while (static_cast<int>(side.size()) < n) {
@@ -232,8 +239,10 @@ struct Workspace {
   }
 };
 
+thread_local std::vector<std::unique_ptr<Workspace>> t_workspaces;  // per device, this thread's
+
 Workspace& workspace() {
-  thread_local std::vector<std::unique_ptr<Workspace>> per_device;
+  std::vector<std::unique_ptr<Workspace>>& per_device = t_workspaces;
   int dev = t_device;
   if (static_cast<int>(per_device.size()) <= dev) per_device.resize(dev + 1);
   if (!per_device[dev]) {
@@ -875,7 +884,7 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     // Scratch for all groups at once, within the budget: grids shrink in
     // proportion when the slots would not fit.
     {
-      const size_t budget = size_t{64} << 30;
+      const size_t budget = t_scratch_budget != 0 ? t_scratch_budget : size_t{64} << 30;
       size_t total = 0;
       for (const Launch& L : launches) total += static_cast<size_t>(L.grid) * L.slot_bytes;
       if (total > budget) {
@@ -1024,6 +1033,11 @@ T* upload(Arena& A, const T* p, int w, int h, int64_t stride, cudaStream_t s) {
 }
 
 }  // namespace
+
+void validate_request(const r3dgpu_pair& p) { validate_pair(p); }
+void set_thread_scratch_budget(size_t bytes) { t_scratch_budget = bytes; }
+void set_thread_error(const std::string& message) { t_error = message; }
+
 }  // namespace r3dgpu
 
 using namespace r3dgpu;
@@ -1063,6 +1077,16 @@ r3dgpu_status r3dgpu_set_device(int32_t device) {
     if (device < 0) fail(R3DGPU_EINVAL, "r3dgpu: negative device index");
     t_device = device;
     (void)workspace();
+  });
+}
+
+r3dgpu_status r3dgpu_release_workspace(void) {
+  return guarded([&] {
+    if (t_device < static_cast<int>(t_workspaces.size()) && t_workspaces[t_device]) {
+      R3D_CUDA(cudaSetDevice(t_device));
+      R3D_CUDA(cudaDeviceSynchronize());
+      t_workspaces[t_device].reset();
+    }
   });
 }
 

@@ -20,8 +20,8 @@ from typing import Iterable, Sequence
 import numpy as np
 
 from . import _native
-from .types import (CDisparityMap, COptions, CPair, CViewU8, CViewU16, DisparityMap, LabelRanges, StereoOptions,
-                    to_c_options)
+from .types import (CDisparityMap, COptions, CPair, CRequestTimes, CServerConfig, CViewU8, CViewU16, DisparityMap,
+                    LabelRanges, StereoOptions, to_c_options)
 
 
 def lift_u8(img: np.ndarray) -> np.ndarray:
@@ -266,6 +266,82 @@ class Matcher:
 
 
 _default: Matcher | None = None
+
+
+class Server:
+    """The serving loop of include/r3dgpu_server.h: submit pair requests
+    (host arrays) from any thread, wait on their tickets.
+
+    Requests run in continuous batches on `workers` CUDA streams; the
+    estimated device memory of the admitted requests stays within
+    `hbm_budget` bytes. Each result equals Matcher.match_stereo on the same
+    pair, whatever else ran beside it.
+    """
+
+    def __init__(self, lib_path: str | None = None, device: int = 0, workers: int = 2, max_batch: int = 16,
+                 hbm_budget: int = 64 << 30, scratch_budget: int = 0):
+        self.lib = _native.load(lib_path)
+        cfg = CServerConfig(device, workers, max_batch, 0, hbm_budget, scratch_budget)
+        h = ctypes.c_void_p()
+        _native.check(self.lib, self.lib.r3dgpu_server_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self._live: dict[int, tuple] = {}  # ticket -> (request, host arrays it points into)
+
+    def submit(self, left, right, left_valid=None, right_valid=None, disparity_min: int = 0,
+               num_disparities: int = 64, options: StereoOptions | None = None, out=None) -> int:
+        """Queues a pair. `out` = (disparity, confidence or None): caller-owned
+        float32 arrays of the left image's shape (page-locked memory makes the
+        copies asynchronous); by default both are allocated here."""
+        L, R = _u16(left), _u16(right)
+        lv = None if left_valid is None else np.ascontiguousarray(left_valid, dtype=np.uint8)
+        rv = None if right_valid is None else np.ascontiguousarray(right_valid, dtype=np.uint8)
+        h, w = L.shape
+        if out is None:
+            disp, conf = np.empty((h, w), np.float32), np.empty((h, w), np.float32)
+        else:
+            disp, conf = out
+            for a in (disp, conf):
+                if a is not None and (a.shape != (h, w) or a.dtype != np.float32 or not a.flags.c_contiguous):
+                    raise _native.StereoError(1, "server: output arrays must be contiguous float32 of the image shape")
+        req = CPair()
+        req.left, req.right = _view16(L), _view16(R)
+        req.left_valid, req.right_valid = _view8(lv), _view8(rv)
+        req.disparity_min, req.num_disparities = int(disparity_min), int(num_disparities)
+        req.options = _opts(options)
+        req.out.disparity, req.out.stride = disp.ctypes.data, w
+        req.out.confidence = conf.ctypes.data if conf is not None else None
+        ticket = ctypes.c_uint64()
+        _native.check(self.lib, self.lib.r3dgpu_server_submit(self._h, ctypes.byref(req), ctypes.byref(ticket)))
+        self._live[ticket.value] = (req, (L, R, lv, rv, disp, conf))
+        return ticket.value
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0) -> tuple[DisparityMap, dict]:
+        req, arrays = self._live[ticket]
+        t = CRequestTimes()
+        st = self.lib.r3dgpu_server_wait(self._h, ticket, float(timeout_ms), ctypes.byref(req), ctypes.byref(t))
+        if st != 5:  # R3DGPU_ETIMEOUT keeps the ticket
+            del self._live[ticket]
+        _native.check(self.lib, st)
+        disp, conf = arrays[4], arrays[5]
+        times = {"queued_ms": t.queued_ms, "run_ms": t.run_ms, "total_ms": t.total_ms,
+                 "device_bytes": int(t.device_bytes), "batch_size": t.batch_size, "worker": t.worker}
+        return DisparityMap(disp, conf, req.out.disparity_min, req.out.num_disparities, req.out.levels,
+                            int(req.out.cells)), times
+
+    def pending(self) -> int:
+        return int(self.lib.r3dgpu_server_pending(self._h))
+
+    def close(self) -> None:
+        if self._h:
+            _native.check(self.lib, self.lib.r3dgpu_server_destroy(self._h))
+            self._h = ctypes.c_void_p()
+            self._live.clear()
+
+    def __enter__(self) -> "Server":
+        return self
+
+    def __exit__(self, *exc) -> None:
+        self.close()
 
 
 def default_matcher() -> Matcher:

@@ -133,6 +133,28 @@ class CPair(ctypes.Structure):
     ]
 
 
+class CServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("workers", ctypes.c_int32),
+        ("max_batch", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("hbm_budget", ctypes.c_uint64),
+        ("scratch_budget", ctypes.c_uint64),
+    ]
+
+
+class CRequestTimes(ctypes.Structure):
+    _fields_ = [
+        ("queued_ms", ctypes.c_double),
+        ("run_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+        ("device_bytes", ctypes.c_uint64),
+        ("batch_size", ctypes.c_int32),
+        ("worker", ctypes.c_int32),
+    ]
+
+
 class CProfile(ctypes.Structure):
     _fields_ = [
         ("sgm_ms", ctypes.c_double),

@@ -27,7 +27,7 @@ def cuda_lib():
 
 
 def test_exports_every_declared_symbol(cuda_lib):
-    names = _declared("r3dgpu.h") | _declared("r3dgpu_synth.h")
+    names = _declared("r3dgpu.h") | _declared("r3dgpu_server.h") | _declared("r3dgpu_synth.h")
     assert len(names) >= 15
     for n in sorted(names):
         assert hasattr(cuda_lib, n), n
@@ -37,7 +37,7 @@ def test_exports_every_declared_symbol(cuda_lib):
 
 
 def test_emulator_exports_the_same_matcher_symbols(simt_matcher):
-    names = _declared("r3dgpu.h")
+    names = _declared("r3dgpu.h") | _declared("r3dgpu_server.h")
     for n in sorted(names):
         assert hasattr(simt_matcher.lib, n), n
 

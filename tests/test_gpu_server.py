@@ -1,0 +1,74 @@
+"""The serving loop on the B200: requests of uneven size, label range and
+hierarchy depth, submitted from several client threads and run in
+continuous batches on two worker streams, give exactly the maps of the same
+pairs matched alone; a tight device-memory budget serialises them without
+changing any result."""
+
+from __future__ import annotations
+
+import threading
+
+import numpy as np
+import pytest
+
+from images import mismatch_report, same_disparities
+from regard3d_mvs_b200 import Server, StereoOptions
+from test_gpu_parity import _synthetic_pair
+
+pytestmark = pytest.mark.gpu
+
+SPECS = ((640, 480, 128, 0), (768, 512, 256, 3), (400, 300, 96, -1), (1024, 700, 192, 2), (320, 240, 64, 0),
+         (900, 600, 128, 1))
+
+
+@pytest.fixture(scope="module")
+def pairs():
+    out = []
+    for i, (w, h, nd, lv) in enumerate(SPECS):
+        left, right = _synthetic_pair(w, h, nd, 30 + i)
+        o = StereoOptions(levels=lv, range_radius=0, range_margin=8) if lv else StereoOptions(levels=lv)
+        out.append(dict(left=left, right=right, disparity_min=0, num_disparities=nd, options=o))
+    return out
+
+
+@pytest.fixture(scope="module")
+def alone(gpu_matcher, pairs):
+    return [gpu_matcher.match_stereo(p["left"], p["right"], None, None, 0, p["num_disparities"], p["options"])
+            for p in pairs]
+
+
+def _same(a, b):
+    assert same_disparities(a.disparity, b.disparity), mismatch_report(a.disparity, b.disparity)
+    assert np.array_equal(a.confidence, b.confidence)
+    assert (a.cells, a.levels, a.num_disparities) == (b.cells, b.levels, b.num_disparities)
+
+
+def test_server_mix_equals_alone(pairs, alone):
+    got, times = {}, {}
+    lock = threading.Lock()
+    with Server(workers=2, max_batch=3, hbm_budget=16 << 30, scratch_budget=8 << 30) as srv:
+        def client(idxs):
+            tickets = [(i, srv.submit(**pairs[i])) for i in idxs]
+            for i, t in tickets:
+                m, tm = srv.wait(t)
+                with lock:
+                    got[i], times[i] = m, tm
+
+        threads = [threading.Thread(target=client, args=(list(range(k, len(pairs), 3)),)) for k in range(3)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+    for i, a in enumerate(alone):
+        _same(got[i], a)
+    assert {t["worker"] for t in times.values()} <= {0, 1}
+
+
+def test_server_tight_budget(pairs, alone):
+    # Every request is larger than the budget: each runs alone, one at a time.
+    with Server(workers=2, max_batch=8, hbm_budget=1) as srv:
+        tickets = [srv.submit(**p) for p in pairs]
+        res = [srv.wait(t) for t in tickets]
+    for a, (m, tm) in zip(alone, res):
+        _same(m, a)
+        assert tm["batch_size"] == 1
