@@ -172,7 +172,7 @@ def measured_peaks():
 
 def sgm_traffic_per_cell():
     """DRAM bytes per aggregated cell of the SGM kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "sgm_tile_kernel_traffic.json")
+    path = os.path.join(ROOT, "profiles", "sgm_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
             d = json.load(f)
