@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OBJ_DIR = os.path.join(HERE, "_lib", "obj")
 LIB = os.path.join(OUT_DIR, "libr3dgpu.so")
-SOURCES = ("image_kernels.cu", "sgm.cu", "sgm_full.cu", "sgm_ranged.cu", "noalloc.cu", "matcher.cpp", "server.cpp", "synth.cpp")
+SOURCES = ("image_kernels.cu", "sgm.cu", "sgm_full.cu", "sgm_ranged.cu", "noalloc.cu", "matcher.cpp", "server.cpp", "tuning.cpp", "synth.cpp")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
          "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3"]
@@ -57,7 +57,8 @@ def build(force: bool = False) -> str:
         return LIB
     with cf.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
         objs = list(ex.map(_compile, SOURCES))
-    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static", "-o", LIB, *objs]
+    cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-cudart", "static", "-o", LIB, *objs,
+           "-ldl", "-lpthread"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

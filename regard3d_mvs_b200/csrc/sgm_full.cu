@@ -25,6 +25,7 @@
 #include "sgm.h"
 #include "sgm_full.h"
 #include "sgm_simd.cuh"
+#include "tuning.h"
 
 namespace r3dgpu {
 
@@ -652,6 +653,16 @@ SgmFullPlan sgm_full_plan(int nd, int smem_optin) {
   else if (nd <= 768) p.shape = {32, 12};
   else return p;
   int max_rows = 1 << 20;
+  // The autotuner's entry for this label count, if any.
+  {
+    const auto& table = tuning().full;
+    const auto it = table.find(nd);
+    if (it != table.end() && 2 * it->second.g * it->second.k >= nd &&
+        sgm_full_shape_compiled({it->second.g, it->second.k})) {
+      p.shape = {it->second.g, it->second.k};
+      max_rows = it->second.rows;
+    }
+  }
   if (const char* e = std::getenv("R3DGPU_FULL_SHAPE")) {
     int g = 0, k = 0;
     if (std::sscanf(e, "%d,%d", &g, &k) == 2 && 2 * g * k >= nd && sgm_full_shape_compiled({g, k})) p.shape = {g, k};

@@ -30,6 +30,7 @@
 #include "sgm.h"
 #include "sgm_ranged.h"
 #include "sgm_simd.cuh"
+#include "tuning.h"
 
 namespace r3dgpu {
 
@@ -964,7 +965,7 @@ int sgm_ranged_width_for(const int* stats, int64_t pixels) {
     int g = 0, k = 0;
     if (std::sscanf(e, "%d,%d", &g, &k) == 2 && ranged_shape_compiled({g, k})) return 2 * g * k;
   }
-  double frac = 0.002;
+  double frac = tuning().ranged_wide_frac >= 0.0 ? tuning().ranged_wide_frac : 0.002;
   if (const char* e = std::getenv("R3DGPU_RANGED_WIDE_FRAC")) frac = std::atof(e);
   const double allowed = frac * static_cast<double>(pixels);
   // stats[1 + i]: pixels with more labels than tile_stat_width(i).
@@ -981,6 +982,10 @@ SgmRangedShape sgm_ranged_shape_for_width(int width) {
 
 SgmRangedPlan sgm_ranged_plan(SgmRangedShape shape, int smem_optin) {
   SgmRangedPlan p{shape, 32};
+  {
+    const auto it = tuning().ranged_rows.find(2 * shape.g_ * shape.k_);
+    if (it != tuning().ranged_rows.end()) p.rows = it->second;
+  }
   const int rpw = 32 / p.shape.g_;
   const int max_rows = (p.shape.k_ >= 8 ? 256 : kSgmRangedThreads) / 32 * rpw;
   if (const char* e = std::getenv("R3DGPU_RANGED_ROWS")) p.rows = std::atoi(e);
