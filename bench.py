@@ -244,6 +244,82 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# Multi-view combination (r3dgpu_combine_pairs) of one view: 2048 x 1536 grid,
+# 4 partner pairs. Algorithmic bytes per grid pixel: per pair one disparity
+# and one confidence sample (4 + 4 B), plus depth, confidence and pair mask
+# written (4 + 4 + 2 B).
+COMBINE_W, COMBINE_H, COMBINE_PAIRS = 2048, 1536, 4
+COMBINE_BYTES_PER_PIXEL = COMBINE_PAIRS * 8 + 10
+
+
+def measure_combine(lib, dev, stream, steps: int, warmup: int, peak: float) -> dict:
+    """Device time of the combination of 4 matched pairs into a depth map,
+    the oracle's time on the same view (all host threads) beside it."""
+    import torch
+
+    from oracle import oracle as orc
+    from regard3d_mvs_b200.multi_view import Plane, Rig, c_grid, c_pairs, plane_disparity
+    from regard3d_mvs_b200.types import CPairGeometry, MultiStereoOptions
+
+    rig = Rig(w=COMBINE_W, h=COMBINE_H, f=1800.0,
+              partners=((0.6, 0.0, 0.0), (-0.5, 0.3, 0.1), (0.2, -0.55, 0.0), (-0.3, -0.4, 0.2)))
+    plane = Plane()
+    rng = np.random.default_rng(3)
+    pairs = []
+    for p, shift in zip(rig.partners, (0.0, 0.5, 6.0, 0.0)):
+        q = rig.rectify(p)
+        d = plane_disparity(rig, q, plane, shift)
+        d += rng.normal(0, 0.3, d.shape).astype(np.float32)
+        d[rng.random(d.shape) < 0.08] = np.inf
+        q["disparity"] = d
+        q["confidence"] = rng.random(d.shape).astype(np.float32)
+        pairs.append(q)
+    grid = rig.grid()
+    g = c_grid(grid)
+    harr, keep = c_pairs(grid, pairs)
+    darr = (CPairGeometry * COMBINE_PAIRS)()
+    dev_maps = []
+    for i, q in enumerate(pairs):
+        darr[i] = harr[i]
+        dd = torch.from_numpy(q["disparity"]).to(dev)
+        dc = torch.from_numpy(q["confidence"]).to(dev)
+        dev_maps += [dd, dc]
+        darr[i].disparity, darr[i].confidence = dd.data_ptr(), dc.data_ptr()
+    depth = torch.empty((COMBINE_H, COMBINE_W), dtype=torch.float32, device=dev)
+    conf = torch.empty_like(depth)
+    mask = torch.empty((COMBINE_H, COMBINE_W), dtype=torch.int16, device=dev)
+    o = MultiStereoOptions().c()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def run():
+        _native_check(lib, lib.r3dgpu_combine_pairs(ctypes.byref(g), darr, COMBINE_PAIRS, ctypes.byref(o),
+                                                    depth.data_ptr(), conf.data_ptr(), mask.data_ptr(), COMBINE_W,
+                                                    sptr))
+
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(steps):
+        run()
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b) / steps
+    px = COMBINE_W * COMBINE_H
+    achieved = COMBINE_BYTES_PER_PIXEL * px / (ms * 1e-3) / 1e9
+    t0 = time.perf_counter()
+    ref = orc.combine_pairs(grid, pairs)
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ref.depth, depth.cpu().numpy()))
+    return {"workload": f"combine_pairs, {COMBINE_W}x{COMBINE_H} grid, {COMBINE_PAIRS} pairs, plane + noise",
+            "value": px / (ms * 1e-3) / 1e9, "unit": "Gpixels/s", "ms": ms, "bit_exact_vs_oracle": same,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "alg_bytes_per_pixel": COMBINE_BYTES_PER_PIXEL},
+            "cpu_baseline": {"value": px / cpu_s / 1e9, "unit": "Gpixels/s", "cores": orc.max_threads(),
+                             "kind": "port", "sample": "the same view, once"}}
+
+
 SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
 SERVE_REQUEST_BUDGET = 118 << 30  # config 3's 150 GB: 118 GB for admitted requests + 2 x 16 GB worker scratch
 SERVE_WORKERS = 2
@@ -530,6 +606,7 @@ def main():
             line["batched_vs_per_pair"] = value / per_pair["value"]
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(specs)
+            line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
         if args.serve and world == 1:
             # In a fresh process, with this one's device memory given back.
             del dL, dR, dD, dC

@@ -201,6 +201,62 @@ r3dgpu_status r3dgpu_remove_speckles_no_alloc(float* disparity, int32_t width, i
  * Replaces r3d::median_filter_3x3, src/r3d/stereo/stereo_matcher.hpp:91. */
 r3dgpu_status r3dgpu_median_filter_3x3_host(const float* disparity, int32_t width, int32_t height, float* out);
 
+/* ------------------------------------------------------------------ multi-view
+ * Combination of up to 16 matched pairs that share a base camera into one
+ * depth map (the consumer of the matcher in the multi-view stage).
+ * Replaces r3d::combine_pairs, src/r3d/mvs/multi_stereo.hpp:43-44
+ * (implementation src/r3d/mvs/multi_stereo.cpp:74-216). The caller passes
+ * the geometry the reference derives with Eigen from the cameras. */
+
+/* The depth map's grid camera (r3d::PinholeCamera): K^-1 and R^T (row-major)
+ * and the centre. */
+typedef struct r3dgpu_depth_grid {
+  double k_inv[9];
+  double rot_t[9];
+  double center[3];
+  int32_t width;
+  int32_t height;
+} r3dgpu_depth_grid;
+
+/* One pair (multi_stereo.cpp:24-33 PairGeometry): grid pixel -> rectified
+ * left pixel homography K_r R_r R_g^T K_g^-1 (row-major), focal * baseline,
+ * disparity offset (cx_left - cx_right), the partner camera's centre, and the
+ * pair's disparity map (and confidence, or NULL) in the rectified left image. */
+typedef struct r3dgpu_pair_geometry {
+  double grid_to_rect[9];
+  double fb;
+  double offset;
+  double partner_center[3];
+  const float* disparity;
+  const float* confidence;
+  int32_t width;
+  int32_t height;
+  int64_t stride;
+} r3dgpu_pair_geometry;
+
+/* MultiStereoOptions, src/r3d/mvs/multi_stereo.hpp:25-30 (same defaults). */
+typedef struct r3dgpu_multi_stereo_options {
+  double inlier_px;
+  double max_reprojection_px;
+  double min_angle_deg;
+  int32_t min_pairs;
+  int32_t reserved;
+} r3dgpu_multi_stereo_options;
+
+void r3dgpu_default_multi_stereo_options(r3dgpu_multi_stereo_options* out);
+
+/* Depth (0 = none), confidence and pair mask (bit i: pair i was used) of
+ * every grid pixel; maps and outputs in device memory, row stride `stride`
+ * elements; runs on `stream` and synchronises it. */
+r3dgpu_status r3dgpu_combine_pairs(const r3dgpu_depth_grid* grid, const r3dgpu_pair_geometry* pairs, int32_t count,
+                                   const r3dgpu_multi_stereo_options* options, float* depth, float* confidence,
+                                   uint16_t* pair_mask, int64_t stride, void* stream);
+
+/* Same with the pairs' maps and the outputs in host memory (copies inside). */
+r3dgpu_status r3dgpu_combine_pairs_host(const r3dgpu_depth_grid* grid, const r3dgpu_pair_geometry* pairs,
+                                        int32_t count, const r3dgpu_multi_stereo_options* options, float* depth,
+                                        float* confidence, uint16_t* pair_mask, int64_t stride);
+
 /* Frees the device and pinned host buffers that this thread's calls keep on
  * its current device for reuse (they grow to the largest call made so far);
  * the next call allocates them again. No reference counterpart. */

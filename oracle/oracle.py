@@ -48,6 +48,8 @@ def lib():
         L.orc_median_filter_3x3.argtypes = [P, i32, i32, P]
         L.orc_match_stereo.argtypes = [P, i32, i32, P, i32, P, P, i32, i32, P, P, P, P]
         L.orc_match_tiles.argtypes = [P, i32, i32, P, i32, P, P, i32, i32, P, P, P, i32, P, P, P]
+        L.orc_combine_pairs.argtypes = [P, P, i32, P, P, P, P, ctypes.c_int64]
+        L.orc_sample_disparity.argtypes = [P, i32, i32, P, P, i32, P]
         _lib = L
     return _lib
 
@@ -145,6 +147,34 @@ def remove_speckles(disp: np.ndarray, min_size: int, max_diff: float) -> np.ndar
     d = np.array(disp, dtype=np.float32, order="C", copy=True)
     _check(lib().orc_remove_speckles(_ptr(d), d.shape[1], d.shape[0], int(min_size), float(max_diff)))
     return d
+
+
+def combine_pairs(grid: dict, pairs: list, options=None):
+    """r3d::combine_pairs (src/r3d/mvs/multi_stereo.cpp:74-216) on the CPU;
+    grid and pairs as in regard3d_mvs_b200.multi_view."""
+    from regard3d_mvs_b200.multi_view import c_grid, c_pairs
+    from regard3d_mvs_b200.types import DepthMap, MultiStereoOptions
+
+    g = c_grid(grid)
+    arr, keep = c_pairs(grid, pairs)
+    o = (options or MultiStereoOptions()).c()
+    depth = np.empty((g.height, g.width), np.float32)
+    conf = np.empty_like(depth)
+    mask = np.empty((g.height, g.width), np.uint16)
+    _check(lib().orc_combine_pairs(ctypes.byref(g), arr, len(pairs), ctypes.byref(o), _ptr(depth), _ptr(conf),
+                                   _ptr(mask), g.width))
+    del keep
+    return DepthMap(depth, conf, mask)
+
+
+def sample_disparity(disp: np.ndarray, u, v) -> np.ndarray:
+    """r3d::sample_disparity (src/r3d/mvs/multi_stereo.cpp:44-72) at positions (u, v)."""
+    d = _c(disp, np.float32)
+    u = np.ascontiguousarray(np.atleast_1d(u), np.float64)
+    v = np.ascontiguousarray(np.atleast_1d(v), np.float64)
+    out = np.empty(u.shape, np.float32)
+    _check(lib().orc_sample_disparity(_ptr(d), d.shape[1], d.shape[0], _ptr(u), _ptr(v), u.size, _ptr(out)))
+    return out
 
 
 def median_filter_3x3(disp: np.ndarray) -> np.ndarray:

@@ -933,6 +933,170 @@ int guarded(F&& f) {
 }  // namespace orc
 
 // ---------------------------------------------------------------- C ABI (ctypes)
+// ---------------------------------------------------------------- multi-view
+// combine_pairs and sample_disparity (src/r3d/mvs/multi_stereo.cpp:44-216),
+// in the reference's operation order; the geometry (Eigen-derived matrices in
+// the reference) comes precomputed in r3dgpu_depth_grid / r3dgpu_pair_geometry.
+namespace orc {
+
+float sample_disparity(const r3dgpu_pair_geometry& g, double u, double v) {  // multi_stereo.cpp:44-72
+  const int w = g.width, h = g.height;
+  if (!(u > -0.5 && v > -0.5 && u < w - 0.5 && v < h - 0.5)) return kInvalid;
+  const int x0 = std::clamp(static_cast<int>(std::floor(u)), 0, w - 1);
+  const int y0 = std::clamp(static_cast<int>(std::floor(v)), 0, h - 1);
+  const int x1 = std::min(x0 + 1, w - 1);
+  const int y1 = std::min(y0 + 1, h - 1);
+  auto at = [&](int x, int y) { return g.disparity[static_cast<int64_t>(y) * g.stride + x]; };
+  const float d00 = at(x0, y0), d10 = at(x1, y0), d01 = at(x0, y1), d11 = at(x1, y1);
+  if (std::isfinite(d00) && std::isfinite(d10) && std::isfinite(d01) && std::isfinite(d11)) {
+    const float lo = std::min({d00, d10, d01, d11});
+    const float hi = std::max({d00, d10, d01, d11});
+    if (hi - lo <= 1.0F) {
+      const auto fx = static_cast<float>(std::clamp(u - x0, 0.0, 1.0));
+      const auto fy = static_cast<float>(std::clamp(v - y0, 0.0, 1.0));
+      const float top = d00 + fx * (d10 - d00);
+      const float bottom = d01 + fx * (d11 - d01);
+      return top + fy * (bottom - top);
+    }
+  }
+  const int xn = std::clamp(static_cast<int>(std::lround(u)), 0, w - 1);
+  const int yn = std::clamp(static_cast<int>(std::lround(v)), 0, h - 1);
+  return at(xn, yn);
+}
+
+// 3x3 (row-major) times (x, y, z), each row summed left to right.
+void mat_vec(const double* m, double x, double y, double z, double* out) {
+  for (int i = 0; i < 3; ++i) out[i] = m[3 * i] * x + m[3 * i + 1] * y + m[3 * i + 2] * z;
+}
+
+void normalize3(double* v) {
+  const double n = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+  if (n > 0.0) {
+    const double s = std::sqrt(n);
+    for (int k = 0; k < 3; ++k) v[k] /= s;
+  }
+}
+
+void combine_pairs(const r3dgpu_depth_grid& grid, const r3dgpu_pair_geometry* geo, int count,
+                   const r3dgpu_multi_stereo_options& options, float* depth, float* confidence, uint16_t* mask,
+                   int64_t stride) {  // multi_stereo.cpp:74-216
+  constexpr int kMaxPairs = 16;
+  if (count > kMaxPairs) throw Failure("combine_pairs: at most 16 pairs per view");
+  struct Candidate {
+    double w = 0.0, k = 0.0;
+    float confidence = 0.0F;
+    int pair = 0;
+  };
+  const double cos_min_angle = std::cos(options.min_angle_deg * 3.14159265358979323846 / 180.0);
+  const int min_pairs = std::max(1, options.min_pairs);
+  const int w = grid.width, h = grid.height;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 8)
+#endif
+  for (int yy = 0; yy < h; ++yy) {
+    Candidate cand[kMaxPairs];
+    int used[kMaxPairs];
+    for (int x = 0; x < w; ++x) {
+      const int64_t o = static_cast<int64_t>(yy) * stride + x;
+      depth[o] = 0.0F;
+      confidence[o] = 0.0F;
+      mask[o] = 0;
+      int n = 0;
+      for (int i = 0; i < count; ++i) {
+        const r3dgpu_pair_geometry& g = geo[i];
+        double r[3];
+        mat_vec(g.grid_to_rect, x, yy, 1.0, r);
+        const double c = r[2];
+        if (!(c > 1e-9)) continue;
+        const double u = r[0] / c;
+        const double v = r[1] / c;
+        const float d = sample_disparity(g, u, v);
+        if (!std::isfinite(d) || d <= g.offset) continue;
+        Candidate& cd = cand[n++];
+        cd.k = g.fb / c;
+        cd.w = (d - g.offset) / cd.k;
+        cd.pair = i;
+        cd.confidence = 0.0F;
+        if (g.confidence != nullptr) {
+          const int xn = std::clamp(static_cast<int>(std::lround(u)), 0, g.width - 1);
+          const int yn = std::clamp(static_cast<int>(std::lround(v)), 0, g.height - 1);
+          cd.confidence = g.confidence[static_cast<int64_t>(yn) * g.stride + xn];
+        }
+      }
+      if (n < min_pairs) continue;
+      int best = -1, best_support = 0;
+      float best_conf = -1.0F;
+      for (int i = 0; i < n; ++i) {
+        int support = 0;
+        float conf = 0.0F;
+        for (int j = 0; j < n; ++j) {
+          if (std::abs(cand[j].k * (cand[j].w - cand[i].w)) <= options.inlier_px) {
+            ++support;
+            conf += cand[j].confidence;
+          }
+        }
+        if (support > best_support || (support == best_support && conf > best_conf)) {
+          best = i;
+          best_support = support;
+          best_conf = conf;
+        }
+      }
+      int m = 0;
+      for (int j = 0; j < n; ++j)
+        if (std::abs(cand[j].k * (cand[j].w - cand[best].w)) <= options.inlier_px) used[m++] = j;
+      double w_opt = 0.0;
+      while (m > 0) {
+        double sw = 0.0, swx = 0.0;
+        for (int t = 0; t < m; ++t) {
+          const Candidate& cd = cand[used[t]];
+          sw += cd.k * cd.k;
+          swx += cd.k * cd.k * cd.w;
+        }
+        w_opt = swx / sw;
+        int worst = -1;
+        double worst_res = options.max_reprojection_px;
+        for (int t = 0; t < m; ++t) {
+          const Candidate& cd = cand[used[t]];
+          const double res = std::abs(cd.k * (cd.w - w_opt));
+          if (res > worst_res) {
+            worst_res = res;
+            worst = t;
+          }
+        }
+        if (worst < 0) break;
+        used[worst] = used[--m];
+      }
+      const bool majority = m > n - m || (m >= 2 && m >= n - m);
+      if (m < min_pairs || !majority || !(w_opt > 0.0)) continue;
+      const double z = 1.0 / w_opt;
+      double a[3], ray[3], xw[3], tb[3];
+      mat_vec(grid.k_inv, x, yy, 1.0, a);
+      mat_vec(grid.rot_t, a[0], a[1], a[2], ray);
+      for (int k = 0; k < 3; ++k) xw[k] = grid.center[k] + z * ray[k];
+      for (int k = 0; k < 3; ++k) tb[k] = grid.center[k] - xw[k];
+      normalize3(tb);
+      bool wide = false;
+      float conf = 0.0F;
+      uint16_t msk = 0;
+      for (int t = 0; t < m; ++t) {
+        const Candidate& cd = cand[used[t]];
+        msk = static_cast<uint16_t>(msk | (1U << cd.pair));
+        double tp[3];
+        for (int k = 0; k < 3; ++k) tp[k] = geo[cd.pair].partner_center[k] - xw[k];
+        normalize3(tp);
+        wide = wide || (tb[0] * tp[0] + tb[1] * tp[1] + tb[2] * tp[2]) <= cos_min_angle;
+        conf += cd.confidence;
+      }
+      if (!wide) continue;
+      depth[o] = static_cast<float>(z);
+      confidence[o] = conf / static_cast<float>(m);
+      mask[o] = msk;
+    }
+  }
+}
+
+}  // namespace orc
+
 extern "C" {
 
 const char* orc_last_error() { return orc::g_error.c_str(); }
@@ -1067,6 +1231,25 @@ int orc_match_tiles(const uint16_t* left, int wl, int h, const uint16_t* right, 
     std::copy(m.disp.px.begin(), m.disp.px.end(), disp);
     if (conf) std::copy(m.conf.px.begin(), m.conf.px.end(), conf);
     *cells = m.cells;
+  });
+}
+
+// combine_pairs on host maps (pairs' disparity/confidence pointers are host pointers).
+int orc_combine_pairs(const r3dgpu_depth_grid* grid, const r3dgpu_pair_geometry* pairs, int count,
+                      const r3dgpu_multi_stereo_options* options, float* depth, float* confidence, uint16_t* mask,
+                      int64_t stride) {
+  return orc::guarded([&] { orc::combine_pairs(*grid, pairs, count, *options, depth, confidence, mask, stride); });
+}
+
+// sample_disparity at n positions.
+int orc_sample_disparity(const float* disp, int w, int h, const double* u, const double* v, int n, float* out) {
+  return orc::guarded([&] {
+    r3dgpu_pair_geometry g{};
+    g.disparity = disp;
+    g.width = w;
+    g.height = h;
+    g.stride = w;
+    for (int i = 0; i < n; ++i) out[i] = orc::sample_disparity(g, u[i], v[i]);
   });
 }
 

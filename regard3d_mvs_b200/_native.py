@@ -10,8 +10,8 @@ from __future__ import annotations
 import ctypes
 import os
 
-from .types import (CDisparityMap, COptions, CPair, CProfile, CRequestTimes, CServerConfig, CSynthParams, CViewU8,
-                    CViewU16)
+from .types import (CDepthGrid, CDisparityMap, CMultiStereoOptions, COptions, CPair, CPairGeometry, CProfile,
+                    CRequestTimes, CServerConfig, CSynthParams, CViewU8, CViewU16)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libr3dgpu.so")
@@ -42,6 +42,9 @@ EXPORTS = (
     "r3dgpu_remove_speckles_host",
     "r3dgpu_remove_speckles_no_alloc",
     "r3dgpu_median_filter_3x3_host",
+    "r3dgpu_default_multi_stereo_options",
+    "r3dgpu_combine_pairs",
+    "r3dgpu_combine_pairs_host",
     "r3dgpu_release_workspace",
     "r3dgpu_launch_count",
     "r3dgpu_profile_enable",
@@ -106,6 +109,13 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_remove_speckles_no_alloc.restype = st
     L.r3dgpu_median_filter_3x3_host.argtypes = [P, i32, i32, P]
     L.r3dgpu_median_filter_3x3_host.restype = st
+    L.r3dgpu_default_multi_stereo_options.argtypes = [ctypes.POINTER(CMultiStereoOptions)]
+    L.r3dgpu_default_multi_stereo_options.restype = None
+    for name in ("r3dgpu_combine_pairs", "r3dgpu_combine_pairs_host"):
+        f = getattr(L, name)
+        f.argtypes = [ctypes.POINTER(CDepthGrid), ctypes.POINTER(CPairGeometry), i32,
+                      ctypes.POINTER(CMultiStereoOptions), P, P, P, ctypes.c_int64] + ([P] if name == "r3dgpu_combine_pairs" else [])
+        f.restype = st
     L.r3dgpu_release_workspace.argtypes = []
     L.r3dgpu_release_workspace.restype = st
     L.r3dgpu_launch_count.argtypes = []

@@ -167,35 +167,107 @@ R3D_DEVICE void uf_unite(int* parent, int a, int b) {
   }
 }
 
-R3D_GLOBAL void uf_init_kernel(int* parent, int* size, int64_t n) {
+// Tiles of 32 x 32 pixels are united in shared memory first (local indices
+// in row-major order, so a local root is also the smallest global index of
+// its part of the segment); only pixels on tile borders then unite across
+// tiles in global memory.
+constexpr int kUfTile = 32;
+
+R3D_DEVICE int uf_root_local(volatile int* par, int x) {
+  int p = par[x];
+  while (p != x) {
+    x = p;
+    p = par[x];
+  }
+  return x;
+}
+
+R3D_DEVICE void uf_unite_local(int* par, int a, int b) {
+  while (true) {
+    a = uf_root_local(par, a);
+    b = uf_root_local(par, b);
+    if (a == b) return;
+    if (a > b) {
+      const int t = a;
+      a = b;
+      b = t;
+    }
+    const int old = atomicCAS(par + b, b, a);
+    if (old == b) return;
+    b = old;
+  }
+}
+
+// Per tile: local union, then parent[p] = global index of p's local root and
+// size[p] = 0 for every pixel of the tile.
+R3D_GLOBAL void uf_tile_kernel(const float* __restrict__ d, int w, int h, float max_diff, int* parent, int* size) {
+  R3D_DYNAMIC_SMEM(smem);
+  int* par = reinterpret_cast<int*>(smem);
+  float* dv = reinterpret_cast<float*>(smem + sizeof(int) * kUfTile * kUfTile);
+  const int tx0 = static_cast<int>(blockIdx.x) * kUfTile, ty0 = static_cast<int>(blockIdx.y) * kUfTile;
+  const int tw = r3dsimt::imin(kUfTile, w - tx0), th = r3dsimt::imin(kUfTile, h - ty0);
+  const int nt = static_cast<int>(blockDim.x);
+  for (int i = static_cast<int>(threadIdx.x); i < kUfTile * kUfTile; i += nt) {
+    const int lx = i % kUfTile, ly = i / kUfTile;
+    par[i] = i;
+    dv[i] = (lx < tw && ly < th) ? d[static_cast<int64_t>(ty0 + ly) * w + tx0 + lx] : kInf;
+  }
+  r3dsimt::syncthreads();
+  for (int i = static_cast<int>(threadIdx.x); i < kUfTile * kUfTile; i += nt) {
+    const int lx = i % kUfTile, ly = i / kUfTile;
+    const float v = dv[i];
+    if (lx >= tw || ly >= th || !r3dsimt::finitef(v)) continue;
+    if (lx + 1 < tw && fabsf(__fsub_rn(dv[i + 1], v)) <= max_diff) uf_unite_local(par, i, i + 1);
+    if (ly + 1 < th && fabsf(__fsub_rn(dv[i + kUfTile], v)) <= max_diff) uf_unite_local(par, i, i + kUfTile);
+  }
+  r3dsimt::syncthreads();
+  for (int i = static_cast<int>(threadIdx.x); i < kUfTile * kUfTile; i += nt) {
+    const int lx = i % kUfTile, ly = i / kUfTile;
+    if (lx >= tw || ly >= th) continue;
+    const int r = uf_root_local(par, i);
+    const int64_t g = static_cast<int64_t>(ty0 + ly) * w + tx0 + lx;
+    parent[g] = (ty0 + r / kUfTile) * w + tx0 + r % kUfTile;
+    size[g] = 0;
+  }
+}
+
+// Unions across tile borders: the pixel pairs straddling a vertical tile
+// boundary, then those straddling a horizontal one.
+R3D_GLOBAL void uf_border_kernel(const float* __restrict__ d, int w, int h, float max_diff, int* parent) {
+  const int64_t nvx = static_cast<int64_t>((w - 1) / kUfTile) * h;  // vertical boundaries x all rows
+  const int64_t nhy = static_cast<int64_t>((h - 1) / kUfTile) * w;  // horizontal boundaries x all columns
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < n) {
-    parent[i] = static_cast<int>(i);
-    size[i] = 0;
+  int a = -1, b = -1;
+  if (i < nvx) {
+    const int y = static_cast<int>(i % h), k = static_cast<int>(i / h);
+    const int x = (k + 1) * kUfTile - 1;
+    a = y * w + x;
+    b = a + 1;
+  } else if (i < nvx + nhy) {
+    const int64_t j = i - nvx;
+    const int x = static_cast<int>(j % w), k = static_cast<int>(j / w);
+    const int y = (k + 1) * kUfTile - 1;
+    a = y * w + x;
+    b = a + w;
+  } else {
+    return;
   }
+  const float u = d[a], v = d[b];
+  if (r3dsimt::finitef(u) && fabsf(__fsub_rn(v, u)) <= max_diff) uf_unite(parent, a, b);
 }
 
-R3D_GLOBAL void uf_union_kernel(const float* __restrict__ d, int w, int h, float max_diff, int* parent) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= w || y >= h) return;
-  const int i = y * w + x;
-  const float v = d[i];
-  if (!r3dsimt::finitef(v)) return;
-  if (x + 1 < w) {
-    const float u = d[i + 1];
-    if (fabsf(__fsub_rn(u, v)) <= max_diff) uf_unite(parent, i, i + 1);
-  }
-  if (y + 1 < h) {
-    const float u = d[i + w];
-    if (fabsf(__fsub_rn(u, v)) <= max_diff) uf_unite(parent, i, i + w);
-  }
-}
-
+// Segment sizes: the lanes of a warp whose pixels share a root add their
+// count with one atomic; every pixel's parent becomes its root.
 R3D_GLOBAL void uf_count_kernel(const float* __restrict__ d, int64_t n, int* parent, int* size) {
   const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n || !r3dsimt::finitef(d[i])) return;
-  const int r = uf_root(parent, static_cast<int>(i));
-  atomicAdd(size + r, 1);
+  const bool ok = i < n && r3dsimt::finitef(d[i]);
+  const int r = ok ? uf_root(parent, static_cast<int>(i)) : -1;
+  const uint32_t peers = r3dsimt::match_any(static_cast<uint32_t>(r));
+  if (ok) {
+    parent[i] = r;
+    if (static_cast<int>(r3dsimt::lane_id()) == r3dsimt::ffs(peers) - 1)
+      atomicAdd(size + r, r3dsimt::popc64(peers));
+  }
 }
 
 R3D_GLOBAL void uf_filter_kernel(float* __restrict__ d, int64_t n, const int* parent, const int* size, int min_size) {
@@ -548,12 +620,15 @@ void launch_remove_speckles(float* d, int w, int h, int min_size, float max_diff
   const int64_t n = static_cast<int64_t>(w) * h;
   int* parent = scratch;
   int* size = scratch + n;
+  const dim3 tiles(static_cast<unsigned>(ceil_div64(w, kUfTile)), static_cast<unsigned>(ceil_div64(h, kUfTile)));
+  R3D_LAUNCH(uf_tile_kernel, tiles, 256, 2 * sizeof(int) * kUfTile * kUfTile, s, d, w, h, max_diff, parent, size);
+  launched("uf_tile_kernel");
+  const int64_t nb = static_cast<int64_t>((w - 1) / kUfTile) * h + static_cast<int64_t>((h - 1) / kUfTile) * w;
+  if (nb > 0) {
+    R3D_LAUNCH(uf_border_kernel, static_cast<unsigned>(ceil_div64(nb, 256)), 256, 0, s, d, w, h, max_diff, parent);
+    launched("uf_border_kernel");
+  }
   const unsigned g1 = static_cast<unsigned>(ceil_div64(n, 256));
-  R3D_LAUNCH(uf_init_kernel, g1, 256, 0, s, parent, size, n);
-  launched("uf_init_kernel");
-  const dim3 b(32, 8);
-  R3D_LAUNCH(uf_union_kernel, grid2d(w, h, b), b, 0, s, d, w, h, max_diff, parent);
-  launched("uf_union_kernel");
   R3D_LAUNCH(uf_count_kernel, g1, 256, 0, s, d, n, parent, size);
   launched("uf_count_kernel");
   R3D_LAUNCH(uf_filter_kernel, g1, 256, 0, s, d, n, parent, size, min_size);

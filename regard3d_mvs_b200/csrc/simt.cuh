@@ -36,6 +36,7 @@ R3D_DEVICE uint32_t lane_id() { return threadIdx.x & 31u; }
 R3D_DEVICE uint32_t shfl(uint32_t v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 R3D_DEVICE uint32_t shfl_xor(uint32_t v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
 R3D_DEVICE uint32_t ballot(bool p) { return __ballot_sync(0xffffffffu, p); }
+R3D_DEVICE uint32_t match_any(uint32_t v) { return __match_any_sync(0xffffffffu, v); }  // lanes holding v
 R3D_DEVICE int ffs(uint32_t v) { return __ffs(static_cast<int>(v)); }  // 1 + index of the lowest set bit, 0 if none
 R3D_DEVICE void syncwarp() { __syncwarp(); }
 R3D_DEVICE void syncthreads() { __syncthreads(); }
@@ -125,6 +126,7 @@ uint32_t lane_id();
 uint32_t shfl(uint32_t v, int src);
 uint32_t shfl_xor(uint32_t v, int m);
 uint32_t ballot(bool p);
+uint32_t match_any(uint32_t v);
 inline int ffs(uint32_t v) { return __builtin_ffs(static_cast<int>(v)); }
 void syncwarp();
 void syncthreads();

@@ -1,0 +1,138 @@
+"""Geometry of the multi-view combination (r3dgpu_combine_pairs) as ctypes
+structs.
+
+A grid is a dict with the grid camera's ``K`` (3x3), ``R`` (world -> camera
+rotation), ``C`` (centre), ``width`` and ``height``. A pair is a dict with its
+rectified left camera (``K_rect``, ``R_rect``), ``baseline``, the right
+camera's principal point ``cx_right``, the partner's ``centre`` and the
+pair's ``disparity`` (and optional ``confidence``) maps in the rectified left
+image: the quantities src/r3d/mvs/multi_stereo.cpp:85-93 derives per pair.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from .types import CDepthGrid, CPairGeometry
+
+
+def c_grid(grid: dict) -> CDepthGrid:
+    g = CDepthGrid()
+    k_inv = np.linalg.inv(np.asarray(grid["K"], np.float64))
+    rot_t = np.asarray(grid["R"], np.float64).T
+    g.k_inv[:] = [float(v) for v in k_inv.ravel()]
+    g.rot_t[:] = [float(v) for v in rot_t.ravel()]
+    g.center[:] = [float(v) for v in np.asarray(grid["C"], np.float64)]
+    g.width, g.height = int(grid["width"]), int(grid["height"])
+    return g
+
+
+def c_pairs(grid: dict, pairs: list[dict]):
+    """(array of CPairGeometry with host map pointers, the arrays they point into)."""
+    arr = (CPairGeometry * max(len(pairs), 1))()
+    keep = []
+    k_inv = np.linalg.inv(np.asarray(grid["K"], np.float64))
+    r_gt = np.asarray(grid["R"], np.float64).T
+    for i, p in enumerate(pairs):
+        kr = np.asarray(p["K_rect"], np.float64)
+        h = kr @ np.asarray(p["R_rect"], np.float64) @ r_gt @ k_inv
+        d = np.ascontiguousarray(p["disparity"], np.float32)
+        c = p.get("confidence")
+        c = None if c is None else np.ascontiguousarray(c, np.float32)
+        keep += [d, c]
+        q = arr[i]
+        q.grid_to_rect[:] = [float(v) for v in h.ravel()]
+        q.fb = float(kr[0, 0] * p["baseline"])
+        q.offset = float(kr[0, 2] - p["cx_right"])
+        q.partner_center[:] = [float(v) for v in np.asarray(p["centre"], np.float64)]
+        q.disparity = d.ctypes.data
+        q.confidence = None if c is None else c.ctypes.data
+        q.height, q.width = d.shape
+        q.stride = d.shape[1]
+    return arr, keep
+
+
+# ---------------------------------------------------------------- synthetic views
+# A base camera, partner cameras, their rectified pairs (x axis along the
+# baseline, optical axis the mean of the two cameras' axes, as
+# src/r3d/rectify/rectification.hpp:14-20 describes) and the disparity maps of
+# a plane, d = f b / z + (cx_l - cx_r): inputs for tests and benchmarks.
+
+
+def rot_y(a):
+    c, s = np.cos(a), np.sin(a)
+    return np.array([[c, 0, -s], [0, 1, 0], [s, 0, c]], np.float64)
+
+
+def rot_x(a):
+    c, s = np.cos(a), np.sin(a)
+    return np.array([[1, 0, 0], [0, c, s], [0, -s, c]], np.float64)
+
+
+class Rig:
+    """Base camera at the origin looking along +z (world -> camera rotation
+    R), partners around it looking at the scene centre."""
+
+    def __init__(self, w=160, h=120, f=150.0, partners=((0.6, 0.0, 0.0), (-0.5, 0.3, 0.1), (0.2, -0.55, 0.0))):
+        self.w, self.h, self.f = w, h, f
+        self.K = np.array([[f, 0, (w - 1) / 2.0], [0, f, (h - 1) / 2.0], [0, 0, 1]], np.float64)
+        self.R = rot_x(0.02) @ rot_y(-0.03)
+        self.C = np.zeros(3)
+        self.partners = [(rot_y(-0.06 * np.sign(p[0] + 1e-9)) @ self.R, np.array(p, np.float64)) for p in partners]
+
+    def grid(self):
+        return {"K": self.K, "R": self.R, "C": self.C, "width": self.w, "height": self.h}
+
+    def rectify(self, partner, cx_shift=12.0):
+        """Rectified pair of the base camera and `partner` (R_p, C_p)."""
+        Rp, Cp = partner
+        b = Cp - self.C
+        x = b / np.linalg.norm(b)
+        z_mean = self.R[2] + Rp[2]
+        z_mean /= np.linalg.norm(z_mean)
+        y = np.cross(z_mean, x)
+        y /= np.linalg.norm(y)
+        z = np.cross(x, y)
+        R_rect = np.stack([x, y, z])
+        cx_l, cy = (self.w - 1) / 2.0 + 3.0, (self.h - 1) / 2.0 - 2.0
+        K_rect = np.array([[self.f, 0, cx_l], [0, self.f, cy], [0, 0, 1]], np.float64)
+        return {"K_rect": K_rect, "R_rect": R_rect, "baseline": float(np.linalg.norm(b)), "cx_right": cx_l - cx_shift,
+                "centre": Cp}
+
+
+class Plane:
+    """Points X with n . X = dist."""
+
+    def __init__(self, normal=(0.15, -0.1, -1.0), point=(0.0, 0.0, 6.0)):
+        n = np.asarray(normal, np.float64)
+        self.n = n / np.linalg.norm(n)
+        self.dist = float(self.n @ np.asarray(point, np.float64))
+
+    def depth_along(self, origin, direction):
+        """t with origin + t * direction on the plane."""
+        return (self.dist - self.n @ origin) / (direction @ self.n)
+
+
+def plane_disparity(rig: Rig, pair: dict, plane: Plane, shift: float = 0.0) -> np.ndarray:
+    """Disparity of the plane in the rectified left image (rig-sized)."""
+    K_inv = np.linalg.inv(pair["K_rect"])
+    ys, xs = np.mgrid[0:rig.h, 0:rig.w].astype(np.float64)
+    pix = np.stack([xs, ys, np.ones_like(xs)], -1)
+    dirs = pix @ (pair["R_rect"].T @ K_inv).T  # world directions with unit rectified depth
+    t = (plane.dist - plane.n @ rig.C) / (dirs @ plane.n)
+    fb = pair["K_rect"][0, 0] * pair["baseline"]
+    offset = pair["K_rect"][0, 2] - pair["cx_right"]
+    d = fb / t + offset + shift
+    d[~(t > 0)] = np.inf
+    return d.astype(np.float32)
+
+
+def grid_plane_depth(rig: Rig, plane: Plane) -> np.ndarray:
+    """Depth along the grid camera's optical axis of the plane at every grid pixel."""
+    K_inv = np.linalg.inv(rig.K)
+    ys, xs = np.mgrid[0:rig.h, 0:rig.w].astype(np.float64)
+    pix = np.stack([xs, ys, np.ones_like(xs)], -1)
+    dirs = pix @ (rig.R.T @ K_inv).T
+    return (plane.dist - plane.n @ rig.C) / (dirs @ plane.n)

@@ -91,6 +91,25 @@ class Matcher:
                                                       ctypes.byref(out)))
         return DisparityMap(disp, conf, out.disparity_min, out.num_disparities, out.levels, int(out.cells))
 
+    # ---------------------------------------------------------------- r3d::combine_pairs
+    def combine_pairs(self, grid: dict, pairs: list[dict], options=None):
+        """Depth map of the grid camera from matched pairs that share its
+        centre (see regard3d_mvs_b200.multi_view for the dicts)."""
+        from .multi_view import c_grid, c_pairs
+        from .types import DepthMap, MultiStereoOptions
+
+        g = c_grid(grid)
+        arr, keep = c_pairs(grid, pairs)
+        o = (options or MultiStereoOptions()).c()
+        depth = np.empty((g.height, g.width), np.float32)
+        conf = np.empty_like(depth)
+        mask = np.empty((g.height, g.width), np.uint16)
+        self._check(self.lib.r3dgpu_combine_pairs_host(ctypes.byref(g), arr, len(pairs), ctypes.byref(o),
+                                                       depth.ctypes.data, conf.ctypes.data, mask.ctypes.data,
+                                                       g.width))
+        del keep
+        return DepthMap(depth, conf, mask)
+
     # ---------------------------------------------------------------- batched matching
     def match_stereo_batch(self, pairs: Sequence[dict], stream: int | None = None) -> list[DisparityMap]:
         """Matches many pairs in one pass of every stage.

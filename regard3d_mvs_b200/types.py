@@ -133,6 +133,62 @@ class CPair(ctypes.Structure):
     ]
 
 
+class CDepthGrid(ctypes.Structure):
+    _fields_ = [
+        ("k_inv", ctypes.c_double * 9),
+        ("rot_t", ctypes.c_double * 9),
+        ("center", ctypes.c_double * 3),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+    ]
+
+
+class CPairGeometry(ctypes.Structure):
+    _fields_ = [
+        ("grid_to_rect", ctypes.c_double * 9),
+        ("fb", ctypes.c_double),
+        ("offset", ctypes.c_double),
+        ("partner_center", ctypes.c_double * 3),
+        ("disparity", ctypes.c_void_p),
+        ("confidence", ctypes.c_void_p),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("stride", ctypes.c_int64),
+    ]
+
+
+class CMultiStereoOptions(ctypes.Structure):
+    _fields_ = [
+        ("inlier_px", ctypes.c_double),
+        ("max_reprojection_px", ctypes.c_double),
+        ("min_angle_deg", ctypes.c_double),
+        ("min_pairs", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+@dataclass
+class MultiStereoOptions:
+    """MultiStereoOptions, src/r3d/mvs/multi_stereo.hpp:25-30."""
+
+    inlier_px: float = 2.0
+    max_reprojection_px: float = 1.0
+    min_angle_deg: float = 3.0
+    min_pairs: int = 1
+
+    def c(self) -> CMultiStereoOptions:
+        return CMultiStereoOptions(self.inlier_px, self.max_reprojection_px, self.min_angle_deg, self.min_pairs, 0)
+
+
+@dataclass
+class DepthMap:
+    """DepthMap (src/r3d/mvs/depth_map.hpp:17-31): depth 0 = none, pair_mask bit i = pair i used."""
+
+    depth: np.ndarray
+    confidence: np.ndarray
+    pair_mask: np.ndarray
+
+
 class CServerConfig(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32),

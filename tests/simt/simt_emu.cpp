@@ -147,6 +147,17 @@ uint32_t shfl(uint32_t v, int src) {
 
 uint32_t shfl_xor(uint32_t v, int m) { return shfl(v, static_cast<int>(lane_id() ^ static_cast<uint32_t>(m))); }
 
+uint32_t match_any(uint32_t v) {
+  WarpState& ws = (*t_warps)[warp_of(t_cur)];
+  ws.buf[lane_id()] = v;
+  warp_barrier();
+  uint32_t r = 0;
+  for (int i = 0; i < 32; ++i)
+    if (ws.buf[i] == v) r |= 1u << i;
+  warp_barrier();
+  return r;
+}
+
 uint32_t ballot(bool p) {
   WarpState& ws = (*t_warps)[warp_of(t_cur)];
   ws.buf[lane_id()] = p ? 1u : 0u;

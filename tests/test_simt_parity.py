@@ -183,3 +183,20 @@ def test_ranged_kernel_wide_pixels_wta(simt_matcher, oracle, monkeypatch, opts):
     left, right, _ = render_pair(tex, 60, 34, lambda x, y: np.where(y < 15, 9.0 + 0.1 * x, 21.0))
     _same_map(simt_matcher.match_stereo(left, right, None, None, 0, 48, opts),
               oracle.match_stereo(left, right, None, None, 0, 48, opts))
+
+
+def test_speckles_across_union_tiles(simt_matcher, oracle):
+    """Segments spanning many 32 x 32 union tiles (smooth ramps, a large
+    plateau, thin diagonal strips and noise) against the reference BFS."""
+    rng = np.random.default_rng(8)
+    h, w = 97, 131
+    yy, xx = np.mgrid[0:h, 0:w]
+    d = (0.01 * xx + 0.02 * yy).astype(np.float32)                 # one segment crossing every tile
+    d[20:70, 40:100] = 30.0                                       # plateau over tile borders
+    d[(xx + yy) % 17 == 0] = 50.0                                 # diagonal strips (cut at tile corners)
+    noise = rng.random((h, w)) < 0.05
+    d[noise] = np.round(rng.normal(10, 5, noise.sum())).astype(np.float32)
+    d[rng.random((h, w)) < 0.03] = np.inf
+    for size, diff in ((5, 0.5), (40, 1.0), (400, 1.0), (3000, 0.2)):
+        assert same_disparities(simt_matcher.remove_speckles(d.copy(), size, diff),
+                                oracle.remove_speckles(d, size, diff)), (size, diff)
