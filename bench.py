@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640"), default="batch64")
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine"), default="batch64",
+                    help="combine: only the multi-view combination of one view (its own JSON line)")
     ap.add_argument("--pairs", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-per-pair", action="store_true")
@@ -430,6 +431,14 @@ def main():
 
     m = Matcher(device=local)
     lib = m.lib
+    if args.workload == "combine":
+        peak, _ = measured_peaks()
+        dev0 = torch.device(f"cuda:{local}")
+        r = measure_combine(lib, dev0, torch.cuda.current_stream(dev0), args.steps, args.warmup, peak)
+        if rank == 0:
+            print(json.dumps(dict(r, metric="combine_pairs Gpixels/s", n_gpus=world, steps=args.steps,
+                                  warmup=args.warmup, higher_is_better=True, data="synthetic")), flush=True)
+        return
     specs = workload_pairs(args.workload, args.pairs, args.seed + 7919 * rank)
     host = [make_images(lib, s) for s in specs]
     dev = torch.device(f"cuda:{local}")
