@@ -355,6 +355,10 @@ def run_serving(args, sat_pairs_per_s: float) -> dict:
     points = []
     free0, total = torch.cuda.mem_get_info(0)
     peak_used = total - free0
+    # Enough page-locked output maps for the deepest queue, allocated before
+    # the arrivals start (page-locking during the sweep would slow it).
+    for i in range(len(specs)):
+        pool[i] += [take(i) for _ in range(3)]
     with Server(device=0, workers=SERVE_WORKERS, max_batch=16, hbm_budget=SERVE_REQUEST_BUDGET,
                 scratch_budget=16 << 30) as srv:
         # Warm-up: every worker compiles nothing, but allocates its buffers.
@@ -592,6 +596,8 @@ def main():
                          "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "avg_stage_ms": sgm_ms, "stages": rounds,
                          "launches": int(prof.sgm_launches), "alg_bytes_per_stage": alg_bytes,
+                         "stage_ms_of_first_step": [round(e["ms"], 2) for e in launch_log
+                                                    if e["kernel"] == "sgm_round"][:rounds // max(args.steps, 1)],
                          "sgm_share_of_step": prof.sgm_ms / max(ms, 1e-9)},
             "int_roofline": {"ops_per_cell": INT_OPS_PER_CELL, "achieved_tops": int_achieved,
                              "nominal_int32_tops": int_peak, "frac": int_achieved / int_peak},
