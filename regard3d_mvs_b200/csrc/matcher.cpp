@@ -723,49 +723,15 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
   }
   for (auto& P : runs) build_levels(P, A, s);
 
-  // A pair runs its levels (coarsest first) in consecutive rounds starting
-  // at round start[i]. Pairs are independent, so the starts only balance the
-  // rounds: largest pairs first, each where the busiest of its rounds stays
-  // least loaded (estimated aggregated cells: the full range at a pair's
-  // coarsest level, about 32 labels per pixel on the ranged levels).
-  std::vector<int> start(count, 0);
-  {
-    auto level_cells = [&](const PairRun& P, int l) {
-      const double px = static_cast<double>(std::max(1, pairs[&P - runs.data()].left.width >> l)) *
-                        std::max(1, pairs[&P - runs.data()].left.height >> l);
-      const double labels = l == P.levels ? std::max(16, align16(pairs[&P - runs.data()].num_disparities) >> l) : 32;
-      return px * labels * (P.lr_full ? 2.0 : 1.0);
-    };
-    std::vector<double> total(count, 0.0);
-    for (int i = 0; i < count; ++i)
-      for (int l = 0; l <= runs[i].levels; ++l) total[i] += level_cells(runs[i], l);
-    std::vector<int> order(count);
-    for (int i = 0; i < count; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return total[a] > total[b]; });
-    std::vector<double> load(max_levels + 1, 0.0);
-    for (int i : order) {
-      const PairRun& P = runs[i];
-      int best = 0;
-      double best_peak = 0.0;
-      for (int st = 0; st + P.levels <= max_levels; ++st) {
-        double peak = 0.0;
-        for (int l = P.levels; l >= 0; --l) peak = std::max(peak, load[st + P.levels - l] + level_cells(P, l));
-        if (st == 0 || peak < best_peak) {
-          best = st;
-          best_peak = peak;
-        }
-      }
-      start[i] = best;
-      for (int l = P.levels; l >= 0; --l) load[best + P.levels - l] += level_cells(P, l);
-    }
-  }
-
   for (int round = 0; round <= max_levels; ++round) {
     std::vector<PairRun*> active;
-    for (int i = 0; i < count; ++i) {
-      PairRun& P = runs[i];
-      const int l = P.levels - (round - start[i]);
-      if (round >= start[i] && l >= 0) {
+    // Round r runs level max_levels - r of every pair that has it, so that
+    // all pairs reach level 0 (the largest) in the last round, where their
+    // SGM launches overlap. (Spreading single-level pairs over the earlier
+    // rounds measured slower: every round costs at least its slowest tile.)
+    for (auto& P : runs) {
+      const int l = max_levels - round;
+      if (l <= P.levels) {
         P.cur = l;
         active.push_back(&P);
       }
