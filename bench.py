@@ -60,8 +60,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine"), default="batch64",
-                    help="combine: only the multi-view combination of one view (its own JSON line)")
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine", "rectify"), default="batch64",
+                    help="combine / rectify: only the multi-view combination of one view / the rectification "
+                         "resampling of one pair (each its own JSON line)")
     ap.add_argument("--pairs", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-per-pair", action="store_true")
@@ -321,6 +322,120 @@ def measure_combine(lib, dev, stream, steps: int, warmup: int, peak: float) -> d
                              "kind": "port", "sample": "the same view, once"}}
 
 
+# Rectification resampling (r3dgpu_rectify_image_u16) of both images of a
+# pair: 6000 x 4000 u16 photos with brown_t2 distortion into rectified
+# cameras of the same focal length (pyramid level 0), 6120 x 4080 targets.
+# Algorithmic bytes per launch: the source read once (2 B per source pixel),
+# the target image and validity mask written (2 + 1 B per target pixel).
+RECT_W, RECT_H = 6000, 4000
+RECT_TW, RECT_TH = 6120, 4080
+RECT_BYTES_PER_LAUNCH = 2 * RECT_W * RECT_H + 3 * RECT_TW * RECT_TH
+L2_FLUSH_BYTES = 256 << 20
+
+
+def rectify_setup():
+    """Cameras, rotations and source images of the rectified pair."""
+    from regard3d_mvs_b200.multi_view import rot_x, rot_y
+
+    cams, rots, srcs = [], [], []
+    rng = np.random.default_rng(5)
+    for i, (ry, rx) in enumerate(((0.04, -0.015), (-0.035, 0.01))):
+        cams.append({"model": 3, "width": RECT_W, "height": RECT_H, "fx": 5200.0, "fy": 5203.0,
+                     "cx": (RECT_W - 1) / 2 + 11 - 4 * i, "cy": (RECT_H - 1) / 2 - 6,
+                     "params": (-0.09, 0.03, -0.004, 0.0008, -0.0011)})
+        rots.append((rot_y(ry) @ rot_x(rx)) @ rot_x(0.012).T)
+        y, x = np.mgrid[0:RECT_H, 0:RECT_W]
+        img = 32768 + 12000 * np.sin(x / 23.0 + i) * np.cos(y / 17.0) + rng.normal(0, 3000, (RECT_H, RECT_W))
+        srcs.append(np.clip(img, 0, 65535).astype(np.uint16))
+    target = {"width": RECT_TW, "height": RECT_TH, "fx": 5200.0, "fy": 5200.0, "cx": (RECT_TW - 1) / 2,
+              "cy": (RECT_TH - 1) / 2 + 2}
+    return cams, rots, srcs, target
+
+
+def measure_rectify(lib, dev, stream, steps: int, warmup: int, peak: float) -> dict:
+    """Device time of rectify_image on both images of a pair (L2 flushed
+    before each launch), end-to-end time through the host entry point, and
+    the oracle on the host's cores on one image."""
+    import torch
+
+    from oracle import oracle as orc
+    from regard3d_mvs_b200.types import CViewU16, camera_struct, pinhole_struct
+
+    cams, rots, srcs, target = rectify_setup()
+    k = pinhole_struct(target)
+    cs = [camera_struct(c) for c in cams]
+    ms_ = [np.ascontiguousarray(r).reshape(9) for r in rots]
+    dsrc = [torch.from_numpy(a.view(np.int16)).to(dev) for a in srcs]
+    views = [CViewU16(d.data_ptr(), RECT_W, RECT_H, RECT_W) for d in dsrc]
+    dout = [torch.empty((RECT_TH, RECT_TW), dtype=torch.int16, device=dev) for _ in srcs]
+    dval = [torch.empty((RECT_TH, RECT_TW), dtype=torch.uint8, device=dev) for _ in srcs]
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def run(i):
+        _native_check(lib, lib.r3dgpu_rectify_image_u16(ctypes.byref(views[i]), ctypes.byref(cs[i]),
+                                                        ms_[i].ctypes.data, ctypes.byref(k), dout[i].data_ptr(),
+                                                        RECT_TW, dval[i].data_ptr(), RECT_TW, sptr))
+
+    for _ in range(warmup):
+        run(0)
+        run(1)
+    torch.cuda.synchronize(dev)
+    total_ms = 0.0
+    launches0 = int(lib.r3dgpu_launch_count())
+    for _ in range(steps):
+        for i in range(2):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            run(i)
+            b.record(stream)
+            torch.cuda.synchronize(dev)
+            total_ms += a.elapsed_time(b)
+    launches = int(lib.r3dgpu_launch_count()) - launches0
+    ms = total_ms / (2 * steps)  # per launch
+    px = RECT_TW * RECT_TH
+    achieved = RECT_BYTES_PER_LAUNCH / (ms * 1e-3) / 1e9
+
+    # End to end through the host entry point: pinned host source in, image
+    # and mask out, every step.
+    hsrc = [torch.from_numpy(a.view(np.int16)).pin_memory() for a in srcs]
+    hout = [torch.empty((RECT_TH, RECT_TW), dtype=torch.int16).pin_memory() for _ in srcs]
+    hval = [torch.empty((RECT_TH, RECT_TW), dtype=torch.uint8).pin_memory() for _ in srcs]
+    hviews = [CViewU16(h.data_ptr(), RECT_W, RECT_H, RECT_W) for h in hsrc]
+
+    def run_host(i):
+        _native_check(lib, lib.r3dgpu_rectify_image_u16_host(ctypes.byref(hviews[i]), ctypes.byref(cs[i]),
+                                                             ms_[i].ctypes.data, ctypes.byref(k), hout[i].data_ptr(),
+                                                             RECT_TW, hval[i].data_ptr(), RECT_TW))
+
+    for _ in range(max(1, warmup)):
+        run_host(0)
+        run_host(1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run_host(0)
+        run_host(1)
+    e2e_s = (time.perf_counter() - t0) / (2 * steps)
+
+    got = [dout[i].cpu().numpy().view(np.uint16) for i in range(2)]
+    t0 = time.perf_counter()
+    ref, ref_valid = orc.rectify_image(srcs[0], cams[0], rots[0], target)
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ref, got[0]) and np.array_equal(ref_valid, dval[0].cpu().numpy())
+                and np.array_equal(hout[1].numpy().view(np.uint16), got[1]))
+    return {"workload": f"rectify_image u16, brown_t2 {RECT_W}x{RECT_H} -> {RECT_TW}x{RECT_TH}, level 0, "
+                        "both images of a pair",
+            "value": px / (ms * 1e-3) / 1e9, "unit": "Gpixels/s", "ms_per_launch": ms, "gpu_launches": launches,
+            "bit_exact_vs_oracle": same, "l2": f"flushed before each launch ({L2_FLUSH_BYTES >> 20} MiB write)",
+            "e2e": {"value": px / e2e_s / 1e9, "unit": "Gpixels/s", "h2d_bytes_per_step": 2 * 2 * RECT_W * RECT_H,
+                    "d2h_bytes_per_step": 2 * 3 * px},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "alg_bytes_per_launch": RECT_BYTES_PER_LAUNCH},
+            "cpu_baseline": {"value": px / cpu_s / 1e9, "unit": "Gpixels/s", "cores": orc.max_threads(),
+                             "kind": "port", "sample": "one image of the pair, once"}}
+
+
 SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
 SERVE_REQUEST_BUDGET = 118 << 30  # config 3's 150 GB: 118 GB for admitted requests + 2 x 16 GB worker scratch
 SERVE_WORKERS = 2
@@ -441,6 +556,14 @@ def main():
         r = measure_combine(lib, dev0, torch.cuda.current_stream(dev0), args.steps, args.warmup, peak)
         if rank == 0:
             print(json.dumps(dict(r, metric="combine_pairs Gpixels/s", n_gpus=world, steps=args.steps,
+                                  warmup=args.warmup, higher_is_better=True, data="synthetic")), flush=True)
+        return
+    if args.workload == "rectify":
+        peak, _ = measured_peaks()
+        dev0 = torch.device(f"cuda:{local}")
+        r = measure_rectify(lib, dev0, torch.cuda.current_stream(dev0), args.steps, args.warmup, peak)
+        if rank == 0:
+            print(json.dumps(dict(r, metric="rectify_image Gpixels/s", n_gpus=world, steps=args.steps,
                                   warmup=args.warmup, higher_is_better=True, data="synthetic")), flush=True)
         return
     specs = workload_pairs(args.workload, args.pairs, args.seed + 7919 * rank)
@@ -622,6 +745,7 @@ def main():
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(specs)
             line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
+            line["rectify"] = measure_rectify(lib, dev, stream, args.steps, args.warmup, peak)
         if args.serve and world == 1:
             # In a fresh process, with this one's device memory given back.
             del dL, dR, dD, dC

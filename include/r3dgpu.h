@@ -201,6 +201,50 @@ r3dgpu_status r3dgpu_remove_speckles_no_alloc(float* disparity, int32_t width, i
  * Replaces r3d::median_filter_3x3, src/r3d/stereo/stereo_matcher.hpp:91. */
 r3dgpu_status r3dgpu_median_filter_3x3_host(const float* disparity, int32_t width, int32_t height, float* out);
 
+/* ------------------------------------------------------------------ rectification
+ * Resampling of a source image into a rectified (or any rotated pinhole)
+ * camera with the same centre: Catmull-Rom bicubic sampling of the source
+ * (of a pyramid level of it when the target has less than 1/1.5 of its
+ * resolution), pixels without a source 0, an optional validity mask (255 /
+ * 0). Replaces r3d::rectify_image, src/r3d/rectify/rectification.hpp:75-88
+ * (implementation src/r3d/rectify/rectification.cpp:287-350), for single
+ * channel u16 and f32 images. */
+
+/* CameraIntrinsics, src/r3d/core/camera_model.hpp:32-41; model: 0 pinhole,
+ * 1 radial_k1, 2 radial_k3, 3 brown_t2, 4 fisheye (params as there). */
+typedef struct r3dgpu_camera {
+  int32_t model;
+  int32_t width;
+  int32_t height;
+  int32_t reserved;
+  double fx, fy, cx, cy;
+  double params[5];
+} r3dgpu_camera;
+
+/* PinholeIntrinsics of the target camera. */
+typedef struct r3dgpu_pinhole {
+  int32_t width;
+  int32_t height;
+  double fx, fy, cx, cy;
+} r3dgpu_pinhole;
+
+/* source_from_target: R_source R_target^T (row-major), the rotation that
+ * takes target camera rays to source camera rays. Device images; `valid` may
+ * be NULL; runs on `stream` and synchronises it. */
+r3dgpu_status r3dgpu_rectify_image_u16(const r3dgpu_view_u16* src, const r3dgpu_camera* cam,
+                                       const double* source_from_target, const r3dgpu_pinhole* target, uint16_t* out,
+                                       int64_t out_stride, uint8_t* valid, int64_t valid_stride, void* stream);
+r3dgpu_status r3dgpu_rectify_image_f32(const float* src, int64_t src_stride, const r3dgpu_camera* cam,
+                                       const double* source_from_target, const r3dgpu_pinhole* target, float* out,
+                                       int64_t out_stride, uint8_t* valid, int64_t valid_stride, void* stream);
+/* Same with host images (copies inside). */
+r3dgpu_status r3dgpu_rectify_image_u16_host(const r3dgpu_view_u16* src, const r3dgpu_camera* cam,
+                                            const double* source_from_target, const r3dgpu_pinhole* target,
+                                            uint16_t* out, int64_t out_stride, uint8_t* valid, int64_t valid_stride);
+r3dgpu_status r3dgpu_rectify_image_f32_host(const float* src, int64_t src_stride, const r3dgpu_camera* cam,
+                                            const double* source_from_target, const r3dgpu_pinhole* target,
+                                            float* out, int64_t out_stride, uint8_t* valid, int64_t valid_stride);
+
 /* ------------------------------------------------------------------ multi-view
  * Combination of up to 16 matched pairs that share a base camera into one
  * depth map (the consumer of the matcher in the multi-view stage).

@@ -50,6 +50,8 @@ def lib():
         L.orc_match_tiles.argtypes = [P, i32, i32, P, i32, P, P, i32, i32, P, P, P, i32, P, P, P]
         L.orc_combine_pairs.argtypes = [P, P, i32, P, P, P, P, ctypes.c_int64]
         L.orc_sample_disparity.argtypes = [P, i32, i32, P, P, i32, P]
+        L.orc_rectify_image.argtypes = [i32, P, P, P, P, P, P]
+        L.orc_distort_pixel.argtypes = [P, P, i32, P]
         _lib = L
     return _lib
 
@@ -175,6 +177,36 @@ def sample_disparity(disp: np.ndarray, u, v) -> np.ndarray:
     out = np.empty(u.shape, np.float32)
     _check(lib().orc_sample_disparity(_ptr(d), d.shape[1], d.shape[0], _ptr(u), _ptr(v), u.size, _ptr(out)))
     return out
+
+
+def distort_pixel(camera: dict, pixels) -> np.ndarray:
+    """CameraIntrinsics::distort_pixel (src/r3d/core/camera_model.cpp:142-146)
+    of an (n, 2) array of pixels."""
+    from regard3d_mvs_b200.types import camera_struct
+
+    cam = camera_struct(camera)
+    p = np.ascontiguousarray(np.reshape(pixels, (-1, 2)), np.float64)
+    out = np.empty_like(p)
+    _check(lib().orc_distort_pixel(ctypes.byref(cam), _ptr(p), len(p), _ptr(out)))
+    return out
+
+
+def rectify_image(src: np.ndarray, camera: dict, source_from_target, target: dict):
+    """r3d::rectify_image (src/r3d/rectify/rectification.cpp:287-350) on the
+    CPU for a one-channel u16 or f32 image; returns (image, valid)."""
+    from regard3d_mvs_b200.types import camera_struct, pinhole_struct
+
+    cam, k = camera_struct(camera), pinhole_struct(target)
+    is_float = src.dtype == np.float32
+    img = _c(src, np.float32 if is_float else np.uint16)
+    if img.shape != (cam.height, cam.width):
+        raise OracleError(f"rectify_image: image is {img.shape}, camera is {cam.height}x{cam.width}")
+    m = np.ascontiguousarray(source_from_target, dtype=np.float64).reshape(9)
+    out = np.empty((k.height, k.width), np.float32 if is_float else np.uint16)
+    valid = np.empty((k.height, k.width), np.uint8)
+    _check(lib().orc_rectify_image(int(is_float), _ptr(img), ctypes.byref(cam), _ptr(m), ctypes.byref(k), _ptr(out),
+                                   _ptr(valid)))
+    return out, valid
 
 
 def median_filter_3x3(disp: np.ndarray) -> np.ndarray:

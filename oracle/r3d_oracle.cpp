@@ -31,6 +31,7 @@
 #include <limits>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -1095,6 +1096,136 @@ void combine_pairs(const r3dgpu_depth_grid& grid, const r3dgpu_pair_geometry* ge
   }
 }
 
+// ---------------------------------------------------------------- rectification
+// rectify_image (src/r3d/rectify/rectification.cpp:287-350) for one-channel
+// u16 and f32 images: pyramid level for anti-aliasing, target ray rotated
+// into the source camera, projection through the camera model
+// (src/r3d/core/camera_model.cpp:67-100, 148-151), Catmull-Rom bicubic
+// sampling with clamped taps (src/r3d/core/sampling.hpp:15-55).
+
+// pyramid.cpp:33-83 with float accumulators: sums of the horizontal pass kept
+// per row, then the vertical pass, times 1/256.
+Img<float> pyramid_down_f32(const Img<float>& s) {
+  const int w = s.w, h = s.h, dw = (w + 1) / 2, dh = (h + 1) / 2;
+  Img<float> tmp(dw, h);
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < dw; ++x) {
+      const int c = 2 * x;
+      auto v = [&](int xx) { return s(std::clamp(xx, 0, w - 1), y); };
+      tmp(x, y) = v(c - 2) + v(c + 2) + 4.0F * (v(c - 1) + v(c + 1)) + 6.0F * v(c);
+    }
+  Img<float> out(dw, dh);
+  for (int y = 0; y < dh; ++y) {
+    const int c = 2 * y;
+    for (int x = 0; x < dw; ++x) {
+      auto v = [&](int yy) { return tmp(x, std::clamp(yy, 0, h - 1)); };
+      out(x, y) = (v(c - 2) + v(c + 2) + 4.0F * (v(c - 1) + v(c + 1)) + 6.0F * v(c)) * (1.0F / 256.0F);
+    }
+  }
+  return out;
+}
+
+Img<uint16_t> level_down(const Img<uint16_t>& s) { return pyramid_down(s); }
+Img<float> level_down(const Img<float>& s) { return pyramid_down_f32(s); }
+
+// camera_model.cpp:67-100.
+void distort(const r3dgpu_camera& c, double ux, double uy, double& dx, double& dy) {
+  const double r2 = ux * ux + uy * uy;
+  const double* p = c.params;
+  dx = ux;
+  dy = uy;
+  if (c.model == 1) {
+    dx = ux * (1.0 + p[0] * r2);
+    dy = uy * (1.0 + p[0] * r2);
+  } else if (c.model == 2) {
+    const double f = 1.0 + r2 * (p[0] + r2 * (p[1] + r2 * p[2]));
+    dx = ux * f;
+    dy = uy * f;
+  } else if (c.model == 3) {
+    const double radial = r2 * (p[0] + r2 * (p[1] + r2 * p[2]));
+    dx = ux + ux * radial + (p[4] * (r2 + 2.0 * ux * ux) + 2.0 * p[3] * ux * uy);
+    dy = uy + uy * radial + (p[3] * (r2 + 2.0 * uy * uy) + 2.0 * p[4] * ux * uy);
+  } else if (c.model == 4) {
+    const double r = std::sqrt(r2);
+    if (r > 1e-8) {
+      const double th = std::atan(r), th2 = th * th;
+      const double f = th * (1.0 + th2 * (p[0] + th2 * (p[1] + th2 * (p[2] + th2 * p[3])))) / r;
+      dx = ux * f;
+      dy = uy * f;
+    }
+  }
+}
+
+// sampling.hpp:21-26.
+std::array<float, 4> cubic_weights(float t) {
+  const float t2 = t * t, t3 = t2 * t;
+  return {-0.5F * t3 + t2 - 0.5F * t, 1.5F * t3 - 2.5F * t2 + 1.0F, -1.5F * t3 + 2.0F * t2 + 0.5F * t,
+          0.5F * t3 - 0.5F * t2};
+}
+
+// rectification.cpp:140-148.
+template <class T>
+T to_pixel(float v) {
+  if constexpr (std::is_floating_point_v<T>) {
+    return v;
+  } else {
+    return static_cast<T>(std::clamp(std::round(v), 0.0F, 65535.0F));
+  }
+}
+
+template <class T>
+void rectify(const Img<T>& src, const r3dgpu_camera& cam, const double* m, const r3dgpu_pinhole& k, T* out,
+             uint8_t* valid) {
+  if (src.w != cam.width || src.h != cam.height) throw Failure("rectify_image: image and camera sizes differ");
+  int level = 0;
+  while (cam.fx / k.fx > 1.5 * std::ldexp(1.0, level) && (cam.width >> (level + 1)) >= 16 &&
+         (cam.height >> (level + 1)) >= 16)
+    ++level;
+  Img<T> img = src;
+  for (int l = 0; l < level; ++l) img = level_down(img);
+  r3dgpu_camera c = cam;
+  const double scale = std::ldexp(1.0, -level);
+  c.fx *= scale;
+  c.fy *= scale;
+  c.cx *= scale;
+  c.cy *= scale;
+#pragma omp parallel for schedule(static)
+  for (int y = 0; y < k.height; ++y) {
+    const double ry = (y - k.cy) / k.fy;
+    for (int x = 0; x < k.width; ++x) {
+      const double rx = (x - k.cx) / k.fx;
+      double r[3];
+      for (int i = 0; i < 3; ++i) r[i] = m[3 * i] * rx + m[3 * i + 1] * ry + m[3 * i + 2] * 1.0;
+      bool inside = r[2] > 1e-9;
+      double sx = 0.0, sy = 0.0;
+      if (inside) {
+        double dx, dy;
+        distort(c, r[0] / r[2], r[1] / r[2], dx, dy);
+        sx = c.fx * dx + c.cx;
+        sy = c.fy * dy + c.cy;
+        inside = sx >= -0.5 && sy >= -0.5 && sx <= img.w - 0.5 && sy <= img.h - 0.5;
+      }
+      T v{};
+      if (inside) {
+        const double flx = std::floor(sx), fly = std::floor(sy);
+        const auto wx = cubic_weights(static_cast<float>(sx - flx));
+        const auto wy = cubic_weights(static_cast<float>(sy - fly));
+        const int x0 = static_cast<int>(flx) - 1, y0 = static_cast<int>(fly) - 1;
+        float acc_y = 0.0F;
+        for (int j = 0; j < 4; ++j) {
+          const int yy = std::clamp(y0 + j, 0, img.h - 1);
+          float acc = 0.0F;
+          for (int i = 0; i < 4; ++i) acc += wx[i] * static_cast<float>(img(std::clamp(x0 + i, 0, img.w - 1), yy));
+          acc_y += wy[j] * acc;
+        }
+        v = to_pixel<T>(acc_y);
+      }
+      out[static_cast<size_t>(y) * k.width + x] = v;
+      if (valid != nullptr) valid[static_cast<size_t>(y) * k.width + x] = inside ? 255 : 0;
+    }
+  }
+}
+
 }  // namespace orc
 
 extern "C" {
@@ -1239,6 +1370,33 @@ int orc_combine_pairs(const r3dgpu_depth_grid* grid, const r3dgpu_pair_geometry*
                       const r3dgpu_multi_stereo_options* options, float* depth, float* confidence, uint16_t* mask,
                       int64_t stride) {
   return orc::guarded([&] { orc::combine_pairs(*grid, pairs, count, *options, depth, confidence, mask, stride); });
+}
+
+// rectify_image of a contiguous host image (u16, or f32 when is_float) into
+// contiguous host outputs; `valid` may be NULL.
+int orc_rectify_image(int is_float, const void* src, const r3dgpu_camera* cam, const double* m,
+                      const r3dgpu_pinhole* k, void* out, uint8_t* valid) {
+  return orc::guarded([&] {
+    if (is_float)
+      orc::rectify(orc::wrap(static_cast<const float*>(src), cam->width, cam->height), *cam, m, *k,
+                   static_cast<float*>(out), valid);
+    else
+      orc::rectify(orc::wrap(static_cast<const uint16_t*>(src), cam->width, cam->height), *cam, m, *k,
+                   static_cast<uint16_t*>(out), valid);
+  });
+}
+
+// distort_pixel (src/r3d/core/camera_model.cpp:142-146) at n pixels
+// (xy pairs), for the camera-model golden vectors.
+int orc_distort_pixel(const r3dgpu_camera* cam, const double* px, int n, double* out) {
+  return orc::guarded([&] {
+    for (int i = 0; i < n; ++i) {
+      double dx, dy;
+      orc::distort(*cam, (px[2 * i] - cam->cx) / cam->fx, (px[2 * i + 1] - cam->cy) / cam->fy, dx, dy);
+      out[2 * i] = cam->fx * dx + cam->cx;
+      out[2 * i + 1] = cam->fy * dy + cam->cy;
+    }
+  });
 }
 
 // sample_disparity at n positions.

@@ -10,7 +10,7 @@ from __future__ import annotations
 import ctypes
 import os
 
-from .types import (CDepthGrid, CDisparityMap, CMultiStereoOptions, COptions, CPair, CPairGeometry, CProfile,
+from .types import (CCamera, CDepthGrid, CDisparityMap, CMultiStereoOptions, COptions, CPair, CPairGeometry, CPinhole, CProfile,
                     CRequestTimes, CServerConfig, CSynthParams, CViewU8, CViewU16)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -42,6 +42,10 @@ EXPORTS = (
     "r3dgpu_remove_speckles_host",
     "r3dgpu_remove_speckles_no_alloc",
     "r3dgpu_median_filter_3x3_host",
+    "r3dgpu_rectify_image_u16",
+    "r3dgpu_rectify_image_f32",
+    "r3dgpu_rectify_image_u16_host",
+    "r3dgpu_rectify_image_f32_host",
     "r3dgpu_default_multi_stereo_options",
     "r3dgpu_combine_pairs",
     "r3dgpu_combine_pairs_host",
@@ -109,6 +113,14 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_remove_speckles_no_alloc.restype = st
     L.r3dgpu_median_filter_3x3_host.argtypes = [P, i32, i32, P]
     L.r3dgpu_median_filter_3x3_host.restype = st
+    cam, pin, i64 = ctypes.POINTER(CCamera), ctypes.POINTER(CPinhole), ctypes.c_int64
+    L.r3dgpu_rectify_image_u16.argtypes = [ctypes.POINTER(CViewU16), cam, P, pin, P, i64, P, i64, P]
+    L.r3dgpu_rectify_image_f32.argtypes = [P, i64, cam, P, pin, P, i64, P, i64, P]
+    L.r3dgpu_rectify_image_u16_host.argtypes = [ctypes.POINTER(CViewU16), cam, P, pin, P, i64, P, i64]
+    L.r3dgpu_rectify_image_f32_host.argtypes = [P, i64, cam, P, pin, P, i64, P, i64]
+    for name in ("r3dgpu_rectify_image_u16", "r3dgpu_rectify_image_f32", "r3dgpu_rectify_image_u16_host",
+                 "r3dgpu_rectify_image_f32_host"):
+        getattr(L, name).restype = st
     L.r3dgpu_default_multi_stereo_options.argtypes = [ctypes.POINTER(CMultiStereoOptions)]
     L.r3dgpu_default_multi_stereo_options.restype = None
     for name in ("r3dgpu_combine_pairs", "r3dgpu_combine_pairs_host"):

@@ -110,6 +110,38 @@ class Matcher:
         del keep
         return DepthMap(depth, conf, mask)
 
+    # ---------------------------------------------------------------- r3d::rectify_image
+    def rectify_image(self, src: np.ndarray, camera: dict, source_from_target, target: dict):
+        """Resamples a one-channel u16 or f32 image of `camera` ({model, width,
+        height, fx, fy, cx, cy, params}) into the pinhole camera `target`
+        ({width, height, fx, fy, cx, cy}) rotated by R_source R_target^T =
+        `source_from_target` about the same centre; returns (image, valid)
+        with valid 255 where the target pixel sees the source.
+        r3d::rectify_image, src/r3d/rectify/rectification.hpp:75-88."""
+        from .types import camera_struct, pinhole_struct
+
+        cam, k = camera_struct(camera), pinhole_struct(target)
+        m = np.ascontiguousarray(source_from_target, dtype=np.float64).reshape(9)
+        valid = np.empty((k.height, k.width), np.uint8)
+        if src.dtype == np.float32:
+            img = np.ascontiguousarray(src)
+            if img.ndim != 2 or img.shape != (cam.height, cam.width):
+                raise _native.StereoError(1, f"rectify_image: image is {img.shape}, camera is "
+                                             f"{cam.height}x{cam.width}")
+            out = np.empty((k.height, k.width), np.float32)
+            st = self.lib.r3dgpu_rectify_image_f32_host(img.ctypes.data, img.shape[1],
+                                                         ctypes.byref(cam), m.ctypes.data, ctypes.byref(k),
+                                                         out.ctypes.data, k.width, valid.ctypes.data, k.width)
+        else:
+            img = _u16(src)
+            out = np.empty((k.height, k.width), np.uint16)
+            view = CViewU16(img.ctypes.data, img.shape[1], img.shape[0], img.shape[1])
+            st = self.lib.r3dgpu_rectify_image_u16_host(ctypes.byref(view), ctypes.byref(cam), m.ctypes.data,
+                                                         ctypes.byref(k), out.ctypes.data, k.width,
+                                                         valid.ctypes.data, k.width)
+        self._check(st)
+        return out, valid
+
     # ---------------------------------------------------------------- batched matching
     def match_stereo_batch(self, pairs: Sequence[dict], stream: int | None = None) -> list[DisparityMap]:
         """Matches many pairs in one pass of every stage.

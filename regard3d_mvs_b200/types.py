@@ -189,6 +189,59 @@ class DepthMap:
     pair_mask: np.ndarray
 
 
+# Camera models of CameraIntrinsics (src/r3d/core/camera_model.hpp:15-21).
+CAMERA_MODELS = {"pinhole": 0, "radial_k1": 1, "radial_k3": 2, "brown_t2": 3, "fisheye": 4}
+
+
+class CCamera(ctypes.Structure):
+    """r3dgpu_camera: CameraIntrinsics, src/r3d/core/camera_model.hpp:32-41."""
+
+    _fields_ = [
+        ("model", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("fx", ctypes.c_double),
+        ("fy", ctypes.c_double),
+        ("cx", ctypes.c_double),
+        ("cy", ctypes.c_double),
+        ("params", ctypes.c_double * 5),
+    ]
+
+
+class CPinhole(ctypes.Structure):
+    """r3dgpu_pinhole: PinholeIntrinsics of a rectified camera."""
+
+    _fields_ = [
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("fx", ctypes.c_double),
+        ("fy", ctypes.c_double),
+        ("cx", ctypes.c_double),
+        ("cy", ctypes.c_double),
+    ]
+
+
+def camera_struct(cam: dict) -> CCamera:
+    """CCamera from {model (name or number), width, height, fx, fy, cx, cy, params}."""
+    model = cam.get("model", 0)
+    model = CAMERA_MODELS[model] if isinstance(model, str) else int(model)
+    params = list(cam.get("params", ()))
+    if len(params) > 5:
+        raise ValueError("at most 5 distortion parameters")
+    c = CCamera(model, int(cam["width"]), int(cam["height"]), 0, float(cam["fx"]), float(cam["fy"]),
+                float(cam["cx"]), float(cam["cy"]))
+    for i, v in enumerate(params):
+        c.params[i] = float(v)
+    return c
+
+
+def pinhole_struct(k: dict) -> CPinhole:
+    """CPinhole from {width, height, fx, fy, cx, cy}."""
+    return CPinhole(int(k["width"]), int(k["height"]), float(k["fx"]), float(k["fy"]), float(k["cx"]),
+                    float(k["cy"]))
+
+
 class CServerConfig(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32),
