@@ -301,6 +301,115 @@ r3dgpu_status r3dgpu_combine_pairs_host(const r3dgpu_depth_grid* grid, const r3d
                                         int32_t count, const r3dgpu_multi_stereo_options* options, float* depth,
                                         float* confidence, uint16_t* pair_mask, int64_t stride);
 
+/* ------------------------------------------------------------------ depth maps
+ * Multi-view geometric consistency of depth maps (the step after the
+ * combination). Replaces prepare_depth_map, check_consistency,
+ * filter_depth_maps, erode_depth_edges, remove_weak_depths,
+ * remove_depth_halos and remove_depth_speckles,
+ * src/r3d/mvs/consistency.hpp:97-125 (implementation
+ * src/r3d/mvs/consistency.cpp:57-487). */
+
+/* PinholeCamera (src/r3d/core/camera.hpp:26-80): intrinsics, pose (R maps
+ * world to camera axes, C is the centre; row-major), and K^-1 as the caller
+ * computes it (the reference takes Eigen's K().inverse()). */
+typedef struct r3dgpu_pinhole_camera {
+  r3dgpu_pinhole intrinsics;
+  double rotation[9];
+  double center[3];
+  double k_inv[9];
+} r3dgpu_pinhole_camera;
+
+/* DepthMap (src/r3d/mvs/depth_map.hpp:17-41) in device memory (host memory
+ * for _host calls). depth 0 = invalid; `support` is written by the check;
+ * `color` is RGB interleaved (or NULL: weak-texture and halo removal then do
+ * nothing); `stride` is the row stride of depth, confidence, pair_mask and
+ * support in elements, `color_stride` that of color in bytes. */
+#define R3DGPU_MAX_PARTNERS 16
+typedef struct r3dgpu_depth_map {
+  r3dgpu_pinhole_camera camera;
+  float* depth;
+  float* confidence;
+  uint16_t* pair_mask;
+  uint8_t* support;
+  const uint8_t* color;
+  int64_t stride;
+  int64_t color_stride;
+  int32_t width;
+  int32_t height;
+  uint32_t view;
+  uint32_t num_partners;
+  uint32_t partners[R3DGPU_MAX_PARTNERS];
+} r3dgpu_depth_map;
+
+/* ConsistencyOptions, src/r3d/mvs/consistency.hpp:59-78: same fields, same
+ * defaults (r3dgpu_default_consistency_options). max_neighbours belongs to
+ * the caller's neighbour selection and is not read here. */
+typedef struct r3dgpu_consistency_options {
+  double max_relative_depth_error;
+  double max_reprojection_px;
+  int32_t min_views;
+  int32_t min_evidence;
+  float min_confidence;
+  int32_t edge_erosion;
+  double discontinuity;
+  int32_t erode_holes;
+  int32_t max_neighbours;
+  int32_t independent_support;
+  int32_t average_depths;
+  double weak_texture;
+  double weak_segment;
+  int32_t reject_weak;
+  int32_t halo_px;
+  int32_t halo_colour;
+  int32_t speckle_size;
+  double speckle_step;
+} r3dgpu_consistency_options;
+
+/* ConsistencyStats, src/r3d/mvs/consistency.hpp:80-89. */
+typedef struct r3dgpu_consistency_stats {
+  uint64_t input, unconfident, eroded, rejected, weak, halo, speckles, output;
+} r3dgpu_consistency_stats;
+
+void r3dgpu_default_consistency_options(r3dgpu_consistency_options* out);
+
+/* At most this many neighbours per map in one check. */
+#define R3DGPU_MAX_NEIGHBOURS 64
+
+/* prepare_depth_map: removes unconfident depths and depth edges in place;
+ * counts are added to *stats (may be NULL). Runs on `stream`, synchronises it. */
+r3dgpu_status r3dgpu_prepare_depth_map(r3dgpu_depth_map* map, const r3dgpu_consistency_options* options,
+                                       r3dgpu_consistency_stats* stats, void* stream);
+
+/* check_consistency: checks `map` against its prepared neighbours (read
+ * only), fills map->support, removes unconfirmed depths, weak depths, halos
+ * and speckles; counts are added to *stats. */
+r3dgpu_status r3dgpu_check_consistency(r3dgpu_depth_map* map, const r3dgpu_depth_map* neighbours, int32_t count,
+                                       const r3dgpu_consistency_options* options, r3dgpu_consistency_stats* stats,
+                                       void* stream);
+
+/* filter_depth_maps: both steps for all maps in place; the neighbours of
+ * map i are maps[neighbour_index[neighbour_offset[i] .. neighbour_offset[i+1])]
+ * (count + 1 offsets). All checks read the prepared, unfiltered maps. *stats
+ * (may be NULL) is set, not added to. */
+r3dgpu_status r3dgpu_filter_depth_maps(r3dgpu_depth_map* maps, int32_t count, const int32_t* neighbour_offset,
+                                       const int32_t* neighbour_index, const r3dgpu_consistency_options* options,
+                                       r3dgpu_consistency_stats* stats, void* stream);
+/* Same with the maps in host memory (copies inside). */
+r3dgpu_status r3dgpu_filter_depth_maps_host(r3dgpu_depth_map* maps, int32_t count, const int32_t* neighbour_offset,
+                                            const int32_t* neighbour_index,
+                                            const r3dgpu_consistency_options* options,
+                                            r3dgpu_consistency_stats* stats);
+
+/* The single filters (device maps); *removed receives the pixels removed. */
+r3dgpu_status r3dgpu_erode_depth_edges(r3dgpu_depth_map* map, int32_t radius, double discontinuity, int32_t holes,
+                                       uint64_t* removed, void* stream);
+r3dgpu_status r3dgpu_remove_weak_depths(r3dgpu_depth_map* map, const r3dgpu_consistency_options* options,
+                                        uint64_t* removed, void* stream);
+r3dgpu_status r3dgpu_remove_depth_halos(r3dgpu_depth_map* map, int32_t max_px, int32_t colour_step,
+                                        uint64_t* removed, void* stream);
+r3dgpu_status r3dgpu_remove_depth_speckles(r3dgpu_depth_map* map, int32_t min_size, double max_relative_step,
+                                           uint64_t* removed, void* stream);
+
 /* Frees the device and pinned host buffers that this thread's calls keep on
  * its current device for reuse (they grow to the largest call made so far);
  * the next call allocates them again. No reference counterpart. */

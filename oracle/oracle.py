@@ -52,6 +52,14 @@ def lib():
         L.orc_sample_disparity.argtypes = [P, i32, i32, P, P, i32, P]
         L.orc_rectify_image.argtypes = [i32, P, P, P, P, P, P]
         L.orc_distort_pixel.argtypes = [P, P, i32, P]
+        L.orc_mvs_last_error.restype = ctypes.c_char_p
+        L.orc_filter_depth_maps.argtypes = [P, i32, P, P, P, P]
+        L.orc_prepare_depth_map.argtypes = [P, P, P]
+        L.orc_check_consistency.argtypes = [P, P, i32, P, P]
+        L.orc_erode_depth_edges.argtypes = [P, i32, ctypes.c_double, i32, P]
+        L.orc_remove_weak_depths.argtypes = [P, P, P]
+        L.orc_remove_depth_halos.argtypes = [P, i32, i32, P]
+        L.orc_remove_depth_speckles.argtypes = [P, i32, ctypes.c_double, P]
         _lib = L
     return _lib
 
@@ -189,6 +197,91 @@ def distort_pixel(camera: dict, pixels) -> np.ndarray:
     out = np.empty_like(p)
     _check(lib().orc_distort_pixel(ctypes.byref(cam), _ptr(p), len(p), _ptr(out)))
     return out
+
+
+# ------------------------------------------------------------------ depth-map consistency
+# src/r3d/mvs/consistency.cpp:57-485 on host maps (dicts as in
+# regard3d_mvs_b200.depth_maps); depth and support are updated in place.
+def _mvs_check(rc: int) -> None:
+    if rc != 0:
+        raise OracleError(lib().orc_mvs_last_error().decode())
+
+
+def _host_maps(maps):
+    from regard3d_mvs_b200.depth_maps import CDepthMap, c_depth_map, normalise
+
+    norm = [normalise(m) for m in maps]
+    arr = (CDepthMap * max(1, len(norm)))()
+    for i, n in enumerate(norm):
+        arr[i] = c_depth_map(n, lambda a: a.ctypes.data)
+    return norm, arr
+
+
+def _back(maps, norm):
+    for m, n in zip(maps, norm):
+        m["depth"], m["support"] = n["depth"], n["support"]
+
+
+def filter_depth_maps(maps, neighbours, options=None) -> dict:
+    from regard3d_mvs_b200.depth_maps import CConsistencyStats, ConsistencyOptions, neighbour_lists
+
+    norm, arr = _host_maps(maps)
+    off, idx = neighbour_lists(neighbours)
+    st = CConsistencyStats()
+    o = (options or ConsistencyOptions()).c()
+    _mvs_check(lib().orc_filter_depth_maps(arr, len(maps), _ptr(off), _ptr(idx), ctypes.byref(o), ctypes.byref(st)))
+    _back(maps, norm)
+    return st.as_dict()
+
+
+def prepare_depth_map(m, options=None) -> dict:
+    from regard3d_mvs_b200.depth_maps import CConsistencyStats, ConsistencyOptions
+
+    norm, arr = _host_maps([m])
+    st = CConsistencyStats()
+    o = (options or ConsistencyOptions()).c()
+    _mvs_check(lib().orc_prepare_depth_map(ctypes.byref(arr[0]), ctypes.byref(o), ctypes.byref(st)))
+    _back([m], norm)
+    return st.as_dict()
+
+
+def check_consistency(m, neighbours, options=None) -> dict:
+    from regard3d_mvs_b200.depth_maps import CConsistencyStats, ConsistencyOptions
+
+    norm, arr = _host_maps([m])
+    nnorm, nbs = _host_maps(neighbours)
+    st = CConsistencyStats()
+    o = (options or ConsistencyOptions()).c()
+    _mvs_check(lib().orc_check_consistency(ctypes.byref(arr[0]), nbs, len(neighbours), ctypes.byref(o),
+                                           ctypes.byref(st)))
+    del nnorm
+    _back([m], norm)
+    return st.as_dict()
+
+
+def _single(m, call) -> int:
+    norm, arr = _host_maps([m])
+    removed = ctypes.c_uint64(0)
+    _mvs_check(call(ctypes.byref(arr[0]), ctypes.byref(removed)))
+    _back([m], norm)
+    return int(removed.value)
+
+
+def erode_depth_edges(m, radius: int, discontinuity: float, holes: bool = False) -> int:
+    return _single(m, lambda c, r: lib().orc_erode_depth_edges(c, radius, discontinuity, int(holes), r))
+
+
+def remove_weak_depths(m, options) -> int:
+    o = options.c()
+    return _single(m, lambda c, r: lib().orc_remove_weak_depths(c, ctypes.byref(o), r))
+
+
+def remove_depth_halos(m, max_px: int, colour_step: int) -> int:
+    return _single(m, lambda c, r: lib().orc_remove_depth_halos(c, max_px, colour_step, r))
+
+
+def remove_depth_speckles(m, min_size: int, max_relative_step: float) -> int:
+    return _single(m, lambda c, r: lib().orc_remove_depth_speckles(c, min_size, max_relative_step, r))
 
 
 def rectify_image(src: np.ndarray, camera: dict, source_from_target, target: dict):

@@ -46,6 +46,15 @@ EXPORTS = (
     "r3dgpu_rectify_image_f32",
     "r3dgpu_rectify_image_u16_host",
     "r3dgpu_rectify_image_f32_host",
+    "r3dgpu_default_consistency_options",
+    "r3dgpu_prepare_depth_map",
+    "r3dgpu_check_consistency",
+    "r3dgpu_filter_depth_maps",
+    "r3dgpu_filter_depth_maps_host",
+    "r3dgpu_erode_depth_edges",
+    "r3dgpu_remove_weak_depths",
+    "r3dgpu_remove_depth_halos",
+    "r3dgpu_remove_depth_speckles",
     "r3dgpu_default_multi_stereo_options",
     "r3dgpu_combine_pairs",
     "r3dgpu_combine_pairs_host",
@@ -120,6 +129,24 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_rectify_image_f32_host.argtypes = [P, i64, cam, P, pin, P, i64, P, i64]
     for name in ("r3dgpu_rectify_image_u16", "r3dgpu_rectify_image_f32", "r3dgpu_rectify_image_u16_host",
                  "r3dgpu_rectify_image_f32_host"):
+        getattr(L, name).restype = st
+    from .depth_maps import CConsistencyOptions, CConsistencyStats, CDepthMap
+
+    dm, co, cs, u64p = (ctypes.POINTER(CDepthMap), ctypes.POINTER(CConsistencyOptions),
+                        ctypes.POINTER(CConsistencyStats), ctypes.POINTER(ctypes.c_uint64))
+    L.r3dgpu_default_consistency_options.argtypes = [co]
+    L.r3dgpu_default_consistency_options.restype = None
+    L.r3dgpu_prepare_depth_map.argtypes = [dm, co, cs, P]
+    L.r3dgpu_check_consistency.argtypes = [dm, dm, i32, co, cs, P]
+    L.r3dgpu_filter_depth_maps.argtypes = [dm, i32, P, P, co, cs, P]
+    L.r3dgpu_filter_depth_maps_host.argtypes = [dm, i32, P, P, co, cs]
+    L.r3dgpu_erode_depth_edges.argtypes = [dm, i32, ctypes.c_double, i32, u64p, P]
+    L.r3dgpu_remove_weak_depths.argtypes = [dm, co, u64p, P]
+    L.r3dgpu_remove_depth_halos.argtypes = [dm, i32, i32, u64p, P]
+    L.r3dgpu_remove_depth_speckles.argtypes = [dm, i32, ctypes.c_double, u64p, P]
+    for name in ("r3dgpu_prepare_depth_map", "r3dgpu_check_consistency", "r3dgpu_filter_depth_maps",
+                 "r3dgpu_filter_depth_maps_host", "r3dgpu_erode_depth_edges", "r3dgpu_remove_weak_depths",
+                 "r3dgpu_remove_depth_halos", "r3dgpu_remove_depth_speckles"):
         getattr(L, name).restype = st
     L.r3dgpu_default_multi_stereo_options.argtypes = [ctypes.POINTER(CMultiStereoOptions)]
     L.r3dgpu_default_multi_stereo_options.restype = None

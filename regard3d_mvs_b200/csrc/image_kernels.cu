@@ -615,11 +615,8 @@ void launch_apply_bad(float* map, const uint8_t* bad, int64_t n, cudaStream_t s)
   launched("apply_bad_kernel");
 }
 
-void launch_remove_speckles(float* d, int w, int h, int min_size, float max_diff, int* scratch, cudaStream_t s) {
-  if (min_size <= 1 || w <= 0 || h <= 0) return;
+void launch_segments(const float* d, int w, int h, float max_diff, int* parent, int* size, cudaStream_t s) {
   const int64_t n = static_cast<int64_t>(w) * h;
-  int* parent = scratch;
-  int* size = scratch + n;
   const dim3 tiles(static_cast<unsigned>(ceil_div64(w, kUfTile)), static_cast<unsigned>(ceil_div64(h, kUfTile)));
   R3D_LAUNCH(uf_tile_kernel, tiles, 256, 2 * sizeof(int) * kUfTile * kUfTile, s, d, w, h, max_diff, parent, size);
   launched("uf_tile_kernel");
@@ -631,6 +628,15 @@ void launch_remove_speckles(float* d, int w, int h, int min_size, float max_diff
   const unsigned g1 = static_cast<unsigned>(ceil_div64(n, 256));
   R3D_LAUNCH(uf_count_kernel, g1, 256, 0, s, d, n, parent, size);
   launched("uf_count_kernel");
+}
+
+void launch_remove_speckles(float* d, int w, int h, int min_size, float max_diff, int* scratch, cudaStream_t s) {
+  if (min_size <= 1 || w <= 0 || h <= 0) return;
+  const int64_t n = static_cast<int64_t>(w) * h;
+  int* parent = scratch;
+  int* size = scratch + n;
+  launch_segments(d, w, h, max_diff, parent, size, s);
+  const unsigned g1 = static_cast<unsigned>(ceil_div64(n, 256));
   R3D_LAUNCH(uf_filter_kernel, g1, 256, 0, s, d, n, parent, size, min_size);
   launched("uf_filter_kernel");
 }

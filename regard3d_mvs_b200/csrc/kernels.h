@@ -30,6 +30,10 @@ void launch_intervals(const uint8_t* mask, int64_t stride, int w, int h, RowInte
 void launch_lr_check(const float* map, const float* other, int w, int h, int wo, int sign, int max_diff,
                      uint8_t* bad, cudaStream_t s);
 void launch_apply_bad(float* map, const uint8_t* bad, int64_t n, cudaStream_t s);
+// Segments of 4-neighbours of the contiguous map d (w x h, invalid = +inf)
+// whose values differ by at most max_diff: afterwards parent[i] is the root
+// (smallest index) of valid pixel i's segment and size[root] its pixel count.
+void launch_segments(const float* d, int w, int h, float max_diff, int* parent, int* size, cudaStream_t s);
 // In place; scratch: 2 * w * h ints.
 void launch_remove_speckles(float* d, int w, int h, int min_size, float max_diff, int* scratch, cudaStream_t s);
 // Same filter with the scratch in a static device array (noalloc.cu); the

@@ -142,6 +142,96 @@ class Matcher:
         self._check(st)
         return out, valid
 
+    # ---------------------------------------------------------------- depth-map consistency
+    # src/r3d/mvs/consistency.hpp:97-125. Maps are dicts (regard3d_mvs_b200.depth_maps);
+    # their depth and support arrays are updated in place.
+    def _device_maps(self, maps: Sequence[dict], keep: list):
+        from .depth_maps import CDepthMap, c_depth_map, normalise
+
+        norm = [normalise(m) for m in maps]
+        dev: dict[int, object] = {}
+
+        def ptr(a):
+            p = self._to_device(a, keep)
+            dev[id(a)] = keep[-1]
+            return p
+
+        arr = (CDepthMap * max(1, len(norm)))()
+        for i, n in enumerate(norm):
+            arr[i] = c_depth_map(n, ptr)
+        return norm, arr, dev
+
+    def _maps_back(self, maps: Sequence[dict], norm: list, dev: dict) -> None:
+        for m, n in zip(maps, norm):
+            if not self.host_is_device:
+                n["depth"][...] = dev[id(n["depth"])].cpu().numpy()
+                n["support"][...] = dev[id(n["support"])].cpu().numpy()
+            m["depth"], m["support"] = n["depth"], n["support"]
+
+    def _single(self, m: dict, call) -> int:
+        keep: list = []
+        norm, arr, dev = self._device_maps([m], keep)
+        removed = ctypes.c_uint64(0)
+        self._check(call(ctypes.byref(arr[0]), ctypes.byref(removed)))
+        self._maps_back([m], norm, dev)
+        return int(removed.value)
+
+    def prepare_depth_map(self, m: dict, options=None) -> dict:
+        from .depth_maps import CConsistencyStats, ConsistencyOptions
+
+        keep: list = []
+        norm, arr, dev = self._device_maps([m], keep)
+        st = CConsistencyStats()
+        o = (options or ConsistencyOptions()).c()
+        self._check(self.lib.r3dgpu_prepare_depth_map(ctypes.byref(arr[0]), ctypes.byref(o), ctypes.byref(st), None))
+        self._maps_back([m], norm, dev)
+        return st.as_dict()
+
+    def check_consistency(self, m: dict, neighbours: Sequence[dict], options=None) -> dict:
+        from .depth_maps import CConsistencyStats, ConsistencyOptions
+
+        keep: list = []
+        norm, arr, dev = self._device_maps([m], keep)
+        _, nbs, _ = self._device_maps(neighbours, keep)
+        st = CConsistencyStats()
+        o = (options or ConsistencyOptions()).c()
+        self._check(self.lib.r3dgpu_check_consistency(ctypes.byref(arr[0]), nbs, len(neighbours), ctypes.byref(o),
+                                                      ctypes.byref(st), None))
+        self._maps_back([m], norm, dev)
+        return st.as_dict()
+
+    def filter_depth_maps(self, maps: list[dict], neighbours: Sequence[Sequence[int]], options=None) -> dict:
+        """filter_depth_maps through the host entry point (copies inside)."""
+        from .depth_maps import CConsistencyStats, CDepthMap, ConsistencyOptions, c_depth_map, neighbour_lists, normalise
+
+        norm = [normalise(m) for m in maps]
+        arr = (CDepthMap * max(1, len(norm)))()
+        for i, n in enumerate(norm):
+            arr[i] = c_depth_map(n, lambda a: a.ctypes.data)
+        off, idx = neighbour_lists(neighbours)
+        st = CConsistencyStats()
+        o = (options or ConsistencyOptions()).c()
+        self._check(self.lib.r3dgpu_filter_depth_maps_host(arr, len(maps), off.ctypes.data, idx.ctypes.data,
+                                                           ctypes.byref(o), ctypes.byref(st)))
+        for m, n in zip(maps, norm):
+            m["depth"], m["support"] = n["depth"], n["support"]
+        return st.as_dict()
+
+    def erode_depth_edges(self, m: dict, radius: int, discontinuity: float, holes: bool = False) -> int:
+        return self._single(m, lambda c, r: self.lib.r3dgpu_erode_depth_edges(c, radius, discontinuity, int(holes),
+                                                                              r, None))
+
+    def remove_weak_depths(self, m: dict, options) -> int:
+        o = options.c()
+        return self._single(m, lambda c, r: self.lib.r3dgpu_remove_weak_depths(c, ctypes.byref(o), r, None))
+
+    def remove_depth_halos(self, m: dict, max_px: int, colour_step: int) -> int:
+        return self._single(m, lambda c, r: self.lib.r3dgpu_remove_depth_halos(c, max_px, colour_step, r, None))
+
+    def remove_depth_speckles(self, m: dict, min_size: int, max_relative_step: float) -> int:
+        return self._single(m, lambda c, r: self.lib.r3dgpu_remove_depth_speckles(c, min_size, max_relative_step, r,
+                                                                                  None))
+
     # ---------------------------------------------------------------- batched matching
     def match_stereo_batch(self, pairs: Sequence[dict], stream: int | None = None) -> list[DisparityMap]:
         """Matches many pairs in one pass of every stage.
