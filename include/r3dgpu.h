@@ -410,6 +410,70 @@ r3dgpu_status r3dgpu_remove_depth_halos(r3dgpu_depth_map* map, int32_t max_px, i
 r3dgpu_status r3dgpu_remove_depth_speckles(r3dgpu_depth_map* map, int32_t min_size, double max_relative_step,
                                            uint64_t* removed, void* stream);
 
+/* ------------------------------------------------------------------ refinement
+ * Patch-based depth refinement: per valid pixel an inverse-depth plane
+ * (w, a, b) fitted by Gauss-Newton on 2 - 2 NCC of the window warped into the
+ * neighbouring views. Replaces make_refinement_image and refine_depth_map,
+ * src/r3d/mvs/refinement.hpp:33-68 (implementation
+ * src/r3d/mvs/refinement.cpp:1-451). */
+
+/* RefinementOptions (refinement.hpp:33-44, same defaults), plus `fp32`:
+ * 0 computes the window terms in double precision as the reference does;
+ * 1 computes them in float (the 3x3 solve stays double). */
+typedef struct r3dgpu_refinement_options {
+  int32_t radius;
+  int32_t step;
+  int32_t iterations;
+  int32_t max_views;
+  double min_ncc;
+  double max_shift_px;
+  double min_gain;
+  double min_texture;
+  double blur_sigma;
+  int32_t drop_unconfirmed;
+  int32_t fp32;
+} r3dgpu_refinement_options;
+
+/* RefinementStats (refinement.hpp:46-51). */
+typedef struct r3dgpu_refinement_stats {
+  uint64_t input, refined, kept, unconfirmed;
+} r3dgpu_refinement_stats;
+
+/* RefinementImage (refinement.hpp:53-58): a view's intensity (0..255) and its
+ * x / y derivatives, three interleaved floats per pixel on the camera's grid
+ * (camera.intrinsics.width x height); `stride` in floats per row. */
+typedef struct r3dgpu_refinement_image {
+  r3dgpu_pinhole_camera camera;
+  const float* data;
+  int64_t stride;
+} r3dgpu_refinement_image;
+
+void r3dgpu_default_refinement_options(r3dgpu_refinement_options* out);
+
+/* make_refinement_image (refinement.hpp:60-63): gray (width x height,
+ * `gray_stride` floats per row), optionally Gaussian-smoothed by blur_sigma
+ * pixels, into out (3 floats per pixel, `out_stride` floats per row).
+ * Device pointers; runs on `stream` and synchronises it. */
+r3dgpu_status r3dgpu_make_refinement_image(const float* gray, int64_t gray_stride, int32_t width, int32_t height,
+                                           double blur_sigma, float* out, int64_t out_stride, void* stream);
+
+/* refine_depth_map (refinement.hpp:65-68): refines the depth map (depth and
+ * confidence, width x height at `stride` floats per row, on `camera`'s grid)
+ * in place; `base` is on the same grid, `views` are the neighbouring images
+ * (at most options->max_views, and at most 8, are used). *stats may be NULL.
+ * Device pointers; runs on `stream` and synchronises it. */
+r3dgpu_status r3dgpu_refine_depth_map(float* depth, float* confidence, int64_t stride,
+                                      const r3dgpu_pinhole_camera* camera, int32_t width, int32_t height,
+                                      const r3dgpu_refinement_image* base, const r3dgpu_refinement_image* views,
+                                      int32_t num_views, const r3dgpu_refinement_options* options,
+                                      r3dgpu_refinement_stats* stats, void* stream);
+/* Same with host maps and images (copies inside). */
+r3dgpu_status r3dgpu_refine_depth_map_host(float* depth, float* confidence, int64_t stride,
+                                           const r3dgpu_pinhole_camera* camera, int32_t width, int32_t height,
+                                           const r3dgpu_refinement_image* base,
+                                           const r3dgpu_refinement_image* views, int32_t num_views,
+                                           const r3dgpu_refinement_options* options, r3dgpu_refinement_stats* stats);
+
 /* Frees the device and pinned host buffers that this thread's calls keep on
  * its current device for reuse (they grow to the largest call made so far);
  * the next call allocates them again. No reference counterpart. */

@@ -60,6 +60,8 @@ def lib():
         L.orc_remove_weak_depths.argtypes = [P, P, P]
         L.orc_remove_depth_halos.argtypes = [P, i32, i32, P]
         L.orc_remove_depth_speckles.argtypes = [P, i32, ctypes.c_double, P]
+        L.orc_make_refinement_image.argtypes = [P, i32, i32, ctypes.c_double, P]
+        L.orc_refine_depth_map.argtypes = [P, P, ctypes.c_int64, P, i32, i32, P, P, i32, P, P]
         _lib = L
     return _lib
 
@@ -256,6 +258,41 @@ def check_consistency(m, neighbours, options=None) -> dict:
                                            ctypes.byref(st)))
     del nnorm
     _back([m], norm)
+    return st.as_dict()
+
+
+def make_refinement_image(gray: np.ndarray, blur_sigma: float = 0.0) -> np.ndarray:
+    """make_refinement_image (src/r3d/mvs/refinement.cpp:242-269): H x W x 3."""
+    g = _c(gray, np.float32)
+    h, w = g.shape
+    out = np.empty((h, w, 3), np.float32)
+    _mvs_check(lib().orc_make_refinement_image(_ptr(g), w, h, blur_sigma, _ptr(out)))
+    return out
+
+
+def refine_depth_map(m, base, views, options=None) -> dict:
+    """refine_depth_map (src/r3d/mvs/refinement.cpp:271-449) in double
+    precision; m["depth"] and m["confidence"] are updated in place."""
+    from regard3d_mvs_b200.depth_maps import (CRefinementImage, CRefinementStats, RefinementOptions, c_camera,
+                                              c_refinement_image)
+
+    depth = np.ascontiguousarray(m["depth"], np.float32)
+    conf = np.ascontiguousarray(m["confidence"], np.float32) if m.get("confidence") is not None \
+        else np.zeros_like(depth)
+    h, w = depth.shape
+    host = lambda a: a.ctypes.data  # noqa: E731
+    bdata = np.ascontiguousarray(base["data"], np.float32)
+    cb = c_refinement_image({"camera": base["camera"], "data": bdata}, host)
+    vdata = [np.ascontiguousarray(v["data"], np.float32) for v in views]
+    cv = (CRefinementImage * max(1, len(views)))()
+    for i, (v, d) in enumerate(zip(views, vdata)):
+        cv[i] = c_refinement_image({"camera": v["camera"], "data": d}, host)
+    cam = c_camera(m["camera"])
+    st = CRefinementStats()
+    o = (options or RefinementOptions()).c()
+    _mvs_check(lib().orc_refine_depth_map(_ptr(depth), _ptr(conf), w, ctypes.byref(cam), w, h, ctypes.byref(cb), cv,
+                                          len(views), ctypes.byref(o), ctypes.byref(st)))
+    m["depth"], m["confidence"] = depth, conf
     return st.as_dict()
 
 

@@ -46,6 +46,10 @@ EXPORTS = (
     "r3dgpu_rectify_image_f32",
     "r3dgpu_rectify_image_u16_host",
     "r3dgpu_rectify_image_f32_host",
+    "r3dgpu_default_refinement_options",
+    "r3dgpu_make_refinement_image",
+    "r3dgpu_refine_depth_map",
+    "r3dgpu_refine_depth_map_host",
     "r3dgpu_default_consistency_options",
     "r3dgpu_prepare_depth_map",
     "r3dgpu_check_consistency",
@@ -144,6 +148,19 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_remove_weak_depths.argtypes = [dm, co, u64p, P]
     L.r3dgpu_remove_depth_halos.argtypes = [dm, i32, i32, u64p, P]
     L.r3dgpu_remove_depth_speckles.argtypes = [dm, i32, ctypes.c_double, u64p, P]
+    from .depth_maps import CPinholeCamera, CRefinementImage, CRefinementOptions, CRefinementStats
+
+    ro, ri, rs = (ctypes.POINTER(CRefinementOptions), ctypes.POINTER(CRefinementImage),
+                  ctypes.POINTER(CRefinementStats))
+    L.r3dgpu_default_refinement_options.argtypes = [ro]
+    L.r3dgpu_default_refinement_options.restype = None
+    L.r3dgpu_make_refinement_image.argtypes = [P, ctypes.c_int64, i32, i32, ctypes.c_double, P, ctypes.c_int64, P]
+    L.r3dgpu_refine_depth_map.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(CPinholeCamera), i32, i32, ri, ri,
+                                          i32, ro, rs, P]
+    L.r3dgpu_refine_depth_map_host.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(CPinholeCamera), i32, i32, ri,
+                                               ri, i32, ro, rs]
+    for name in ("r3dgpu_make_refinement_image", "r3dgpu_refine_depth_map", "r3dgpu_refine_depth_map_host"):
+        getattr(L, name).restype = st
     for name in ("r3dgpu_prepare_depth_map", "r3dgpu_check_consistency", "r3dgpu_filter_depth_maps",
                  "r3dgpu_filter_depth_maps_host", "r3dgpu_erode_depth_edges", "r3dgpu_remove_weak_depths",
                  "r3dgpu_remove_depth_halos", "r3dgpu_remove_depth_speckles"):

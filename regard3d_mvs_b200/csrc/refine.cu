@@ -1,0 +1,807 @@
+// Patch-based depth refinement (r3dgpu_refine_depth_map) and its input images
+// (r3dgpu_make_refinement_image), the reference's src/r3d/mvs/refinement.cpp.
+//
+// One warp per depth-map pixel. The window samples (25 for the default 9 x 9
+// window at step 2, 49 for a 7 x 7 window at step 1, at most 225) are spread
+// over the lanes: each lane warps, samples and normalises its samples, and
+// every sum of the NCC and of the Gauss-Newton terms is an xor-butterfly
+// reduction. After a butterfly every lane holds the same bits (the partial
+// sums meet in mirrored order, and IEEE addition commutes), so the per-pixel
+// control flow — view selection, the damped Gauss-Newton loop with step
+// shrinking, the acceptance test — is uniform over the warp and runs in every
+// lane, with no shared memory and no barriers. The window terms compute in
+// double precision as the reference does, or in float (fp32 = 1); the 3 x 3
+// LDL^T solve is double in both. Sums run in a different order than the
+// reference's sequential loops, so results agree with a double-precision CPU
+// restatement to rounding, not bit for bit.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "matcher_internal.h"
+
+namespace r3dgpu {
+namespace {
+
+constexpr int kMaxSamples = 225;  // refinement.cpp:21
+constexpr int kMaxViews = 8;      // refinement.cpp:22
+constexpr double kDiscontinuity = 0.05;
+enum : int { kInput, kRefined, kUnconfirmed, kCounters };
+
+// Plane-induced warp into a view (refinement.cpp:24-30): h = m (qx, qy, 1) + b w(q).
+struct ViewGeo {
+  double m[9];  // K_j R_j R_0^T K_0^-1, row-major
+  double b[3];  // K_j R_j (C_0 - C_j)
+  const float* data;
+  int64_t stride;
+  int width, height;
+};
+
+struct Params {
+  int width, height;
+  int radius, step, side, n;  // `side` samples per window row, n = side^2
+  int iterations, num_views;
+  double min_ncc, max_shift_px, min_gain, min_texture2n;
+  int drop_unconfirmed;
+};
+
+template <class T>
+R3D_DEVICE T shfl_xor_t(T v, int mask) {
+  uint32_t w[sizeof(T) / 4];
+  memcpy(w, &v, sizeof(T));
+  for (int i = 0; i < static_cast<int>(sizeof(T) / 4); ++i) w[i] = r3dsimt::shfl_xor(w[i], mask);
+  memcpy(&v, w, sizeof(T));
+  return v;
+}
+
+// Butterfly sums of K values at once (every lane gets the totals).
+template <class T, int K>
+R3D_DEVICE void warp_sums(T (&v)[K]) {
+  for (int m = 16; m >= 1; m >>= 1) {
+#pragma unroll
+    for (int i = 0; i < K; ++i) v[i] += shfl_xor_t(v[i], m);
+  }
+}
+
+template <class T>
+R3D_DEVICE T warp_sum(T v) {
+  T a[1] = {v};
+  warp_sums(a);
+  return a[0];
+}
+
+// Finite (neither infinite nor NaN): v - v is 0 exactly then, NaN otherwise.
+R3D_DEVICE bool finite_d(double v) { return v - v == 0.0; }
+
+R3D_DEVICE double row3(const double* m, int i, double x, double y, double z) {
+  return (m[3 * i] * x + m[3 * i + 1] * y) + m[3 * i + 2] * z;
+}
+
+// Per-lane sample s = lane + 32 k: window offset and the offset / radius.
+struct SampleAt {
+  bool on;
+  int dx, dy;
+};
+R3D_DEVICE SampleAt sample_at(const Params& p, int k) {
+  const int s = static_cast<int>(r3dsimt::lane_id()) + 32 * k;
+  if (s >= p.n) return {false, 0, 0};
+  return {true, (s % p.side) * p.step - p.radius, (s / p.side) * p.step - p.radius};
+}
+
+// refinement.cpp:46-152 for one view: NCC of the warped window with the
+// normalised base window n0 and, with JAC, J^T J (upper triangle: xx xy xz
+// yy yz zz) and J^T e of sum (n_q - n0_q)^2 in (w, a, b). False if a sample
+// leaves the image or the window has no texture.
+template <class T, int PER, bool JAC>
+R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double* theta, const Params& p,
+                              const T (&n0)[PER], T& ncc_out, T (&hh)[6], T (&gg)[3]) {
+  const T hc0 = static_cast<T>(row3(g.m, 0, x, y, 1.0)), hc1 = static_cast<T>(row3(g.m, 1, x, y, 1.0)),
+          hc2 = static_cast<T>(row3(g.m, 2, x, y, 1.0));
+  const T b0 = static_cast<T>(g.b[0]), b1 = static_cast<T>(g.b[1]), b2 = static_cast<T>(g.b[2]);
+  const T max_x = static_cast<T>(g.width - 1), max_y = static_cast<T>(g.height - 1);
+  const T th0 = static_cast<T>(theta[0]), th1 = static_cast<T>(theta[1]), th2 = static_cast<T>(theta[2]);
+  // In float, pixel positions of a few thousand carry about 1e-4 px of
+  // rounding, which the NCC gradient turns into depth noise. The float path
+  // therefore projects the window centre at the current depth in double once
+  // and each sample as a small float offset from it:
+  // (H + d).xy / (H + d).z = c + (d.xy - c d.z) / (H + d).z, c = H.xy / H.z.
+  const bool rel = sizeof(T) == 4;
+  double c0 = 0.0, c1 = 0.0, hz = 0.0;
+  int ic0 = 0, ic1 = 0;
+  T fc0 = 0, fc1 = 0, cf0 = 0, cf1 = 0, hzf = 0;
+  if (rel) {
+    const double H0 = row3(g.m, 0, x, y, 1.0) + g.b[0] * theta[0];
+    const double H1 = row3(g.m, 1, x, y, 1.0) + g.b[1] * theta[0];
+    hz = row3(g.m, 2, x, y, 1.0) + g.b[2] * theta[0];
+    if (hz > 0.0) {
+      c0 = H0 / hz;
+      c1 = H1 / hz;
+      const double f0 = floor(c0), f1 = floor(c1);
+      if (fabs(f0) < 1e8 && fabs(f1) < 1e8) {
+        ic0 = static_cast<int>(f0);
+        ic1 = static_cast<int>(f1);
+        fc0 = static_cast<T>(c0 - f0);
+        fc1 = static_cast<T>(c1 - f1);
+        cf0 = static_cast<T>(c0);
+        cf1 = static_cast<T>(c1);
+        hzf = static_cast<T>(hz);
+      } else {
+        hz = 0.0;
+      }
+    }
+  }
+  const bool offsets = rel && hz > 0.0;
+  T v[PER], dv[PER];
+  bool bad = false;
+  T sum = 0;
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    v[k] = 0;
+    dv[k] = 0;
+    const SampleAt sm = sample_at(p, k);
+    if (!sm.on || bad) continue;
+    const T dx = static_cast<T>(sm.dx), dy = static_cast<T>(sm.dy);
+    const T sx = dx / static_cast<T>(p.radius), sy = dy / static_cast<T>(p.radius);
+    T h2, inv_z, px, py;
+    int ix, iy;
+    T fx, fy;
+    if (offsets) {
+      const T ws = th1 * sx + th2 * sy;  // w(q) - w at the window centre
+      const T d0 = (static_cast<T>(g.m[0]) * dx + static_cast<T>(g.m[1]) * dy) + b0 * ws;
+      const T d1 = (static_cast<T>(g.m[3]) * dx + static_cast<T>(g.m[4]) * dy) + b1 * ws;
+      const T d2 = (static_cast<T>(g.m[6]) * dx + static_cast<T>(g.m[7]) * dy) + b2 * ws;
+      h2 = hzf + d2;
+      if (!(h2 > T(0))) {
+        bad = true;
+        continue;
+      }
+      inv_z = T(1) / h2;
+      const T q0 = fc0 + (d0 - cf0 * d2) * inv_z, q1 = fc1 + (d1 - cf1 * d2) * inv_z;
+      if (!(fabs(q0) < T(1e6) && fabs(q1) < T(1e6))) {
+        bad = true;
+        continue;
+      }
+      const T fl0 = floor(q0), fl1 = floor(q1);
+      ix = ic0 + static_cast<int>(fl0);
+      iy = ic1 + static_cast<int>(fl1);
+      fx = q0 - fl0;
+      fy = q1 - fl1;
+      px = static_cast<T>(ix) + fx;
+      py = static_cast<T>(iy) + fy;
+      // px in [0, width - 1) and py in [0, height - 1), as below.
+      if (!(ix >= 0 && iy >= 0 && ix <= g.width - 2 && iy <= g.height - 2)) {
+        bad = true;
+        continue;
+      }
+    } else {
+      const T wq = (th0 + th1 * sx) + th2 * sy;
+      const T h0 = ((hc0 + static_cast<T>(g.m[0]) * dx) + static_cast<T>(g.m[1]) * dy) + b0 * wq;
+      const T h1 = ((hc1 + static_cast<T>(g.m[3]) * dx) + static_cast<T>(g.m[4]) * dy) + b1 * wq;
+      h2 = ((hc2 + static_cast<T>(g.m[6]) * dx) + static_cast<T>(g.m[7]) * dy) + b2 * wq;
+      if (!(h2 > T(0))) {
+        bad = true;
+        continue;
+      }
+      inv_z = T(1) / h2;
+      px = h0 * inv_z;
+      py = h1 * inv_z;
+      if (!(px >= T(0) && py >= T(0) && px < max_x && py < max_y)) {
+        bad = true;
+        continue;
+      }
+      ix = static_cast<int>(px);
+      iy = static_cast<int>(py);
+      fx = px - static_cast<T>(ix);
+      fy = py - static_cast<T>(iy);
+    }
+    const float* r0 = g.data + static_cast<int64_t>(iy) * g.stride + 3 * ix;
+    const float* r1 = r0 + g.stride;
+    const T ax = T(1) - fx, ay = T(1) - fy;
+    auto bil = [&](int c) {
+      return ay * (ax * static_cast<T>(__ldg(r0 + c)) + fx * static_cast<T>(__ldg(r0 + 3 + c))) +
+             fy * (ax * static_cast<T>(__ldg(r1 + c)) + fx * static_cast<T>(__ldg(r1 + 3 + c)));
+    };
+    v[k] = bil(0);
+    sum += v[k];
+    if (JAC) {
+      const T dpx = (b0 - px * b2) * inv_z, dpy = (b1 - py * b2) * inv_z;
+      dv[k] = bil(1) * dpx + bil(2) * dpy;
+    }
+  }
+  if (r3dsimt::ballot(bad) != 0) return false;
+  const T n = static_cast<T>(p.n);
+  const T mean = warp_sum(sum) / n;
+  T norm2 = 0;
+#pragma unroll
+  for (int k = 0; k < PER; ++k)
+    if (sample_at(p, k).on) {
+      v[k] -= mean;
+      norm2 += v[k] * v[k];
+    }
+  norm2 = warp_sum(norm2);
+  if (!(norm2 > T(1e-6) * n)) return false;
+  const T inv_norm = T(1) / sqrt(norm2);
+  T ncc = 0;
+#pragma unroll
+  for (int k = 0; k < PER; ++k)
+    if (sample_at(p, k).on) {
+      v[k] *= inv_norm;
+      ncc += v[k] * n0[k];
+    }
+  ncc_out = warp_sum(ncc);
+  if (!JAC) return true;
+  // d(v - mean) per parameter, then dn = (I - n n^T) d(v - mean) / |v - mean|.
+  T dm[3] = {0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const SampleAt sm = sample_at(p, k);
+    if (!sm.on) continue;
+    const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
+    dm[0] += dv[k];
+    dm[1] += dv[k] * sx;
+    dm[2] += dv[k] * sy;
+  }
+  warp_sums(dm);
+  for (int i = 0; i < 3; ++i) dm[i] /= n;
+  T pr[3] = {0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const SampleAt sm = sample_at(p, k);
+    if (!sm.on) continue;
+    const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
+    pr[0] += v[k] * (dv[k] - dm[0]);
+    pr[1] += v[k] * (dv[k] * sx - dm[1]);
+    pr[2] += v[k] * (dv[k] * sy - dm[2]);
+  }
+  warp_sums(pr);
+  T acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const SampleAt sm = sample_at(p, k);
+    if (!sm.on) continue;
+    const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
+    const T ns = v[k];
+    const T j0 = ((dv[k] - dm[0]) - ns * pr[0]) * inv_norm;
+    const T j1 = ((dv[k] * sx - dm[1]) - ns * pr[1]) * inv_norm;
+    const T j2 = ((dv[k] * sy - dm[2]) - ns * pr[2]) * inv_norm;
+    const T e = ns - n0[k];
+    acc[0] += j0 * j0;
+    acc[1] += j0 * j1;
+    acc[2] += j0 * j2;
+    acc[3] += j1 * j1;
+    acc[4] += j1 * j2;
+    acc[5] += j2 * j2;
+    acc[6] += j0 * e;
+    acc[7] += j1 * e;
+    acc[8] += j2 * e;
+  }
+  warp_sums(acc);
+  for (int i = 0; i < 6; ++i) hh[i] = acc[i];
+  for (int i = 0; i < 3; ++i) gg[i] = acc[6 + i];
+  return true;
+}
+
+// refinement.cpp:155-165: pixels of motion in the view per unit of inverse depth.
+R3D_DEVICE double centre_motion(const ViewGeo& g, double x, double y, double w) {
+  const double h0 = row3(g.m, 0, x, y, 1.0) + g.b[0] * w;
+  const double h1 = row3(g.m, 1, x, y, 1.0) + g.b[1] * w;
+  const double h2 = row3(g.m, 2, x, y, 1.0) + g.b[2] * w;
+  if (!(h2 > 0.0)) return 0.0;
+  const double px = h0 / h2, py = h1 / h2;
+  return hypot(g.b[0] - px * g.b[2], g.b[1] - py * g.b[2]) / h2;
+}
+
+// refinement.cpp:167-196: inverse-depth slope from the neighbours at +-1.
+R3D_DEVICE double initial_slope(const float* depth, int w, int h, int x, int y, int ax, int ay) {
+  const float z = depth[static_cast<int64_t>(y) * w + x];
+  auto neighbour = [&](int k, double& wn) {
+    const int nx = x + k * ax, ny = y + k * ay;
+    if (nx < 0 || ny < 0 || nx >= w || ny >= h) return false;
+    const float zn = depth[static_cast<int64_t>(ny) * w + nx];
+    if (!(zn > 0.0F) || static_cast<double>(fabsf(zn - z)) > kDiscontinuity * static_cast<double>(fminf(z, zn)))
+      return false;
+    wn = 1.0 / zn;
+    return true;
+  };
+  double wp = 0.0, wm = 0.0;
+  const bool pl = neighbour(1, wp);
+  const bool mi = neighbour(-1, wm);
+  const double w0 = 1.0 / z;
+  if (pl && mi) return 0.5 * (wp - wm);
+  if (pl) return wp - w0;
+  if (mi) return w0 - wm;
+  return 0.0;
+}
+
+// delta = -(H (1 + 1e-6 on the diagonal) + 1e-12 I)^-1 g by LDL^T with
+// symmetric diagonal pivoting (the largest remaining diagonal first).
+R3D_DEVICE void solve_damped(const double* hh, const double* gg, double* delta) {
+  double a[3][3] = {{hh[0], hh[1], hh[2]}, {hh[1], hh[3], hh[4]}, {hh[2], hh[4], hh[5]}};
+  for (int i = 0; i < 3; ++i) a[i][i] = a[i][i] * (1.0 + 1e-6) + 1e-12;
+  int perm[3] = {0, 1, 2};
+  double l[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}, d[3];
+  for (int k = 0; k < 3; ++k) {
+    int piv = k;
+    for (int i = k + 1; i < 3; ++i)
+      if (fabs(a[i][i]) > fabs(a[piv][piv])) piv = i;
+    if (piv != k) {
+      for (int j = 0; j < 3; ++j) {
+        const double t = a[k][j];
+        a[k][j] = a[piv][j];
+        a[piv][j] = t;
+      }
+      for (int i = 0; i < 3; ++i) {
+        const double t = a[i][k];
+        a[i][k] = a[i][piv];
+        a[i][piv] = t;
+      }
+      for (int j = 0; j < k; ++j) {
+        const double t = l[k][j];
+        l[k][j] = l[piv][j];
+        l[piv][j] = t;
+      }
+      const int t = perm[k];
+      perm[k] = perm[piv];
+      perm[piv] = t;
+    }
+    d[k] = a[k][k];
+    for (int i = k + 1; i < 3; ++i) l[i][k] = d[k] != 0.0 ? a[i][k] / d[k] : 0.0;
+    for (int i = k + 1; i < 3; ++i)
+      for (int j = k + 1; j <= i; ++j) {
+        a[i][j] -= l[i][k] * d[k] * l[j][k];
+        a[j][i] = a[i][j];
+      }
+  }
+  double y[3];
+  for (int i = 0; i < 3; ++i) {
+    y[i] = gg[perm[i]];
+    for (int j = 0; j < i; ++j) y[i] -= l[i][j] * y[j];
+  }
+  for (int i = 0; i < 3; ++i) y[i] = d[i] != 0.0 ? y[i] / d[i] : 0.0;
+  for (int i = 2; i >= 0; --i)
+    for (int j = i + 1; j < 3; ++j) y[i] -= l[j][i] * y[j];
+  for (int i = 0; i < 3; ++i) delta[perm[i]] = -y[i];
+}
+
+template <class T, int PER>
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
+    refine_kernel(const float* R3D_RESTRICT input, float* depth, float* conf, int64_t stride,
+                  const float* R3D_RESTRICT base, int64_t bstride, const ViewGeo* R3D_RESTRICT views, Params p,
+                  unsigned long long* counters) {
+  const int64_t pix = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (pix >= static_cast<int64_t>(p.width) * p.height) return;  // whole warp
+  const bool lead = r3dsimt::lane_id() == 0;
+  const int y = static_cast<int>(pix / p.width), x = static_cast<int>(pix - static_cast<int64_t>(y) * p.width);
+  const float z0 = input[pix];
+  if (!(z0 > 0.0F)) return;
+  const int64_t at = static_cast<int64_t>(y) * stride + x;
+  if (lead) {
+    atomicAdd(counters + kInput, 1ULL);
+    conf[at] = 0.0F;
+  }
+  const int r = p.radius;
+  if (p.num_views == 0 || x < r || y < r || x >= p.width - r || y >= p.height - r) return;
+
+  // Normalised base window.
+  T n0[PER];
+  T sum = 0;
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const SampleAt sm = sample_at(p, k);
+    n0[k] = sm.on ? static_cast<T>(base[static_cast<int64_t>(y + sm.dy) * bstride + 3 * (x + sm.dx)]) : T(0);
+    sum += n0[k];
+  }
+  const T mean = warp_sum(sum) / static_cast<T>(p.n);
+  T norm2 = 0;
+#pragma unroll
+  for (int k = 0; k < PER; ++k)
+    if (sample_at(p, k).on) {
+      n0[k] -= mean;
+      norm2 += n0[k] * n0[k];
+    }
+  norm2 = warp_sum(norm2);
+  if (static_cast<double>(norm2) < p.min_texture2n) return;
+  const T inv_norm = T(1) / sqrt(norm2);
+#pragma unroll
+  for (int k = 0; k < PER; ++k) n0[k] *= inv_norm;
+
+  const double w0 = 1.0 / z0;
+  const double theta0[3] = {w0, r * initial_slope(input, p.width, p.height, x, y, 1, 0),
+                            r * initial_slope(input, p.width, p.height, x, y, 0, 1)};
+  const double xd = x, yd = y;
+
+  // Local view selection at the initial plane.
+  int used[kMaxViews];
+  int m = 0;
+  double s0 = 0.0;
+  T hh_t[6], gg_t[3];
+  for (int j = 0; j < p.num_views; ++j) {
+    T ncc;
+    if (evaluate_view<T, PER, false>(views[j], xd, yd, theta0, p, n0, ncc, hh_t, gg_t) &&
+        static_cast<double>(ncc) >= p.min_ncc) {
+      used[m++] = j;
+      s0 += static_cast<double>(ncc);
+    }
+  }
+  if (m == 0) {
+    if (p.drop_unconfirmed && lead) {
+      depth[at] = 0.0F;
+      atomicAdd(counters + kUnconfirmed, 1ULL);
+    }
+    return;
+  }
+  s0 /= m;
+  if (lead) conf[at] = static_cast<float>(s0);
+  double max_motion = 0.0;
+  for (int t = 0; t < m; ++t) max_motion = fmax(max_motion, centre_motion(views[used[t]], xd, yd, w0));
+
+  // Mean NCC and Gauss-Newton terms over the used views; -inf if a view drops out.
+  auto evaluate = [&](const double* theta, double* hh, double* gg) {
+    for (int i = 0; i < 6; ++i) hh[i] = 0.0;
+    for (int i = 0; i < 3; ++i) gg[i] = 0.0;
+    double score = 0.0;
+    for (int t = 0; t < m; ++t) {
+      T ncc;
+      if (!evaluate_view<T, PER, true>(views[used[t]], xd, yd, theta, p, n0, ncc, hh_t, gg_t))
+        return -__builtin_huge_val();
+      score += static_cast<double>(ncc);
+      for (int i = 0; i < 6; ++i) hh[i] += static_cast<double>(hh_t[i]);
+      for (int i = 0; i < 3; ++i) gg[i] += static_cast<double>(gg_t[i]);
+    }
+    return score / m;
+  };
+
+  double hh[6], gg[3];
+  double best[3] = {theta0[0], theta0[1], theta0[2]};
+  double best_score = evaluate(best, hh, gg);
+  if (!finite_d(best_score)) return;
+  double scale = 1.0;
+  for (int it = 0; it < p.iterations; ++it) {
+    double delta[3];
+    solve_damped(hh, gg, delta);
+    if (!(finite_d(delta[0]) && finite_d(delta[1]) && finite_d(delta[2]))) break;
+    // At most one pixel of motion per step at the window border.
+    const double motion = max_motion * ((fabs(delta[0]) + fabs(delta[1])) + fabs(delta[2]));
+    if (motion > 1.0)
+      for (int i = 0; i < 3; ++i) delta[i] /= motion;
+    for (int i = 0; i < 3; ++i) delta[i] *= scale;
+    if (max_motion * ((fabs(delta[0]) + fabs(delta[1])) + fabs(delta[2])) < 1e-3) break;
+    double h2[6], g2[3];
+    const double cand[3] = {best[0] + delta[0], best[1] + delta[1], best[2] + delta[2]};
+    const double score = evaluate(cand, h2, g2);
+    if (score > best_score) {
+      for (int i = 0; i < 3; ++i) best[i] = cand[i];
+      best_score = score;
+      for (int i = 0; i < 6; ++i) hh[i] = h2[i];
+      for (int i = 0; i < 3; ++i) gg[i] = g2[i];
+      scale = 1.0;
+    } else {
+      scale *= 0.25;
+    }
+  }
+  if (best_score > s0 + p.min_gain && best[0] > 0.0 && max_motion * fabs(best[0] - w0) <= p.max_shift_px) {
+    if (lead) {
+      depth[at] = static_cast<float>(1.0 / best[0]);
+      conf[at] = static_cast<float>(best_score);
+      atomicAdd(counters + kRefined, 1ULL);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ refinement images
+// refinement.cpp:198-238: separable Gaussian, taps (normalised floats) from the host.
+R3D_GLOBAL void blur_rows_kernel(const float* in, int64_t istride, int w, int h, const float* taps, int r,
+                                 float* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const float* row = in + static_cast<int64_t>(y) * istride;
+  float acc = 0.0F;
+  for (int i = -r; i <= r; ++i) {
+    const int xx = x + i < 0 ? 0 : (x + i > w - 1 ? w - 1 : x + i);
+    acc = __fadd_rn(acc, __fmul_rn(taps[i + r], row[xx]));
+  }
+  out[static_cast<int64_t>(y) * w + x] = acc;
+}
+
+R3D_GLOBAL void blur_cols_kernel(const float* in, int w, int h, const float* taps, int r, float* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  float acc = 0.0F;
+  for (int i = -r; i <= r; ++i) {
+    const int yy = y + i < 0 ? 0 : (y + i > h - 1 ? h - 1 : y + i);
+    acc = __fadd_rn(acc, __fmul_rn(taps[i + r], in[static_cast<int64_t>(yy) * w + x]));
+  }
+  out[static_cast<int64_t>(y) * w + x] = acc;
+}
+
+// refinement.cpp:249-266: intensity and central-difference derivatives.
+R3D_GLOBAL void gradient_kernel(const float* gray, int64_t gstride, int w, int h, float* out, int64_t ostride) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const float* row = gray + static_cast<int64_t>(y) * gstride;
+  const float* up = gray + static_cast<int64_t>(y > 0 ? y - 1 : 0) * gstride;
+  const float* down = gray + static_cast<int64_t>(y < h - 1 ? y + 1 : h - 1) * gstride;
+  const float sy = (y > 0 && y < h - 1) ? 0.5F : 1.0F;
+  const int xl = x > 0 ? x - 1 : 0, xr = x < w - 1 ? x + 1 : w - 1;
+  float* o = out + static_cast<int64_t>(y) * ostride + 3 * x;
+  o[0] = row[x];
+  o[1] = __fdiv_rn(__fsub_rn(row[xr], row[xl]), static_cast<float>(xr - xl > 1 ? xr - xl : 1));
+  o[2] = __fmul_rn(__fsub_rn(down[x], up[x]), h > 1 ? sy : 0.0F);
+}
+
+// ------------------------------------------------------------------ host side
+struct Scratch {
+  DeviceBuffer<unsigned long long> counters;
+  DeviceBuffer<float> input, blur_tmp, blur_out, taps;
+  DeviceBuffer<ViewGeo> views;
+};
+
+Scratch& scratch() {
+  thread_local Scratch s;
+  s.counters.reserve(kCounters);
+  s.views.reserve(kMaxViews);
+  return s;
+}
+
+template <class F>
+r3dgpu_status guard(F&& f) {
+  try {
+    set_thread_error("");
+    f();
+    return R3DGPU_OK;
+  } catch (const Error& e) {
+    set_thread_error(e.what());
+    return e.status;
+  } catch (const std::exception& e) {
+    set_thread_error(e.what());
+    return R3DGPU_EDEVICE;
+  }
+}
+
+// Row-major 3x3 products in the reference's left-to-right order.
+void mat3(const double* a, const double* b, double* out) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) out[3 * i + j] = (a[3 * i] * b[j] + a[3 * i + 1] * b[3 + j]) + a[3 * i + 2] * b[6 + j];
+}
+
+// refinement.cpp:297-309.
+ViewGeo view_geometry(const r3dgpu_pinhole_camera& c0, const r3dgpu_refinement_image& v) {
+  const r3dgpu_pinhole_camera& cj = v.camera;
+  const double kj[9] = {cj.intrinsics.fx, 0.0, cj.intrinsics.cx, 0.0, cj.intrinsics.fy, cj.intrinsics.cy,
+                        0.0, 0.0, 1.0};
+  double r0t[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r0t[3 * i + j] = c0.rotation[3 * j + i];
+  double kr[9], krr[9];
+  ViewGeo g{};
+  mat3(kj, cj.rotation, kr);
+  mat3(kr, r0t, krr);
+  mat3(krr, c0.k_inv, g.m);
+  const double dc[3] = {c0.center[0] - cj.center[0], c0.center[1] - cj.center[1], c0.center[2] - cj.center[2]};
+  for (int i = 0; i < 3; ++i) g.b[i] = (kr[3 * i] * dc[0] + kr[3 * i + 1] * dc[1]) + kr[3 * i + 2] * dc[2];
+  g.data = v.data;
+  g.stride = v.stride;
+  g.width = cj.intrinsics.width;
+  g.height = cj.intrinsics.height;
+  return g;
+}
+
+r3dgpu_refinement_options options_or_default(const r3dgpu_refinement_options* o) {
+  r3dgpu_refinement_options out{};
+  if (o != nullptr) return *o;
+  r3dgpu_default_refinement_options(&out);
+  return out;
+}
+
+template <class T, int PER>
+void launch_refine(const float* input, float* depth, float* conf, int64_t stride, const float* base,
+                   int64_t bstride, const ViewGeo* views, const Params& p, unsigned long long* counters,
+                   cudaStream_t s) {
+  const int64_t warps = static_cast<int64_t>(p.width) * p.height;
+  auto kernel = refine_kernel<T, PER>;
+  R3D_LAUNCH(kernel, static_cast<unsigned>(ceil_div64(warps, 8)), 256, 0, s, input, depth, conf, stride, base, bstride,
+             views, p, counters);
+  launched(sizeof(T) == 8 ? "refine_kernel<f64>" : "refine_kernel<f32>");
+}
+
+template <class T>
+void launch_refine_t(int per, const float* input, float* depth, float* conf, int64_t stride, const float* base,
+                     int64_t bstride, const ViewGeo* views, const Params& p, unsigned long long* counters,
+                     cudaStream_t s) {
+  if (per <= 1)
+    launch_refine<T, 1>(input, depth, conf, stride, base, bstride, views, p, counters, s);
+  else if (per <= 2)
+    launch_refine<T, 2>(input, depth, conf, stride, base, bstride, views, p, counters, s);
+  else if (per <= 4)
+    launch_refine<T, 4>(input, depth, conf, stride, base, bstride, views, p, counters, s);
+  else
+    launch_refine<T, 8>(input, depth, conf, stride, base, bstride, views, p, counters, s);
+}
+
+void refine(float* depth, float* conf, int64_t stride, const r3dgpu_pinhole_camera& cam, int w, int h,
+            const r3dgpu_refinement_image& base, const r3dgpu_refinement_image* views, int num_views,
+            const r3dgpu_refinement_options& o, r3dgpu_refinement_stats* stats, cudaStream_t s) {
+  if (o.radius < 1 || o.step < 1 || o.iterations < 0)
+    fail(R3DGPU_EINVAL, "refinement: invalid window (radius " + std::to_string(o.radius) + ", step " +
+                            std::to_string(o.step) + ") or iterations " + std::to_string(o.iterations));
+  if (base.camera.intrinsics.width != w || base.camera.intrinsics.height != h || base.data == nullptr ||
+      base.stride < 3LL * w)
+    fail(R3DGPU_EINVAL, "refinement: base image does not match the depth map");
+  if (w < 0 || h < 0 || (w > 0 && h > 0 && (depth == nullptr || conf == nullptr || stride < w)))
+    fail(R3DGPU_EINVAL, "refinement: bad depth map");
+  const int side = 2 * o.radius / o.step + 1;
+  const int n = side * side;
+  if (n > kMaxSamples)
+    fail(R3DGPU_EINVAL, "refinement: window of " + std::to_string(n) + " samples (at most 225)");
+  if (num_views < 0 || (num_views > 0 && views == nullptr)) fail(R3DGPU_EINVAL, "refinement: null views");
+  const int nv = std::min(num_views, std::min(o.max_views, kMaxViews));
+  Scratch& sc = scratch();
+  ViewGeo geo[kMaxViews];
+  for (int j = 0; j < nv; ++j) {
+    const r3dgpu_refinement_image& v = views[j];
+    if (v.data == nullptr || v.camera.intrinsics.width < 2 || v.camera.intrinsics.height < 2 ||
+        v.stride < 3LL * v.camera.intrinsics.width)
+      fail(R3DGPU_EINVAL, "refinement: view " + std::to_string(j) + " has no image");
+    geo[j] = view_geometry(cam, v);
+  }
+  R3D_CUDA(cudaMemsetAsync(sc.counters.get(), 0, sizeof(unsigned long long) * kCounters, s));
+  if (w > 0 && h > 0) {
+    if (nv > 0)
+      R3D_CUDA(cudaMemcpyAsync(sc.views.get(), geo, sizeof(ViewGeo) * nv, cudaMemcpyHostToDevice, s));
+    sc.input.reserve(static_cast<size_t>(w) * h);
+    R3D_CUDA(cudaMemcpy2DAsync(sc.input.get(), sizeof(float) * w, depth, sizeof(float) * stride, sizeof(float) * w,
+                               h, cudaMemcpyDeviceToDevice, s));
+    Params p{w, h, o.radius, o.step, side, n, o.iterations, nv, o.min_ncc, o.max_shift_px, o.min_gain,
+             o.min_texture * o.min_texture * n, o.drop_unconfirmed};
+    const int per = (n + 31) / 32;
+    if (o.fp32)
+      launch_refine_t<float>(per, sc.input.get(), depth, conf, stride, base.data, base.stride, sc.views.get(), p,
+                             sc.counters.get(), s);
+    else
+      launch_refine_t<double>(per, sc.input.get(), depth, conf, stride, base.data, base.stride, sc.views.get(), p,
+                              sc.counters.get(), s);
+  }
+  unsigned long long c[kCounters];
+  R3D_CUDA(cudaMemcpyAsync(c, sc.counters.get(), sizeof(c), cudaMemcpyDeviceToHost, s));
+  R3D_CUDA(cudaStreamSynchronize(s));
+  if (stats != nullptr) *stats = r3dgpu_refinement_stats{c[kInput], c[kRefined], c[kInput] - c[kRefined] - c[kUnconfirmed],
+                                                         c[kUnconfirmed]};
+}
+
+void make_image(const float* gray, int64_t gstride, int w, int h, double sigma, float* out, int64_t ostride,
+                cudaStream_t s) {
+  if (w < 0 || h < 0 || (w > 0 && h > 0 && (gray == nullptr || out == nullptr || gstride < w || ostride < 3LL * w)))
+    fail(R3DGPU_EINVAL, "refinement image: bad size, stride or pointer");
+  if (w == 0 || h == 0) return;
+  const dim3 b(32, 8), g(static_cast<unsigned>(ceil_div(w, 32)), static_cast<unsigned>(ceil_div(h, 8)));
+  const float* src = gray;
+  int64_t sstride = gstride;
+  if (sigma > 0.0) {
+    // refinement.cpp:200-210: taps up to 3 sigma, normalised in float.
+    const int r = std::max(1, static_cast<int>(std::ceil(3.0 * sigma)));
+    std::vector<float> k(static_cast<size_t>(2 * r + 1));
+    float ksum = 0.0F;
+    for (int i = -r; i <= r; ++i) {
+      k[i + r] = static_cast<float>(std::exp(-0.5 * i * i / (sigma * sigma)));
+      ksum += k[i + r];
+    }
+    for (float& v : k) v /= ksum;
+    Scratch& sc = scratch();
+    sc.taps.reserve(k.size());
+    sc.blur_tmp.reserve(static_cast<size_t>(w) * h);
+    sc.blur_out.reserve(static_cast<size_t>(w) * h);
+    float* taps = sc.taps.get();
+    float* tmp = sc.blur_tmp.get();
+    float* blurred = sc.blur_out.get();
+    R3D_CUDA(cudaMemcpyAsync(taps, k.data(), sizeof(float) * k.size(), cudaMemcpyHostToDevice, s));
+    R3D_LAUNCH(blur_rows_kernel, g, b, 0, s, gray, gstride, w, h, taps, r, tmp);
+    launched("blur_rows_kernel");
+    R3D_LAUNCH(blur_cols_kernel, g, b, 0, s, tmp, w, h, taps, r, blurred);
+    launched("blur_cols_kernel");
+    src = blurred;
+    sstride = w;
+  }
+  R3D_LAUNCH(gradient_kernel, g, b, 0, s, src, sstride, w, h, out, ostride);
+  launched("gradient_kernel");
+}
+
+}  // namespace
+}  // namespace r3dgpu
+
+using namespace r3dgpu;
+
+extern "C" {
+
+void r3dgpu_default_refinement_options(r3dgpu_refinement_options* out) {
+  if (out == nullptr) return;
+  *out = r3dgpu_refinement_options{4, 2, 6, 4, 0.3, 2.0, 0.02, 1.0, 0.0, 1, 0};
+}
+
+r3dgpu_status r3dgpu_make_refinement_image(const float* gray, int64_t gray_stride, int32_t width, int32_t height,
+                                           double blur_sigma, float* out, int64_t out_stride, void* stream) {
+  return guard([&] {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    make_image(gray, gray_stride, width, height, blur_sigma, out, out_stride, s);
+    R3D_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+r3dgpu_status r3dgpu_refine_depth_map(float* depth, float* confidence, int64_t stride,
+                                      const r3dgpu_pinhole_camera* camera, int32_t width, int32_t height,
+                                      const r3dgpu_refinement_image* base, const r3dgpu_refinement_image* views,
+                                      int32_t num_views, const r3dgpu_refinement_options* options,
+                                      r3dgpu_refinement_stats* stats, void* stream) {
+  return guard([&] {
+    if (camera == nullptr || base == nullptr) fail(R3DGPU_EINVAL, "refinement: null argument");
+    refine(depth, confidence, stride, *camera, width, height, *base, views, num_views, options_or_default(options),
+           stats, static_cast<cudaStream_t>(stream));
+  });
+}
+
+r3dgpu_status r3dgpu_refine_depth_map_host(float* depth, float* confidence, int64_t stride,
+                                           const r3dgpu_pinhole_camera* camera, int32_t width, int32_t height,
+                                           const r3dgpu_refinement_image* base,
+                                           const r3dgpu_refinement_image* views, int32_t num_views,
+                                           const r3dgpu_refinement_options* options, r3dgpu_refinement_stats* stats) {
+  return guard([&] {
+    if (camera == nullptr || base == nullptr) fail(R3DGPU_EINVAL, "refinement: null argument");
+    if (num_views < 0 || (num_views > 0 && views == nullptr)) fail(R3DGPU_EINVAL, "refinement: null views");
+    if (width < 0 || height < 0 || stride < width || (width > 0 && height > 0 && (depth == nullptr || confidence == nullptr)))
+      fail(R3DGPU_EINVAL, "refinement: bad depth map");
+    const r3dgpu_refinement_options o = options_or_default(options);
+    const int nv = std::min(num_views, std::min(o.max_views, kMaxViews));
+    cudaStream_t s = nullptr;
+    auto up = [](size_t n) { return (n + 255) & ~static_cast<size_t>(255); };
+    auto image_bytes = [](const r3dgpu_refinement_image& v) {
+      return sizeof(float) * 3 * static_cast<size_t>(v.camera.intrinsics.width) * v.camera.intrinsics.height;
+    };
+    const size_t px = static_cast<size_t>(width) * height;
+    size_t bytes = 2 * up(4 * px) + up(image_bytes(*base));
+    for (int j = 0; j < nv; ++j) bytes += up(image_bytes(views[j]));
+    thread_local DeviceBuffer<unsigned char> io;
+    io.reserve(bytes > 0 ? bytes : 1);
+    unsigned char* p = io.get();
+    auto take = [&](size_t n) {
+      unsigned char* at = p;
+      p += up(n);
+      return at;
+    };
+    auto upload = [&](const r3dgpu_refinement_image& v) {
+      r3dgpu_refinement_image d = v;
+      const int vw = v.camera.intrinsics.width, vh = v.camera.intrinsics.height;
+      float* dst = reinterpret_cast<float*>(take(image_bytes(v)));
+      if (vw > 0 && vh > 0) {
+        if (v.data == nullptr || v.stride < 3LL * vw) fail(R3DGPU_EINVAL, "refinement: image without data");
+        R3D_CUDA(cudaMemcpy2DAsync(dst, sizeof(float) * 3 * vw, v.data, sizeof(float) * v.stride,
+                                   sizeof(float) * 3 * vw, vh, cudaMemcpyHostToDevice, s));
+      }
+      d.data = dst;
+      d.stride = 3LL * vw;
+      return d;
+    };
+    float* dd = reinterpret_cast<float*>(take(4 * px));
+    float* dc = reinterpret_cast<float*>(take(4 * px));
+    if (px > 0) {
+      R3D_CUDA(cudaMemcpy2DAsync(dd, 4 * static_cast<size_t>(width), depth, 4 * stride, 4 * static_cast<size_t>(width),
+                                 height, cudaMemcpyHostToDevice, s));
+      R3D_CUDA(cudaMemcpy2DAsync(dc, 4 * static_cast<size_t>(width), confidence, 4 * stride,
+                                 4 * static_cast<size_t>(width), height, cudaMemcpyHostToDevice, s));
+    }
+    const r3dgpu_refinement_image dbase = upload(*base);
+    std::vector<r3dgpu_refinement_image> dviews;
+    for (int j = 0; j < nv; ++j) dviews.push_back(upload(views[j]));
+    refine(dd, dc, width, *camera, width, height, dbase, dviews.data(), nv, o, stats, s);
+    if (px > 0) {
+      R3D_CUDA(cudaMemcpy2DAsync(depth, 4 * stride, dd, 4 * static_cast<size_t>(width), 4 * static_cast<size_t>(width),
+                                 height, cudaMemcpyDeviceToHost, s));
+      R3D_CUDA(cudaMemcpy2DAsync(confidence, 4 * stride, dc, 4 * static_cast<size_t>(width),
+                                 4 * static_cast<size_t>(width), height, cudaMemcpyDeviceToHost, s));
+    }
+    R3D_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+}  // extern "C"

@@ -175,3 +175,63 @@ def neighbour_lists(neighbours) -> tuple[np.ndarray, np.ndarray]:
         off[i + 1] = off[i] + len(nb)
     idx = np.array([j for nb in neighbours for j in nb], np.int32)
     return off, (idx if idx.size else np.zeros(1, np.int32))
+
+
+# ------------------------------------------------------------------ refinement
+class CRefinementOptions(ctypes.Structure):
+    _fields_ = [
+        ("radius", ctypes.c_int32),
+        ("step", ctypes.c_int32),
+        ("iterations", ctypes.c_int32),
+        ("max_views", ctypes.c_int32),
+        ("min_ncc", ctypes.c_double),
+        ("max_shift_px", ctypes.c_double),
+        ("min_gain", ctypes.c_double),
+        ("min_texture", ctypes.c_double),
+        ("blur_sigma", ctypes.c_double),
+        ("drop_unconfirmed", ctypes.c_int32),
+        ("fp32", ctypes.c_int32),
+    ]
+
+
+class CRefinementStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("input", "refined", "kept", "unconfirmed")]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+class CRefinementImage(ctypes.Structure):
+    _fields_ = [("camera", CPinholeCamera), ("data", ctypes.c_void_p), ("stride", ctypes.c_int64)]
+
+
+@dataclass
+class RefinementOptions:
+    """RefinementOptions, src/r3d/mvs/refinement.hpp:33-44 (same defaults);
+    fp32 computes the window terms in float."""
+
+    radius: int = 4
+    step: int = 2
+    iterations: int = 6
+    max_views: int = 4
+    min_ncc: float = 0.3
+    max_shift_px: float = 2.0
+    min_gain: float = 0.02
+    min_texture: float = 1.0
+    blur_sigma: float = 0.0
+    drop_unconfirmed: bool = True
+    fp32: bool = False
+
+    def c(self) -> CRefinementOptions:
+        return CRefinementOptions(*[int(v) if isinstance(v, bool) else v
+                                    for v in (getattr(self, f.name) for f in fields(self))])
+
+
+def c_refinement_image(img: dict, ptr) -> CRefinementImage:
+    """img: {camera, data (H x W x 3 float32)}."""
+    data = img["data"]
+    c = CRefinementImage()
+    c.camera = c_camera(img["camera"])
+    c.data = ptr(data)
+    c.stride = 3 * data.shape[1]
+    return c

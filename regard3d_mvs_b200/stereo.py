@@ -232,6 +232,44 @@ class Matcher:
         return self._single(m, lambda c, r: self.lib.r3dgpu_remove_depth_speckles(c, min_size, max_relative_step, r,
                                                                                   None))
 
+    # ---------------------------------------------------------------- depth refinement
+    # src/r3d/mvs/refinement.hpp:53-68.
+    def make_refinement_image(self, gray: np.ndarray, blur_sigma: float = 0.0) -> np.ndarray:
+        """Intensity and x / y derivatives (H x W x 3 float32) of a float image."""
+        g = np.ascontiguousarray(gray, np.float32)
+        h, w = g.shape
+        keep: list = []
+        dg = self._to_device(g, keep)
+        ptr, obj = self._empty_device((h, w, 3), keep)
+        self._check(self.lib.r3dgpu_make_refinement_image(dg, w, w, h, blur_sigma, ptr, 3 * w, None))
+        return self._to_host((ptr, obj), (h, w, 3))
+
+    def refine_depth_map(self, m: dict, base: dict, views: Sequence[dict], options=None) -> dict:
+        """Refines m["depth"] and m["confidence"] in place (host entry point).
+        base and views: {camera, data (H x W x 3 float32 refinement image)}."""
+        from .depth_maps import (CRefinementImage, CRefinementStats, RefinementOptions, c_camera,
+                                 c_refinement_image)
+
+        depth = np.ascontiguousarray(m["depth"], np.float32)
+        conf = np.ascontiguousarray(m["confidence"], np.float32) if m.get("confidence") is not None \
+            else np.zeros_like(depth)
+        h, w = depth.shape
+        host = lambda a: a.ctypes.data  # noqa: E731
+        cb = c_refinement_image({"camera": base["camera"], "data": np.ascontiguousarray(base["data"], np.float32)},
+                                host)
+        vdata = [np.ascontiguousarray(v["data"], np.float32) for v in views]
+        cv = (CRefinementImage * max(1, len(views)))()
+        for i, (v, d) in enumerate(zip(views, vdata)):
+            cv[i] = c_refinement_image({"camera": v["camera"], "data": d}, host)
+        cam = c_camera(m["camera"])
+        st = CRefinementStats()
+        o = (options or RefinementOptions()).c()
+        self._check(self.lib.r3dgpu_refine_depth_map_host(depth.ctypes.data, conf.ctypes.data, w, ctypes.byref(cam), w,
+                                                          h, ctypes.byref(cb), cv, len(views), ctypes.byref(o),
+                                                          ctypes.byref(st)))
+        m["depth"], m["confidence"] = depth, conf
+        return st.as_dict()
+
     # ---------------------------------------------------------------- batched matching
     def match_stereo_batch(self, pairs: Sequence[dict], stream: int | None = None) -> list[DisparityMap]:
         """Matches many pairs in one pass of every stage.

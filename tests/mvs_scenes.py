@@ -74,8 +74,8 @@ def plane_depth_map(cam: dict, plane: Plane, view: int, partner: int) -> dict:
 class MultiRig:
     """test_mvs.cpp:95-113."""
 
-    def __init__(self):
-        self.k = pinhole()
+    def __init__(self, scale: float = 1.0):
+        self.k = pinhole(int(320 * scale), int(240 * scale), 280.0 * scale, 161.2 * scale, 118.7 * scale)
         self.base = camera(self.k, rotation(2.0, -3.0, 1.0), (0.1, -0.2, 0.0))
         self.partners = []
         for i, off in enumerate(((0.8, 0.05, 0.1), (-0.7, 0.1, 0.0), (0.1, 0.75, -0.1))):
@@ -148,3 +148,68 @@ def copy_maps(maps):
                 c[key] = c[key].copy()
         out.append(c)
     return out
+
+
+# ------------------------------------------------------------------ refinement scenes
+def unit_orthogonal(n: np.ndarray) -> np.ndarray:
+    """A unit vector orthogonal to n (the rule of Eigen's unitOrthogonal for 3-vectors)."""
+    x, y, z = n
+    if abs(x) > 1e-12 * abs(z) or abs(y) > 1e-12 * abs(z):
+        inv = 1.0 / np.hypot(x, y)
+        return np.array([-y * inv, x * inv, 0.0])
+    inv = 1.0 / np.hypot(y, z)
+    return np.array([0.0, -z * inv, y * inv])
+
+
+WAVES = ((31.0, 7.0, 0.3), (-11.0, 23.0, 1.1), (5.0, -13.0, 2.0), (43.0, 29.0, 0.7), (-37.0, 47.0, 2.9))
+
+
+def render_plane(cam: dict, plane: Plane, phase: float) -> np.ndarray:
+    """test_mvs.cpp:386-414: smooth texture on a plane, 4 x 4 supersampled."""
+    u = unit_orthogonal(plane.normal)
+    v = np.cross(plane.normal, u)
+    h, w = cam["height"], cam["width"]
+    y, x = np.mgrid[0:h, 0:w].astype(np.float64)
+    acc = np.zeros((h, w))
+    for sy in range(4):
+        for sx in range(4):
+            px, py = x - 0.375 + 0.25 * sx, y - 0.375 + 0.25 * sy
+            d = np.stack([(px - cam["cx"]) / cam["fx"], (py - cam["cy"]) / cam["fy"], np.ones_like(px)], -1)
+            dirs = d @ cam["rotation"]
+            t = plane.intersect(cam["center"], dirs)
+            xw = cam["center"] + t[..., None] * dirs - plane.point
+            pu, pv = xw @ u, xw @ v
+            for kx, ky, ph in WAVES:
+                acc += np.sin(kx * pu + ky * pv + ph + phase)
+    return (128.0 + 20.0 * acc / 16.0).astype(np.float32)
+
+
+def refinement_scene(make_image, scale: int = 1):
+    """test_mvs.cpp:431-467 (at scale 1): the rig's base view cropped to its
+    central 160 x 120, a plane at 42 degrees, rendered views, and an SGM-like input
+    (constant depth per 4 x 4 block times a smooth error of up to 1 %).
+    make_image(gray) builds a refinement image. Returns (map, truth, base,
+    views, wrong_views)."""
+    rig = MultiRig(scale)
+    cam0 = dict(rig.base, width=160 * scale, height=120 * scale, cx=rig.base["cx"] - 80.0 * scale,
+                cy=rig.base["cy"] - 60.0 * scale)
+    vd = view_direction(rig.base)
+    n = vd + rig.base["rotation"].T @ np.array([0.8, 0.4, 0.0])
+    plane = Plane(n / np.linalg.norm(n), rig.base["center"] + 5.0 * vd)
+    truth = plane_depth_map(cam0, plane, 0, 1)
+    base = {"camera": cam0, "data": make_image(render_plane(cam0, plane, 0.0))}
+    views = [{"camera": p, "data": make_image(render_plane(p, plane, 0.0))} for p in rig.partners]
+    wrong = [{"camera": p, "data": make_image(render_plane(p, plane, 1.7))} for p in rig.partners]
+    h, w = truth["depth"].shape
+    y, x = np.mgrid[0:h, 0:w]
+    block = truth["depth"][np.minimum(y // 4 * 4 + 2, h - 1), np.minimum(x // 4 * 4 + 2, w - 1)]
+    depth = (block * (1.0 + 0.01 * np.sin(x / 9.0) * np.cos(y / 13.0)).astype(np.float32)).astype(np.float32)
+    m = {"camera": cam0, "depth": depth, "confidence": truth["confidence"].copy()}
+    return m, truth, base, views, wrong
+
+
+def relative_depth_rms(m: dict, truth: dict, border: int) -> float:
+    """test_mvs.cpp:416-428."""
+    d = m["depth"][border:-border, border:-border].astype(np.float64)
+    t = truth["depth"][border:-border, border:-border].astype(np.float64)
+    return float(np.sqrt(np.mean(((d - t) / t) ** 2)))
