@@ -60,9 +60,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine", "rectify"), default="batch64",
-                    help="combine / rectify: only the multi-view combination of one view / the rectification "
-                         "resampling of one pair (each its own JSON line)")
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine", "rectify", "depth"),
+                    default="batch64",
+                    help="combine / rectify / depth: only the multi-view combination of one view / the "
+                         "rectification resampling of one pair / the depth stage after the combination "
+                         "(refinement and consistency of 8 views; each its own JSON line)")
     ap.add_argument("--pairs", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-per-pair", action="store_true")
@@ -436,6 +438,201 @@ def measure_rectify(lib, dev, stream, steps: int, warmup: int, peak: float) -> d
                              "kind": "port", "sample": "one image of the pair, once"}}
 
 
+# Depth stage after the combination (config 4's refinement and consistency):
+# 8 views of 2048 x 1536, each refined against its 4 nearest views with a
+# 7 x 7 window (radius 3, step 1), then one consistency filter of all 8 maps
+# (4 neighbours each). Algorithmic bytes per view: its refinement image and
+# the 4 partners' (12 B per pixel each), depth and confidence in and out
+# (16 B per pixel), the consistency pass over depth, pair mask, colour and
+# support (about 20 B per pixel): about 96 B per pixel.
+DEPTH_VIEWS, DEPTH_W, DEPTH_H = 8, 2048, 1536
+DEPTH_BYTES_PER_PIXEL = 96
+DEPTH_CROP = (512, 384)
+
+
+def measure_depth(lib, dev, stream, steps: int, warmup: int, peak: float) -> dict:
+    """Device time of the depth stage of 8 views (float and double refinement
+    paths), end-to-end time through the host entry points, the float path's
+    depth error against the double-precision oracle, and the oracle's time,
+    both on a crop of one view."""
+    import torch
+
+    from oracle import oracle as orc
+    from regard3d_mvs_b200.depth_maps import (CConsistencyStats, CDepthMap, ConsistencyOptions, CRefinementImage,
+                                              CRefinementStats, RefinementOptions, c_camera, neighbour_lists)
+    from regard3d_mvs_b200.multi_view import depth_stage_scene
+
+    scene = depth_stage_scene(DEPTH_VIEWS, DEPTH_W, DEPTH_H)
+    views, partners = scene["views"], scene["partners"]
+    n, w, h = len(views), DEPTH_W, DEPTH_H
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    cams = [c_camera(v["camera"]) for v in views]
+    images = []
+    for v in views:
+        g = torch.from_numpy(v["gray"]).to(dev)
+        img = torch.empty((h, w, 3), dtype=torch.float32, device=dev)
+        _native_check(lib, lib.r3dgpu_make_refinement_image(g.data_ptr(), w, w, h, 0.0, img.data_ptr(), 3 * w, sptr))
+        images.append(img)
+    rimg = []
+    for i in range(n):
+        r = CRefinementImage()
+        r.camera, r.data, r.stride = cams[i], images[i].data_ptr(), 3 * w
+        rimg.append(r)
+    partner_arr = []
+    for i in range(n):
+        arr = (CRefinementImage * len(partners[i]))()
+        for k, j in enumerate(partners[i]):
+            arr[k] = rimg[j]
+        partner_arr.append(arr)
+    pristine = [torch.from_numpy(v["depth"]).to(dev) for v in views]
+    depth = [torch.empty_like(d) for d in pristine]
+    conf = [torch.zeros_like(d) for d in pristine]
+    mask = [torch.full((h, w), 1, dtype=torch.int16, device=dev) for _ in views]
+    support = [torch.zeros((h, w), dtype=torch.uint8, device=dev) for _ in views]
+    color = [torch.from_numpy(v["color"]).to(dev) for v in views]
+    maps = (CDepthMap * n)()
+    for i, v in enumerate(views):
+        mp = maps[i]
+        mp.camera = cams[i]
+        mp.depth, mp.confidence = depth[i].data_ptr(), conf[i].data_ptr()
+        mp.pair_mask, mp.support, mp.color = mask[i].data_ptr(), support[i].data_ptr(), color[i].data_ptr()
+        mp.stride, mp.color_stride, mp.width, mp.height = w, 3 * w, w, h
+        mp.view, mp.num_partners = i, len(partners[i])
+        for k, j in enumerate(partners[i]):
+            mp.partners[k] = j
+    off, idx = neighbour_lists(partners)
+    copts = ConsistencyOptions().c()
+    rstats, cstats = CRefinementStats(), CConsistencyStats()
+
+    def step(opts):
+        for i in range(n):
+            depth[i].copy_(pristine[i])
+        for i in range(n):
+            _native_check(lib, lib.r3dgpu_refine_depth_map(depth[i].data_ptr(), conf[i].data_ptr(), w,
+                                                           ctypes.byref(cams[i]), w, h, ctypes.byref(rimg[i]),
+                                                           partner_arr[i], len(partners[i]), ctypes.byref(opts),
+                                                           ctypes.byref(rstats), sptr))
+        _native_check(lib, lib.r3dgpu_filter_depth_maps(maps, n, off.ctypes.data, idx.ctypes.data,
+                                                        ctypes.byref(copts), ctypes.byref(cstats), sptr))
+
+    def timed(opts):
+        for _ in range(warmup):
+            step(opts)
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = int(lib.r3dgpu_launch_count())
+        a.record(stream)
+        for _ in range(steps):
+            step(opts)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / steps, (int(lib.r3dgpu_launch_count()) - l0) // steps
+
+    f32 = RefinementOptions(radius=3, step=1, fp32=True).c()
+    f64 = RefinementOptions(radius=3, step=1).c()
+    ms32, launches = timed(f32)
+    refine_stats, filter_stats = rstats.as_dict(), cstats.as_dict()
+    ms64, _ = timed(f64)
+    # Refinement alone (float path), for the kernel's share.
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for i in range(n):
+        depth[i].copy_(pristine[i])
+    torch.cuda.synchronize(dev)
+    a.record(stream)
+    for i in range(n):
+        _native_check(lib, lib.r3dgpu_refine_depth_map(depth[i].data_ptr(), conf[i].data_ptr(), w,
+                                                       ctypes.byref(cams[i]), w, h, ctypes.byref(rimg[i]),
+                                                       partner_arr[i], len(partners[i]), ctypes.byref(f32),
+                                                       ctypes.byref(rstats), sptr))
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    refine_ms = a.elapsed_time(b) / n
+
+    # End to end through the host entry points (host maps and images, copies inside).
+    himg = [im.cpu().numpy() for im in images]
+    hrimg = []
+    for i in range(n):
+        r = CRefinementImage()
+        r.camera, r.data, r.stride = cams[i], himg[i].ctypes.data, 3 * w
+        hrimg.append(r)
+    hpartner = []
+    for i in range(n):
+        arr = (CRefinementImage * len(partners[i]))()
+        for k, j in enumerate(partners[i]):
+            arr[k] = hrimg[j]
+        hpartner.append(arr)
+    hdepth = [np.empty((h, w), np.float32) for _ in views]
+    hconf = [np.zeros((h, w), np.float32) for _ in views]
+    hmask = [np.ones((h, w), np.uint16) for _ in views]
+    hsup = [np.zeros((h, w), np.uint8) for _ in views]
+    hmaps = (CDepthMap * n)()
+    for i, v in enumerate(views):
+        hmaps[i] = maps[i]
+        hmaps[i].depth, hmaps[i].confidence = hdepth[i].ctypes.data, hconf[i].ctypes.data
+        hmaps[i].pair_mask, hmaps[i].support, hmaps[i].color = hmask[i].ctypes.data, hsup[i].ctypes.data, \
+            v["color"].ctypes.data
+
+    def host_step():
+        for i in range(n):
+            hdepth[i][...] = views[i]["depth"]
+            _native_check(lib, lib.r3dgpu_refine_depth_map_host(hdepth[i].ctypes.data, hconf[i].ctypes.data, w,
+                                                                ctypes.byref(cams[i]), w, h, ctypes.byref(hrimg[i]),
+                                                                hpartner[i], len(partners[i]), ctypes.byref(f32),
+                                                                ctypes.byref(rstats)))
+        _native_check(lib, lib.r3dgpu_filter_depth_maps_host(hmaps, n, off.ctypes.data, idx.ctypes.data,
+                                                             ctypes.byref(copts), ctypes.byref(cstats)))
+
+    host_step()
+    t0 = time.perf_counter()
+    for _ in range(max(1, steps // 2)):
+        host_step()
+    e2e_s = (time.perf_counter() - t0) / max(1, steps // 2)
+    img_bytes = 12 * w * h
+    h2d = n * (img_bytes * (1 + len(partners[0])) + 8 * w * h) + n * (4 + 4 + 2 + 3) * w * h
+    d2h = n * 8 * w * h + n * 5 * w * h
+
+    # The float path's error and the oracle's time on a crop of view 0.
+    cw, ch = DEPTH_CROP
+    x0, y0 = (w - cw) // 2, (h - ch) // 2
+    cam0 = dict(views[0]["camera"], width=cw, height=ch, cx=views[0]["camera"]["cx"] - x0,
+                cy=views[0]["camera"]["cy"] - y0)
+    crop_img = np.ascontiguousarray(himg[0][y0:y0 + ch, x0:x0 + cw])
+    base = {"camera": cam0, "data": crop_img}
+    pviews = [{"camera": views[j]["camera"], "data": himg[j]} for j in partners[0]]
+    crop = {"camera": cam0, "depth": np.ascontiguousarray(views[0]["depth"][y0:y0 + ch, x0:x0 + cw]),
+            "confidence": np.zeros((ch, cw), np.float32)}
+    from regard3d_mvs_b200.stereo import Matcher
+
+    mm = Matcher(device=dev.index or 0)
+    g32 = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in crop.items()}
+    mm.refine_depth_map(g32, base, pviews, RefinementOptions(radius=3, step=1, fp32=True))
+    o64 = {k: (v.copy() if isinstance(v, np.ndarray) else v) for k, v in crop.items()}
+    t0 = time.perf_counter()
+    ost = orc.refine_depth_map(o64, base, pviews, RefinementOptions(radius=3, step=1))
+    cpu_s = time.perf_counter() - t0
+    both = (g32["depth"] > 0) & (o64["depth"] > 0)
+    rel = np.abs(g32["depth"][both].astype(np.float64) - o64["depth"][both]) / o64["depth"][both]
+    flips = int(((g32["depth"] > 0) != (o64["depth"] > 0)).sum())
+    achieved = DEPTH_BYTES_PER_PIXEL * w * h / (ms32 / n * 1e-3) / 1e9
+    return {"workload": f"depth stage: {n} views {w}x{h}, refinement 7x7 (radius 3, step 1) against 4 views, "
+                        "consistency over 4 neighbours",
+            "value": n / (ms32 * 1e-3), "unit": "depth maps/s", "ms_per_step": ms32, "dtype": "f32 window terms",
+            "f64_path": {"value": n / (ms64 * 1e-3), "ms_per_step": ms64},
+            "refine_ms_per_view_f32": refine_ms, "gpu_launches": launches,
+            "refinement": refine_stats, "consistency": filter_stats,
+            "fp32_vs_f64_oracle": {"sample": f"{cw}x{ch} crop of view 0", "pixels_compared": int(both.sum()),
+                                   "decision_flips": flips, "rel_depth_error_p50": float(np.percentile(rel, 50)),
+                                   "p99": float(np.percentile(rel, 99)), "max": float(rel.max())},
+            "e2e": {"value": n / e2e_s, "unit": "depth maps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "alg_bytes_per_pixel": DEPTH_BYTES_PER_PIXEL},
+            "cpu_baseline": {"value": (cw * ch) / cpu_s / (w * h), "unit": "depth maps/s (refinement only)",
+                             "cores": orc.max_threads(), "kind": "port",
+                             "sample": f"double-precision refinement of a {cw}x{ch} crop of view 0, scaled to "
+                                       f"{w}x{h}", "refined": ost["refined"]}}
+
+
 SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
 SERVE_REQUEST_BUDGET = 118 << 30  # config 3's 150 GB: 118 GB for admitted requests + 2 x 16 GB worker scratch
 SERVE_WORKERS = 2
@@ -557,6 +754,14 @@ def main():
         if rank == 0:
             print(json.dumps(dict(r, metric="combine_pairs Gpixels/s", n_gpus=world, steps=args.steps,
                                   warmup=args.warmup, higher_is_better=True, data="synthetic")), flush=True)
+        return
+    if args.workload == "depth":
+        peak, _ = measured_peaks()
+        dev0 = torch.device(f"cuda:{local}")
+        r = measure_depth(lib, dev0, torch.cuda.current_stream(dev0), args.steps, args.warmup, peak)
+        if rank == 0:
+            print(json.dumps(dict(r, metric="depth maps/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
+                                  higher_is_better=True, data="synthetic")), flush=True)
         return
     if args.workload == "rectify":
         peak, _ = measured_peaks()

@@ -10,8 +10,10 @@
 // control flow — view selection, the damped Gauss-Newton loop with step
 // shrinking, the acceptance test — is uniform over the warp and runs in every
 // lane, with no shared memory and no barriers. The window terms compute in
-// double precision as the reference does, or in float (fp32 = 1); the 3 x 3
-// LDL^T solve is double in both. Sums run in a different order than the
+// double precision as the reference does; with fp32 = 1 the Gauss-Newton
+// terms (Jacobian, J^T J, J^T e: the bulk of the work) are float while the
+// objective that decides which steps are taken (sampled values, window
+// normalisation, NCC) and the 3 x 3 LDL^T solve stay double. Sums run in a different order than the
 // reference's sequential loops, so results agree with a double-precision CPU
 // restatement to rounding, not bit for bit.
 #include <cmath>
@@ -97,7 +99,7 @@ R3D_DEVICE SampleAt sample_at(const Params& p, int k) {
 // leaves the image or the window has no texture.
 template <class T, int PER, bool JAC>
 R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double* theta, const Params& p,
-                              const T (&n0)[PER], T& ncc_out, T (&hh)[6], T (&gg)[3]) {
+                              const double (&n0)[PER], double& ncc_out, T (&hh)[6], T (&gg)[3]) {
   const T hc0 = static_cast<T>(row3(g.m, 0, x, y, 1.0)), hc1 = static_cast<T>(row3(g.m, 1, x, y, 1.0)),
           hc2 = static_cast<T>(row3(g.m, 2, x, y, 1.0));
   const T b0 = static_cast<T>(g.b[0]), b1 = static_cast<T>(g.b[1]), b2 = static_cast<T>(g.b[2]);
@@ -134,9 +136,12 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
     }
   }
   const bool offsets = rel && hz > 0.0;
-  T v[PER], dv[PER];
+  // The sampled values and the NCC are double in both paths (they decide
+  // which steps are taken); the Jacobian terms are T.
+  double v[PER];
+  T dv[PER];
   bool bad = false;
-  T sum = 0;
+  double sum = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k) {
     v[k] = 0;
@@ -204,7 +209,11 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
       return ay * (ax * static_cast<T>(__ldg(r0 + c)) + fx * static_cast<T>(__ldg(r0 + 3 + c))) +
              fy * (ax * static_cast<T>(__ldg(r1 + c)) + fx * static_cast<T>(__ldg(r1 + 3 + c)));
     };
-    v[k] = bil(0);
+    {
+      const double fxd = fx, fyd = fy;
+      v[k] = (1.0 - fyd) * ((1.0 - fxd) * static_cast<double>(__ldg(r0)) + fxd * static_cast<double>(__ldg(r0 + 3))) +
+             fyd * ((1.0 - fxd) * static_cast<double>(__ldg(r1)) + fxd * static_cast<double>(__ldg(r1 + 3)));
+    }
     sum += v[k];
     if (JAC) {
       const T dpx = (b0 - px * b2) * inv_z, dpy = (b1 - py * b2) * inv_z;
@@ -212,9 +221,9 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
     }
   }
   if (r3dsimt::ballot(bad) != 0) return false;
-  const T n = static_cast<T>(p.n);
-  const T mean = warp_sum(sum) / n;
-  T norm2 = 0;
+  const double nd = p.n;
+  const double mean = warp_sum(sum) / nd;
+  double norm2 = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k)
     if (sample_at(p, k).on) {
@@ -222,17 +231,19 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
       norm2 += v[k] * v[k];
     }
   norm2 = warp_sum(norm2);
-  if (!(norm2 > T(1e-6) * n)) return false;
-  const T inv_norm = T(1) / sqrt(norm2);
-  T ncc = 0;
+  if (!(norm2 > 1e-6 * nd)) return false;
+  const double inv_norm_d = 1.0 / sqrt(norm2);
+  double ncc = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k)
     if (sample_at(p, k).on) {
-      v[k] *= inv_norm;
+      v[k] *= inv_norm_d;
       ncc += v[k] * n0[k];
     }
   ncc_out = warp_sum(ncc);
   if (!JAC) return true;
+  const T n = static_cast<T>(p.n);
+  const T inv_norm = static_cast<T>(inv_norm_d);
   // d(v - mean) per parameter, then dn = (I - n n^T) d(v - mean) / |v - mean|.
   T dm[3] = {0, 0, 0};
 #pragma unroll
@@ -252,9 +263,10 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
     const SampleAt sm = sample_at(p, k);
     if (!sm.on) continue;
     const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
-    pr[0] += v[k] * (dv[k] - dm[0]);
-    pr[1] += v[k] * (dv[k] * sx - dm[1]);
-    pr[2] += v[k] * (dv[k] * sy - dm[2]);
+    const T ns = static_cast<T>(v[k]);
+    pr[0] += ns * (dv[k] - dm[0]);
+    pr[1] += ns * (dv[k] * sx - dm[1]);
+    pr[2] += ns * (dv[k] * sy - dm[2]);
   }
   warp_sums(pr);
   T acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -263,11 +275,11 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
     const SampleAt sm = sample_at(p, k);
     if (!sm.on) continue;
     const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
-    const T ns = v[k];
+    const T ns = static_cast<T>(v[k]);
     const T j0 = ((dv[k] - dm[0]) - ns * pr[0]) * inv_norm;
     const T j1 = ((dv[k] * sx - dm[1]) - ns * pr[1]) * inv_norm;
     const T j2 = ((dv[k] * sy - dm[2]) - ns * pr[2]) * inv_norm;
-    const T e = ns - n0[k];
+    const T e = static_cast<T>(v[k] - n0[k]);
     acc[0] += j0 * j0;
     acc[1] += j0 * j1;
     acc[2] += j0 * j2;
@@ -386,16 +398,16 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
   if (p.num_views == 0 || x < r || y < r || x >= p.width - r || y >= p.height - r) return;
 
   // Normalised base window.
-  T n0[PER];
-  T sum = 0;
+  double n0[PER];
+  double sum = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k) {
     const SampleAt sm = sample_at(p, k);
-    n0[k] = sm.on ? static_cast<T>(base[static_cast<int64_t>(y + sm.dy) * bstride + 3 * (x + sm.dx)]) : T(0);
+    n0[k] = sm.on ? static_cast<double>(base[static_cast<int64_t>(y + sm.dy) * bstride + 3 * (x + sm.dx)]) : 0.0;
     sum += n0[k];
   }
-  const T mean = warp_sum(sum) / static_cast<T>(p.n);
-  T norm2 = 0;
+  const double mean = warp_sum(sum) / p.n;
+  double norm2 = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k)
     if (sample_at(p, k).on) {
@@ -403,8 +415,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
       norm2 += n0[k] * n0[k];
     }
   norm2 = warp_sum(norm2);
-  if (static_cast<double>(norm2) < p.min_texture2n) return;
-  const T inv_norm = T(1) / sqrt(norm2);
+  if (norm2 < p.min_texture2n) return;
+  const double inv_norm = 1.0 / sqrt(norm2);
 #pragma unroll
   for (int k = 0; k < PER; ++k) n0[k] *= inv_norm;
 
@@ -419,7 +431,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
   double s0 = 0.0;
   T hh_t[6], gg_t[3];
   for (int j = 0; j < p.num_views; ++j) {
-    T ncc;
+    double ncc;
     if (evaluate_view<T, PER, false>(views[j], xd, yd, theta0, p, n0, ncc, hh_t, gg_t) &&
         static_cast<double>(ncc) >= p.min_ncc) {
       used[m++] = j;
@@ -444,7 +456,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
     for (int i = 0; i < 3; ++i) gg[i] = 0.0;
     double score = 0.0;
     for (int t = 0; t < m; ++t) {
-      T ncc;
+      double ncc;
       if (!evaluate_view<T, PER, true>(views[used[t]], xd, yd, theta, p, n0, ncc, hh_t, gg_t))
         return -__builtin_huge_val();
       score += static_cast<double>(ncc);

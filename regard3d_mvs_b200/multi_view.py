@@ -136,3 +136,55 @@ def grid_plane_depth(rig: Rig, plane: Plane) -> np.ndarray:
     pix = np.stack([xs, ys, np.ones_like(xs)], -1)
     dirs = pix @ (rig.R.T @ K_inv).T
     return (plane.dist - plane.n @ rig.C) / (dirs @ plane.n)
+
+
+# ---------------------------------------------------------------- depth-stage scene
+# Views on an arc around a textured slanted plane, for the depth stage after
+# the combination (refinement and consistency): each view's camera, its gray
+# image (a sum of plane-coordinate sine waves scaled to about 11 px per
+# wavelength at any resolution), an SGM-like depth map (constant per 4 x 4
+# block times a smooth error of up to 1 %, as the reference's refinement test
+# builds, tests/test_mvs.cpp:459-466), its colour, and the 4 nearest views as
+# refinement partners and consistency neighbours.
+DEPTH_WAVES = ((31.0, 7.0, 0.3), (-11.0, 23.0, 1.1), (5.0, -13.0, 2.0), (43.0, 29.0, 0.7), (-37.0, 47.0, 2.9))
+
+
+def depth_stage_scene(n_views: int, width: int, height: int, partners: int = 4) -> dict:
+    f = 0.9 * width
+    target = np.array([0.0, 0.0, 5.0])
+    normal = np.array([0.35, -0.2, -1.0])
+    normal /= np.linalg.norm(normal)
+    wave_scale = f / 280.0
+    u = np.cross(normal, [0.0, 1.0, 0.0])
+    u /= np.linalg.norm(u)
+    v = np.cross(normal, u)
+    views = []
+    y, x = np.mgrid[0:height, 0:width].astype(np.float64)
+    for i in range(n_views):
+        a = np.deg2rad(-18.0 + 36.0 * i / max(1, n_views - 1))
+        c = np.array([5.0 * np.sin(a), 0.3 * np.cos(3.0 * a), 5.0 - 5.0 * np.cos(a)])
+        z = target - c
+        z /= np.linalg.norm(z)
+        xa = np.cross([0.0, 1.0, 0.0], z)
+        xa /= np.linalg.norm(xa)
+        r = np.stack([xa, np.cross(z, xa), z])
+        cam = {"width": width, "height": height, "fx": f, "fy": f, "cx": (width - 1) / 2 + 0.4,
+               "cy": (height - 1) / 2 - 0.3, "rotation": r, "center": c}
+        d = np.stack([(x - cam["cx"]) / f, (y - cam["cy"]) / f, np.ones_like(x)], -1) @ r
+        t = ((target - c) @ normal) / (d @ normal)
+        pts = c + t[..., None] * d - target
+        pu, pv = pts @ u, pts @ v
+        acc = np.zeros_like(x)
+        for kx, ky, ph in DEPTH_WAVES:
+            acc += np.sin(wave_scale * (kx * pu + ky * pv) + ph)
+        gray = (128.0 + 20.0 * acc).astype(np.float32)
+        depth_true = (t * d[..., 2]).astype(np.float32)  # depth along the optical axis
+        block = depth_true[np.minimum(y.astype(int) // 4 * 4 + 2, height - 1),
+                           np.minimum(x.astype(int) // 4 * 4 + 2, width - 1)]
+        depth = (block * (1.0 + 0.01 * np.sin(x / 9.0) * np.cos(y / 13.0))).astype(np.float32)
+        g8 = np.clip(gray, 0, 255).astype(np.uint8)
+        views.append({"camera": cam, "gray": gray, "depth": depth, "depth_true": depth_true,
+                      "color": np.repeat(g8[..., None], 3, axis=2)})
+    order = [sorted((j for j in range(n_views) if j != i), key=lambda j: (abs(j - i), j))[:partners]
+             for i in range(n_views)]
+    return {"views": views, "partners": order}

@@ -4,8 +4,9 @@ The kernel sums the window terms in a different order than the oracle, and
 CUDA's hypot may round differently from the host's, so the double path agrees
 with the oracle to rounding: refinement decisions (refined / kept /
 unconfirmed) on all but a handful of pixels, and refined depths within 1e-6
-relative for 99 % of the pixels. The float path (fp32) keeps 99 % of the
-depths within 1e-5 relative of the double oracle.
+relative for 99 % of the pixels. The float path (fp32: the Gauss-Newton
+terms in float, the NCC objective that decides the steps in double) meets
+the same bounds.
 """
 
 from __future__ import annotations
@@ -55,10 +56,10 @@ def test_float_path_close_to_oracle(gpu_matcher, oracle, scene):
     ia = gpu_matcher.refine_depth_map(a, base, views, RefinementOptions(min_gain=0.0, radius=3, step=1, fp32=True))
     ib = oracle.refine_depth_map(b, base, views, opts)
     assert ia["input"] == ib["input"]
-    assert abs(ia["refined"] - ib["refined"]) <= max(3, ib["input"] // 200)
+    assert abs(ia["refined"] - ib["refined"]) <= max(3, ib["input"] // 1000)
     flips, rel = agreement(a, b, ia, ib)
-    assert flips <= 5e-3
-    assert np.percentile(rel, 99) <= 1e-5 and rel.max() <= 1e-3, (np.percentile(rel, 99), rel.max())
+    assert flips <= 1e-3
+    assert np.percentile(rel, 99) <= 1e-6 and rel.max() <= 1e-4, (np.percentile(rel, 99), rel.max())
 
 
 def test_unrelated_views(gpu_matcher, oracle, scene):

@@ -5,7 +5,9 @@ The double-precision oracle is pinned by the reference's refinement test
 between the CUDA kernels (on the SIMT emulator) and the oracle; the refined
 depths of the kernel agree with the oracle's to rounding (the kernel sums the
 window terms in a butterfly instead of a sequential loop): the same pixels
-are refined and their depths differ by at most 2e-6 relative.
+are refined and their depths differ by at most 2e-6 relative. The float
+path (fp32: Gauss-Newton terms in float, the objective in double) stays
+within 1e-5 relative of the double oracle.
 """
 
 from __future__ import annotations
@@ -74,7 +76,7 @@ def test_refinement_image_equals_oracle(simt_matcher, oracle, sigma):
                                   oracle.make_refinement_image(gray, sigma).view(np.uint32))
 
 
-def sparse(m, seed, clusters=40):
+def sparse(m, seed, clusters=16):
     """Keeps 3 x 3 clusters of valid depth around random pixels (so that the
     slopes see neighbours), the rest invalid: a few hundred warps for the
     emulator."""
@@ -125,18 +127,16 @@ def fp32_error(a, b):
 
 
 def test_kernel_fp32_close_to_oracle(simt_matcher, oracle, scene):
-    """Window terms in float: the same decisions on this scene; 99 % of the
-    depths within 1e-5 relative of the double oracle, all within 1e-4 (float
-    noise in the NCC score can move the Gauss-Newton stop by one step, whose
-    size the stop rule bounds at 1e-3 px of motion)."""
+    """Gauss-Newton terms in float, objective in double: the same decisions,
+    depths within 1e-5 relative of the double oracle (measured: one float ulp)."""
     m, _, base, views, _ = scene
-    a, b = sparse(m, 3, 60), sparse(m, 3, 60)
-    ia = simt_matcher.refine_depth_map(a, base, views, RefinementOptions(min_gain=0.0, fp32=True))
-    ib = oracle.refine_depth_map(b, base, views, RefinementOptions(min_gain=0.0))
+    a, b = sparse(m, 3, 40), sparse(m, 3, 40)
+    ia = simt_matcher.refine_depth_map(a, base, views, RefinementOptions(min_gain=0.0, radius=3, step=1, fp32=True))
+    ib = oracle.refine_depth_map(b, base, views, RefinementOptions(min_gain=0.0, radius=3, step=1))
     assert ia == ib
     np.testing.assert_array_equal(a["depth"] > 0, b["depth"] > 0)
     rel = fp32_error(a, b)
-    assert np.percentile(rel, 99) <= 1e-5 and rel.max() <= 1e-4, (np.percentile(rel, 99), rel.max())
+    assert np.percentile(rel, 99) <= 1e-6 and rel.max() <= 1e-5, (np.percentile(rel, 99), rel.max())
 
 
 def test_kernel_rejects_bad_options(simt_matcher, scene):
