@@ -82,36 +82,60 @@ R3D_DEVICE double row3(const double* m, int i, double x, double y, double z) {
   return (m[3 * i] * x + m[3 * i + 1] * y) + m[3 * i + 2] * z;
 }
 
-// Per-lane sample s = lane + 32 k: window offset and the offset / radius.
-struct SampleAt {
-  bool on;
-  int dx, dy;
+// This lane's window samples s = lane + 32 k: offsets, offsets / radius and
+// the normalised base window (computed once per pixel).
+template <class T, int PER>
+struct Lanes {
+  bool on[PER];
+  T dx[PER], dy[PER], sx[PER], sy[PER];
+  double n0[PER];
 };
-R3D_DEVICE SampleAt sample_at(const Params& p, int k) {
-  const int s = static_cast<int>(r3dsimt::lane_id()) + 32 * k;
-  if (s >= p.n) return {false, 0, 0};
-  return {true, (s % p.side) * p.step - p.radius, (s / p.side) * p.step - p.radius};
+
+template <class T, int PER>
+R3D_DEVICE void init_lanes(const Params& p, Lanes<T, PER>& L) {
+#pragma unroll
+  for (int k = 0; k < PER; ++k) {
+    const int s = static_cast<int>(r3dsimt::lane_id()) + 32 * k;
+    L.on[k] = s < p.n;
+    const int dx = L.on[k] ? (s % p.side) * p.step - p.radius : 0;
+    const int dy = L.on[k] ? (s / p.side) * p.step - p.radius : 0;
+    L.dx[k] = static_cast<T>(dx);
+    L.dy[k] = static_cast<T>(dy);
+    L.sx[k] = static_cast<T>(static_cast<double>(dx) / p.radius);
+    L.sy[k] = static_cast<T>(static_cast<double>(dy) / p.radius);
+    L.n0[k] = 0.0;
+  }
 }
 
 // refinement.cpp:46-152 for one view: NCC of the warped window with the
-// normalised base window n0 and, with JAC, J^T J (upper triangle: xx xy xz
-// yy yz zz) and J^T e of sum (n_q - n0_q)^2 in (w, a, b). False if a sample
-// leaves the image or the window has no texture.
+// normalised base window n0 and, with JAC, J^T J (xx xy xz yy yz zz) and
+// J^T e of sum (n_q - n0_q)^2 in (w, a, b). False if a sample leaves the
+// image or the window has no texture.
+//
+// One pass: every lane accumulates its samples' raw moments and one
+// butterfly sums them. With v = (raw - mean) / |raw - mean| (so sum v = 0 and
+// sum v^2 = 1), a = dv (1, sx, sy), d = a - mean(a) and p = sum v d, the
+// reference's terms are ncc = sum raw n0 / |raw - mean| (n0 has zero mean),
+// J^T J = (sum d d^T - p p^T) / |raw - mean|^2 and
+// J^T e = (p ncc - sum a n0) / |raw - mean|. The objective moments are double
+// (with intensities shifted by `shift`, the base window's mean, to keep the
+// variance well conditioned); the Jacobian moments are T.
 template <class T, int PER, bool JAC>
 R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double* theta, const Params& p,
-                              const double (&n0)[PER], double& ncc_out, T (&hh)[6], T (&gg)[3]) {
+                              const Lanes<T, PER>& L, double shift, double& ncc_out, double* hh, double* gg) {
   const T hc0 = static_cast<T>(row3(g.m, 0, x, y, 1.0)), hc1 = static_cast<T>(row3(g.m, 1, x, y, 1.0)),
           hc2 = static_cast<T>(row3(g.m, 2, x, y, 1.0));
   const T b0 = static_cast<T>(g.b[0]), b1 = static_cast<T>(g.b[1]), b2 = static_cast<T>(g.b[2]);
+  const T m0 = static_cast<T>(g.m[0]), m1 = static_cast<T>(g.m[1]), m3 = static_cast<T>(g.m[3]),
+          m4 = static_cast<T>(g.m[4]), m6 = static_cast<T>(g.m[6]), m7 = static_cast<T>(g.m[7]);
   const T max_x = static_cast<T>(g.width - 1), max_y = static_cast<T>(g.height - 1);
   const T th0 = static_cast<T>(theta[0]), th1 = static_cast<T>(theta[1]), th2 = static_cast<T>(theta[2]);
   // In float, pixel positions of a few thousand carry about 1e-4 px of
-  // rounding, which the NCC gradient turns into depth noise. The float path
-  // therefore projects the window centre at the current depth in double once
-  // and each sample as a small float offset from it:
+  // rounding. The float path therefore projects the window centre at the
+  // current depth in double once and each sample as a small float offset:
   // (H + d).xy / (H + d).z = c + (d.xy - c d.z) / (H + d).z, c = H.xy / H.z.
   const bool rel = sizeof(T) == 4;
-  double c0 = 0.0, c1 = 0.0, hz = 0.0;
+  double hz = 0.0;
   int ic0 = 0, ic1 = 0;
   T fc0 = 0, fc1 = 0, cf0 = 0, cf1 = 0, hzf = 0;
   if (rel) {
@@ -119,8 +143,7 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
     const double H1 = row3(g.m, 1, x, y, 1.0) + g.b[1] * theta[0];
     hz = row3(g.m, 2, x, y, 1.0) + g.b[2] * theta[0];
     if (hz > 0.0) {
-      c0 = H0 / hz;
-      c1 = H1 / hz;
+      const double c0 = H0 / hz, c1 = H1 / hz;
       const double f0 = floor(c0), f1 = floor(c1);
       if (fabs(f0) < 1e8 && fabs(f1) < 1e8) {
         ic0 = static_cast<int>(f0);
@@ -136,29 +159,25 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
     }
   }
   const bool offsets = rel && hz > 0.0;
-  // The sampled values and the NCC are double in both paths (they decide
-  // which steps are taken); the Jacobian terms are T.
-  double v[PER];
-  T dv[PER];
+  // Moments: objective (double) raw, raw^2, raw n0; Jacobian (T) a, raw a,
+  // a a^T (upper triangle), n0 a.
+  double ob[3] = {0.0, 0.0, 0.0};
+  T jm[15];
+#pragma unroll
+  for (int i = 0; i < 15; ++i) jm[i] = T(0);
   bool bad = false;
-  double sum = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k) {
-    v[k] = 0;
-    dv[k] = 0;
-    const SampleAt sm = sample_at(p, k);
-    if (!sm.on || bad) continue;
-    const T dx = static_cast<T>(sm.dx), dy = static_cast<T>(sm.dy);
-    const T sx = dx / static_cast<T>(p.radius), sy = dy / static_cast<T>(p.radius);
-    T h2, inv_z, px, py;
+    if (!L.on[k] || bad) continue;
+    const T dx = L.dx[k], dy = L.dy[k], sx = L.sx[k], sy = L.sy[k];
+    T inv_z, px, py, fx, fy;
     int ix, iy;
-    T fx, fy;
     if (offsets) {
       const T ws = th1 * sx + th2 * sy;  // w(q) - w at the window centre
-      const T d0 = (static_cast<T>(g.m[0]) * dx + static_cast<T>(g.m[1]) * dy) + b0 * ws;
-      const T d1 = (static_cast<T>(g.m[3]) * dx + static_cast<T>(g.m[4]) * dy) + b1 * ws;
-      const T d2 = (static_cast<T>(g.m[6]) * dx + static_cast<T>(g.m[7]) * dy) + b2 * ws;
-      h2 = hzf + d2;
+      const T d0 = (m0 * dx + m1 * dy) + b0 * ws;
+      const T d1 = (m3 * dx + m4 * dy) + b1 * ws;
+      const T d2 = (m6 * dx + m7 * dy) + b2 * ws;
+      const T h2 = hzf + d2;
       if (!(h2 > T(0))) {
         bad = true;
         continue;
@@ -183,9 +202,9 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
       }
     } else {
       const T wq = (th0 + th1 * sx) + th2 * sy;
-      const T h0 = ((hc0 + static_cast<T>(g.m[0]) * dx) + static_cast<T>(g.m[1]) * dy) + b0 * wq;
-      const T h1 = ((hc1 + static_cast<T>(g.m[3]) * dx) + static_cast<T>(g.m[4]) * dy) + b1 * wq;
-      h2 = ((hc2 + static_cast<T>(g.m[6]) * dx) + static_cast<T>(g.m[7]) * dy) + b2 * wq;
+      const T h0 = ((hc0 + m0 * dx) + m1 * dy) + b0 * wq;
+      const T h1 = ((hc1 + m3 * dx) + m4 * dy) + b1 * wq;
+      const T h2 = ((hc2 + m6 * dx) + m7 * dy) + b2 * wq;
       if (!(h2 > T(0))) {
         bad = true;
         continue;
@@ -204,95 +223,62 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
     }
     const float* r0 = g.data + static_cast<int64_t>(iy) * g.stride + 3 * ix;
     const float* r1 = r0 + g.stride;
-    const T ax = T(1) - fx, ay = T(1) - fy;
-    auto bil = [&](int c) {
-      return ay * (ax * static_cast<T>(__ldg(r0 + c)) + fx * static_cast<T>(__ldg(r0 + 3 + c))) +
-             fy * (ax * static_cast<T>(__ldg(r1 + c)) + fx * static_cast<T>(__ldg(r1 + 3 + c)));
-    };
-    {
-      const double fxd = fx, fyd = fy;
-      v[k] = (1.0 - fyd) * ((1.0 - fxd) * static_cast<double>(__ldg(r0)) + fxd * static_cast<double>(__ldg(r0 + 3))) +
-             fyd * ((1.0 - fxd) * static_cast<double>(__ldg(r1)) + fxd * static_cast<double>(__ldg(r1 + 3)));
-    }
-    sum += v[k];
+    const double fxd = fx, fyd = fy;
+    const double raw =
+        ((1.0 - fyd) * ((1.0 - fxd) * static_cast<double>(__ldg(r0)) + fxd * static_cast<double>(__ldg(r0 + 3))) +
+         fyd * ((1.0 - fxd) * static_cast<double>(__ldg(r1)) + fxd * static_cast<double>(__ldg(r1 + 3)))) -
+        shift;
+    ob[0] += raw;
+    ob[1] += raw * raw;
+    ob[2] += raw * L.n0[k];
     if (JAC) {
+      const T ax = T(1) - fx, ay = T(1) - fy;
+      auto bil = [&](int c) {
+        return ay * (ax * __ldg(r0 + c) + fx * __ldg(r0 + 3 + c)) + fy * (ax * __ldg(r1 + c) + fx * __ldg(r1 + 3 + c));
+      };
       const T dpx = (b0 - px * b2) * inv_z, dpy = (b1 - py * b2) * inv_z;
-      dv[k] = bil(1) * dpx + bil(2) * dpy;
+      const T dv = bil(1) * dpx + bil(2) * dpy;
+      const T a0 = dv, a1 = dv * sx, a2 = dv * sy;
+      const T rf = static_cast<T>(raw), nf = static_cast<T>(L.n0[k]);
+      jm[0] += a0;
+      jm[1] += a1;
+      jm[2] += a2;
+      jm[3] += rf * a0;
+      jm[4] += rf * a1;
+      jm[5] += rf * a2;
+      jm[6] += a0 * a0;
+      jm[7] += a0 * a1;
+      jm[8] += a0 * a2;
+      jm[9] += a1 * a1;
+      jm[10] += a1 * a2;
+      jm[11] += a2 * a2;
+      jm[12] += nf * a0;
+      jm[13] += nf * a1;
+      jm[14] += nf * a2;
     }
   }
   if (r3dsimt::ballot(bad) != 0) return false;
+  warp_sums(ob);
+  if (JAC) warp_sums(jm);
   const double nd = p.n;
-  const double mean = warp_sum(sum) / nd;
-  double norm2 = 0.0;
-#pragma unroll
-  for (int k = 0; k < PER; ++k)
-    if (sample_at(p, k).on) {
-      v[k] -= mean;
-      norm2 += v[k] * v[k];
-    }
-  norm2 = warp_sum(norm2);
+  const double mean = ob[0] / nd;  // of the shifted values
+  const double norm2 = ob[1] - ob[0] * mean;
   if (!(norm2 > 1e-6 * nd)) return false;
-  const double inv_norm_d = 1.0 / sqrt(norm2);
-  double ncc = 0.0;
-#pragma unroll
-  for (int k = 0; k < PER; ++k)
-    if (sample_at(p, k).on) {
-      v[k] *= inv_norm_d;
-      ncc += v[k] * n0[k];
-    }
-  ncc_out = warp_sum(ncc);
+  const double inv_norm = 1.0 / sqrt(norm2);
+  const double ncc = ob[2] * inv_norm;
+  ncc_out = ncc;
   if (!JAC) return true;
-  const T n = static_cast<T>(p.n);
-  const T inv_norm = static_cast<T>(inv_norm_d);
-  // d(v - mean) per parameter, then dn = (I - n n^T) d(v - mean) / |v - mean|.
-  T dm[3] = {0, 0, 0};
+  const T inv = static_cast<T>(inv_norm), n = static_cast<T>(p.n), meanf = static_cast<T>(mean);
+  const T dm[3] = {jm[0] / n, jm[1] / n, jm[2] / n};
+  const T pr[3] = {inv * (jm[3] - meanf * jm[0]), inv * (jm[4] - meanf * jm[1]), inv * (jm[5] - meanf * jm[2])};
+  // sum d d^T = sum a a^T - dm (sum a)^T, then minus p p^T, times inv^2.
+  const int ti[6] = {0, 0, 0, 1, 1, 2}, tj[6] = {0, 1, 2, 1, 2, 2};
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const SampleAt sm = sample_at(p, k);
-    if (!sm.on) continue;
-    const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
-    dm[0] += dv[k];
-    dm[1] += dv[k] * sx;
-    dm[2] += dv[k] * sy;
-  }
-  warp_sums(dm);
-  for (int i = 0; i < 3; ++i) dm[i] /= n;
-  T pr[3] = {0, 0, 0};
+  for (int e = 0; e < 6; ++e)
+    hh[e] = static_cast<double>(inv * inv * ((jm[6 + e] - dm[ti[e]] * jm[tj[e]]) - pr[ti[e]] * pr[tj[e]]));
+  const T nccf = static_cast<T>(ncc);
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const SampleAt sm = sample_at(p, k);
-    if (!sm.on) continue;
-    const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
-    const T ns = static_cast<T>(v[k]);
-    pr[0] += ns * (dv[k] - dm[0]);
-    pr[1] += ns * (dv[k] * sx - dm[1]);
-    pr[2] += ns * (dv[k] * sy - dm[2]);
-  }
-  warp_sums(pr);
-  T acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const SampleAt sm = sample_at(p, k);
-    if (!sm.on) continue;
-    const T sx = static_cast<T>(sm.dx) / static_cast<T>(p.radius), sy = static_cast<T>(sm.dy) / static_cast<T>(p.radius);
-    const T ns = static_cast<T>(v[k]);
-    const T j0 = ((dv[k] - dm[0]) - ns * pr[0]) * inv_norm;
-    const T j1 = ((dv[k] * sx - dm[1]) - ns * pr[1]) * inv_norm;
-    const T j2 = ((dv[k] * sy - dm[2]) - ns * pr[2]) * inv_norm;
-    const T e = static_cast<T>(v[k] - n0[k]);
-    acc[0] += j0 * j0;
-    acc[1] += j0 * j1;
-    acc[2] += j0 * j2;
-    acc[3] += j1 * j1;
-    acc[4] += j1 * j2;
-    acc[5] += j2 * j2;
-    acc[6] += j0 * e;
-    acc[7] += j1 * e;
-    acc[8] += j2 * e;
-  }
-  warp_sums(acc);
-  for (int i = 0; i < 6; ++i) hh[i] = acc[i];
-  for (int i = 0; i < 3; ++i) gg[i] = acc[6 + i];
+  for (int i = 0; i < 3; ++i) gg[i] = static_cast<double>(inv * (pr[i] * nccf - jm[12 + i]));
   return true;
 }
 
@@ -378,8 +364,10 @@ R3D_DEVICE void solve_damped(const double* hh, const double* gg, double* delta) 
   for (int i = 0; i < 3; ++i) delta[perm[i]] = -y[i];
 }
 
+// Two blocks per SM (128 registers) for the common windows of up to 64
+// samples; the larger windows keep their registers.
 template <class T, int PER>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, (PER <= 2 ? 2 : 1))
     refine_kernel(const float* R3D_RESTRICT input, float* depth, float* conf, int64_t stride,
                   const float* R3D_RESTRICT base, int64_t bstride, const ViewGeo* R3D_RESTRICT views, Params p,
                   unsigned long long* counters) {
@@ -397,28 +385,30 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
   const int r = p.radius;
   if (p.num_views == 0 || x < r || y < r || x >= p.width - r || y >= p.height - r) return;
 
-  // Normalised base window.
-  double n0[PER];
+  // This lane's samples and the normalised base window.
+  Lanes<T, PER> L;
+  init_lanes(p, L);
   double sum = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k) {
-    const SampleAt sm = sample_at(p, k);
-    n0[k] = sm.on ? static_cast<double>(base[static_cast<int64_t>(y + sm.dy) * bstride + 3 * (x + sm.dx)]) : 0.0;
-    sum += n0[k];
+    L.n0[k] = L.on[k] ? static_cast<double>(base[static_cast<int64_t>(y + static_cast<int>(L.dy[k])) * bstride +
+                                                 3 * (x + static_cast<int>(L.dx[k]))])
+                      : 0.0;
+    sum += L.n0[k];
   }
   const double mean = warp_sum(sum) / p.n;
   double norm2 = 0.0;
 #pragma unroll
   for (int k = 0; k < PER; ++k)
-    if (sample_at(p, k).on) {
-      n0[k] -= mean;
-      norm2 += n0[k] * n0[k];
+    if (L.on[k]) {
+      L.n0[k] -= mean;
+      norm2 += L.n0[k] * L.n0[k];
     }
   norm2 = warp_sum(norm2);
   if (norm2 < p.min_texture2n) return;
   const double inv_norm = 1.0 / sqrt(norm2);
 #pragma unroll
-  for (int k = 0; k < PER; ++k) n0[k] *= inv_norm;
+  for (int k = 0; k < PER; ++k) L.n0[k] *= inv_norm;
 
   const double w0 = 1.0 / z0;
   const double theta0[3] = {w0, r * initial_slope(input, p.width, p.height, x, y, 1, 0),
@@ -429,13 +419,12 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
   int used[kMaxViews];
   int m = 0;
   double s0 = 0.0;
-  T hh_t[6], gg_t[3];
+  double hh_v[6], gg_v[3];
   for (int j = 0; j < p.num_views; ++j) {
     double ncc;
-    if (evaluate_view<T, PER, false>(views[j], xd, yd, theta0, p, n0, ncc, hh_t, gg_t) &&
-        static_cast<double>(ncc) >= p.min_ncc) {
+    if (evaluate_view<T, PER, false>(views[j], xd, yd, theta0, p, L, mean, ncc, hh_v, gg_v) && ncc >= p.min_ncc) {
       used[m++] = j;
-      s0 += static_cast<double>(ncc);
+      s0 += ncc;
     }
   }
   if (m == 0) {
@@ -457,11 +446,11 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(256)
     double score = 0.0;
     for (int t = 0; t < m; ++t) {
       double ncc;
-      if (!evaluate_view<T, PER, true>(views[used[t]], xd, yd, theta, p, n0, ncc, hh_t, gg_t))
+      if (!evaluate_view<T, PER, true>(views[used[t]], xd, yd, theta, p, L, mean, ncc, hh_v, gg_v))
         return -__builtin_huge_val();
-      score += static_cast<double>(ncc);
-      for (int i = 0; i < 6; ++i) hh[i] += static_cast<double>(hh_t[i]);
-      for (int i = 0; i < 3; ++i) gg[i] += static_cast<double>(gg_t[i]);
+      score += ncc;
+      for (int i = 0; i < 6; ++i) hh[i] += hh_v[i];
+      for (int i = 0; i < 3; ++i) gg[i] += gg_v[i];
     }
     return score / m;
   };

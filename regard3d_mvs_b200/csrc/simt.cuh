@@ -22,6 +22,7 @@
 #define R3D_HOSTDEV __host__ __device__ __forceinline__
 #define R3D_RESTRICT __restrict__
 #define R3D_LAUNCH_BOUNDS(n) __launch_bounds__(n)
+#define R3D_LAUNCH_BOUNDS_MIN(n, blocks) __launch_bounds__(n, blocks)
 #define R3D_DYNAMIC_SMEM(name) extern __shared__ __align__(16) unsigned char name[]
 #define R3D_LAUNCH(kernel, grid, block, smem, stream, ...) kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__)
 
@@ -78,6 +79,7 @@ R3D_DEVICE void cp_async_wait() {
 #define R3D_HOSTDEV inline
 #define R3D_RESTRICT
 #define R3D_LAUNCH_BOUNDS(n)
+#define R3D_LAUNCH_BOUNDS_MIN(n, blocks)
 #define R3D_DYNAMIC_SMEM(name) unsigned char* name = ::r3dsimt::dynamic_smem()
 #define R3D_LAUNCH(kernel, grid, block, smem, stream, ...) \
   ::r3dsimt::launch((grid), (block), (smem), [=]() { kernel(__VA_ARGS__); })
