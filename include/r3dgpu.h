@@ -410,6 +410,21 @@ r3dgpu_status r3dgpu_remove_depth_halos(r3dgpu_depth_map* map, int32_t max_px, i
 r3dgpu_status r3dgpu_remove_depth_speckles(r3dgpu_depth_map* map, int32_t min_size, double max_relative_step,
                                            uint64_t* removed, void* stream);
 
+/* Depth-map files (.r3dd, format version 2). Replace write_depth_map and
+ * read_depth_map, src/r3d/mvs/depth_map.hpp:57-59 (implementation
+ * src/r3d/mvs/depth_map.cpp:135-239): the same bytes, so served maps feed the
+ * reference pipeline's --reuse. The map's images are host memory, or device
+ * memory when `device` != 0 (copied on `stream` first); NULL images are
+ * written as zeros. */
+r3dgpu_status r3dgpu_write_depth_map(const char* path, const r3dgpu_depth_map* map, int32_t device, void* stream);
+/* Reading takes two calls: _info fills the camera (and K^-1 of its
+ * intrinsics), width, height, view and partners without touching the image
+ * pointers; the caller allocates host images of that size and
+ * r3dgpu_read_depth_map fills the non-NULL ones (at map->stride and
+ * map->color_stride). */
+r3dgpu_status r3dgpu_read_depth_map_info(const char* path, r3dgpu_depth_map* map);
+r3dgpu_status r3dgpu_read_depth_map(const char* path, r3dgpu_depth_map* map);
+
 /* ------------------------------------------------------------------ refinement
  * Patch-based depth refinement: per valid pixel an inverse-depth plane
  * (w, a, b) fitted by Gauss-Newton on 2 - 2 NCC of the window warped into the

@@ -46,6 +46,9 @@ EXPORTS = (
     "r3dgpu_rectify_image_f32",
     "r3dgpu_rectify_image_u16_host",
     "r3dgpu_rectify_image_f32_host",
+    "r3dgpu_write_depth_map",
+    "r3dgpu_read_depth_map_info",
+    "r3dgpu_read_depth_map",
     "r3dgpu_default_refinement_options",
     "r3dgpu_make_refinement_image",
     "r3dgpu_refine_depth_map",
@@ -159,6 +162,11 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
                                           i32, ro, rs, P]
     L.r3dgpu_refine_depth_map_host.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(CPinholeCamera), i32, i32, ri,
                                                ri, i32, ro, rs]
+    L.r3dgpu_write_depth_map.argtypes = [ctypes.c_char_p, dm, i32, P]
+    L.r3dgpu_read_depth_map_info.argtypes = [ctypes.c_char_p, dm]
+    L.r3dgpu_read_depth_map.argtypes = [ctypes.c_char_p, dm]
+    for name in ("r3dgpu_write_depth_map", "r3dgpu_read_depth_map_info", "r3dgpu_read_depth_map"):
+        getattr(L, name).restype = st
     for name in ("r3dgpu_make_refinement_image", "r3dgpu_refine_depth_map", "r3dgpu_refine_depth_map_host"):
         getattr(L, name).restype = st
     for name in ("r3dgpu_prepare_depth_map", "r3dgpu_check_consistency", "r3dgpu_filter_depth_maps",

@@ -235,3 +235,38 @@ def c_refinement_image(img: dict, ptr) -> CRefinementImage:
     c.data = ptr(data)
     c.stride = 3 * data.shape[1]
     return c
+
+
+# ------------------------------------------------------------------ .r3dd files
+def write_depth_map(lib, path: str, m: dict) -> None:
+    """write_depth_map (src/r3d/mvs/depth_map.hpp:58) of a host map."""
+    from . import _native
+
+    n = normalise(m)
+    if n["color"] is None:
+        n["color"] = np.zeros(n["depth"].shape + (3,), np.uint8)
+    c = c_depth_map(n, lambda a: a.ctypes.data)
+    _native.check(lib, lib.r3dgpu_write_depth_map(str(path).encode(), ctypes.byref(c), 0, None))
+
+
+def read_depth_map(lib, path: str) -> dict:
+    """read_depth_map (src/r3d/mvs/depth_map.hpp:59): a map dict."""
+    from . import _native
+
+    c = CDepthMap()
+    _native.check(lib, lib.r3dgpu_read_depth_map_info(str(path).encode(), ctypes.byref(c)))
+    h, w = c.height, c.width
+    m = {"depth": np.empty((h, w), np.float32), "confidence": np.empty((h, w), np.float32),
+         "pair_mask": np.empty((h, w), np.uint16), "support": np.empty((h, w), np.uint8),
+         "color": np.empty((h, w, 3), np.uint8)}
+    c.depth, c.confidence = m["depth"].ctypes.data, m["confidence"].ctypes.data
+    c.pair_mask, c.support, c.color = m["pair_mask"].ctypes.data, m["support"].ctypes.data, m["color"].ctypes.data
+    c.stride, c.color_stride = w, 3 * w
+    _native.check(lib, lib.r3dgpu_read_depth_map(str(path).encode(), ctypes.byref(c)))
+    k = c.camera.intrinsics
+    m["camera"] = {"width": k.width, "height": k.height, "fx": k.fx, "fy": k.fy, "cx": k.cx, "cy": k.cy,
+                   "rotation": np.array(c.camera.rotation[:]).reshape(3, 3), "center": np.array(c.camera.center[:]),
+                   "k_inv": np.array(c.camera.k_inv[:]).reshape(3, 3)}
+    m["view"] = int(c.view)
+    m["partners"] = [int(c.partners[i]) for i in range(c.num_partners)]
+    return m
