@@ -59,10 +59,31 @@ R3D_DEVICE T shfl_xor_t(T v, int mask) {
   return v;
 }
 
-// Butterfly sums of K values at once (every lane gets the totals).
+// The value of lane `src` (every lane reads one source lane).
+template <class T>
+R3D_DEVICE T shfl_t(T v, int src) {
+  uint32_t w[sizeof(T) / 4];
+  memcpy(w, &v, sizeof(T));
+  for (int i = 0; i < static_cast<int>(sizeof(T) / 4); ++i) w[i] = r3dsimt::shfl(w[i], src);
+  memcpy(&v, w, sizeof(T));
+  return v;
+}
+
+// Butterfly sums of K values over aligned groups of `width` lanes (masks
+// below width), and from there across the groups (masks width .. 16). After
+// each, all lanes of a group (or of the warp) hold the same bits: the partial
+// sums meet in mirrored order and IEEE addition commutes.
 template <class T, int K>
-R3D_DEVICE void warp_sums(T (&v)[K]) {
-  for (int m = 16; m >= 1; m >>= 1) {
+R3D_DEVICE void sums_below(T (&v)[K], int width) {
+  for (int m = 1; m < width; m <<= 1) {
+#pragma unroll
+    for (int i = 0; i < K; ++i) v[i] += shfl_xor_t(v[i], m);
+  }
+}
+
+template <class T, int K>
+R3D_DEVICE void sums_from(T (&v)[K], int width) {
+  for (int m = width; m < 32; m <<= 1) {
 #pragma unroll
     for (int i = 0; i < K; ++i) v[i] += shfl_xor_t(v[i], m);
   }
@@ -71,7 +92,7 @@ R3D_DEVICE void warp_sums(T (&v)[K]) {
 template <class T>
 R3D_DEVICE T warp_sum(T v) {
   T a[1] = {v};
-  warp_sums(a);
+  sums_below(a, 32);
   return a[0];
 }
 
@@ -82,192 +103,200 @@ R3D_DEVICE double row3(const double* m, int i, double x, double y, double z) {
   return (m[3 * i] * x + m[3 * i + 1] * y) + m[3 * i + 2] * z;
 }
 
-// This lane's window samples s = lane + 32 k: offsets, offsets / radius and
-// the normalised base window (computed once per pixel).
-template <class T, int PER>
-struct Lanes {
-  bool on[PER];
-  T dx[PER], dy[PER], sx[PER], sy[PER];
-  double n0[PER];
-};
+// Smallest power of two >= m (m in 1..8): the number of lane groups.
+R3D_DEVICE int groups_for(int m) { return m <= 1 ? 1 : (m <= 2 ? 2 : (m <= 4 ? 4 : 8)); }
 
-template <class T, int PER>
-R3D_DEVICE void init_lanes(const Params& p, Lanes<T, PER>& L) {
-#pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    const int s = static_cast<int>(r3dsimt::lane_id()) + 32 * k;
-    L.on[k] = s < p.n;
-    const int dx = L.on[k] ? (s % p.side) * p.step - p.radius : 0;
-    const int dy = L.on[k] ? (s / p.side) * p.step - p.radius : 0;
-    L.dx[k] = static_cast<T>(dx);
-    L.dy[k] = static_cast<T>(dy);
-    L.sx[k] = static_cast<T>(static_cast<double>(dx) / p.radius);
-    L.sy[k] = static_cast<T>(static_cast<double>(dy) / p.radius);
-    L.n0[k] = 0.0;
-  }
-}
+// Per warp in shared memory: the normalised base window n0[s] and the
+// window coordinates (offset / radius) of each window column.
+constexpr int kWarpTableDoubles = kMaxSamples + 16;
 
-// refinement.cpp:46-152 for one view: NCC of the warped window with the
-// normalised base window n0 and, with JAC, J^T J (xx xy xz yy yz zz) and
-// J^T e of sum (n_q - n0_q)^2 in (w, a, b). False if a sample leaves the
-// image or the window has no texture.
+// One view's terms at plane theta (refinement.cpp:46-152), computed by the
+// `gsize` lanes of a group: lane `gl` of the group takes the window samples
+// gl, gl + gsize, ... NCC of the warped window with the normalised base
+// window and, with JAC, J^T J (xx xy xz yy yz zz) and J^T e of
+// sum (n_q - n0_q)^2 in (w, a, b). `valid` is false if a sample leaves the
+// image or the window has no texture. All lanes of the group return the same
+// values; `active` false (a group without a view) returns zeros and valid.
 //
-// One pass: every lane accumulates its samples' raw moments and one
-// butterfly sums them. With v = (raw - mean) / |raw - mean| (so sum v = 0 and
-// sum v^2 = 1), a = dv (1, sx, sy), d = a - mean(a) and p = sum v d, the
-// reference's terms are ncc = sum raw n0 / |raw - mean| (n0 has zero mean),
+// One pass: the lanes accumulate raw moments and one butterfly sums them.
+// With v = (raw - mean) / |raw - mean| (sum v = 0, sum v^2 = 1),
+// a = dv (1, sx, sy), d = a - mean(a) and p = sum v d, the reference's terms
+// are ncc = sum raw n0 / |raw - mean| (n0 has zero mean),
 // J^T J = (sum d d^T - p p^T) / |raw - mean|^2 and
 // J^T e = (p ncc - sum a n0) / |raw - mean|. The objective moments are double
-// (with intensities shifted by `shift`, the base window's mean, to keep the
+// (intensities shifted by `shift`, the base window's mean, to keep the
 // variance well conditioned); the Jacobian moments are T.
-template <class T, int PER, bool JAC>
-R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double* theta, const Params& p,
-                              const Lanes<T, PER>& L, double shift, double& ncc_out, double* hh, double* gg) {
-  const T hc0 = static_cast<T>(row3(g.m, 0, x, y, 1.0)), hc1 = static_cast<T>(row3(g.m, 1, x, y, 1.0)),
-          hc2 = static_cast<T>(row3(g.m, 2, x, y, 1.0));
-  const T b0 = static_cast<T>(g.b[0]), b1 = static_cast<T>(g.b[1]), b2 = static_cast<T>(g.b[2]);
-  const T m0 = static_cast<T>(g.m[0]), m1 = static_cast<T>(g.m[1]), m3 = static_cast<T>(g.m[3]),
-          m4 = static_cast<T>(g.m[4]), m6 = static_cast<T>(g.m[6]), m7 = static_cast<T>(g.m[7]);
-  const T max_x = static_cast<T>(g.width - 1), max_y = static_cast<T>(g.height - 1);
-  const T th0 = static_cast<T>(theta[0]), th1 = static_cast<T>(theta[1]), th2 = static_cast<T>(theta[2]);
-  // In float, pixel positions of a few thousand carry about 1e-4 px of
-  // rounding. The float path therefore projects the window centre at the
-  // current depth in double once and each sample as a small float offset:
-  // (H + d).xy / (H + d).z = c + (d.xy - c d.z) / (H + d).z, c = H.xy / H.z.
-  const bool rel = sizeof(T) == 4;
-  double hz = 0.0;
-  int ic0 = 0, ic1 = 0;
-  T fc0 = 0, fc1 = 0, cf0 = 0, cf1 = 0, hzf = 0;
-  if (rel) {
-    const double H0 = row3(g.m, 0, x, y, 1.0) + g.b[0] * theta[0];
-    const double H1 = row3(g.m, 1, x, y, 1.0) + g.b[1] * theta[0];
-    hz = row3(g.m, 2, x, y, 1.0) + g.b[2] * theta[0];
-    if (hz > 0.0) {
-      const double c0 = H0 / hz, c1 = H1 / hz;
-      const double f0 = floor(c0), f1 = floor(c1);
-      if (fabs(f0) < 1e8 && fabs(f1) < 1e8) {
-        ic0 = static_cast<int>(f0);
-        ic1 = static_cast<int>(f1);
-        fc0 = static_cast<T>(c0 - f0);
-        fc1 = static_cast<T>(c1 - f1);
-        cf0 = static_cast<T>(c0);
-        cf1 = static_cast<T>(c1);
-        hzf = static_cast<T>(hz);
-      } else {
-        hz = 0.0;
-      }
-    }
-  }
-  const bool offsets = rel && hz > 0.0;
-  // Moments: objective (double) raw, raw^2, raw n0; Jacobian (T) a, raw a,
-  // a a^T (upper triangle), n0 a.
+template <class T, bool JAC>
+R3D_DEVICE void evaluate_group(const ViewGeo& g, bool active, double x, double y, const double* theta,
+                               const Params& p, const double* table, double shift, int gl, int gsize, bool& valid,
+                               double& ncc_out, double* hh, double* gg) {
   double ob[3] = {0.0, 0.0, 0.0};
   T jm[15];
 #pragma unroll
   for (int i = 0; i < 15; ++i) jm[i] = T(0);
   bool bad = false;
-#pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    if (!L.on[k] || bad) continue;
-    const T dx = L.dx[k], dy = L.dy[k], sx = L.sx[k], sy = L.sy[k];
-    T inv_z, px, py, fx, fy;
-    int ix, iy;
-    if (offsets) {
-      const T ws = th1 * sx + th2 * sy;  // w(q) - w at the window centre
-      const T d0 = (m0 * dx + m1 * dy) + b0 * ws;
-      const T d1 = (m3 * dx + m4 * dy) + b1 * ws;
-      const T d2 = (m6 * dx + m7 * dy) + b2 * ws;
-      const T h2 = hzf + d2;
-      if (!(h2 > T(0))) {
-        bad = true;
-        continue;
+  if (active) {
+    const T b0 = static_cast<T>(g.b[0]), b1 = static_cast<T>(g.b[1]), b2 = static_cast<T>(g.b[2]);
+    const T m0 = static_cast<T>(g.m[0]), m1 = static_cast<T>(g.m[1]), m3 = static_cast<T>(g.m[3]),
+            m4 = static_cast<T>(g.m[4]), m6 = static_cast<T>(g.m[6]), m7 = static_cast<T>(g.m[7]);
+    const T max_x = static_cast<T>(g.width - 1), max_y = static_cast<T>(g.height - 1);
+    const T th0 = static_cast<T>(theta[0]), th1 = static_cast<T>(theta[1]), th2 = static_cast<T>(theta[2]);
+    const T hc0 = static_cast<T>(row3(g.m, 0, x, y, 1.0)), hc1 = static_cast<T>(row3(g.m, 1, x, y, 1.0)),
+            hc2 = static_cast<T>(row3(g.m, 2, x, y, 1.0));
+    // In float, pixel positions of a few thousand carry about 1e-4 px of
+    // rounding. The float path therefore projects the window centre at the
+    // current depth in double once and each sample as a small float offset:
+    // (H + d).xy / (H + d).z = c + (d.xy - c d.z) / (H + d).z, c = H.xy / H.z.
+    const bool rel = sizeof(T) == 4;
+    double hz = 0.0;
+    int ic0 = 0, ic1 = 0;
+    T fc0 = 0, fc1 = 0, cf0 = 0, cf1 = 0, hzf = 0;
+    if (rel) {
+      const double H0 = row3(g.m, 0, x, y, 1.0) + g.b[0] * theta[0];
+      const double H1 = row3(g.m, 1, x, y, 1.0) + g.b[1] * theta[0];
+      hz = row3(g.m, 2, x, y, 1.0) + g.b[2] * theta[0];
+      if (hz > 0.0) {
+        const double c0 = H0 / hz, c1 = H1 / hz;
+        const double f0 = floor(c0), f1 = floor(c1);
+        if (fabs(f0) < 1e8 && fabs(f1) < 1e8) {
+          ic0 = static_cast<int>(f0);
+          ic1 = static_cast<int>(f1);
+          fc0 = static_cast<T>(c0 - f0);
+          fc1 = static_cast<T>(c1 - f1);
+          cf0 = static_cast<T>(c0);
+          cf1 = static_cast<T>(c1);
+          hzf = static_cast<T>(hz);
+        } else {
+          hz = 0.0;
+        }
       }
-      inv_z = T(1) / h2;
-      const T q0 = fc0 + (d0 - cf0 * d2) * inv_z, q1 = fc1 + (d1 - cf1 * d2) * inv_z;
-      if (!(fabs(q0) < T(1e6) && fabs(q1) < T(1e6))) {
-        bad = true;
-        continue;
-      }
-      const T fl0 = floor(q0), fl1 = floor(q1);
-      ix = ic0 + static_cast<int>(fl0);
-      iy = ic1 + static_cast<int>(fl1);
-      fx = q0 - fl0;
-      fy = q1 - fl1;
-      px = static_cast<T>(ix) + fx;
-      py = static_cast<T>(iy) + fy;
-      // px in [0, width - 1) and py in [0, height - 1), as below.
-      if (!(ix >= 0 && iy >= 0 && ix <= g.width - 2 && iy <= g.height - 2)) {
-        bad = true;
-        continue;
-      }
-    } else {
-      const T wq = (th0 + th1 * sx) + th2 * sy;
-      const T h0 = ((hc0 + m0 * dx) + m1 * dy) + b0 * wq;
-      const T h1 = ((hc1 + m3 * dx) + m4 * dy) + b1 * wq;
-      const T h2 = ((hc2 + m6 * dx) + m7 * dy) + b2 * wq;
-      if (!(h2 > T(0))) {
-        bad = true;
-        continue;
-      }
-      inv_z = T(1) / h2;
-      px = h0 * inv_z;
-      py = h1 * inv_z;
-      if (!(px >= T(0) && py >= T(0) && px < max_x && py < max_y)) {
-        bad = true;
-        continue;
-      }
-      ix = static_cast<int>(px);
-      iy = static_cast<int>(py);
-      fx = px - static_cast<T>(ix);
-      fy = py - static_cast<T>(iy);
     }
-    const float* r0 = g.data + static_cast<int64_t>(iy) * g.stride + 3 * ix;
-    const float* r1 = r0 + g.stride;
-    const double fxd = fx, fyd = fy;
-    const double raw =
-        ((1.0 - fyd) * ((1.0 - fxd) * static_cast<double>(__ldg(r0)) + fxd * static_cast<double>(__ldg(r0 + 3))) +
-         fyd * ((1.0 - fxd) * static_cast<double>(__ldg(r1)) + fxd * static_cast<double>(__ldg(r1 + 3)))) -
-        shift;
-    ob[0] += raw;
-    ob[1] += raw * raw;
-    ob[2] += raw * L.n0[k];
-    if (JAC) {
-      const T ax = T(1) - fx, ay = T(1) - fy;
-      auto bil = [&](int c) {
-        return ay * (ax * __ldg(r0 + c) + fx * __ldg(r0 + 3 + c)) + fy * (ax * __ldg(r1 + c) + fx * __ldg(r1 + 3 + c));
-      };
-      const T dpx = (b0 - px * b2) * inv_z, dpy = (b1 - py * b2) * inv_z;
-      const T dv = bil(1) * dpx + bil(2) * dpy;
-      const T a0 = dv, a1 = dv * sx, a2 = dv * sy;
-      const T rf = static_cast<T>(raw), nf = static_cast<T>(L.n0[k]);
-      jm[0] += a0;
-      jm[1] += a1;
-      jm[2] += a2;
-      jm[3] += rf * a0;
-      jm[4] += rf * a1;
-      jm[5] += rf * a2;
-      jm[6] += a0 * a0;
-      jm[7] += a0 * a1;
-      jm[8] += a0 * a2;
-      jm[9] += a1 * a1;
-      jm[10] += a1 * a2;
-      jm[11] += a2 * a2;
-      jm[12] += nf * a0;
-      jm[13] += nf * a1;
-      jm[14] += nf * a2;
+    const bool offsets = rel && hz > 0.0;
+    const double* n0s = table;
+    const double* coord = table + kMaxSamples;  // offset / radius of window column c
+    // Window column and row of sample s, advanced by gsize per step.
+    int col = gl % p.side, row = gl / p.side;
+    const int dcol = gsize % p.side, drow = gsize / p.side;
+    for (int s = gl; s < p.n; s += gsize) {
+      const T dx = static_cast<T>(col * p.step - p.radius), dy = static_cast<T>(row * p.step - p.radius);
+      const T sx = static_cast<T>(coord[col]), sy = static_cast<T>(coord[row]);
+      col += dcol;
+      row += drow;
+      if (col >= p.side) {
+        col -= p.side;
+        ++row;
+      }
+      T inv_z, px, py, fx, fy;
+      int ix, iy;
+      if (offsets) {
+        const T ws = th1 * sx + th2 * sy;  // w(q) - w at the window centre
+        const T d0 = (m0 * dx + m1 * dy) + b0 * ws;
+        const T d1 = (m3 * dx + m4 * dy) + b1 * ws;
+        const T d2 = (m6 * dx + m7 * dy) + b2 * ws;
+        const T h2 = hzf + d2;
+        if (!(h2 > T(0))) {
+          bad = true;
+          break;
+        }
+        inv_z = T(1) / h2;
+        const T q0 = fc0 + (d0 - cf0 * d2) * inv_z, q1 = fc1 + (d1 - cf1 * d2) * inv_z;
+        if (!(fabs(q0) < T(1e6) && fabs(q1) < T(1e6))) {
+          bad = true;
+          break;
+        }
+        const T fl0 = floor(q0), fl1 = floor(q1);
+        ix = ic0 + static_cast<int>(fl0);
+        iy = ic1 + static_cast<int>(fl1);
+        fx = q0 - fl0;
+        fy = q1 - fl1;
+        px = static_cast<T>(ix) + fx;
+        py = static_cast<T>(iy) + fy;
+        // px in [0, width - 1) and py in [0, height - 1), as below.
+        if (!(ix >= 0 && iy >= 0 && ix <= g.width - 2 && iy <= g.height - 2)) {
+          bad = true;
+          break;
+        }
+      } else {
+        const T wq = (th0 + th1 * sx) + th2 * sy;
+        const T h0 = ((hc0 + m0 * dx) + m1 * dy) + b0 * wq;
+        const T h1 = ((hc1 + m3 * dx) + m4 * dy) + b1 * wq;
+        const T h2 = ((hc2 + m6 * dx) + m7 * dy) + b2 * wq;
+        if (!(h2 > T(0))) {
+          bad = true;
+          break;
+        }
+        inv_z = T(1) / h2;
+        px = h0 * inv_z;
+        py = h1 * inv_z;
+        if (!(px >= T(0) && py >= T(0) && px < max_x && py < max_y)) {
+          bad = true;
+          break;
+        }
+        ix = static_cast<int>(px);
+        iy = static_cast<int>(py);
+        fx = px - static_cast<T>(ix);
+        fy = py - static_cast<T>(iy);
+      }
+      const float* r0 = g.data + static_cast<int64_t>(iy) * g.stride + 3 * ix;
+      const float* r1 = r0 + g.stride;
+      const double fxd = fx, fyd = fy;
+      const double raw =
+          ((1.0 - fyd) * ((1.0 - fxd) * static_cast<double>(__ldg(r0)) + fxd * static_cast<double>(__ldg(r0 + 3))) +
+           fyd * ((1.0 - fxd) * static_cast<double>(__ldg(r1)) + fxd * static_cast<double>(__ldg(r1 + 3)))) -
+          shift;
+      const double n0 = n0s[s];
+      ob[0] += raw;
+      ob[1] += raw * raw;
+      ob[2] += raw * n0;
+      if (JAC) {
+        const T ax = T(1) - fx, ay = T(1) - fy;
+        auto bil = [&](int c) {
+          return ay * (ax * __ldg(r0 + c) + fx * __ldg(r0 + 3 + c)) + fy * (ax * __ldg(r1 + c) + fx * __ldg(r1 + 3 + c));
+        };
+        const T dpx = (b0 - px * b2) * inv_z, dpy = (b1 - py * b2) * inv_z;
+        const T dv = bil(1) * dpx + bil(2) * dpy;
+        const T a0 = dv, a1 = dv * sx, a2 = dv * sy;
+        const T rf = static_cast<T>(raw), nf = static_cast<T>(n0);
+        jm[0] += a0;
+        jm[1] += a1;
+        jm[2] += a2;
+        jm[3] += rf * a0;
+        jm[4] += rf * a1;
+        jm[5] += rf * a2;
+        jm[6] += a0 * a0;
+        jm[7] += a0 * a1;
+        jm[8] += a0 * a2;
+        jm[9] += a1 * a1;
+        jm[10] += a1 * a2;
+        jm[11] += a2 * a2;
+        jm[12] += nf * a0;
+        jm[13] += nf * a1;
+        jm[14] += nf * a2;
+      }
     }
   }
-  if (r3dsimt::ballot(bad) != 0) return false;
-  warp_sums(ob);
-  if (JAC) warp_sums(jm);
+  // The group is invalid if any of its lanes left the image.
+  const uint32_t lane = r3dsimt::lane_id();
+  const uint32_t gmask = (gsize == 32 ? 0xFFFFFFFFu : ((1u << gsize) - 1u) << (lane & ~static_cast<uint32_t>(gsize - 1)));
+  const bool group_bad = (r3dsimt::ballot(bad) & gmask) != 0;
+  sums_below(ob, gsize);
+  if (JAC) sums_below(jm, gsize);
+  for (int i = 0; i < 6; ++i) hh[i] = 0.0;
+  for (int i = 0; i < 3; ++i) gg[i] = 0.0;
+  ncc_out = 0.0;
+  valid = true;
+  if (!active) return;
   const double nd = p.n;
   const double mean = ob[0] / nd;  // of the shifted values
   const double norm2 = ob[1] - ob[0] * mean;
-  if (!(norm2 > 1e-6 * nd)) return false;
+  if (group_bad || !(norm2 > 1e-6 * nd)) {
+    valid = false;
+    return;
+  }
   const double inv_norm = 1.0 / sqrt(norm2);
   const double ncc = ob[2] * inv_norm;
   ncc_out = ncc;
-  if (!JAC) return true;
+  if (!JAC) return;
   const T inv = static_cast<T>(inv_norm), n = static_cast<T>(p.n), meanf = static_cast<T>(mean);
   const T dm[3] = {jm[0] / n, jm[1] / n, jm[2] / n};
   const T pr[3] = {inv * (jm[3] - meanf * jm[0]), inv * (jm[4] - meanf * jm[1]), inv * (jm[5] - meanf * jm[2])};
@@ -279,7 +308,6 @@ R3D_DEVICE bool evaluate_view(const ViewGeo& g, double x, double y, const double
   const T nccf = static_cast<T>(ncc);
 #pragma unroll
   for (int i = 0; i < 3; ++i) gg[i] = static_cast<double>(inv * (pr[i] * nccf - jm[12 + i]));
-  return true;
 }
 
 // refinement.cpp:155-165: pixels of motion in the view per unit of inverse depth.
@@ -364,16 +392,19 @@ R3D_DEVICE void solve_damped(const double* hh, const double* gg, double* delta) 
   for (int i = 0; i < 3; ++i) delta[perm[i]] = -y[i];
 }
 
-// Two blocks per SM (128 registers) for the common windows of up to 64
-// samples; the larger windows keep their registers.
-template <class T, int PER>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, (PER <= 2 ? 2 : 1))
+// One warp per depth-map pixel; per warp a table of kWarpTableDoubles
+// doubles in dynamic shared memory.
+template <class T>
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, 2)
     refine_kernel(const float* R3D_RESTRICT input, float* depth, float* conf, int64_t stride,
                   const float* R3D_RESTRICT base, int64_t bstride, const ViewGeo* R3D_RESTRICT views, Params p,
                   unsigned long long* counters) {
+  R3D_DYNAMIC_SMEM(smem);
   const int64_t pix = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   if (pix >= static_cast<int64_t>(p.width) * p.height) return;  // whole warp
-  const bool lead = r3dsimt::lane_id() == 0;
+  const int lane = static_cast<int>(r3dsimt::lane_id());
+  const bool lead = lane == 0;
+  double* table = reinterpret_cast<double*>(smem) + (threadIdx.x >> 5) * kWarpTableDoubles;
   const int y = static_cast<int>(pix / p.width), x = static_cast<int>(pix - static_cast<int64_t>(y) * p.width);
   const float z0 = input[pix];
   if (!(z0 > 0.0F)) return;
@@ -385,46 +416,62 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, (PER <= 2 ? 2 : 1))
   const int r = p.radius;
   if (p.num_views == 0 || x < r || y < r || x >= p.width - r || y >= p.height - r) return;
 
-  // This lane's samples and the normalised base window.
-  Lanes<T, PER> L;
-  init_lanes(p, L);
+  // The normalised base window (sample s = lane + 32 k) into the table.
+  double nb[kMaxSamples / 32 + 1];
   double sum = 0.0;
 #pragma unroll
-  for (int k = 0; k < PER; ++k) {
-    L.n0[k] = L.on[k] ? static_cast<double>(base[static_cast<int64_t>(y + static_cast<int>(L.dy[k])) * bstride +
-                                                 3 * (x + static_cast<int>(L.dx[k]))])
-                      : 0.0;
-    sum += L.n0[k];
+  for (int k = 0; k < kMaxSamples / 32 + 1; ++k) {
+    const int s = lane + 32 * k;
+    nb[k] = 0.0;
+    if (s < p.n) {
+      const int dx = (s % p.side) * p.step - r, dy = (s / p.side) * p.step - r;
+      nb[k] = base[static_cast<int64_t>(y + dy) * bstride + 3 * (x + dx)];
+      sum += nb[k];
+    }
   }
   const double mean = warp_sum(sum) / p.n;
   double norm2 = 0.0;
 #pragma unroll
-  for (int k = 0; k < PER; ++k)
-    if (L.on[k]) {
-      L.n0[k] -= mean;
-      norm2 += L.n0[k] * L.n0[k];
+  for (int k = 0; k < kMaxSamples / 32 + 1; ++k)
+    if (lane + 32 * k < p.n) {
+      nb[k] -= mean;
+      norm2 += nb[k] * nb[k];
     }
   norm2 = warp_sum(norm2);
   if (norm2 < p.min_texture2n) return;
   const double inv_norm = 1.0 / sqrt(norm2);
 #pragma unroll
-  for (int k = 0; k < PER; ++k) L.n0[k] *= inv_norm;
+  for (int k = 0; k < kMaxSamples / 32 + 1; ++k)
+    if (lane + 32 * k < p.n) table[lane + 32 * k] = nb[k] * inv_norm;
+  if (lane < p.side) table[kMaxSamples + lane] = static_cast<double>(lane * p.step - r) / r;
+  r3dsimt::syncwarp();
 
   const double w0 = 1.0 / z0;
   const double theta0[3] = {w0, r * initial_slope(input, p.width, p.height, x, y, 1, 0),
                             r * initial_slope(input, p.width, p.height, x, y, 0, 1)};
   const double xd = x, yd = y;
+  double hh_v[6], gg_v[3];
 
-  // Local view selection at the initial plane.
+  // Local view selection at the initial plane: all views at once, one lane
+  // group per view.
   int used[kMaxViews];
   int m = 0;
   double s0 = 0.0;
-  double hh_v[6], gg_v[3];
-  for (int j = 0; j < p.num_views; ++j) {
+  {
+    const int gsize = 32 / groups_for(p.num_views);
+    const int t = lane / gsize;
+    const bool active = t < p.num_views;
+    bool valid;
     double ncc;
-    if (evaluate_view<T, PER, false>(views[j], xd, yd, theta0, p, L, mean, ncc, hh_v, gg_v) && ncc >= p.min_ncc) {
-      used[m++] = j;
-      s0 += ncc;
+    evaluate_group<T, false>(views[active ? t : 0], active, xd, yd, theta0, p, table, mean, lane % gsize, gsize,
+                             valid, ncc, hh_v, gg_v);
+    const uint32_t ok = r3dsimt::ballot(active && valid && ncc >= p.min_ncc);
+    for (int j = 0; j < p.num_views; ++j) {
+      const double nj = shfl_t(ncc, j * gsize);  // group j's value
+      if ((ok >> (j * gsize)) & 1u) {
+        used[m++] = j;
+        s0 += nj;
+      }
     }
   }
   if (m == 0) {
@@ -439,20 +486,23 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, (PER <= 2 ? 2 : 1))
   double max_motion = 0.0;
   for (int t = 0; t < m; ++t) max_motion = fmax(max_motion, centre_motion(views[used[t]], xd, yd, w0));
 
-  // Mean NCC and Gauss-Newton terms over the used views; -inf if a view drops out.
+  // Mean NCC and Gauss-Newton terms over the used views (one lane group
+  // each); -inf if a view drops out.
+  const int gsize = 32 / groups_for(m);
+  const int my_t = lane / gsize;
+  const bool my_active = my_t < m;
+  const ViewGeo& my_view = views[used[my_active ? my_t : 0]];
   auto evaluate = [&](const double* theta, double* hh, double* gg) {
-    for (int i = 0; i < 6; ++i) hh[i] = 0.0;
-    for (int i = 0; i < 3; ++i) gg[i] = 0.0;
-    double score = 0.0;
-    for (int t = 0; t < m; ++t) {
-      double ncc;
-      if (!evaluate_view<T, PER, true>(views[used[t]], xd, yd, theta, p, L, mean, ncc, hh_v, gg_v))
-        return -__builtin_huge_val();
-      score += ncc;
-      for (int i = 0; i < 6; ++i) hh[i] += hh_v[i];
-      for (int i = 0; i < 3; ++i) gg[i] += gg_v[i];
-    }
-    return score / m;
+    bool valid;
+    double ncc;
+    evaluate_group<T, true>(my_view, my_active, xd, yd, theta, p, table, mean, lane % gsize, gsize, valid, ncc,
+                            hh_v, gg_v);
+    if (r3dsimt::ballot(!valid) != 0) return -__builtin_huge_val();
+    double tot[10] = {ncc, hh_v[0], hh_v[1], hh_v[2], hh_v[3], hh_v[4], hh_v[5], gg_v[0], gg_v[1], gg_v[2]};
+    sums_from(tot, gsize);
+    for (int i = 0; i < 6; ++i) hh[i] = tot[1 + i];
+    for (int i = 0; i < 3; ++i) gg[i] = tot[7 + i];
+    return tot[0] / m;
   };
 
   double hh[6], gg[3];
@@ -597,29 +647,16 @@ r3dgpu_refinement_options options_or_default(const r3dgpu_refinement_options* o)
   return out;
 }
 
-template <class T, int PER>
+template <class T>
 void launch_refine(const float* input, float* depth, float* conf, int64_t stride, const float* base,
                    int64_t bstride, const ViewGeo* views, const Params& p, unsigned long long* counters,
                    cudaStream_t s) {
   const int64_t warps = static_cast<int64_t>(p.width) * p.height;
-  auto kernel = refine_kernel<T, PER>;
-  R3D_LAUNCH(kernel, static_cast<unsigned>(ceil_div64(warps, 8)), 256, 0, s, input, depth, conf, stride, base, bstride,
-             views, p, counters);
+  const size_t smem = sizeof(double) * kWarpTableDoubles * 8;
+  auto kernel = refine_kernel<T>;
+  R3D_LAUNCH(kernel, static_cast<unsigned>(ceil_div64(warps, 8)), 256, smem, s, input, depth, conf, stride, base,
+             bstride, views, p, counters);
   launched(sizeof(T) == 8 ? "refine_kernel<f64>" : "refine_kernel<f32>");
-}
-
-template <class T>
-void launch_refine_t(int per, const float* input, float* depth, float* conf, int64_t stride, const float* base,
-                     int64_t bstride, const ViewGeo* views, const Params& p, unsigned long long* counters,
-                     cudaStream_t s) {
-  if (per <= 1)
-    launch_refine<T, 1>(input, depth, conf, stride, base, bstride, views, p, counters, s);
-  else if (per <= 2)
-    launch_refine<T, 2>(input, depth, conf, stride, base, bstride, views, p, counters, s);
-  else if (per <= 4)
-    launch_refine<T, 4>(input, depth, conf, stride, base, bstride, views, p, counters, s);
-  else
-    launch_refine<T, 8>(input, depth, conf, stride, base, bstride, views, p, counters, s);
 }
 
 void refine(float* depth, float* conf, int64_t stride, const r3dgpu_pinhole_camera& cam, int w, int h,
@@ -657,13 +694,12 @@ void refine(float* depth, float* conf, int64_t stride, const r3dgpu_pinhole_came
                                h, cudaMemcpyDeviceToDevice, s));
     Params p{w, h, o.radius, o.step, side, n, o.iterations, nv, o.min_ncc, o.max_shift_px, o.min_gain,
              o.min_texture * o.min_texture * n, o.drop_unconfirmed};
-    const int per = (n + 31) / 32;
     if (o.fp32)
-      launch_refine_t<float>(per, sc.input.get(), depth, conf, stride, base.data, base.stride, sc.views.get(), p,
-                             sc.counters.get(), s);
+      launch_refine<float>(sc.input.get(), depth, conf, stride, base.data, base.stride, sc.views.get(), p,
+                           sc.counters.get(), s);
     else
-      launch_refine_t<double>(per, sc.input.get(), depth, conf, stride, base.data, base.stride, sc.views.get(), p,
-                              sc.counters.get(), s);
+      launch_refine<double>(sc.input.get(), depth, conf, stride, base.data, base.stride, sc.views.get(), p,
+                            sc.counters.get(), s);
   }
   unsigned long long c[kCounters];
   R3D_CUDA(cudaMemcpyAsync(c, sc.counters.get(), sizeof(c), cudaMemcpyDeviceToHost, s));
