@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "api_guard.h"
 #include "matcher_internal.h"
 
 namespace r3dgpu {
@@ -519,21 +520,6 @@ void count_output(const r3dgpu_depth_map& m, cudaStream_t s) {
   unsigned long long* c = scratch().counters.get() + kOutput;
   R3D_LAUNCH(count_valid_kernel, grid_of(m.width, m.height), b, 0, s, m, c);
   launched("count_valid_kernel");
-}
-
-template <class F>
-r3dgpu_status guard(F&& f) {
-  try {
-    set_thread_error("");
-    f();
-    return R3DGPU_OK;
-  } catch (const Error& e) {
-    set_thread_error(e.what());
-    return e.status;
-  } catch (const std::exception& e) {
-    set_thread_error(e.what());
-    return R3DGPU_EDEVICE;
-  }
 }
 
 // Device filter of `count` maps (device pointers in `maps`).

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "api_guard.h"
 #include "matcher_internal.h"
 
 namespace r3dgpu {
@@ -81,7 +82,7 @@ void check_map(const r3dgpu_depth_map* m) {
     fail(R3DGPU_EINVAL, "depth map: colour stride below 3 x width");
 }
 
-// Header fields up to the images; returns (width, height).
+// Header fields up to the images (sets the camera, K^-1, view, partners, width and height).
 void read_header(std::FILE* f, const std::string& path, r3dgpu_depth_map& m) {
   char magic[4];
   uint32_t version = 0;
@@ -116,21 +117,6 @@ void read_header(std::FILE* f, const std::string& path, r3dgpu_depth_map& m) {
   // replace it).
   const double ki[9] = {1.0 / k.fx, 0.0, -k.cx / k.fx, 0.0, 1.0 / k.fy, -k.cy / k.fy, 0.0, 0.0, 1.0};
   std::memcpy(m.camera.k_inv, ki, sizeof(ki));
-}
-
-template <class F>
-r3dgpu_status guard(F&& f) {
-  try {
-    set_thread_error("");
-    f();
-    return R3DGPU_OK;
-  } catch (const Error& e) {
-    set_thread_error(e.what());
-    return e.status;
-  } catch (const std::exception& e) {
-    set_thread_error(e.what());
-    return R3DGPU_EDEVICE;
-  }
 }
 
 }  // namespace

@@ -18,6 +18,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "api_guard.h"
 #include "matcher_internal.h"
 
 namespace r3dgpu {
@@ -185,21 +186,6 @@ R3D_GLOBAL void combine_pairs_kernel(r3dgpu_depth_grid grid, const r3dgpu_pair_g
   depth[out] = static_cast<float>(z);
   confidence[out] = __fdiv_rn(conf, static_cast<float>(m));
   pair_mask[out] = static_cast<uint16_t>(mask);
-}
-
-template <class F>
-r3dgpu_status guard(F&& f) {
-  try {
-    set_thread_error("");
-    f();
-    return R3DGPU_OK;
-  } catch (const Error& e) {
-    set_thread_error(e.what());
-    return e.status;
-  } catch (const std::exception& e) {
-    set_thread_error(e.what());
-    return R3DGPU_EDEVICE;
-  }
 }
 
 void check_args(const r3dgpu_depth_grid* grid, const r3dgpu_pair_geometry* pairs, int count, float* depth,

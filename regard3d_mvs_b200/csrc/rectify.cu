@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "api_guard.h"
 #include "matcher_internal.h"
 
 namespace r3dgpu {
@@ -269,21 +270,6 @@ void check(const void* src, int src_width, int src_height, int64_t src_stride, c
     fail(R3DGPU_EINVAL, "rectify_image: no output image or its stride is below the target width");
   if (has_pixels && valid != nullptr && vstride < k->width)
     fail(R3DGPU_EINVAL, "rectify_image: validity stride below the target width");
-}
-
-template <class F>
-r3dgpu_status guard(F&& f) {
-  try {
-    set_thread_error("");
-    f();
-    return R3DGPU_OK;
-  } catch (const Error& e) {
-    set_thread_error(e.what());
-    return e.status;
-  } catch (const std::exception& e) {
-    set_thread_error(e.what());
-    return R3DGPU_EDEVICE;
-  }
 }
 
 // Host images: copy in, rectify, copy out (one per-thread staging buffer).

@@ -23,6 +23,7 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "api_guard.h"
 #include "matcher_internal.h"
 
 namespace r3dgpu {
@@ -595,21 +596,6 @@ Scratch& scratch() {
   s.counters.reserve(kCounters);
   s.views.reserve(kMaxViews);
   return s;
-}
-
-template <class F>
-r3dgpu_status guard(F&& f) {
-  try {
-    set_thread_error("");
-    f();
-    return R3DGPU_OK;
-  } catch (const Error& e) {
-    set_thread_error(e.what());
-    return e.status;
-  } catch (const std::exception& e) {
-    set_thread_error(e.what());
-    return R3DGPU_EDEVICE;
-  }
 }
 
 // Row-major 3x3 products in the reference's left-to-right order.
