@@ -951,6 +951,7 @@ def main():
             line["cpu_baseline"] = cpu_baseline(specs)
             line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
             line["rectify"] = measure_rectify(lib, dev, stream, args.steps, args.warmup, peak)
+            line["depth_stage"] = measure_depth(lib, dev, stream, args.steps, args.warmup, peak)
         if args.serve and world == 1:
             # In a fresh process, with this one's device memory given back.
             del dL, dR, dD, dC

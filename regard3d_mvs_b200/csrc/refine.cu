@@ -17,6 +17,7 @@
 // reference's sequential loops, so results agree with a double-precision CPU
 // restatement to rounding, not bit for bit.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -38,8 +39,8 @@ enum : int { kInput, kRefined, kUnconfirmed, kCounters };
 struct ViewGeo {
   double m[9];  // K_j R_j R_0^T K_0^-1, row-major
   double b[3];  // K_j R_j (C_0 - C_j)
-  const float* data;
-  int64_t stride;
+  const float4* data;  // (intensity, d/dx, d/dy, 0) per pixel, repacked from the 3-channel image
+  int64_t stride;      // in pixels
   int width, height;
 };
 
@@ -127,7 +128,7 @@ constexpr int kWarpTableDoubles = kMaxSamples + 16;
 // J^T e = (p ncc - sum a n0) / |raw - mean|. The objective moments are double
 // (intensities shifted by `shift`, the base window's mean, to keep the
 // variance well conditioned); the Jacobian moments are T.
-template <class T, bool JAC>
+template <class T, bool JAC, int U>
 R3D_DEVICE void evaluate_group(const ViewGeo& g, bool active, double x, double y, const double* theta,
                                const Params& p, const double* table, double shift, int gl, int gsize, bool& valid,
                                double& ncc_out, double* hh, double* gg) {
@@ -178,6 +179,7 @@ R3D_DEVICE void evaluate_group(const ViewGeo& g, bool active, double x, double y
     // Window column and row of sample s, advanced by gsize per step.
     int col = gl % p.side, row = gl / p.side;
     const int dcol = gsize % p.side, drow = gsize / p.side;
+#pragma unroll(U)
     for (int s = gl; s < p.n; s += gsize) {
       const T dx = static_cast<T>(col * p.step - p.radius), dy = static_cast<T>(row * p.step - p.radius);
       const T sx = static_cast<T>(coord[col]), sy = static_cast<T>(coord[row]);
@@ -238,24 +240,22 @@ R3D_DEVICE void evaluate_group(const ViewGeo& g, bool active, double x, double y
         fx = px - static_cast<T>(ix);
         fy = py - static_cast<T>(iy);
       }
-      const float* r0 = g.data + static_cast<int64_t>(iy) * g.stride + 3 * ix;
-      const float* r1 = r0 + g.stride;
+      const float4* r0 = g.data + static_cast<int64_t>(iy) * g.stride + ix;
+      const float4 c00 = __ldg(r0), c01 = __ldg(r0 + 1), c10 = __ldg(r0 + g.stride), c11 = __ldg(r0 + g.stride + 1);
       const double fxd = fx, fyd = fy;
-      const double raw =
-          ((1.0 - fyd) * ((1.0 - fxd) * static_cast<double>(__ldg(r0)) + fxd * static_cast<double>(__ldg(r0 + 3))) +
-           fyd * ((1.0 - fxd) * static_cast<double>(__ldg(r1)) + fxd * static_cast<double>(__ldg(r1 + 3)))) -
-          shift;
+      const double raw = ((1.0 - fyd) * ((1.0 - fxd) * static_cast<double>(c00.x) + fxd * static_cast<double>(c01.x)) +
+                          fyd * ((1.0 - fxd) * static_cast<double>(c10.x) + fxd * static_cast<double>(c11.x))) -
+                         shift;
       const double n0 = n0s[s];
       ob[0] += raw;
       ob[1] += raw * raw;
       ob[2] += raw * n0;
       if (JAC) {
         const T ax = T(1) - fx, ay = T(1) - fy;
-        auto bil = [&](int c) {
-          return ay * (ax * __ldg(r0 + c) + fx * __ldg(r0 + 3 + c)) + fy * (ax * __ldg(r1 + c) + fx * __ldg(r1 + 3 + c));
-        };
+        const T gx = ay * (ax * c00.y + fx * c01.y) + fy * (ax * c10.y + fx * c11.y);
+        const T gy = ay * (ax * c00.z + fx * c01.z) + fy * (ax * c10.z + fx * c11.z);
         const T dpx = (b0 - px * b2) * inv_z, dpy = (b1 - py * b2) * inv_z;
-        const T dv = bil(1) * dpx + bil(2) * dpy;
+        const T dv = gx * dpx + gy * dpy;
         const T a0 = dv, a1 = dv * sx, a2 = dv * sy;
         const T rf = static_cast<T>(raw), nf = static_cast<T>(n0);
         jm[0] += a0;
@@ -395,7 +395,7 @@ R3D_DEVICE void solve_damped(const double* hh, const double* gg, double* delta) 
 
 // One warp per depth-map pixel; per warp a table of kWarpTableDoubles
 // doubles in dynamic shared memory.
-template <class T>
+template <class T, int U>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, 2)
     refine_kernel(const float* R3D_RESTRICT input, float* depth, float* conf, int64_t stride,
                   const float* R3D_RESTRICT base, int64_t bstride, const ViewGeo* R3D_RESTRICT views, Params p,
@@ -464,7 +464,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, 2)
     const bool active = t < p.num_views;
     bool valid;
     double ncc;
-    evaluate_group<T, false>(views[active ? t : 0], active, xd, yd, theta0, p, table, mean, lane % gsize, gsize,
+    evaluate_group<T, false, U>(views[active ? t : 0], active, xd, yd, theta0, p, table, mean, lane % gsize, gsize,
                              valid, ncc, hh_v, gg_v);
     const uint32_t ok = r3dsimt::ballot(active && valid && ncc >= p.min_ncc);
     for (int j = 0; j < p.num_views; ++j) {
@@ -496,7 +496,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, 2)
   auto evaluate = [&](const double* theta, double* hh, double* gg) {
     bool valid;
     double ncc;
-    evaluate_group<T, true>(my_view, my_active, xd, yd, theta, p, table, mean, lane % gsize, gsize, valid, ncc,
+    evaluate_group<T, true, U>(my_view, my_active, xd, yd, theta, p, table, mean, lane % gsize, gsize, valid, ncc,
                             hh_v, gg_v);
     if (r3dsimt::ballot(!valid) != 0) return -__builtin_huge_val();
     double tot[10] = {ncc, hh_v[0], hh_v[1], hh_v[2], hh_v[3], hh_v[4], hh_v[5], gg_v[0], gg_v[1], gg_v[2]};
@@ -584,11 +584,21 @@ R3D_GLOBAL void gradient_kernel(const float* gray, int64_t gstride, int w, int h
   o[2] = __fmul_rn(__fsub_rn(down[x], up[x]), h > 1 ? sy : 0.0F);
 }
 
+// A view's 3-channel refinement image as one float4 per pixel (one 16-byte
+// load per bilinear corner in the refinement kernel).
+R3D_GLOBAL void repack_kernel(const float* in, int64_t istride, int w, int h, float4* out) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const float* p = in + static_cast<int64_t>(y) * istride + 3 * x;
+  out[static_cast<int64_t>(y) * w + x] = make_float4(p[0], p[1], p[2], 0.0F);
+}
+
 // ------------------------------------------------------------------ host side
 struct Scratch {
   DeviceBuffer<unsigned long long> counters;
   DeviceBuffer<float> input, blur_tmp, blur_out, taps;
   DeviceBuffer<ViewGeo> views;
+  DeviceBuffer<float4> packed;  // the views' repacked images
 };
 
 Scratch& scratch() {
@@ -619,8 +629,8 @@ ViewGeo view_geometry(const r3dgpu_pinhole_camera& c0, const r3dgpu_refinement_i
   mat3(krr, c0.k_inv, g.m);
   const double dc[3] = {c0.center[0] - cj.center[0], c0.center[1] - cj.center[1], c0.center[2] - cj.center[2]};
   for (int i = 0; i < 3; ++i) g.b[i] = (kr[3 * i] * dc[0] + kr[3 * i + 1] * dc[1]) + kr[3 * i + 2] * dc[2];
-  g.data = v.data;
-  g.stride = v.stride;
+  g.data = nullptr;  // set to the repacked image by the caller
+  g.stride = cj.intrinsics.width;
   g.width = cj.intrinsics.width;
   g.height = cj.intrinsics.height;
   return g;
@@ -639,7 +649,12 @@ void launch_refine(const float* input, float* depth, float* conf, int64_t stride
                    cudaStream_t s) {
   const int64_t warps = static_cast<int64_t>(p.width) * p.height;
   const size_t smem = sizeof(double) * kWarpTableDoubles * 8;
-  auto kernel = refine_kernel<T>;
+  // The window-sample loop unrolled by 1 (default) or 2 (R3DGPU_REFINE_UNROLL=2).
+  static const int unroll = [] {
+    const char* e = std::getenv("R3DGPU_REFINE_UNROLL");
+    return e != nullptr && std::atoi(e) == 2 ? 2 : 1;
+  }();
+  auto kernel = unroll == 2 ? refine_kernel<T, 2> : refine_kernel<T, 1>;
   R3D_LAUNCH(kernel, static_cast<unsigned>(ceil_div64(warps, 8)), 256, smem, s, input, depth, conf, stride, base,
              bstride, views, p, counters);
   launched(sizeof(T) == 8 ? "refine_kernel<f64>" : "refine_kernel<f32>");
@@ -673,6 +688,21 @@ void refine(float* depth, float* conf, int64_t stride, const r3dgpu_pinhole_came
   }
   R3D_CUDA(cudaMemsetAsync(sc.counters.get(), 0, sizeof(unsigned long long) * kCounters, s));
   if (w > 0 && h > 0) {
+    // The views' images as one float4 per pixel.
+    size_t total = 0;
+    for (int j = 0; j < nv; ++j)
+      total += static_cast<size_t>(views[j].camera.intrinsics.width) * views[j].camera.intrinsics.height;
+    sc.packed.reserve(total > 0 ? total : 1);
+    size_t off = 0;
+    for (int j = 0; j < nv; ++j) {
+      const int vw = views[j].camera.intrinsics.width, vh = views[j].camera.intrinsics.height;
+      float4* dst = sc.packed.get() + off;
+      const dim3 b(32, 8), g(static_cast<unsigned>(ceil_div(vw, 32)), static_cast<unsigned>(ceil_div(vh, 8)));
+      R3D_LAUNCH(repack_kernel, g, b, 0, s, views[j].data, views[j].stride, vw, vh, dst);
+      launched("repack_kernel");
+      geo[j].data = dst;
+      off += static_cast<size_t>(vw) * vh;
+    }
     if (nv > 0)
       R3D_CUDA(cudaMemcpyAsync(sc.views.get(), geo, sizeof(ViewGeo) * nv, cudaMemcpyHostToDevice, s));
     sc.input.reserve(static_cast<size_t>(w) * h);

@@ -103,10 +103,14 @@ struct alignas(16) uint4 {
 struct alignas(8) uint2 {
   unsigned x, y;
 };
+struct alignas(16) float4 {
+  float x, y, z, w;
+};
 inline int4 make_int4(int x, int y, int z, int w) { return int4{x, y, z, w}; }
 inline int2 make_int2(int x, int y) { return int2{x, y}; }
 inline uint4 make_uint4(unsigned x, unsigned y, unsigned z, unsigned w) { return uint4{x, y, z, w}; }
 inline uint2 make_uint2(unsigned x, unsigned y) { return uint2{x, y}; }
+inline float4 make_float4(float x, float y, float z, float w) { return float4{x, y, z, w}; }
 
 namespace r3dsimt {
 
