@@ -17,7 +17,6 @@
 // reference's sequential loops, so results agree with a double-precision CPU
 // restatement to rounding, not bit for bit.
 #include <cmath>
-#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -128,7 +127,7 @@ constexpr int kWarpTableDoubles = kMaxSamples + 16;
 // J^T e = (p ncc - sum a n0) / |raw - mean|. The objective moments are double
 // (intensities shifted by `shift`, the base window's mean, to keep the
 // variance well conditioned); the Jacobian moments are T.
-template <class T, bool JAC, int U>
+template <class T, bool JAC>
 R3D_DEVICE void evaluate_group(const ViewGeo& g, bool active, double x, double y, const double* theta,
                                const Params& p, const double* table, double shift, int gl, int gsize, bool& valid,
                                double& ncc_out, double* hh, double* gg) {
@@ -179,7 +178,6 @@ R3D_DEVICE void evaluate_group(const ViewGeo& g, bool active, double x, double y
     // Window column and row of sample s, advanced by gsize per step.
     int col = gl % p.side, row = gl / p.side;
     const int dcol = gsize % p.side, drow = gsize / p.side;
-#pragma unroll(U)
     for (int s = gl; s < p.n; s += gsize) {
       const T dx = static_cast<T>(col * p.step - p.radius), dy = static_cast<T>(row * p.step - p.radius);
       const T sx = static_cast<T>(coord[col]), sy = static_cast<T>(coord[row]);
@@ -395,7 +393,7 @@ R3D_DEVICE void solve_damped(const double* hh, const double* gg, double* delta) 
 
 // One warp per depth-map pixel; per warp a table of kWarpTableDoubles
 // doubles in dynamic shared memory.
-template <class T, int U>
+template <class T>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, 2)
     refine_kernel(const float* R3D_RESTRICT input, float* depth, float* conf, int64_t stride,
                   const float* R3D_RESTRICT base, int64_t bstride, const ViewGeo* R3D_RESTRICT views, Params p,
@@ -464,7 +462,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, 2)
     const bool active = t < p.num_views;
     bool valid;
     double ncc;
-    evaluate_group<T, false, U>(views[active ? t : 0], active, xd, yd, theta0, p, table, mean, lane % gsize, gsize,
+    evaluate_group<T, false>(views[active ? t : 0], active, xd, yd, theta0, p, table, mean, lane % gsize, gsize,
                              valid, ncc, hh_v, gg_v);
     const uint32_t ok = r3dsimt::ballot(active && valid && ncc >= p.min_ncc);
     for (int j = 0; j < p.num_views; ++j) {
@@ -496,7 +494,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(256, 2)
   auto evaluate = [&](const double* theta, double* hh, double* gg) {
     bool valid;
     double ncc;
-    evaluate_group<T, true, U>(my_view, my_active, xd, yd, theta, p, table, mean, lane % gsize, gsize, valid, ncc,
+    evaluate_group<T, true>(my_view, my_active, xd, yd, theta, p, table, mean, lane % gsize, gsize, valid, ncc,
                             hh_v, gg_v);
     if (r3dsimt::ballot(!valid) != 0) return -__builtin_huge_val();
     double tot[10] = {ncc, hh_v[0], hh_v[1], hh_v[2], hh_v[3], hh_v[4], hh_v[5], gg_v[0], gg_v[1], gg_v[2]};
@@ -649,12 +647,7 @@ void launch_refine(const float* input, float* depth, float* conf, int64_t stride
                    cudaStream_t s) {
   const int64_t warps = static_cast<int64_t>(p.width) * p.height;
   const size_t smem = sizeof(double) * kWarpTableDoubles * 8;
-  // The window-sample loop unrolled by 1 (default) or 2 (R3DGPU_REFINE_UNROLL=2).
-  static const int unroll = [] {
-    const char* e = std::getenv("R3DGPU_REFINE_UNROLL");
-    return e != nullptr && std::atoi(e) == 2 ? 2 : 1;
-  }();
-  auto kernel = unroll == 2 ? refine_kernel<T, 2> : refine_kernel<T, 1>;
+  auto kernel = refine_kernel<T>;
   R3D_LAUNCH(kernel, static_cast<unsigned>(ceil_div64(warps, 8)), 256, smem, s, input, depth, conf, stride, base,
              bstride, views, p, counters);
   launched(sizeof(T) == 8 ? "refine_kernel<f64>" : "refine_kernel<f32>");
