@@ -947,7 +947,8 @@ def main():
         if per_pair is not None:
             line["per_pair"] = per_pair
             line["batched_vs_per_pair"] = value / per_pair["value"]
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
+            # The CPU baseline and the other stages' lines at N = 1 only.
             line["cpu_baseline"] = cpu_baseline(specs)
             line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
             line["rectify"] = measure_rectify(lib, dev, stream, args.steps, args.warmup, peak)
