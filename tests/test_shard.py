@@ -116,3 +116,85 @@ def test_lost_rank_ends_the_exchange_with_an_error(simt_matcher):
         p.join(timeout=120)
     assert rank == 0 and outcome.startswith("error")
     assert procs[1].exitcode == 3
+
+
+# ------------------------------------------------------------------ depth stage
+def _depth_inputs():
+    """Four small views with sparse depths (a few hundred refinement warps)."""
+    from regard3d_mvs_b200.multi_view import depth_stage_scene
+
+    scene = depth_stage_scene(4, 40, 30, partners=2)
+    rng = np.random.default_rng(5)
+    maps, images = [], []
+    for i, v in enumerate(scene["views"]):
+        keep = np.zeros(v["depth"].shape, bool)
+        for _ in range(8):
+            y, x = rng.integers(4, 26), rng.integers(4, 36)
+            keep[y - 1:y + 2, x - 1:x + 2] = True
+        keep[10:20, 10:30] = True  # a block the consistency check sees in the neighbours
+        maps.append({"camera": v["camera"], "depth": np.where(keep, v["depth"], 0).astype(np.float32),
+                     "confidence": np.zeros(v["depth"].shape, np.float32),
+                     "pair_mask": np.ones(v["depth"].shape, np.uint16), "color": v["color"], "view": i,
+                     "partners": scene["partners"][i]})
+        images.append({"camera": v["camera"], "data": None, "gray": v["gray"]})
+    return maps, images, scene["partners"]
+
+
+def _depth_rank(rank, world, port, q):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=300))
+    try:
+        from regard3d_mvs_b200 import Matcher
+        from regard3d_mvs_b200.depth_maps import RefinementOptions
+        from regard3d_mvs_b200.shard import depth_stage_sharded
+
+        m = Matcher(SIMT_LIB, host_is_device=True)
+        maps, images, partners = _depth_inputs()
+        for im in images:
+            im["data"] = m.make_refinement_image(im.pop("gray"))
+        res, rst, cst = depth_stage_sharded(m, maps, images, partners, rank, world,
+                                            RefinementOptions(radius=2, step=2))
+        q.put((rank, [(r["depth"], r["support"]) for r in res], rst, cst))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_run_the_depth_stage(simt_matcher):
+    """Refinement of each rank's views, exchange, consistency of each rank's
+    views: the same maps and statistics as one process refining every view
+    and filtering all maps."""
+    from regard3d_mvs_b200.depth_maps import ConsistencyOptions, RefinementOptions
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_depth_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = {}
+    for _ in procs:
+        rank, res, rst, cst = q.get(timeout=600)
+        got[rank] = (res, rst, cst)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    maps, images, partners = _depth_inputs()
+    for im in images:
+        im["data"] = simt_matcher.make_refinement_image(im.pop("gray"))
+    rst = {"input": 0, "refined": 0, "kept": 0, "unconfirmed": 0}
+    for i, mp_ in enumerate(maps):
+        st = simt_matcher.refine_depth_map(mp_, images[i], [images[j] for j in partners[i]],
+                                           RefinementOptions(radius=2, step=2))
+        rst = {k: rst[k] + st[k] for k in rst}
+    cst = simt_matcher.filter_depth_maps(maps, partners, ConsistencyOptions())
+    assert rst["refined"] > 0 and cst["output"] > 0
+    for rank in (0, 1):
+        res, r_rst, r_cst = got[rank]
+        assert r_rst == rst and r_cst == cst
+        for (d, sup), ref in zip(res, maps):
+            assert np.array_equal(d, ref["depth"]) and np.array_equal(sup, ref["support"])
