@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "geom.cuh"
 #include "kernels.h"
 #include "api_guard.h"
 #include "matcher_internal.h"
@@ -34,13 +35,6 @@ R3D_DEVICE void count_warp(unsigned long long* counter, bool pred) {
 
 R3D_DEVICE int64_t at(const r3dgpu_depth_map& m, int x, int y) { return static_cast<int64_t>(y) * m.stride + x; }
 
-// Row i of a row-major 3x3 matrix times v, and row i of its transpose.
-R3D_DEVICE double row3(const double* m, int i, double x, double y, double z) {
-  return (m[3 * i] * x + m[3 * i + 1] * y) + m[3 * i + 2] * z;
-}
-R3D_DEVICE double col3(const double* m, int i, double x, double y, double z) {
-  return (m[i] * x + m[3 + i] * y) + m[6 + i] * z;
-}
 
 // ------------------------------------------------------------------ prepare
 // consistency.cpp:438-447 (confidence) and the valid-pixel count.

@@ -18,6 +18,7 @@
 #include <string>
 
 #include "common.cuh"
+#include "geom.cuh"
 #include "api_guard.h"
 #include "matcher_internal.h"
 
@@ -58,10 +59,6 @@ R3D_DEVICE float sample_disparity(const r3dgpu_pair_geometry& g, double u, doubl
   return g.disparity[yn * g.stride + xn];
 }
 
-// Row i of a row-major 3x3 matrix times (x, y, z).
-R3D_DEVICE double row3(const double* m, int i, double x, double y, double z) {
-  return (m[3 * i] * x + m[3 * i + 1] * y) + m[3 * i + 2] * z;
-}
 
 struct Cand {
   double w, k;

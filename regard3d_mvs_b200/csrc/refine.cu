@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "geom.cuh"
 #include "kernels.h"
 #include "api_guard.h"
 #include "matcher_internal.h"
@@ -100,9 +101,6 @@ R3D_DEVICE T warp_sum(T v) {
 // Finite (neither infinite nor NaN): v - v is 0 exactly then, NaN otherwise.
 R3D_DEVICE bool finite_d(double v) { return v - v == 0.0; }
 
-R3D_DEVICE double row3(const double* m, int i, double x, double y, double z) {
-  return (m[3 * i] * x + m[3 * i + 1] * y) + m[3 * i + 2] * z;
-}
 
 // Smallest power of two >= m (m in 1..8): the number of lane groups.
 R3D_DEVICE int groups_for(int m) { return m <= 1 ? 1 : (m <= 2 ? 2 : (m <= 4 ? 4 : 8)); }
