@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine", "rectify", "depth"),
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine", "rectify", "depth", "view"),
                     default="batch64",
                     help="combine / rectify / depth: only the multi-view combination of one view / the "
                          "rectification resampling of one pair / the depth stage after the combination "
@@ -633,6 +633,105 @@ def measure_depth(lib, dev, stream, steps: int, warmup: int, peak: float) -> dic
                                        f"{w}x{h}", "refined": ost["refined"]}}
 
 
+# A view's depth map on the device (r3dgpu_compute_depth_map): a 2048 x 1536
+# base image and 4 partners of a textured plane, each pair rectified (both
+# images), the 4 pairs matched in one batch (reference default options:
+# automatic hierarchy, +-4 ranges), combined into the grid's depth map.
+VIEW_W, VIEW_H, VIEW_F = 2048, 1536, 1800.0
+VIEW_PARTNERS = ((0.6, 0.0, 0.0), (-0.5, 0.3, 0.1), (0.2, -0.55, 0.0), (-0.3, -0.4, 0.2))
+
+
+def measure_view(lib, dev, stream, steps: int, warmup: int) -> dict:
+    """Device time of compute_depth_map for one view (inputs resident), end
+    to end through Matcher.compute_depth_map (host images in, maps out), and
+    the oracle's chain (rectify, match, combine) on the same view."""
+    import torch
+
+    from oracle import oracle as orc
+    from regard3d_mvs_b200.multi_view import CViewPair, c_grid, pair_geometry, pipeline_scene
+    from regard3d_mvs_b200.stereo import Matcher
+    from regard3d_mvs_b200.types import (CViewU16, MultiStereoOptions, StereoOptions, camera_struct, pinhole_struct,
+                                         to_c_options)
+
+    rig, base, pairs = pipeline_scene(VIEW_W, VIEW_H, VIEW_F, VIEW_PARTNERS, seed=4)
+    w, h = VIEW_W, VIEW_H
+    cam = {"model": 0, "width": w, "height": h, "fx": rig.K[0, 0], "fy": rig.K[1, 1], "cx": rig.K[0, 2],
+           "cy": rig.K[1, 2]}
+    keep = []
+
+    def dev_u16(a):
+        t = torch.from_numpy(a.view(np.int16)).to(dev)
+        keep.append(t)
+        return t.data_ptr()
+
+    cb = camera_struct(cam)
+    vb = CViewU16(dev_u16(base), w, h, w)
+    arr = (CViewPair * len(pairs))()
+    for i, p in enumerate(pairs):
+        q = arr[i]
+        q.partner = CViewU16(dev_u16(p["image"]), w, h, w)
+        q.partner_camera = camera_struct(cam)
+        q.base_from_rect[:] = [float(v) for v in (rig.R @ p["R_rect"].T).ravel()]
+        q.partner_from_rect[:] = [float(v) for v in (p["R_partner"] @ p["R_rect"].T).ravel()]
+        q.left, q.right = pinhole_struct(p["left"]), pinhole_struct(p["right"])
+        q.disparity_min, q.num_disparities = p["disparity_min"], p["num_disparities"]
+        q.geometry = pair_geometry(rig.grid(), p)
+    g = c_grid(rig.grid())
+    depth = torch.empty((h, w), dtype=torch.float32, device=dev)
+    conf = torch.empty_like(depth)
+    mask = torch.empty((h, w), dtype=torch.int16, device=dev)
+    so, mo = to_c_options(StereoOptions()), MultiStereoOptions().c()
+    cells = ctypes.c_uint64(0)
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def run():
+        _native_check(lib, lib.r3dgpu_compute_depth_map(ctypes.byref(vb), ctypes.byref(cb), ctypes.byref(g), arr,
+                                                        len(pairs), ctypes.byref(so), ctypes.byref(mo),
+                                                        depth.data_ptr(), conf.data_ptr(), mask.data_ptr(), w,
+                                                        ctypes.byref(cells), sptr))
+
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = int(lib.r3dgpu_launch_count())
+    a.record(stream)
+    for _ in range(steps):
+        run()
+    b.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b) / steps
+    launches = (int(lib.r3dgpu_launch_count()) - l0) // steps
+    full_cells = sum(w * h * p["num_disparities"] for p in pairs)
+    m = Matcher(device=dev.index or 0)
+    m.compute_depth_map(base, rig.grid(), pairs)
+    t0 = time.perf_counter()
+    for _ in range(max(1, steps // 2)):
+        got, _ = m.compute_depth_map(base, rig.grid(), pairs)
+    e2e_s = (time.perf_counter() - t0) / max(1, steps // 2)
+    # The oracle's chain on the same view (once).
+    t0 = time.perf_counter()
+    matched = []
+    for p in pairs:
+        left, lmask = orc.rectify_image(base, cam, rig.R @ p["R_rect"].T, p["left"])
+        right, rmask = orc.rectify_image(p["image"], cam, p["R_partner"] @ p["R_rect"].T, p["right"])
+        mt = orc.match_stereo(left, right, lmask, rmask, p["disparity_min"], p["num_disparities"], StereoOptions())
+        matched.append(dict(p, disparity=mt.disparity, confidence=mt.confidence))
+    ref = orc.combine_pairs(rig.grid(), matched, MultiStereoOptions())
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ref.depth, got.depth) and np.array_equal(ref.pair_mask, got.pair_mask))
+    return {"workload": f"a view's depth map: {w}x{h} base and 4 partners (plane scene), rectify + match (reference "
+                        "default options, one batch) + combine on the device",
+            "value": 1000.0 / ms, "unit": "depth maps/s", "ms_per_view": ms, "gpu_launches": launches,
+            "full_range_cells": full_cells, "aggregated_cells": int(cells.value),
+            "label_ranges": [p["num_disparities"] for p in pairs], "bit_exact_vs_oracle": same,
+            "valid_fraction": float((got.depth > 0).mean()),
+            "e2e": {"value": 1.0 / e2e_s, "unit": "depth maps/s", "h2d_bytes_per_step": 2 * w * h * (1 + len(pairs)),
+                    "d2h_bytes_per_step": 10 * w * h},
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "depth maps/s", "cores": orc.max_threads(), "kind": "port",
+                             "sample": "the same view once: rectify, match_stereo and combine_pairs of the oracle"}}
+
+
 SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
 SERVE_REQUEST_BUDGET = 118 << 30  # config 3's 150 GB: 118 GB for admitted requests + 2 x 16 GB worker scratch
 SERVE_WORKERS = 2
@@ -754,6 +853,13 @@ def main():
         if rank == 0:
             print(json.dumps(dict(r, metric="combine_pairs Gpixels/s", n_gpus=world, steps=args.steps,
                                   warmup=args.warmup, higher_is_better=True, data="synthetic")), flush=True)
+        return
+    if args.workload == "view":
+        dev0 = torch.device(f"cuda:{local}")
+        r = measure_view(lib, dev0, torch.cuda.current_stream(dev0), args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps(dict(r, metric="depth maps/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
+                                  higher_is_better=True, data="synthetic")), flush=True)
         return
     if args.workload == "depth":
         peak, _ = measured_peaks()
@@ -953,6 +1059,7 @@ def main():
             line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
             line["rectify"] = measure_rectify(lib, dev, stream, args.steps, args.warmup, peak)
             line["depth_stage"] = measure_depth(lib, dev, stream, args.steps, args.warmup, peak)
+            line["view_depth_map"] = measure_view(lib, dev, stream, args.steps, args.warmup)
         if args.serve and world == 1:
             # In a fresh process, with this one's device memory given back.
             del dL, dR, dD, dC

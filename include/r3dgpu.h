@@ -301,6 +301,37 @@ r3dgpu_status r3dgpu_combine_pairs_host(const r3dgpu_depth_grid* grid, const r3d
                                         int32_t count, const r3dgpu_multi_stereo_options* options, float* depth,
                                         float* confidence, uint16_t* pair_mask, int64_t stride);
 
+/* ------------------------------------------------------------------ a view's depth map
+ * The multi-view stage for one view on the device: every partner pair is
+ * rectified (r3dgpu_rectify_image_u16 of the base and the partner image),
+ * all pairs are matched in one batch (r3dgpu_match_stereo_batch) and the
+ * matched pairs are combined into the grid's depth map (r3dgpu_combine_pairs);
+ * rectified images and disparity maps never leave the device. Replaces the
+ * loop of r3d::compute_depth_map, src/r3d/mvs/multi_stereo.hpp:76-79
+ * (implementation src/r3d/mvs/multi_stereo.cpp:243-304), from the rectified
+ * pairs' geometry (which the caller's compute_rectification provides) on. */
+typedef struct r3dgpu_view_pair {
+  r3dgpu_view_u16 partner;           /* the partner's image (device memory) */
+  r3dgpu_camera partner_camera;
+  double base_from_rect[9];          /* R_base R_rect^T, row-major */
+  double partner_from_rect[9];       /* R_partner R_rect^T */
+  r3dgpu_pinhole left;               /* rectified base camera */
+  r3dgpu_pinhole right;              /* rectified partner camera (same height) */
+  int32_t disparity_min;
+  int32_t num_disparities;
+  r3dgpu_pair_geometry geometry;     /* grid_to_rect, fb, offset, partner_center (map pointers ignored) */
+} r3dgpu_view_pair;
+
+/* Depth, confidence and pair mask of the grid (device memory, `stride`
+ * elements per row) from the base image (device) and up to 16 pairs;
+ * *cells (may be NULL) receives the matched cells of all pairs. Runs on
+ * `stream` and synchronises it. */
+r3dgpu_status r3dgpu_compute_depth_map(const r3dgpu_view_u16* base, const r3dgpu_camera* base_camera,
+                                       const r3dgpu_depth_grid* grid, const r3dgpu_view_pair* pairs, int32_t count,
+                                       const r3dgpu_stereo_options* stereo,
+                                       const r3dgpu_multi_stereo_options* multi, float* depth, float* confidence,
+                                       uint16_t* pair_mask, int64_t stride, uint64_t* cells, void* stream);
+
 /* ------------------------------------------------------------------ depth maps
  * Multi-view geometric consistency of depth maps (the step after the
  * combination). Replaces prepare_depth_map, check_consistency,

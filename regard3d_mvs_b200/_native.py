@@ -53,6 +53,7 @@ EXPORTS = (
     "r3dgpu_make_refinement_image",
     "r3dgpu_refine_depth_map",
     "r3dgpu_refine_depth_map_host",
+    "r3dgpu_compute_depth_map",
     "r3dgpu_default_consistency_options",
     "r3dgpu_prepare_depth_map",
     "r3dgpu_check_consistency",
@@ -162,6 +163,13 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
                                           i32, ro, rs, P]
     L.r3dgpu_refine_depth_map_host.argtypes = [P, P, ctypes.c_int64, ctypes.POINTER(CPinholeCamera), i32, i32, ri,
                                                ri, i32, ro, rs]
+    from .multi_view import CViewPair
+
+    L.r3dgpu_compute_depth_map.argtypes = [ctypes.POINTER(CViewU16), ctypes.POINTER(CCamera),
+                                           ctypes.POINTER(CDepthGrid), ctypes.POINTER(CViewPair), i32,
+                                           ctypes.POINTER(COptions), ctypes.POINTER(CMultiStereoOptions), P, P, P,
+                                           ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64), P]
+    L.r3dgpu_compute_depth_map.restype = st
     L.r3dgpu_write_depth_map.argtypes = [ctypes.c_char_p, dm, i32, P]
     L.r3dgpu_read_depth_map_info.argtypes = [ctypes.c_char_p, dm]
     L.r3dgpu_read_depth_map.argtypes = [ctypes.c_char_p, dm]

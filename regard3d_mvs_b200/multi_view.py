@@ -15,7 +15,7 @@ import ctypes
 
 import numpy as np
 
-from .types import CDepthGrid, CPairGeometry
+from .types import CCamera, CDepthGrid, CPairGeometry, CPinhole, CViewU16
 
 
 def c_grid(grid: dict) -> CDepthGrid:
@@ -29,24 +29,32 @@ def c_grid(grid: dict) -> CDepthGrid:
     return g
 
 
+def pair_geometry(grid: dict, p: dict) -> CPairGeometry:
+    """The combination geometry of a pair (no maps): grid-to-rectified
+    homography K_r R_r R_g^T K_g^-1, f * b, disparity offset, partner centre."""
+    q = CPairGeometry()
+    k_inv = np.linalg.inv(np.asarray(grid["K"], np.float64))
+    r_gt = np.asarray(grid["R"], np.float64).T
+    kr = np.asarray(p["K_rect"], np.float64)
+    h = kr @ np.asarray(p["R_rect"], np.float64) @ r_gt @ k_inv
+    q.grid_to_rect[:] = [float(v) for v in h.ravel()]
+    q.fb = float(kr[0, 0] * p["baseline"])
+    q.offset = float(kr[0, 2] - p["cx_right"])
+    q.partner_center[:] = [float(v) for v in np.asarray(p["centre"], np.float64)]
+    return q
+
+
 def c_pairs(grid: dict, pairs: list[dict]):
     """(array of CPairGeometry with host map pointers, the arrays they point into)."""
     arr = (CPairGeometry * max(len(pairs), 1))()
     keep = []
-    k_inv = np.linalg.inv(np.asarray(grid["K"], np.float64))
-    r_gt = np.asarray(grid["R"], np.float64).T
     for i, p in enumerate(pairs):
-        kr = np.asarray(p["K_rect"], np.float64)
-        h = kr @ np.asarray(p["R_rect"], np.float64) @ r_gt @ k_inv
         d = np.ascontiguousarray(p["disparity"], np.float32)
         c = p.get("confidence")
         c = None if c is None else np.ascontiguousarray(c, np.float32)
         keep += [d, c]
+        arr[i] = pair_geometry(grid, p)
         q = arr[i]
-        q.grid_to_rect[:] = [float(v) for v in h.ravel()]
-        q.fb = float(kr[0, 0] * p["baseline"])
-        q.offset = float(kr[0, 2] - p["cx_right"])
-        q.partner_center[:] = [float(v) for v in np.asarray(p["centre"], np.float64)]
         q.disparity = d.ctypes.data
         q.confidence = None if c is None else c.ctypes.data
         q.height, q.width = d.shape
@@ -188,3 +196,62 @@ def depth_stage_scene(n_views: int, width: int, height: int, partners: int = 4) 
     order = [sorted((j for j in range(n_views) if j != i), key=lambda j: (abs(j - i), j))[:partners]
              for i in range(n_views)]
     return {"views": views, "partners": order}
+
+
+# ---------------------------------------------------------------- a view's depth map on the device
+class CViewPair(ctypes.Structure):
+    """r3dgpu_view_pair: one partner pair of r3dgpu_compute_depth_map."""
+
+    _fields_ = [
+        ("partner", CViewU16),
+        ("partner_camera", CCamera),
+        ("base_from_rect", ctypes.c_double * 9),
+        ("partner_from_rect", ctypes.c_double * 9),
+        ("left", CPinhole),
+        ("right", CPinhole),
+        ("disparity_min", ctypes.c_int32),
+        ("num_disparities", ctypes.c_int32),
+        ("geometry", CPairGeometry),
+    ]
+
+
+def pipeline_scene(w: int, h: int, f: float, partners, seed: int = 0, plane=None):
+    """A base view and partners of Rig looking at a textured plane: source
+    images (u16, pinhole cameras), each pair's rectification (rotations
+    R_source R_rect^T, rectified cameras), disparity range and combination
+    geometry. Returns (rig, base image, list of pair dicts)."""
+    rig = Rig(w=w, h=h, f=f, partners=partners)
+    plane = plane or Plane()
+    rng = np.random.default_rng(seed)
+    u = np.cross(plane.n, [0.0, 1.0, 0.0])
+    u /= np.linalg.norm(u)
+    v = np.cross(plane.n, u)
+    scale = f / 150.0 * 8.0
+
+    def render(R, C):
+        K_inv = np.linalg.inv(rig.K)
+        ys, xs = np.mgrid[0:h, 0:w].astype(np.float64)
+        dirs = np.stack([xs, ys, np.ones_like(xs)], -1) @ (R.T @ K_inv).T
+        t = (plane.dist - plane.n @ C) / (dirs @ plane.n)
+        pts = C + t[..., None] * dirs
+        pu, pv = pts @ u, pts @ v
+        acc = np.zeros_like(xs)
+        for kx, ky, ph in DEPTH_WAVES:
+            acc += np.sin(scale * (kx * pu + ky * pv) / 4.0 + ph)
+        img = 128.0 + 22.0 * acc + rng.normal(0, 1.5, acc.shape)
+        return (np.clip(img, 0, 255).astype(np.uint16) * 257).astype(np.uint16)
+
+    base = render(rig.R, rig.C)
+    pairs = []
+    for (Rp, Cp) in rig.partners:
+        rp = rig.rectify((Rp, Cp))
+        d = plane_disparity(rig, rp, plane)
+        fin = d[np.isfinite(d)]
+        dmin = int(np.floor(fin.min())) - 8
+        nd = (int(np.ceil(fin.max())) + 8 - dmin + 1 + 15) // 16 * 16
+        K = rp["K_rect"]
+        pairs.append(dict(rp, image=render(Rp, Cp), R_partner=Rp, disparity_min=dmin, num_disparities=nd,
+                          left={"width": w, "height": h, "fx": K[0, 0], "fy": K[1, 1], "cx": K[0, 2], "cy": K[1, 2]},
+                          right={"width": w, "height": h, "fx": K[0, 0], "fy": K[1, 1], "cx": rp["cx_right"],
+                                 "cy": K[1, 2]}))
+    return rig, base, pairs

@@ -110,6 +110,58 @@ class Matcher:
         del keep
         return DepthMap(depth, conf, mask)
 
+    # ---------------------------------------------------------------- a view's depth map
+    def compute_depth_map(self, base: np.ndarray, grid: dict, pairs: list[dict], stereo: StereoOptions | None = None,
+                          multi=None):
+        """r3dgpu_compute_depth_map: rectification, batch matching and
+        combination of a view's pairs on the device. `grid` as for
+        combine_pairs (pinhole K, R, C, size; also the base camera); each pair
+        carries its partner image ("image"), the partner's rotation
+        ("R_partner"), the rectification ("R_rect", "K_rect", "baseline",
+        "cx_right", "centre", "left" and "right" pinholes) and its disparity
+        range. Returns (DepthMap, matched cells)."""
+        from .multi_view import CViewPair, c_grid, pair_geometry
+        from .types import DepthMap, MultiStereoOptions, camera_struct, pinhole_struct
+
+        keep: list = []
+        b = _u16(base)
+        h, w = b.shape
+        K = np.asarray(grid["K"], np.float64)
+        cam = {"model": 0, "width": w, "height": h, "fx": K[0, 0], "fy": K[1, 1], "cx": K[0, 2], "cy": K[1, 2]}
+        cb = camera_struct(cam)
+        vb = CViewU16(self._to_device(b, keep), w, h, w)
+        arr = (CViewPair * max(1, len(pairs)))()
+        R_base = np.asarray(grid["R"], np.float64)
+        for i, p in enumerate(pairs):
+            q = arr[i]
+            img = _u16(p["image"])
+            ph, pw = img.shape
+            q.partner = CViewU16(self._to_device(img, keep), pw, ph, pw)
+            q.partner_camera = camera_struct(dict(cam, width=pw, height=ph))
+            R_rect = np.asarray(p["R_rect"], np.float64)
+            q.base_from_rect[:] = [float(v) for v in (R_base @ R_rect.T).ravel()]
+            q.partner_from_rect[:] = [float(v) for v in (np.asarray(p["R_partner"], np.float64) @ R_rect.T).ravel()]
+            q.left, q.right = pinhole_struct(p["left"]), pinhole_struct(p["right"])
+            q.disparity_min, q.num_disparities = int(p["disparity_min"]), int(p["num_disparities"])
+            q.geometry = pair_geometry(grid, p)
+        g = c_grid(grid)
+        gh, gw = g.height, g.width
+        dp, dobj = self._empty_device((gh, gw), keep)
+        cp, cobj = self._empty_device((gh, gw), keep)
+        mp, mobj = self._empty_device((gh, gw), keep)  # float32-sized buffer holds the u16 mask
+        o = _opts(stereo)
+        mo = (multi or MultiStereoOptions()).c()
+        cells = ctypes.c_uint64(0)
+        self._check(self.lib.r3dgpu_compute_depth_map(ctypes.byref(vb), ctypes.byref(cb), ctypes.byref(g), arr,
+                                                      len(pairs), ctypes.byref(o), ctypes.byref(mo), dp, cp, mp, gw,
+                                                      ctypes.byref(cells), None))
+        depth = self._to_host((dp, dobj), (gh, gw))
+        conf = self._to_host((cp, cobj), (gh, gw))
+        # The u16 mask is dense (gw per row) in the first half of its float-sized buffer.
+        mask = np.ascontiguousarray(self._to_host((mp, mobj), (gh, gw))).reshape(-1).view(np.uint16)[:gh * gw]
+        mask = mask.reshape(gh, gw)
+        return DepthMap(depth.copy(), conf.copy(), mask.copy()), int(cells.value)
+
     # ---------------------------------------------------------------- r3d::rectify_image
     def rectify_image(self, src: np.ndarray, camera: dict, source_from_target, target: dict):
         """Resamples a one-channel u16 or f32 image of `camera` ({model, width,
