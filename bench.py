@@ -555,12 +555,6 @@ def measure_depth(lib, dev, stream, steps: int, warmup: int, peak: float) -> dic
         r = CRefinementImage()
         r.camera, r.data, r.stride = cams[i], himg[i].ctypes.data, 3 * w
         hrimg.append(r)
-    hpartner = []
-    for i in range(n):
-        arr = (CRefinementImage * len(partners[i]))()
-        for k, j in enumerate(partners[i]):
-            arr[k] = hrimg[j]
-        hpartner.append(arr)
     hdepth = [np.empty((h, w), np.float32) for _ in views]
     hconf = [np.zeros((h, w), np.float32) for _ in views]
     hmask = [np.ones((h, w), np.uint16) for _ in views]
@@ -575,21 +569,21 @@ def measure_depth(lib, dev, stream, steps: int, warmup: int, peak: float) -> dic
     def host_step():
         for i in range(n):
             hdepth[i][...] = views[i]["depth"]
-            _native_check(lib, lib.r3dgpu_refine_depth_map_host(hdepth[i].ctypes.data, hconf[i].ctypes.data, w,
-                                                                ctypes.byref(cams[i]), w, h, ctypes.byref(hrimg[i]),
-                                                                hpartner[i], len(partners[i]), ctypes.byref(f32),
-                                                                ctypes.byref(rstats)))
-        _native_check(lib, lib.r3dgpu_filter_depth_maps_host(hmaps, n, off.ctypes.data, idx.ctypes.data,
-                                                             ctypes.byref(copts), ctypes.byref(cstats)))
+            hconf[i][...] = 0.0
+        _native_check(lib, lib.r3dgpu_depth_stage_host(hmaps, hrimg_arr, n, off.ctypes.data, idx.ctypes.data,
+                                                       ctypes.byref(f32), ctypes.byref(copts), ctypes.byref(rstats),
+                                                       ctypes.byref(cstats)))
 
+    hrimg_arr = (CRefinementImage * n)(*hrimg)
     host_step()
     t0 = time.perf_counter()
     for _ in range(max(1, steps // 2)):
         host_step()
     e2e_s = (time.perf_counter() - t0) / max(1, steps // 2)
-    img_bytes = 12 * w * h
-    h2d = n * (img_bytes * (1 + len(partners[0])) + 8 * w * h) + n * (4 + 4 + 2 + 3) * w * h
-    d2h = n * 8 * w * h + n * 5 * w * h
+    # One call per step: every refinement image and map in once (12 + 13 B per
+    # pixel), depth, confidence and support out (9 B per pixel).
+    h2d = n * 25 * w * h
+    d2h = n * 9 * w * h
 
     # The float path's error and the oracle's time on a crop of view 0.
     cw, ch = DEPTH_CROP

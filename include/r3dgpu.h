@@ -520,6 +520,20 @@ r3dgpu_status r3dgpu_refine_depth_map_host(float* depth, float* confidence, int6
                                            const r3dgpu_refinement_image* views, int32_t num_views,
                                            const r3dgpu_refinement_options* options, r3dgpu_refinement_stats* stats);
 
+/* The depth stage of a set of views in one call (host maps and images):
+ * every view refined against its neighbours' refinement images
+ * (r3dgpu_refine_depth_map with views = its neighbour list, in order), then
+ * r3dgpu_filter_depth_maps of all maps over the same neighbour lists; each
+ * image is copied to the device once, and depth, confidence and support come
+ * back. The reference runs the two stages view by view
+ * (src/r3d/mvs/refinement.hpp:65-68, src/r3d/mvs/consistency.hpp:110-115). */
+r3dgpu_status r3dgpu_depth_stage_host(r3dgpu_depth_map* maps, const r3dgpu_refinement_image* images, int32_t count,
+                                      const int32_t* neighbour_offset, const int32_t* neighbour_index,
+                                      const r3dgpu_refinement_options* refine,
+                                      const r3dgpu_consistency_options* consistency,
+                                      r3dgpu_refinement_stats* refine_stats,
+                                      r3dgpu_consistency_stats* consistency_stats);
+
 /* Frees the device and pinned host buffers that this thread's calls keep on
  * its current device for reuse (they grow to the largest call made so far);
  * the next call allocates them again. No reference counterpart. */

@@ -54,6 +54,7 @@ EXPORTS = (
     "r3dgpu_refine_depth_map",
     "r3dgpu_refine_depth_map_host",
     "r3dgpu_compute_depth_map",
+    "r3dgpu_depth_stage_host",
     "r3dgpu_default_consistency_options",
     "r3dgpu_prepare_depth_map",
     "r3dgpu_check_consistency",
@@ -170,6 +171,8 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
                                            ctypes.POINTER(COptions), ctypes.POINTER(CMultiStereoOptions), P, P, P,
                                            ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64), P]
     L.r3dgpu_compute_depth_map.restype = st
+    L.r3dgpu_depth_stage_host.argtypes = [dm, ri, i32, P, P, ro, co, rs, cs]
+    L.r3dgpu_depth_stage_host.restype = st
     L.r3dgpu_write_depth_map.argtypes = [ctypes.c_char_p, dm, i32, P]
     L.r3dgpu_read_depth_map_info.argtypes = [ctypes.c_char_p, dm]
     L.r3dgpu_read_depth_map.argtypes = [ctypes.c_char_p, dm]

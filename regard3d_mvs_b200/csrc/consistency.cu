@@ -574,6 +574,82 @@ r3dgpu_status single_filter(r3dgpu_depth_map* map, const char* what, uint64_t* r
   });
 }
 
+// Device copies of host maps (depth, confidence, pair mask, support, colour)
+// in one per-thread staging buffer, followed by `extra` bytes for the caller;
+// download() copies depth, support and, if asked, confidence back.
+struct HostMaps {
+  r3dgpu_depth_map* host;
+  int count;
+  std::vector<r3dgpu_depth_map> dev;
+  unsigned char* extra = nullptr;
+
+  HostMaps(r3dgpu_depth_map* maps, int n, size_t extra_bytes, cudaStream_t s) : host(maps), count(n) {
+    if (n < 0 || (n > 0 && maps == nullptr)) fail(R3DGPU_EINVAL, "filter_depth_maps: null argument");
+    for (int i = 0; i < n; ++i) check_map(&maps[i], "filter_depth_maps");
+    auto up = [](size_t b) { return (b + 255) & ~static_cast<size_t>(255); };
+    size_t bytes = extra_bytes;
+    for (int i = 0; i < n; ++i) {
+      const size_t px = static_cast<size_t>(maps[i].width) * maps[i].height;
+      bytes += up(4 * px) + up(4 * px) + up(2 * px) + up(px) + (maps[i].color ? up(3 * px) : 0);
+    }
+    thread_local DeviceBuffer<unsigned char> io;
+    io.reserve(bytes > 0 ? bytes : 1);
+    unsigned char* p = io.get();
+    auto take = [&](size_t b) {
+      unsigned char* at = p;
+      p += up(b);
+      return at;
+    };
+    dev.assign(maps, maps + n);
+    for (int i = 0; i < n; ++i) {
+      const r3dgpu_depth_map& h = maps[i];
+      r3dgpu_depth_map& d = dev[i];
+      const size_t w = static_cast<size_t>(h.width), px = w * h.height;
+      d.stride = h.width;
+      d.depth = reinterpret_cast<float*>(take(4 * px));
+      d.confidence = reinterpret_cast<float*>(take(4 * px));
+      d.pair_mask = reinterpret_cast<uint16_t*>(take(2 * px));
+      d.support = reinterpret_cast<uint8_t*>(take(px));
+      if (h.color != nullptr) {
+        d.color = take(3 * px);
+        d.color_stride = 3 * h.width;
+      }
+      if (px == 0) continue;
+      R3D_CUDA(cudaMemcpy2DAsync(d.depth, 4 * w, h.depth, 4 * h.stride, 4 * w, h.height, cudaMemcpyHostToDevice, s));
+      if (h.confidence != nullptr)
+        R3D_CUDA(cudaMemcpy2DAsync(d.confidence, 4 * w, h.confidence, 4 * h.stride, 4 * w, h.height,
+                                   cudaMemcpyHostToDevice, s));
+      else
+        R3D_CUDA(cudaMemsetAsync(d.confidence, 0, 4 * px, s));
+      if (h.pair_mask != nullptr)
+        R3D_CUDA(cudaMemcpy2DAsync(d.pair_mask, 2 * w, h.pair_mask, 2 * h.stride, 2 * w, h.height,
+                                   cudaMemcpyHostToDevice, s));
+      else
+        R3D_CUDA(cudaMemsetAsync(d.pair_mask, 0, 2 * px, s));
+      if (h.color != nullptr)
+        R3D_CUDA(cudaMemcpy2DAsync(const_cast<uint8_t*>(d.color), 3 * w, h.color, h.color_stride, 3 * w, h.height,
+                                   cudaMemcpyHostToDevice, s));
+    }
+    extra = p;
+  }
+
+  void download(bool confidence, cudaStream_t s) {
+    for (int i = 0; i < count; ++i) {
+      const r3dgpu_depth_map& h = host[i];
+      const r3dgpu_depth_map& d = dev[i];
+      const size_t w = static_cast<size_t>(h.width);
+      if (w == 0 || h.height == 0) continue;
+      R3D_CUDA(cudaMemcpy2DAsync(h.depth, 4 * h.stride, d.depth, 4 * w, 4 * w, h.height, cudaMemcpyDeviceToHost, s));
+      if (confidence && h.confidence != nullptr)
+        R3D_CUDA(cudaMemcpy2DAsync(h.confidence, 4 * h.stride, d.confidence, 4 * w, 4 * w, h.height,
+                                   cudaMemcpyDeviceToHost, s));
+      if (h.support != nullptr)
+        R3D_CUDA(cudaMemcpy2DAsync(h.support, h.stride, d.support, w, w, h.height, cudaMemcpyDeviceToHost, s));
+    }
+    R3D_CUDA(cudaStreamSynchronize(s));
+  }
+};
+
 }  // namespace
 }  // namespace r3dgpu
 
@@ -651,64 +727,70 @@ r3dgpu_status r3dgpu_filter_depth_maps_host(r3dgpu_depth_map* maps, int32_t coun
                                             const r3dgpu_consistency_options* options,
                                             r3dgpu_consistency_stats* stats) {
   return guard([&] {
-    if (count < 0 || (count > 0 && maps == nullptr)) fail(R3DGPU_EINVAL, "filter_depth_maps: null argument");
-    for (int i = 0; i < count; ++i) check_map(&maps[i], "filter_depth_maps");
     cudaStream_t s = nullptr;
-    // One staging buffer: depth, confidence, pair mask, support, colour of every map.
-    auto up = [](size_t n) { return (n + 255) & ~static_cast<size_t>(255); };
-    size_t bytes = 0;
-    for (int i = 0; i < count; ++i) {
-      const size_t px = static_cast<size_t>(maps[i].width) * maps[i].height;
-      bytes += up(4 * px) + up(4 * px) + up(2 * px) + up(px) + (maps[i].color ? up(3 * px) : 0);
-    }
-    thread_local DeviceBuffer<unsigned char> io;
-    io.reserve(bytes > 0 ? bytes : 1);
-    unsigned char* p = io.get();
-    auto take = [&](size_t n) {
-      unsigned char* at = p;
-      p += up(n);
-      return at;
+    HostMaps hm(maps, count, 0, s);
+    filter_maps(hm.dev.data(), count, neighbour_offset, neighbour_index, options_or_default(options), stats, s);
+    hm.download(false, s);
+  });
+}
+
+r3dgpu_status r3dgpu_depth_stage_host(r3dgpu_depth_map* maps, const r3dgpu_refinement_image* images, int32_t count,
+                                      const int32_t* neighbour_offset, const int32_t* neighbour_index,
+                                      const r3dgpu_refinement_options* refine,
+                                      const r3dgpu_consistency_options* consistency,
+                                      r3dgpu_refinement_stats* refine_stats,
+                                      r3dgpu_consistency_stats* consistency_stats) {
+  return guard([&] {
+    if (count > 0 && (images == nullptr || neighbour_offset == nullptr))
+      fail(R3DGPU_EINVAL, "depth_stage: null argument");
+    cudaStream_t s = nullptr;
+    auto image_bytes = [&](int i) {
+      return sizeof(float) * 3 * static_cast<size_t>(images[i].camera.intrinsics.width) *
+             images[i].camera.intrinsics.height;
     };
-    std::vector<r3dgpu_depth_map> dev(maps, maps + count);
+    size_t extra = 0;
+    for (int i = 0; i < count; ++i) extra += (image_bytes(i) + 255) & ~static_cast<size_t>(255);
+    HostMaps hm(maps, count, extra, s);
+    // Every refinement image once.
+    std::vector<r3dgpu_refinement_image> dimg(images, images + count);
+    unsigned char* at = hm.extra;
     for (int i = 0; i < count; ++i) {
-      const r3dgpu_depth_map& h = maps[i];
-      r3dgpu_depth_map& d = dev[i];
-      const size_t w = static_cast<size_t>(h.width), px = w * h.height;
-      d.stride = h.width;
-      d.depth = reinterpret_cast<float*>(take(4 * px));
-      d.confidence = reinterpret_cast<float*>(take(4 * px));
-      d.pair_mask = reinterpret_cast<uint16_t*>(take(2 * px));
-      d.support = reinterpret_cast<uint8_t*>(take(px));
-      if (px == 0) continue;
-      R3D_CUDA(cudaMemcpy2DAsync(d.depth, 4 * w, h.depth, 4 * h.stride, 4 * w, h.height, cudaMemcpyHostToDevice, s));
-      if (h.confidence != nullptr)
-        R3D_CUDA(cudaMemcpy2DAsync(d.confidence, 4 * w, h.confidence, 4 * h.stride, 4 * w, h.height,
-                                   cudaMemcpyHostToDevice, s));
-      else
-        R3D_CUDA(cudaMemsetAsync(d.confidence, 0, 4 * px, s));
-      if (h.pair_mask != nullptr)
-        R3D_CUDA(cudaMemcpy2DAsync(d.pair_mask, 2 * w, h.pair_mask, 2 * h.stride, 2 * w, h.height,
-                                   cudaMemcpyHostToDevice, s));
-      else
-        R3D_CUDA(cudaMemsetAsync(d.pair_mask, 0, 2 * px, s));
-      if (h.color != nullptr) {
-        uint8_t* dc = take(3 * px);
-        R3D_CUDA(cudaMemcpy2DAsync(dc, 3 * w, h.color, h.color_stride, 3 * w, h.height, cudaMemcpyHostToDevice, s));
-        d.color = dc;
-        d.color_stride = 3 * h.width;
+      const int w = images[i].camera.intrinsics.width, h = images[i].camera.intrinsics.height;
+      if (w > 0 && h > 0) {
+        if (images[i].data == nullptr || images[i].stride < 3LL * w)
+          fail(R3DGPU_EINVAL, "depth_stage: image " + std::to_string(i) + " has no data");
+        R3D_CUDA(cudaMemcpy2DAsync(at, sizeof(float) * 3 * w, images[i].data, sizeof(float) * images[i].stride,
+                                   sizeof(float) * 3 * w, h, cudaMemcpyHostToDevice, s));
       }
+      dimg[i].data = reinterpret_cast<const float*>(at);
+      dimg[i].stride = 3LL * w;
+      at += (image_bytes(i) + 255) & ~static_cast<size_t>(255);
     }
-    filter_maps(dev.data(), count, neighbour_offset, neighbour_index, options_or_default(options), stats, s);
+    r3dgpu_refinement_stats total{};
+    std::vector<r3dgpu_refinement_image> views;
     for (int i = 0; i < count; ++i) {
-      const r3dgpu_depth_map& h = maps[i];
-      const r3dgpu_depth_map& d = dev[i];
-      const size_t w = static_cast<size_t>(h.width);
-      if (w == 0 || h.height == 0) continue;
-      R3D_CUDA(cudaMemcpy2DAsync(h.depth, 4 * h.stride, d.depth, 4 * w, 4 * w, h.height, cudaMemcpyDeviceToHost, s));
-      if (h.support != nullptr)
-        R3D_CUDA(cudaMemcpy2DAsync(h.support, h.stride, d.support, w, w, h.height, cudaMemcpyDeviceToHost, s));
+      if (neighbour_offset[i + 1] < neighbour_offset[i]) fail(R3DGPU_EINVAL, "depth_stage: neighbour offsets decrease");
+      views.clear();
+      for (int k = neighbour_offset[i]; k < neighbour_offset[i + 1]; ++k) {
+        if (neighbour_index == nullptr || neighbour_index[k] < 0 || neighbour_index[k] >= count)
+          fail(R3DGPU_EINVAL, "depth_stage: neighbour index out of range");
+        views.push_back(dimg[neighbour_index[k]]);
+      }
+      r3dgpu_depth_map& d = hm.dev[i];
+      r3dgpu_refinement_stats st{};
+      const r3dgpu_status rs = r3dgpu_refine_depth_map(d.depth, d.confidence, d.stride, &d.camera, d.width, d.height,
+                                                       &dimg[i], views.data(), static_cast<int32_t>(views.size()),
+                                                       refine, &st, s);
+      if (rs != R3DGPU_OK) fail(rs, r3dgpu_last_error());
+      total.input += st.input;
+      total.refined += st.refined;
+      total.kept += st.kept;
+      total.unconfirmed += st.unconfirmed;
     }
-    R3D_CUDA(cudaStreamSynchronize(s));
+    filter_maps(hm.dev.data(), count, neighbour_offset, neighbour_index, options_or_default(consistency),
+                consistency_stats, s);
+    hm.download(true, s);
+    if (refine_stats != nullptr) *refine_stats = total;
   });
 }
 

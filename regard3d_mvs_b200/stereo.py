@@ -110,6 +110,35 @@ class Matcher:
         del keep
         return DepthMap(depth, conf, mask)
 
+    def depth_stage(self, maps: list[dict], images: Sequence[dict], neighbours: Sequence[Sequence[int]],
+                    refine=None, consistency=None) -> tuple[dict, dict]:
+        """r3dgpu_depth_stage_host: each view refined against its neighbours'
+        refinement images ({camera, data}), then the consistency filter of
+        all maps over the same neighbour lists; maps' depth, confidence and
+        support are updated in place. Returns (refinement, consistency) statistics."""
+        from .depth_maps import (CConsistencyStats, CDepthMap, ConsistencyOptions, CRefinementImage,
+                                 CRefinementStats, RefinementOptions, c_depth_map, c_refinement_image,
+                                 neighbour_lists, normalise)
+
+        norm = [normalise(m) for m in maps]
+        arr = (CDepthMap * max(1, len(norm)))()
+        for i, n in enumerate(norm):
+            arr[i] = c_depth_map(n, lambda a: a.ctypes.data)
+        data = [np.ascontiguousarray(im["data"], np.float32) for im in images]
+        imgs = (CRefinementImage * max(1, len(images)))()
+        for i, (im, d) in enumerate(zip(images, data)):
+            imgs[i] = c_refinement_image({"camera": im["camera"], "data": d}, lambda a: a.ctypes.data)
+        off, idx = neighbour_lists(neighbours)
+        rst, cst = CRefinementStats(), CConsistencyStats()
+        ro = (refine or RefinementOptions()).c()
+        co = (consistency or ConsistencyOptions()).c()
+        self._check(self.lib.r3dgpu_depth_stage_host(arr, imgs, len(maps), off.ctypes.data, idx.ctypes.data,
+                                                     ctypes.byref(ro), ctypes.byref(co), ctypes.byref(rst),
+                                                     ctypes.byref(cst)))
+        for m, n in zip(maps, norm):
+            m["depth"], m["confidence"], m["support"] = n["depth"], n["confidence"], n["support"]
+        return rst.as_dict(), cst.as_dict()
+
     # ---------------------------------------------------------------- a view's depth map
     def compute_depth_map(self, base: np.ndarray, grid: dict, pairs: list[dict], stereo: StereoOptions | None = None,
                           multi=None):

@@ -145,3 +145,36 @@ def test_kernel_rejects_bad_options(simt_matcher, scene):
         simt_matcher.refine_depth_map(copy_map(m), base, views, RefinementOptions(radius=0))
     with pytest.raises(Exception, match="225"):
         simt_matcher.refine_depth_map(copy_map(m), base, views, RefinementOptions(radius=8, step=1))
+
+
+def test_depth_stage_in_one_call_equals_the_steps(simt_matcher):
+    """r3dgpu_depth_stage_host equals refine_depth_map per view followed by
+    filter_depth_maps (and leaves the inputs' images untouched)."""
+    from regard3d_mvs_b200.depth_maps import ConsistencyOptions
+    from regard3d_mvs_b200.multi_view import depth_stage_scene
+
+    scene = depth_stage_scene(3, 40, 30, partners=2)
+    views, nbs = scene["views"], scene["partners"]
+    rng = np.random.default_rng(2)
+    images, maps = [], []
+    for i, v in enumerate(views):
+        images.append({"camera": v["camera"], "data": simt_matcher.make_refinement_image(v["gray"])})
+        keep = rng.random(v["depth"].shape) < 0.04
+        keep[12:18, 14:26] = True
+        maps.append({"camera": v["camera"], "depth": np.where(keep, v["depth"], 0).astype(np.float32),
+                     "confidence": np.zeros(v["depth"].shape, np.float32),
+                     "pair_mask": np.ones(v["depth"].shape, np.uint16), "color": v["color"], "view": i,
+                     "partners": nbs[i]})
+    opts = RefinementOptions(radius=2, step=2)
+    a = [copy_map(m) for m in maps]
+    ra, ca = simt_matcher.depth_stage(a, images, nbs, opts, ConsistencyOptions())
+    b = [copy_map(m) for m in maps]
+    rb = {"input": 0, "refined": 0, "kept": 0, "unconfirmed": 0}
+    for i, m in enumerate(b):
+        st = simt_matcher.refine_depth_map(m, images[i], [images[j] for j in nbs[i]], opts)
+        rb = {k: rb[k] + st[k] for k in rb}
+    cb = simt_matcher.filter_depth_maps(b, nbs, ConsistencyOptions())
+    assert ra == rb and ca == cb and rb["refined"] > 0
+    for x, y in zip(a, b):
+        assert np.array_equal(x["depth"], y["depth"]) and np.array_equal(x["support"], y["support"])
+        assert np.array_equal(x["confidence"], y["confidence"])
