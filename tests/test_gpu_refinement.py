@@ -77,3 +77,30 @@ def test_refinement_image_equals_oracle(gpu_matcher, oracle, sigma):
     gray = (rng.random((480, 640)) * 255).astype(np.float32)
     np.testing.assert_array_equal(gpu_matcher.make_refinement_image(gray, sigma).view(np.uint32),
                                   oracle.make_refinement_image(gray, sigma).view(np.uint32))
+
+
+def test_depth_stage_in_one_call(gpu_matcher, oracle):
+    """r3dgpu_depth_stage_host on the B200 against the oracle's refinement
+    (double path) and consistency filter of 4 views of 256x192."""
+    from regard3d_mvs_b200.depth_maps import ConsistencyOptions
+    from regard3d_mvs_b200.multi_view import depth_stage_scene
+
+    scene = depth_stage_scene(4, 256, 192, partners=2)
+    views, nbs = scene["views"], scene["partners"]
+    images = [{"camera": v["camera"], "data": oracle.make_refinement_image(v["gray"])} for v in views]
+    maps = [{"camera": v["camera"], "depth": v["depth"].copy(), "confidence": np.zeros_like(v["depth"]),
+             "pair_mask": np.ones(v["depth"].shape, np.uint16), "color": v["color"], "view": i, "partners": nbs[i]}
+            for i, v in enumerate(views)]
+    opts = RefinementOptions(radius=3, step=1)
+    a = [copy_map(m) for m in maps]
+    ra, ca = gpu_matcher.depth_stage(a, images, nbs, opts, ConsistencyOptions())
+    b = [copy_map(m) for m in maps]
+    rb = {"input": 0, "refined": 0, "kept": 0, "unconfirmed": 0}
+    for i, m in enumerate(b):
+        st = oracle.refine_depth_map(m, images[i], [images[j] for j in nbs[i]], opts)
+        rb = {k: rb[k] + st[k] for k in rb}
+    cb = oracle.filter_depth_maps(b, nbs, ConsistencyOptions())
+    assert ra["input"] == rb["input"] and abs(ra["refined"] - rb["refined"]) <= max(3, rb["input"] // 1000)
+    assert abs(ca["output"] - cb["output"]) <= max(5, cb["input"] // 500)
+    agree = [np.mean((x["depth"] > 0) == (y["depth"] > 0)) for x, y in zip(a, b)]
+    assert min(agree) > 0.998, agree
