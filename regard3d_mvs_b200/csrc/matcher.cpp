@@ -24,6 +24,7 @@
 #include "sgm.h"
 #include "sgm_full.h"
 #include "sgm_ranged.h"
+#include "tuning.h"
 
 namespace r3dgpu {
 namespace {
@@ -33,6 +34,14 @@ namespace {
 bool general_ranged_kernel() {
   const char* e = std::getenv("R3DGPU_RANGED_KERNEL");
   return e != nullptr && std::string(e) == "general";
+}
+
+// Ranged tiles whose row shape would be at least this many labels wide go to
+// the general kernel (the tuning table's ranged_general_width, or
+// R3DGPU_RANGED_GENERAL_WIDTH; default: none).
+int general_width() {
+  if (const char* e = std::getenv("R3DGPU_RANGED_GENERAL_WIDTH")) return std::atoi(e) > 0 ? std::atoi(e) : 1 << 30;
+  return tuning().ranged_general_width > 0 ? tuning().ranged_general_width : 1 << 30;
 }
 
 
@@ -806,8 +815,9 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
           continue;
         }
       }
+      const int gw = general_width();
       for (int t = 0; t < nt; ++t) {
-        if (M.ranged && !general_ranged_kernel())
+        if (M.ranged && !general_ranged_kernel() && M.tile_width[t] < gw)
           group_for(kRanged, M.tile_width[t], SgmFullPlan{{0, 0}, 0}).tiles.emplace_back(i, t);
         else
           group_for(kGeneral, 0, SgmFullPlan{{0, 0}, 0}).tiles.emplace_back(i, t);

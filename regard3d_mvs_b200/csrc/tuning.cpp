@@ -42,6 +42,9 @@ Tuning parse(std::istream& in) {
     } else if (kind == "ranged_wide_frac") {
       double f = -1.0;
       if (ss >> f && f >= 0.0) t.ranged_wide_frac = f;
+    } else if (kind == "ranged_general_width") {
+      int w = 0;
+      if (ss >> w && w > 0) t.ranged_general_width = w;
     }
   }
   t.loaded = true;
