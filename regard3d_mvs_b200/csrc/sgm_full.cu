@@ -8,7 +8,10 @@
 // so that a pixel vector is read and written with 64/128-bit shared-memory
 // accesses and the d -+ 1 neighbours come from the lane's own registers plus
 // one word from each side. Rows are skewed by two pixels (pixel u of band row
-// r at step u + 2r). The horizontal path stays in registers (its predecessor
+// r at step u + 2r), and the bands of a tile run back to back as one
+// wavefront: a row starts its next band as soon as it leaves the current one,
+// so the rows drain and fill once per tile rather than once per band. The
+// horizontal path stays in registers (its predecessor
 // is the row's previous pixel; the two boundary words come by shuffle); the
 // vertical and the two diagonal paths go to shared-memory rings of depth 3, 4
 // and 2, read by the row below two, three and one steps later. The last row
@@ -16,8 +19,9 @@
 // band streams back with cp.async. Costs (u8) are computed per tile into the
 // CTA's global scratch, forward partial sums (u16) are stored there too, and
 // both are prefetched two pixels ahead with cp.async. Every instruction of a
-// step is executed by all 32 lanes of a warp (rows idle at the band's edges
-// compute on clamped addresses and store nothing), so shuffles never diverge.
+// step is executed by all 32 lanes of a warp (rows idle at the tile's first
+// and last steps compute on clamped addresses and store nothing), so shuffles
+// never diverge.
 #include <cstdio>
 #include <cstdlib>
 
@@ -145,72 +149,95 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
   uint32_t* mins_up = ring_mins<G, K>(a.smem, rup);
   const int left_lane = (lane + 31) & 31, right_lane = (lane + 1) & 31;
 
-  int band = 0;
-  for (int v0 = 0; v0 < a.h; v0 += a.rows, ++band) {
-    const int Rb = r3dsimt::imin(a.rows, a.h - v0);
-    const bool in_band = r < Rb;
-    const int v = v0 + (in_band ? r : 0);
-    const bool seam_in = in_band && r == 0 && v0 > 0;
-    const bool seam_out = in_band && r == Rb - 1 && v0 + Rb < a.h;
-    unsigned char* gseam_in = a.seam + static_cast<size_t>((band + 1) & 1) * a.w * a.seam_pix;
-    unsigned char* gseam_out = a.seam + static_cast<size_t>(band & 1) * a.w * a.seam_pix;
-    const int2* rrow = a.recs + static_cast<int64_t>(v) * a.w;
-    const int y = a.dir > 0 ? v : a.h - 1 - v;  // image row of this band row
-    const int64_t rowoff = static_cast<int64_t>(y) * a.w * nd;
-
-    auto pixel_off = [&](int u) -> int64_t {
-      const int x = a.dir > 0 ? u : a.w - 1 - u;
-      return rowoff + static_cast<int64_t>(x) * nd;
+  // Bands follow one another without a pause: band row r handles its local
+  // step L (pixel u = L mod P of band L / P) at CTA step L + 2r, so the first
+  // rows of band b + 1 start while the lower rows of band b finish. The period
+  // P is at least the tile width and at least 2 rows + kSgmPF: the last row of
+  // band b writes seam pixel u at step bP + u + 2(rows - 1), strictly before
+  // the first row of band b + 1 prefetches it at step (b + 1)P + u - kSgmPF - 1.
+  // Ring, prefetch and seam slots are indexed by L, which advances by one
+  // across a band change, so consecutive steps never share a slot.
+  {
+    const int R = a.rows;
+    const int nb = (a.h + R - 1) / R;
+    const int P = r3dsimt::imax(a.w, 2 * R + kSgmPF);
+    struct Pos {
+      int b, u, L;  // band, pixel (negative before the row's first step), local step
     };
-    auto prefetch = [&](int u) {
-      if (!in_band || u >= a.w) return;
-      const int64_t off = pixel_off(u);
-      const int slot = u & (kSgmPFSlots - 1);
-      for (int p = t; p < nd / 16; p += G) r3dsimt::cp_async16(cbuf + slot * C::ND + 16 * p, a.cost + off + 16 * p);
+    auto adv = [&](Pos p, int k) -> Pos {
+      p.u += k;
+      p.L += k;
+      if (p.u >= P) {
+        p.u -= P;
+        ++p.b;
+      }
+      return p;
+    };
+    auto valid = [&](const Pos& p) -> bool { return p.u >= 0 && p.u < a.w && p.b * R + r < a.h; };
+    auto row_of = [&](const Pos& p) -> int { return r3dsimt::imin(p.b * R + r, a.h - 1); };  // clamped
+    auto pixel_off = [&](const Pos& p) -> int64_t {
+      const int v = row_of(p);
+      const int y = a.dir > 0 ? v : a.h - 1 - v;
+      const int uc = p.u < 0 ? 0 : (p.u >= a.w ? a.w - 1 : p.u);
+      const int x = a.dir > 0 ? uc : a.w - 1 - uc;
+      return (static_cast<int64_t>(y) * a.w + x) * nd;
+    };
+    auto prefetch = [&](const Pos& p) {
+      if (!valid(p)) return;
+      const int64_t off = pixel_off(p);
+      const int slot = p.L & (kSgmPFSlots - 1);
+      for (int q = t; q < nd / 16; q += G) r3dsimt::cp_async16(cbuf + slot * C::ND + 16 * q, a.cost + off + 16 * q);
       if (a.dir < 0)
-        for (int p = t; p < nd / 8; p += G) r3dsimt::cp_async16(sabuf + slot * C::ND + 8 * p, a.sa + off + 8 * p);
+        for (int q = t; q < nd / 8; q += G) r3dsimt::cp_async16(sabuf + slot * C::ND + 8 * q, a.sa + off + 8 * q);
     };
-    auto prefetch_seam = [&](int u) {
-      if (!seam_in || u >= a.w) return;
-      const int s = u & (kSgmSeamSlots - 1);
+    auto prefetch_seam = [&](const Pos& p) {
+      if (r != 0 || p.b == 0 || !valid(p)) return;
+      unsigned char* gseam_in = a.seam + static_cast<size_t>((p.b + 1) & 1) * a.w * a.seam_pix;
+      const int s = p.L & (kSgmSeamSlots - 1);
       constexpr int pieces = (2 * C::SEAMV) / 16;
-      for (int p = t; p < 3 * pieces + 1; p += G) {
-        if (p < 3 * pieces) {
-          const int path = p / pieces, k = p % pieces;
+      for (int q = t; q < 3 * pieces + 1; q += G) {
+        if (q < 3 * pieces) {
+          const int path = q / pieces, k = q % pieces;
           r3dsimt::cp_async16(seam_vec_s<G, K>(a.smem, a.rows, s, path) + 8 * k,
-                              gseam_vec_f<G, K>(gseam_in, a.seam_pix, u, path) + 8 * k);
+                              gseam_vec_f<G, K>(gseam_in, a.seam_pix, p.u, path) + 8 * k);
         } else {
-          r3dsimt::cp_async16(seam_meta_s<G, K>(a.smem, a.rows, s), gseam_meta_f<G, K>(gseam_in, a.seam_pix, u));
+          r3dsimt::cp_async16(seam_meta_s<G, K>(a.smem, a.rows, s), gseam_meta_f<G, K>(gseam_in, a.seam_pix, p.u));
         }
       }
     };
+    auto rec_at = [&](const Pos& p) -> int2 {
+      return valid(p) ? a.recs[static_cast<int64_t>(p.b * R + r) * a.w + p.u] : make_int2(0, 0);
+    };
 
-    int2 q0 = make_int2(0, 0), q1 = make_int2(0, 0), q2 = make_int2(0, 0);
-    if (in_band) {
-      q0 = rrow[0];
-      if (a.w > 1) q1 = rrow[1];
-      if (a.w > 2) q2 = rrow[2];
-    }
+    Pos cur{0, -2 * r, -2 * r};
+    int2 q0 = rec_at(cur), q1 = rec_at(adv(cur, 1)), q2 = rec_at(adv(cur, 2));
 #pragma unroll
     for (int g = 0; g < kSgmPF; ++g) {
-      prefetch(g);
-      if (g == 0) prefetch_seam(0);
-      prefetch_seam(g + 1);
+      prefetch(adv(cur, g));
+      if (g == 0) prefetch_seam(cur);
+      prefetch_seam(adv(cur, g + 1));
       r3dsimt::cp_async_commit();
     }
     uint32_t hprev[K];  // horizontal path of the row's previous pixel
 #pragma unroll
     for (int j = 0; j < K; ++j) hprev[j] = kSent2;
     uint32_t hmin = 0;
-    const int steps = a.w + 2 * (Rb - 1);
-    for (int st = 0; st < steps; ++st) {
-      const int u = st - 2 * r;
-      const bool active = in_band && u >= 0 && u < a.w;
+    const int last_rows = a.h - (nb - 1) * R;
+    int steps = (nb - 1) * P + a.w + 2 * (last_rows - 1);
+    if (nb > 1) steps = r3dsimt::imax(steps, (nb - 2) * P + a.w + 2 * (R - 1));
+    const int Lend = steps - 2 * r;  // this row's local step at the CTA's last step, plus one
+    for (; cur.L < Lend; cur = adv(cur, 1)) {
+      const int u = cur.u;
+      const bool active = valid(cur);
       const int uc = u < 0 ? 0 : (u >= a.w ? a.w - 1 : u);  // clamped for addressing
+      const int v = row_of(cur);
+      const int Lc = cur.L < 0 ? 0 : cur.L;  // slot index
+      const bool seam_out = active && r == R - 1 && (cur.b + 1) * R < a.h;
+      unsigned char* gseam_out = a.seam + static_cast<size_t>(cur.b & 1) * a.w * a.seam_pix;
       r3dsimt::cp_async_wait<kSgmPF - 1>();
       r3dsimt::syncthreads();
       const int2 rec = q0;
-      const int pslot = uc & (kSgmPFSlots - 1);
+      const int pslot = Lc & (kSgmPFSlots - 1);
       uint32_t c2[K];
       {
         const uint8_t* cb = cbuf + pslot * C::ND + e0;
@@ -232,7 +259,7 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
       qv[0] = nullptr;
       qmin[0] = hmin;
       if (r > 0) {
-        const int u3 = uc % 3, udb = (uc + 3) & 3, uda = (uc + 1) & 1;
+        const int u3 = Lc % 3, udb = (Lc + 3) & 3, uda = (Lc + 1) & 1;
         qv[1] = ring_vec<G, K>(a.smem, rup, u3);
         qmin[1] = mins_up[u3];
         qv[2] = ring_vec<G, K>(a.smem, rup, 3 + udb);
@@ -240,8 +267,8 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
         qv[3] = ring_vec<G, K>(a.smem, rup, 7 + uda);
         qmin[3] = mins_up[7 + uda];
       } else {
-        const int sV = uc & (kSgmSeamSlots - 1), sDB = (uc + kSgmSeamSlots - 1) & (kSgmSeamSlots - 1),
-                  sDA = (uc + 1) & (kSgmSeamSlots - 1);
+        const int sV = Lc & (kSgmSeamSlots - 1), sDB = (Lc + kSgmSeamSlots - 1) & (kSgmSeamSlots - 1),
+                  sDA = (Lc + 1) & (kSgmSeamSlots - 1);
         qv[1] = seam_vec_s<G, K>(a.smem, a.rows, sV, 0);
         qmin[1] = seam_meta_s<G, K>(a.smem, a.rows, sV)[0];
         qv[2] = seam_vec_s<G, K>(a.smem, a.rows, sDB, 1);
@@ -249,7 +276,7 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
         qv[3] = seam_vec_s<G, K>(a.smem, a.rows, sDA, 2);
         qmin[3] = seam_meta_s<G, K>(a.smem, a.rows, sDA)[2];
       }
-      const int ovec[4] = {0, uc % 3, 3 + (uc & 3), 7 + (uc & 1)};
+      const int ovec[4] = {0, Lc % 3, 3 + (Lc & 3), 7 + (Lc & 1)};
       // Boundary words of the horizontal predecessor (all lanes shuffle).
       const uint32_t hl = r3dsimt::shfl(hprev[K - 1], left_lane);
       const uint32_t hr = r3dsimt::shfl(hprev[0], right_lane);
@@ -310,9 +337,9 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
       if (active) {
         hmin = m01 & 0xFFFFu;
         if (t == 0) {
-          mins[uc % 3] = m01 >> 16;
-          mins[3 + (uc & 3)] = m23 & 0xFFFFu;
-          mins[7 + (uc & 1)] = m23 >> 16;
+          mins[Lc % 3] = m01 >> 16;
+          mins[3 + (Lc & 3)] = m23 & 0xFFFFu;
+          mins[7 + (Lc & 1)] = m23 >> 16;
         }
         if (seam_out && t < 4) {
           // Tail sentinels of the seam vectors and the minima.
@@ -328,7 +355,7 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
           }
         }
       }
-      const int64_t off = pixel_off(uc);
+      const int64_t off = pixel_off(cur);
       if (a.dir > 0) {
         if (active) {
           uint32_t* sa32 = reinterpret_cast<uint32_t*>(a.sa + off) + t * K;
@@ -410,17 +437,13 @@ R3D_DEVICE void run_full_pass(const FullPass<G, K>& a) {
           }
         }
       }
-      // Next prefetches and the penalty queue.
-      if (active) {
-        prefetch(u + kSgmPF);
-        prefetch_seam(u + kSgmPF + 1);
-      }
+      // Next prefetches (possibly the next band's first pixels) and the penalty queue.
+      prefetch(adv(cur, kSgmPF));
+      prefetch_seam(adv(cur, kSgmPF + 1));
       r3dsimt::cp_async_commit();
-      if (active) {
-        q0 = q1;
-        q1 = q2;
-        q2 = u + 3 < a.w ? rrow[u + 3] : make_int2(0, 0);
-      }
+      q0 = q1;
+      q1 = q2;
+      q2 = rec_at(adv(cur, 3));
     }
     r3dsimt::cp_async_wait<0>();
     r3dsimt::fence();

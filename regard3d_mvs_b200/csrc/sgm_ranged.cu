@@ -9,7 +9,8 @@
 //
 // Layout. As in sgm_full.cu, G lanes handle one tile row (32 / G rows per
 // warp), lane t holding the K label pairs 2tK .. 2tK + 2K - 1 of the row's
-// current pixel, and rows are skewed by two pixels per row. A pixel whose
+// current pixel, rows are skewed by two pixels per row, and a tile's bands
+// run back to back as one wavefront. A pixel whose
 // range fits the row's ND = 2GK labels ("narrow") keeps its four path
 // vectors in shared-memory rings of ND labels; the vectors of a row are
 // separated by 16 sentinel labels. A narrow predecessor whose lo differs from
@@ -220,27 +221,28 @@ struct RangedPass {
   uint16_t* volume;
 };
 
-// Predecessors of band row rr's pixel uc (band-local row rr, tile row vv):
-// H from the row itself (its previous pixel's range hl/hn and minimum hm),
-// V, DB and DA from the row above, or from the seam for the band's first row.
+// Predecessors of band row rr's pixel uc (band-local row rr, tile row vv,
+// ring slot index lc): H from the row itself (its previous pixel's range
+// hl/hn and minimum hm), V, DB and DA from the row above, or from the seam
+// for the band's first row.
 template <int G, int K>
-R3D_DEVICE void build_preds(const RangedPass& a, unsigned char* gseam_in, int rr, int uc, int vv, int hl, int hn,
-                            uint32_t hm, Pred (&pr)[4], bool (&hasp)[4]) {
+R3D_DEVICE void build_preds(const RangedPass& a, unsigned char* gseam_in, int rr, int uc, int lc, int vv, int hl,
+                            int hn, uint32_t hm, Pred (&pr)[4], bool (&hasp)[4]) {
   const bool has_up = vv > 0;
   hasp[0] = uc > 0;
   hasp[1] = has_up;
   hasp[2] = has_up && uc > 0;
   hasp[3] = has_up && uc + 1 < a.w;
   const uint16_t* wide_r = a.wide + static_cast<int64_t>(rr) * kSgmRangedVecs * a.ndw;
-  const int vh = vec_h(uc + 1);  // pixel uc - 1
+  const int vh = vec_h(lc + 1);  // pixel uc - 1
   pr[0] = Pred{rvec<G, K>(a.smem, rr, vh), wide_r + vh * a.ndw, hl, hn, hm};
   if (rr > 0) {
     const int rup = rr - 1;
     const uint32_t* meta_up = rmeta<G, K>(a.smem, rup);
     const uint32_t* mins_up = rmins<G, K>(a.smem, rup);
     const uint16_t* wide_up = wide_r - static_cast<int64_t>(kSgmRangedVecs) * a.ndw;
-    const int iv = vec_v(uc), idb = vec_db(uc + 3), ida = vec_da(uc + 1);
-    const uint32_t mv = meta_up[uc & 3], mdb = meta_up[(uc + 3) & 3], mda = meta_up[(uc + 1) & 3];
+    const int iv = vec_v(lc), idb = vec_db(lc + 3), ida = vec_da(lc + 1);
+    const uint32_t mv = meta_up[lc & 3], mdb = meta_up[(lc + 3) & 3], mda = meta_up[(lc + 1) & 3];
     pr[1] = Pred{rvec<G, K>(a.smem, rup, iv), wide_up + iv * a.ndw, static_cast<int>(mv & 0xFFFFu),
                  static_cast<int>(mv >> 16), mins_up[iv]};
     pr[2] = Pred{rvec<G, K>(a.smem, rup, idb), wide_up + idb * a.ndw, static_cast<int>(mdb & 0xFFFFu),
@@ -248,8 +250,8 @@ R3D_DEVICE void build_preds(const RangedPass& a, unsigned char* gseam_in, int rr
     pr[3] = Pred{rvec<G, K>(a.smem, rup, ida), wide_up + ida * a.ndw, static_cast<int>(mda & 0xFFFFu),
                  static_cast<int>(mda >> 16), mins_up[ida]};
   } else {
-    const int sv = uc & (kSgmSeamSlots - 1), sdb = (uc + kSgmSeamSlots - 1) & (kSgmSeamSlots - 1),
-              sda = (uc + 1) & (kSgmSeamSlots - 1);
+    const int sv = lc & (kSgmSeamSlots - 1), sdb = (lc + kSgmSeamSlots - 1) & (kSgmSeamSlots - 1),
+              sda = (lc + 1) & (kSgmSeamSlots - 1);
     const int ul = uc > 0 ? uc - 1 : 0, ur = uc + 1 < a.w ? uc + 1 : uc;
     const uint32_t* mv = seam_meta_s<G, K>(a.smem, a.rows, sv);
     const uint32_t* mdb = seam_meta_s<G, K>(a.smem, a.rows, sdb);
@@ -293,63 +295,90 @@ R3D_DEVICE void run_ranged_pass(const RangedPass& a) {
   uint8_t* cbuf = a.smem + S::rows_off + r * S::row_bytes + S::cbuf_off;
   uint16_t* sabuf = reinterpret_cast<uint16_t*>(a.smem + S::rows_off + r * S::row_bytes + S::sabuf_off);
 
-  int band = 0;
-  for (int v0 = 0; v0 < a.h; v0 += a.rows, ++band) {
-    const int Rb = r3dsimt::imin(a.rows, a.h - v0);
-    const bool in_band = r < Rb;
-    const int v = v0 + (in_band ? r : 0);
-    const bool seam_in = in_band && r == 0 && v0 > 0;
-    const bool seam_out = in_band && r == Rb - 1 && v0 + Rb < a.h;
-    unsigned char* gseam_in = a.seam + static_cast<size_t>((band + 1) & 1) * a.w * a.seam_pix;
-    unsigned char* gseam_out = a.seam + static_cast<size_t>(band & 1) * a.w * a.seam_pix;
-    const int4* rrow = a.recs + static_cast<int64_t>(v) * a.w;
-    const int yy = a.h - 1 - v;  // image-order tile row (backward pass)
-
-    auto prefetch = [&](int u, const int4& rec) {
-      if (!in_band || u >= a.w) return;
+  // Bands follow one another without a pause: band row r handles its local
+  // step L (pixel u = L mod P of band L / P) at CTA step L + 2r, so the first
+  // rows of band b + 1 start while the lower rows of band b finish. The period
+  // P is at least the tile width and at least 2 rows + kSgmPF: the last row of
+  // band b writes seam pixel u at step bP + u + 2(rows - 1), strictly before
+  // the first row of band b + 1 prefetches it at step (b + 1)P + u - kSgmPF - 1.
+  // Ring, prefetch and seam slots are indexed by L, which advances by one
+  // across a band change, so consecutive steps never share a slot. The rows
+  // of a warp can be in different bands, so wide pixels take their band from
+  // the row that owns them.
+  {
+    const int R = a.rows;
+    const int nb = (a.h + R - 1) / R;
+    const int P = r3dsimt::imax(a.w, 2 * R + kSgmPF);
+    struct Pos {
+      int b, u, L;  // band, pixel (negative before the row's first step), local step
+    };
+    auto adv = [&](Pos p, int k) -> Pos {
+      p.u += k;
+      p.L += k;
+      if (p.u >= P) {
+        p.u -= P;
+        ++p.b;
+      }
+      return p;
+    };
+    auto valid = [&](const Pos& p) -> bool { return p.u >= 0 && p.u < a.w && p.b * R + r < a.h; };
+    auto seam_buf = [&](int b) -> unsigned char* {
+      return a.seam + static_cast<size_t>(b & 1) * a.w * a.seam_pix;
+    };
+    auto prefetch = [&](const Pos& p, const int4& rec) {
+      if (!valid(p)) return;
       const int num = static_cast<int>(static_cast<uint32_t>(rec.y) >> 16);
       if (num > ND) return;  // wide pixels read global memory directly
-      const int slot = u & (kSgmPFSlots - 1);
-      for (int p = t; p < num / 16; p += G) r3dsimt::cp_async16(cbuf + slot * ND + 16 * p, a.cost + rec.x + 16 * p);
+      const int slot = p.L & (kSgmPFSlots - 1);
+      for (int q = t; q < num / 16; q += G) r3dsimt::cp_async16(cbuf + slot * ND + 16 * q, a.cost + rec.x + 16 * q);
       if (a.dir < 0)
-        for (int p = t; p < num / 8; p += G) r3dsimt::cp_async16(sabuf + slot * ND + 8 * p, a.sa + rec.x + 8 * p);
+        for (int q = t; q < num / 8; q += G) r3dsimt::cp_async16(sabuf + slot * ND + 8 * q, a.sa + rec.x + 8 * q);
     };
-    auto prefetch_seam = [&](int u) {
-      if (!seam_in || u >= a.w) return;
-      const int s = u & (kSgmSeamSlots - 1);
+    auto prefetch_seam = [&](const Pos& p) {
+      if (r != 0 || p.b == 0 || !valid(p)) return;
+      unsigned char* gseam_in = seam_buf(p.b + 1);
+      const int s = p.L & (kSgmSeamSlots - 1);
       constexpr int pieces = ND / 8;
-      for (int p = t; p < 3 * pieces + 1; p += G) {
-        if (p < 3 * pieces) {
-          const int path = p / pieces, k = p % pieces;
+      for (int q = t; q < 3 * pieces + 1; q += G) {
+        if (q < 3 * pieces) {
+          const int path = q / pieces, k = q % pieces;
           r3dsimt::cp_async16(seam_vec_s<G, K>(a.smem, a.rows, s, path) + 8 * k,
-                              gseam_vec(gseam_in, a.seam_pix, u, path, a.ndw) + 8 * k);
+                              gseam_vec(gseam_in, a.seam_pix, p.u, path, a.ndw) + 8 * k);
         } else {
-          r3dsimt::cp_async16(seam_meta_s<G, K>(a.smem, a.rows, s), gseam_meta(gseam_in, a.seam_pix, u));
+          r3dsimt::cp_async16(seam_meta_s<G, K>(a.smem, a.rows, s), gseam_meta(gseam_in, a.seam_pix, p.u));
         }
       }
     };
+    auto rec_at = [&](const Pos& p) -> int4 {
+      return valid(p) ? a.recs[static_cast<int64_t>(p.b * R + r) * a.w + p.u] : make_int4(0, 0, 0, 0);
+    };
 
-    int4 q0 = make_int4(0, 0, 0, 0), q1 = q0, q2 = q0;
-    if (in_band) {
-      q0 = rrow[0];
-      if (a.w > 1) q1 = rrow[1];
-      if (a.w > 2) q2 = rrow[2];
-    }
-    prefetch(0, q0);
-    prefetch_seam(0);
-    prefetch_seam(1);
+    Pos cur{0, -2 * r, -2 * r};
+    int4 q0 = rec_at(cur), q1 = rec_at(adv(cur, 1)), q2 = rec_at(adv(cur, 2));
+    prefetch(cur, q0);
+    prefetch_seam(cur);
+    prefetch_seam(adv(cur, 1));
     r3dsimt::cp_async_commit();
-    prefetch(1, q1);
-    prefetch_seam(2);
+    prefetch(adv(cur, 1), q1);
+    prefetch_seam(adv(cur, 2));
     r3dsimt::cp_async_commit();
 
     uint32_t hmin = 0;  // range and minimum of the row's previous pixel
     int hlo = 0, hnum = 0;
-    const int steps = a.w + 2 * (Rb - 1);
-    for (int st = 0; st < steps; ++st) {
-      const int u = st - 2 * r;
-      const bool active = in_band && u >= 0 && u < a.w;
+    const int last_rows = a.h - (nb - 1) * R;
+    int steps = (nb - 1) * P + a.w + 2 * (last_rows - 1);
+    if (nb > 1) steps = r3dsimt::imax(steps, (nb - 2) * P + a.w + 2 * (R - 1));
+    const int Lend = steps - 2 * r;  // this row's local step at the CTA's last step, plus one
+    for (; cur.L < Lend; cur = adv(cur, 1)) {
+      const int u = cur.u;
+      const bool active = valid(cur);
       const int uc = u < 0 ? 0 : (u >= a.w ? a.w - 1 : u);
+      const int v = r3dsimt::imin(cur.b * R + r, a.h - 1);  // clamped for addressing
+      const int Lc = cur.L < 0 ? 0 : cur.L;                  // slot index
+      const int yy = a.h - 1 - v;                            // image-order tile row (backward pass)
+      const bool seam_out = active && r == R - 1 && (cur.b + 1) * R < a.h;
+      unsigned char* gseam_in = seam_buf(cur.b + 1);
+      unsigned char* gseam_out = seam_buf(cur.b);
       r3dsimt::cp_async_wait<kSgmPF - 1>();
       r3dsimt::syncthreads();
       const int4 rec = q0;
@@ -357,13 +386,13 @@ R3D_DEVICE void run_ranged_pass(const RangedPass& a) {
       const int lo = rec.y & 0xFFFF;
       const int num = active ? static_cast<int>(static_cast<uint32_t>(rec.y) >> 16) : 0;
       const bool wide = num > ND;
-      const int pslot = uc & (kSgmPFSlots - 1);
+      const int pslot = Lc & (kSgmPFSlots - 1);
       Pred pr[4];
       bool hasp[4];
-      build_preds<G, K>(a, gseam_in, r, uc, v, hlo, hnum, hmin, pr, hasp);
+      build_preds<G, K>(a, gseam_in, r, uc, Lc, v, hlo, hnum, hmin, pr, hasp);
       const uint32_t p2v[4] = {static_cast<uint32_t>(rec.z) & 0xFFFFu, static_cast<uint32_t>(rec.z) >> 16,
                                static_cast<uint32_t>(rec.w) & 0xFFFFu, static_cast<uint32_t>(rec.w) >> 16};
-      const int ovec[4] = {vec_h(uc), vec_v(uc), vec_db(uc), vec_da(uc)};
+      const int ovec[4] = {vec_h(Lc), vec_v(Lc), vec_db(Lc), vec_da(Lc)};
       const int x = a.w - 1 - uc;  // image-order tile column (backward pass)
       bool lr_row = false;
       int lr_base = 0;
@@ -452,6 +481,8 @@ R3D_DEVICE void run_ranged_pass(const RangedPass& a) {
         const int gw = src / G;
         const int rw = warp * C::RPW + gw;
         const int ucw = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(uc), src));
+        const int lcw = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(Lc), src));
+        const int bw = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(cur.b), src));
         const int offw = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(off), src));
         const int low = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(lo), src));
         const int numw = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(num), src));
@@ -460,12 +491,13 @@ R3D_DEVICE void run_ranged_pass(const RangedPass& a) {
         const int hlw = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(hlo), src));
         const int hnw = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(hnum), src));
         const uint32_t hmw = r3dsimt::shfl(hmin, src);
-        const int vw = v0 + rw;
+        const int vw = bw * R + rw;
         Pred pw[4];
         bool hw[4];
-        build_preds<G, K>(a, gseam_in, rw, ucw, vw, hlw, hnw, hmw, pw, hw);
-        const bool seam_w = rw == Rb - 1 && v0 + Rb < a.h;
-        const int ovw[4] = {vec_h(ucw), vec_v(ucw), vec_db(ucw), vec_da(ucw)};
+        build_preds<G, K>(a, seam_buf(bw + 1), rw, ucw, lcw, vw, hlw, hnw, hmw, pw, hw);
+        const bool seam_w = rw == R - 1 && (bw + 1) * R < a.h;
+        unsigned char* gseam_out_w = seam_buf(bw);
+        const int ovw[4] = {vec_h(lcw), vec_v(lcw), vec_db(lcw), vec_da(lcw)};
         uint16_t* wide_w = a.wide + static_cast<int64_t>(rw) * kSgmRangedVecs * a.ndw;
         const uint32_t p2w[4] = {recz & 0xFFFFu, recz >> 16, recw & 0xFFFFu, recw >> 16};
         uint32_t pen2[4], negmp[4], pmw[4];
@@ -517,7 +549,7 @@ R3D_DEVICE void run_ranged_pass(const RangedPass& a) {
                 sw += L[k][j];
                 reinterpret_cast<uint32_t*>(wide_w + ovw[k] * a.ndw)[e >> 1] = L[k][j];
                 if (k > 0 && seam_w)
-                  reinterpret_cast<uint32_t*>(gseam_vec(gseam_out, a.seam_pix, ucw, k - 1, a.ndw))[e >> 1] = L[k][j];
+                  reinterpret_cast<uint32_t*>(gseam_vec(gseam_out_w, a.seam_pix, ucw, k - 1, a.ndw))[e >> 1] = L[k][j];
               }
               if (a.dir > 0) {
                 sa32[e >> 1] = sw;
@@ -581,7 +613,7 @@ R3D_DEVICE void run_ranged_pass(const RangedPass& a) {
           mins[ovec[1]] = m01 >> 16;
           mins[ovec[2]] = m23 & 0xFFFFu;
           mins[ovec[3]] = m23 >> 16;
-          meta[uc & 3] = static_cast<uint32_t>(lo) | (static_cast<uint32_t>(num) << 16);
+          meta[Lc & 3] = static_cast<uint32_t>(lo) | (static_cast<uint32_t>(num) << 16);
           if (seam_out) {
             uint32_t* gm = gseam_meta(gseam_out, a.seam_pix, uc);
             gm[0] = m01 >> 16;
@@ -634,16 +666,12 @@ R3D_DEVICE void run_ranged_pass(const RangedPass& a) {
         }
       }
       // Next prefetches and the record queue.
-      if (active) {
-        prefetch(u + kSgmPF, q2);
-        prefetch_seam(u + kSgmPF + 1);
-      }
+      prefetch(adv(cur, kSgmPF), q2);
+      prefetch_seam(adv(cur, kSgmPF + 1));
       r3dsimt::cp_async_commit();
-      if (active) {
-        q0 = q1;
-        q1 = q2;
-        q2 = u + 3 < a.w ? rrow[u + 3] : make_int4(0, 0, 0, 0);
-      }
+      q0 = q1;
+      q1 = q2;
+      q2 = rec_at(adv(cur, 3));
     }
     r3dsimt::cp_async_wait<0>();
     r3dsimt::fence();
