@@ -865,7 +865,14 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
         J.disp = M.tile_disp + M.tile_off[t];
         J.conf = M.tile_conf ? M.tile_conf + M.tile_off[t] : nullptr;
         J.cells = M.d_cells + t;
-        const double steps = 2.0 * ((T.h + L.rows - 1) / L.rows) * (T.w + 2.0 * (L.rows - 1));
+        // Barrier steps of both passes: the full-range and ranged kernels chain
+        // a tile's bands (period max(w, 2 rows + 2)); the general kernel fills
+        // and drains every band.
+        const int nbands = (T.h + L.rows - 1) / L.rows;
+        const double steps =
+            (full || ranged)
+                ? 2.0 * ((nbands - 1.0) * std::max(T.w, 2 * L.rows + 2) + T.w + 2.0 * (T.h - (nbands - 1) * L.rows - 1))
+                : 2.0 * nbands * (T.w + 2.0 * (L.rows - 1));
         work[jb] = steps * (1.0 + kk / 4.0) + static_cast<double>(M.tile_cells[t]) / 256.0;
         L.longest = std::max(L.longest, work[jb]);
         L.cells_sum += M.tile_cells[t];
