@@ -184,66 +184,78 @@ def sgm_traffic_per_cell():
     return None, None
 
 
-def cpu_baseline(specs, seconds_target=15.0):
-    """The oracle on a bounded sample: the smallest pair of the workload,
-    full matcher, all host threads."""
+def oracle_images(spec):
+    """The pair of `spec` from the generator compiled into the oracle library
+    (the same source and bytes as the CUDA library's r3dgpu_synth_pair)."""
     from oracle import oracle
-    from regard3d_mvs_b200 import _native
 
-    lib = _native.load()
+    L, R = oracle.synth_pair(spec["w"], spec["h"], spec["nd"], spec["seed"], spec["textureless"], spec["occluded"])
+    return L.astype(np.uint16) * np.uint16(257), R.astype(np.uint16) * np.uint16(257)
+
+
+def cpu_baseline(specs, gpu_maps=None):
+    """The oracle on a bounded sample: the smallest pair of the workload,
+    full matcher, all host threads. With `gpu_maps` (index -> the GPU
+    disparity map of that pair from the timed batch) the oracle's map is also
+    compared with the GPU's, bit for bit."""
+    from oracle import oracle
+
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
-    spec = min(specs, key=lambda s: s["w"] * s["h"] * s["nd"])
-    L, R = make_images(lib, spec)
+    idx = min(range(len(specs)), key=lambda i: specs[i]["w"] * specs[i]["h"] * specs[i]["nd"])
+    spec = specs[idx]
+    L, R = oracle_images(spec)
     t0 = time.perf_counter()
     r = oracle.match_stereo(L, R, None, None, 0, spec["nd"], options_for(spec))
     dt = time.perf_counter() - t0
     cells = spec["w"] * spec["h"] * ((spec["nd"] + 15) // 16 * 16)
-    return {"value": cells / dt / 1e9, "unit": "Gcells/s", "cores": threads, "kind": "port",
-            "sample": f"one {spec['w']}x{spec['h']} pair, {spec['nd']} labels, levels {spec['levels']}, "
-                      f"{dt:.2f} s, {r.cells} aggregated cells"}
+    out = {"value": cells / dt / 1e9, "unit": "Gcells/s", "cores": threads, "kind": "port",
+           "sample": f"pair {idx}: one {spec['w']}x{spec['h']} pair, {spec['nd']} labels, levels {spec['levels']}, "
+                     f"{dt:.2f} s, {r.cells} aggregated cells"}
+    if gpu_maps is not None and idx in gpu_maps:
+        g = gpu_maps[idx]
+        fa, fb = np.isfinite(g), np.isfinite(r.disparity)
+        out["bit_exact_vs_oracle"] = bool(np.array_equal(fa, fb) and np.array_equal(g[fa], r.disparity[fb]))
+        out["bit_exact_pair"] = idx
+    return out
 
 
 def run_reference(args, rank, world):
-    """The CPU oracle (restatement of the reference matcher) on a bounded
-    sample of the workload: each step matches one pair, cropped to at most
-    1536 px wide, with all host threads."""
+    """The CPU oracle (restatement of the reference matcher, all host threads)
+    on the workload's own pairs, uncropped: each timed step matches the next
+    pair of the list (pairs 0 .. steps - 1); the warm-up steps match the
+    smallest pair. Inputs come from the generator compiled into the oracle
+    library, so no library of the GPU build is loaded."""
     if rank != 0:
         return
     from oracle import oracle
-    from regard3d_mvs_b200 import _native
 
-    lib = _native.load()
     threads = os.cpu_count() or 1
     oracle.set_threads(threads)
     specs = workload_pairs(args.workload, args.pairs, args.seed)
-    sample = []
-    for s in specs:
-        c = dict(s)
-        if c["w"] > 1536:
-            c["h"] = int(round(c["h"] * 1536 / c["w"]))
-            c["w"] = 1536
-        sample.append(c)
-    imgs = [make_images(lib, s) for s in sample[: args.warmup + args.steps]] if len(sample) >= args.warmup + args.steps \
-        else [make_images(lib, sample[i % len(sample)]) for i in range(args.warmup + args.steps)]
+    small = min(specs, key=lambda s: s["w"] * s["h"] * s["nd"])
     cells = 0
     elapsed = 0.0
+    aggregated = 0
     for i in range(args.warmup + args.steps):
-        s = sample[i % len(sample)]
-        L, R = imgs[i]
+        s = small if i < args.warmup else specs[(i - args.warmup) % len(specs)]
+        L, R = oracle_images(s)
         t0 = time.perf_counter()
-        oracle.match_stereo(L, R, None, None, 0, s["nd"], options_for(s))
+        r = oracle.match_stereo(L, R, None, None, 0, s["nd"], options_for(s))
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             elapsed += dt
             cells += s["w"] * s["h"] * ((s["nd"] + 15) // 16 * 16)
+            aggregated += r.cells
     value = cells / elapsed / 1e9
+    sample = (f"pairs 0..{args.steps - 1} of the {args.workload} list, uncropped, one pair per step "
+              f"({aggregated} aggregated cells); warm-up on its smallest pair")
     line = {"metric": METRIC, "value": value, "unit": "Gcells/s", "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-            "config": {"workload": args.workload, "sample": "one pair per step, cropped to <= 1536 px wide"},
+            "config": {"workload": args.workload, "sample": sample, "same_pairs_as_gpu_arm": True},
             "cpu_baseline": {"value": value, "unit": "Gcells/s", "cores": threads, "kind": "port",
-                             "sample": f"{args.steps} pairs of the {args.workload} list, one per step, <= 1536 px wide"},
+                             "sample": sample},
             "e2e": {"value": value, "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -1049,7 +1061,10 @@ def main():
             line["batched_vs_per_pair"] = value / per_pair["value"]
         if not args.no_cpu_baseline and world == 1:
             # The CPU baseline and the other stages' lines at N = 1 only.
-            line["cpu_baseline"] = cpu_baseline(specs)
+            gpu_maps = {i: dD[i].cpu().numpy() for i in range(n)
+                        if specs[i]["w"] * specs[i]["h"] * specs[i]["nd"] ==
+                        min(q["w"] * q["h"] * q["nd"] for q in specs)}
+            line["cpu_baseline"] = cpu_baseline(specs, gpu_maps)
             line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
             line["rectify"] = measure_rectify(lib, dev, stream, args.steps, args.warmup, peak)
             line["depth_stage"] = measure_depth(lib, dev, stream, args.steps, args.warmup, peak)

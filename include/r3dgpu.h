@@ -183,16 +183,23 @@ r3dgpu_status r3dgpu_remove_speckles_host(float* disparity, int32_t width, int32
  * that cannot let the library call cudaMalloc -- an application whose own
  * pool allocator owns the device's memory, or a pipeline that cannot take the
  * device-wide synchronisation of cudaFree. The union-find scratch is a static
- * device array of 32 MiB that every GPU loading this library holds until the
+ * device array of 32 MiB that every GPU using this entry point holds until the
  * process exits; maps above 4,194,304 pixels (2048 x 2048) are rejected with
- * R3DGPU_EINVAL. The work is enqueued on `stream` (cudaStream_t, NULL = legacy
- * default stream) without synchronising it; launch errors are returned, errors
- * during execution surface at the caller's next synchronisation. The first
- * call on a device looks up the array's device address for that device (the
- * current one); make that first call before any stream capture on the device.
- * All calls share the one array, so calls whose work overlaps on the GPU
- * (different streams or host threads without ordering between them) race:
- * order them on one stream or synchronise between them. Results equal
+ * R3DGPU_EINVAL. Like every other entry point it runs on the device this
+ * thread chose with r3dgpu_set_device (device 0 by default) and makes that
+ * device current; the map must be device (or managed) memory of that device,
+ * otherwise R3DGPU_EINVAL before any launch. The work is enqueued on `stream`
+ * (cudaStream_t of that device, NULL = legacy default stream) without
+ * synchronising it; launch errors are returned, errors during execution
+ * surface at the caller's next synchronisation. Set-up: the first call on a
+ * device looks up the array's device address there, which (under CUDA's lazy
+ * module loading, the default) loads the module and reserves the 32 MiB at
+ * that moment; a device without room answers R3DGPU_ENOMEM. Make that first
+ * call -- a call with width = height = 0 does only the set-up -- before the
+ * caller's pool takes the device's memory and before any stream capture on
+ * the device. All calls share the one array, so calls whose work overlaps on
+ * the GPU (different streams or host threads without ordering between them)
+ * race: order them on one stream or synchronise between them. Results equal
  * r3dgpu_remove_speckles_host's. */
 r3dgpu_status r3dgpu_remove_speckles_no_alloc(float* disparity, int32_t width, int32_t height, int32_t min_size,
                                               float max_diff, void* stream);

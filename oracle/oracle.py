@@ -62,6 +62,7 @@ def lib():
         L.orc_remove_depth_speckles.argtypes = [P, i32, ctypes.c_double, P]
         L.orc_make_refinement_image.argtypes = [P, i32, i32, ctypes.c_double, P]
         L.orc_refine_depth_map.argtypes = [P, P, ctypes.c_int64, P, i32, i32, P, P, i32, P, P]
+        L.r3dgpu_synth_pair.argtypes = [P, P, P, P]
         _lib = L
     return _lib
 
@@ -96,6 +97,27 @@ def set_threads(n: int) -> None:
 
 def max_threads() -> int:
     return int(lib().orc_max_threads())
+
+
+class _SynthParams(ctypes.Structure):
+    # include/r3dgpu_synth.h, r3dgpu_synth_params
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("num_disparities", ctypes.c_int32),
+                ("seed", ctypes.c_uint32), ("blur_sigma", ctypes.c_float), ("noise_sigma", ctypes.c_float),
+                ("planes", ctypes.c_int32), ("textureless_fraction", ctypes.c_float),
+                ("occluded_fraction", ctypes.c_float)]
+
+
+def synth_pair(width: int, height: int, num_disparities: int, seed: int, textureless: float = 0.0,
+               occluded: float = 0.0, blur_sigma: float = 1.5, noise_sigma: float = 2.0, planes: int = 8):
+    """The seeded benchmark pair (8-bit left and right images) from the
+    generator compiled into the oracle library: the same source and the same
+    bytes as r3dgpu_synth_pair of the CUDA library, without loading it."""
+    p = _SynthParams(int(width), int(height), int(num_disparities), int(seed) & 0xFFFFFFFF, blur_sigma,
+                     noise_sigma, int(planes), textureless, occluded)
+    left = np.empty((height, width), np.uint8)
+    right = np.empty_like(left)
+    _check(lib().r3dgpu_synth_pair(ctypes.byref(p), _ptr(left), _ptr(right), None))
+    return left, right
 
 
 def census_transform(img: np.ndarray) -> np.ndarray:

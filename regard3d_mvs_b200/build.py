@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OBJ_DIR = os.path.join(HERE, "_lib", "obj")
 LIB = os.path.join(OUT_DIR, "libr3dgpu.so")
-SOURCES = ("image_kernels.cu", "sgm.cu", "sgm_full.cu", "sgm_ranged.cu", "noalloc.cu", "multi_stereo.cu", "rectify.cu", "consistency.cu", "refine.cu", "depth_io.cpp", "pipeline.cpp", "matcher.cpp", "server.cpp", "tuning.cpp", "synth.cpp")
+SOURCES = ("image_kernels.cu", "sgm.cu", "sgm_full.cu", "sgm_path.cu", "sgm_ranged.cu", "noalloc.cu", "multi_stereo.cu", "rectify.cu", "consistency.cu", "refine.cu", "depth_io.cpp", "pipeline.cpp", "matcher.cpp", "server.cpp", "tuning.cpp", "synth.cpp")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "--fmad=false", "-std=c++17",
          "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3"]

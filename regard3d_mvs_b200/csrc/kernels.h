@@ -37,8 +37,8 @@ void launch_segments(const float* d, int w, int h, float max_diff, int* parent, 
 // In place; scratch: 2 * w * h ints.
 void launch_remove_speckles(float* d, int w, int h, int min_size, float max_diff, int* scratch, cudaStream_t s);
 // Same filter with the scratch in a static device array (noalloc.cu); the
-// map is device memory, contiguous, and the work is enqueued on `s`.
-void remove_speckles_static_scratch(float* d, int w, int h, int min_size, float max_diff, cudaStream_t s);
+// map is device memory of `device`, contiguous, and the work is enqueued on `s`.
+void remove_speckles_static_scratch(int device, float* d, int w, int h, int min_size, float max_diff, cudaStream_t s);
 void launch_median3x3(const float* in, int w, int h, float* out, cudaStream_t s);
 // out[y][x] = in[y][w - 1 - x] - offset.
 void launch_unmirror_offset(const float* in, int w, int h, float offset, float* out, cudaStream_t s);

@@ -23,6 +23,7 @@
 #include "matcher_internal.h"
 #include "sgm.h"
 #include "sgm_full.h"
+#include "sgm_path.h"
 #include "sgm_ranged.h"
 #include "tuning.h"
 
@@ -710,6 +711,100 @@ void finish_level(PairRun& P, Arena& A, Pinned& H, cudaStream_t s) {
   }
 }
 
+// Waves of the full-range tiles of a round for the chain passes: tiles in
+// order of kernel shape, a new wave whenever the next tile would take the
+// wave's buffers past `cap_bytes` (a tile larger than that gets a wave of its
+// own). The job tables are copied to the device on s; `max_bytes` receives
+// the largest wave's buffer size.
+void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::vector<Match*>& matches,
+                     size_t cap_bytes, Arena& A, Pinned& H, cudaStream_t s, std::vector<SgmPathWave>& waves,
+                     std::vector<std::vector<SgmPathSegment>>& segs, size_t& max_bytes, uint64_t& cells_sum,
+                     uint64_t& px_sum) {
+  struct Entry {
+    int i, t;
+    SgmPathShape sh;
+    int64_t cells, px, keys;
+  };
+  std::vector<Entry> es;
+  es.reserve(tiles.size());
+  for (const auto& mt : tiles) {
+    const Match& M = *matches[mt.first];
+    const Tile& T = M.layout.tiles[mt.second];
+    const int64_t px = static_cast<int64_t>(T.w) * T.h;
+    es.push_back(Entry{mt.first, mt.second, sgm_path_shape(M.m.nd), px * M.m.nd, px,
+                       M.m.diagonal_lr ? static_cast<int64_t>(T.h) * (T.w + M.m.nd) : 0});
+  }
+  std::stable_sort(es.begin(), es.end(),
+                   [](const Entry& a, const Entry& b) { return a.sh.g_ * a.sh.k_ < b.sh.g_ * b.sh.k_; });
+  max_bytes = 0;
+  cells_sum = 0;
+  px_sum = 0;
+  waves.clear();
+  segs.clear();
+  size_t begin = 0;
+  while (begin < es.size()) {
+    int64_t cells = 0, px = 0, keys = 0;
+    size_t end = begin;
+    while (end < es.size()) {
+      const Entry& e = es[end];
+      if (end > begin && sgm_path_buffers(cells + e.cells, px + e.px, keys + e.keys).total > cap_bytes) break;
+      cells += e.cells;
+      px += e.px;
+      keys += e.keys;
+      ++end;
+    }
+    const int n = static_cast<int>(end - begin);
+    SgmPathJob* hj = H.alloc<SgmPathJob>(n);
+    std::vector<SgmPathSegment> sg;
+    int64_t co = 0, po = 0, ko = 0;
+    for (int q = 0; q < n; ++q) {
+      const Entry& e = es[begin + q];
+      if (sg.empty() || sg.back().shape.g_ != e.sh.g_ || sg.back().shape.k_ != e.sh.k_)
+        sg.push_back(SgmPathSegment{e.sh, q, 0, {0, 0, 0}});
+      SgmPathSegment& g = sg.back();
+      Match& M = *matches[e.i];
+      const Tile& T = M.layout.tiles[e.t];
+      SgmPathJob& J = hj[q];
+      J = SgmPathJob{};
+      J.match = e.i;
+      J.x0 = T.x0;
+      J.y0 = T.y0;
+      J.w = T.w;
+      J.h = T.h;
+      J.cell_off = co;
+      J.px_off = po;
+      J.rk_off = ko;
+      const int cpw = 32 / e.sh.g_;
+      for (int c = 0; c < kPathClasses; ++c) {
+        J.blk[c] = g.blocks[c];
+        g.blocks[c] += (sgm_path_chains(c, T.w, T.h) + cpw - 1) / cpw;
+      }
+      J.disp = M.tile_disp + M.tile_off[e.t];
+      J.conf = M.tile_conf ? M.tile_conf + M.tile_off[e.t] : nullptr;
+      J.cells = M.d_cells + e.t;
+      J.volume = nullptr;
+      ++g.count;
+      co += e.cells;
+      po += e.px;
+      ko += e.keys;
+    }
+    SgmPathJob* dj = A.alloc<SgmPathJob>(n);
+    R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmPathJob) * n, cudaMemcpyHostToDevice, s));
+    SgmPathWave wv{};
+    wv.jobs = dj;
+    wv.njobs = n;
+    wv.cells = co;
+    wv.pixels = po;
+    wv.keys = ko;
+    waves.push_back(wv);
+    segs.push_back(std::move(sg));
+    max_bytes = std::max(max_bytes, sgm_path_buffers(co, po, ko).total);
+    cells_sum += static_cast<uint64_t>(co);
+    px_sum += static_cast<uint64_t>(po);
+    begin = end;
+  }
+}
+
 // Runs a batch of pairs to completion on stream s.
 void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
   Workspace& W = workspace();
@@ -790,7 +885,7 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch) * nm, cudaMemcpyHostToDevice, s));
     // Launch groups: full-range matches by label count; ranged tiles by the
     // kernel shape chosen for each tile (or all into the general kernel).
-    enum Kind { kFull, kRanged, kGeneral };
+    enum Kind { kFull, kRanged, kGeneral, kPath };
     struct Group {
       Kind kind;
       SgmFullPlan plan;
@@ -808,6 +903,12 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
       const Match& M = *matches[i];
       const int nt = static_cast<int>(M.layout.tiles.size());
       if (!M.ranged) {
+        // Full-range tiles of every label count: the chain passes, one group.
+        if (sgm_path_enabled() && sgm_path_shape(M.m.nd).g_ != 0) {
+          Group& g = group_for(kPath, 0, SgmFullPlan{{0, 0}, 0});
+          for (int t = 0; t < nt; ++t) g.tiles.emplace_back(i, t);
+          continue;
+        }
         const SgmFullPlan plan = sgm_full_plan(M.m.nd, W.smem_optin);
         if (plan.shape.g_ != 0) {
           Group& g = group_for(kFull, M.m.nd, plan);
@@ -834,11 +935,24 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
       size_t slot_bytes, scratch_off;
       uint64_t cells_sum, px_sum;
       double longest;
+      // kPath: the waves (one buffer of slot_bytes, reused wave after wave)
+      std::vector<SgmPathWave> waves;
+      std::vector<std::vector<SgmPathSegment>> segs;
     };
     std::vector<Launch> launches;
+    const size_t round_budget = t_scratch_budget != 0 ? t_scratch_budget : size_t{64} << 30;
     for (const Group& g : groups) {
       Launch L{};
       L.g = &g;
+      if (g.kind == kPath) {
+        plan_path_waves(g.tiles, matches, round_budget / 2, A, H, s, L.waves, L.segs, L.slot_bytes, L.cells_sum,
+                        L.px_sum);
+        L.njobs = static_cast<int>(g.tiles.size());
+        L.grid = 1;
+        L.longest = 1e300;  // first: the largest share of the round's work
+        launches.push_back(std::move(L));
+        continue;
+      }
       L.njobs = static_cast<int>(g.tiles.size());
       int max_num = 16;
       for (const auto& mt : g.tiles) max_num = std::max(max_num, matches[mt.first]->tile_maxnum[mt.second]);
@@ -903,7 +1017,7 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     // Scratch for all groups at once, within the budget: grids shrink in
     // proportion when the slots would not fit.
     {
-      const size_t budget = t_scratch_budget != 0 ? t_scratch_budget : size_t{64} << 30;
+      const size_t budget = round_budget;
       size_t total = 0;
       for (const Launch& L : launches) total += static_cast<size_t>(L.grid) * L.slot_bytes;
       if (total > budget) {
@@ -954,7 +1068,15 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
         R3D_CUDA(cudaEventCreate(&ev.b));
         R3D_CUDA(cudaEventRecord(ev.a, gs));
       }
-      if (g.kind == kFull) {
+      if (g.kind == kPath) {
+        for (size_t k = 0; k < L.waves.size(); ++k) {
+          SgmPathWave w = L.waves[k];
+          w.segs = L.segs[k].data();
+          w.nsegs = static_cast<int>(L.segs[k].size());
+          w.buffer = scratch;
+          launch_sgm_path_wave(dm, w, W.sms, gs);
+        }
+      } else if (g.kind == kFull) {
         launch_sgm_full(g.plan.shape, g.nd, dm, L.dj, L.njobs, L.rows, L.grid, scratch, L.slot_bytes, counter, gs);
       } else if (g.kind == kRanged) {
         launch_sgm_ranged(L.rplan.shape, dm, L.dj, L.njobs, L.rows, L.ndw, L.grid, scratch, L.slot_bytes, counter, gs);
@@ -966,8 +1088,11 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
         ev.cells = L.cells_sum;
         ev.pixels = L.px_sum;
         ev.tiles = static_cast<uint64_t>(L.njobs);
-        ev.kernel = g.kind == kFull ? "sgm_full_kernel" : (g.kind == kRanged ? "sgm_ranged_kernel" : "sgm_tile_kernel");
-        ev.shape = g.kind == kFull ? std::to_string(g.plan.shape.g_) + "x" + std::to_string(g.plan.shape.k_) + "/nd" +
+        ev.kernel = g.kind == kPath   ? "sgm_path_kernel"
+                    : g.kind == kFull ? "sgm_full_kernel"
+                                      : (g.kind == kRanged ? "sgm_ranged_kernel" : "sgm_tile_kernel");
+        ev.shape = g.kind == kPath ? "waves" + std::to_string(L.waves.size())
+                   : g.kind == kFull ? std::to_string(g.plan.shape.g_) + "x" + std::to_string(g.plan.shape.k_) + "/nd" +
                                          std::to_string(g.nd)
                    : g.kind == kRanged ? std::to_string(L.rplan.shape.g_) + "x" + std::to_string(L.rplan.shape.k_) +
                                              "/ndw" + std::to_string(L.ndw)
@@ -1318,6 +1443,39 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
     }
     SgmMatch* hm = W.pinned.alloc<SgmMatch>(1);
     fill_match(*hm, o, DView<uint16_t>{dl, wl, h, wl}, cl, cr, wr, il, ir, rlo, rnum, disparity_min, nd, false, false);
+    if (!(ranges_lo && ranges_num) && sgm_path_enabled() && sgm_path_shape(nd).g_ != 0) {
+      // The whole image as one full-range tile through the chain passes.
+      SgmMatch* dm = A.alloc<SgmMatch>(1);
+      R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch), cudaMemcpyHostToDevice, s));
+      const int64_t px = static_cast<int64_t>(wl) * h;
+      SgmPathJob* hj = W.pinned.alloc<SgmPathJob>(1);
+      *hj = SgmPathJob{};
+      hj->w = wl;
+      hj->h = h;
+      const SgmPathShape sh = sgm_path_shape(nd);
+      SgmPathSegment seg{sh, 0, 1, {0, 0, 0}};
+      for (int c = 0; c < kPathClasses; ++c) seg.blocks[c] = (sgm_path_chains(c, wl, h) + 32 / sh.g_ - 1) / (32 / sh.g_);
+      hj->disp = A.alloc<float>(static_cast<size_t>(px));
+      hj->cells = A.alloc<unsigned long long>(1);
+      uint16_t* vol = A.alloc<uint16_t>(cells);
+      hj->volume = vol;
+      SgmPathJob* dj = A.alloc<SgmPathJob>(1);
+      R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmPathJob), cudaMemcpyHostToDevice, s));
+      SgmPathWave wv{};
+      wv.jobs = dj;
+      wv.njobs = 1;
+      wv.segs = &seg;
+      wv.nsegs = 1;
+      wv.cells = static_cast<int64_t>(cells);
+      wv.pixels = px;
+      wv.keys = 0;
+      W.scratch.reserve(sgm_path_buffers(wv.cells, px, 0).total);
+      wv.buffer = W.scratch.get();
+      launch_sgm_path_wave(dm, wv, W.sms, s);
+      R3D_CUDA(cudaMemcpyAsync(out, vol, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s));
+      R3D_CUDA(cudaStreamSynchronize(s));
+      return;
+    }
     const SgmFullPlan plan = (ranges_lo && ranges_num) ? SgmFullPlan{{0, 0}, 0} : sgm_full_plan(nd, W.smem_optin);
     const SgmFullShape sh = plan.shape;
     const bool ranged = !sh.g_ && !general_ranged_kernel();
@@ -1425,7 +1583,10 @@ r3dgpu_status r3dgpu_remove_speckles_host(float* disparity, int32_t width, int32
 r3dgpu_status r3dgpu_remove_speckles_no_alloc(float* disparity, int32_t width, int32_t height, int32_t min_size,
                                               float max_diff, void* stream) {
   return guarded([&] {
-    remove_speckles_static_scratch(disparity, width, height, min_size, max_diff, static_cast<cudaStream_t>(stream));
+    // The device this thread chose with r3dgpu_set_device, as for every other
+    // entry point, but without workspace(): that would allocate.
+    remove_speckles_static_scratch(t_device, disparity, width, height, min_size, max_diff,
+                                   static_cast<cudaStream_t>(stream));
   });
 }
 

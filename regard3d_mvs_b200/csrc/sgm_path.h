@@ -1,0 +1,76 @@
+// Full-range SGM as eight chain passes (sgm_path.cu): the tiles of a wave are
+// aggregated one path direction at a time, every path split into its
+// independent 1-D chains (tile rows, columns or diagonals), many chains in
+// flight per SM. Costs (u8) are computed once per wave; each pass adds its
+// path to the wave's sum volume (u16 per cell), and the last pass also runs
+// the winner-takes-all. The acceptance rules follow in a per-pixel kernel.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "sgm.h"
+
+namespace r3dgpu {
+
+// Chain classes: tile rows (horizontal paths), tile columns (vertical
+// paths) and diagonals (both diagonal directions: w + h - 1 chains).
+constexpr int kPathClasses = 3;
+
+// One tile of a wave. Jobs of a wave are ordered by kernel shape; cell_off
+// and px_off run over the whole wave, blk restarts at 0 with every shape.
+struct SgmPathJob {
+  int match;
+  int x0, y0, w, h;
+  int pad_;
+  int64_t cell_off;           // first cell of the tile in the wave's cost and sum volumes
+  int64_t px_off;             // first pixel of the tile in the wave's WTA records
+  int64_t rk_off;             // first right-WTA key of the tile (diagonal LR only)
+  int64_t blk[kPathClasses];  // first chain block (32 / G chains) of the tile, per chain class
+  float* disp;
+  float* conf;
+  unsigned long long* cells;
+  uint16_t* volume;
+};
+
+// G lanes per chain, K label pairs per lane (2 G K >= nd).
+struct SgmPathShape {
+  int g_;
+  int k_;
+};
+
+// Narrowest compiled shape for nd labels ({0, 0}: more labels than the path
+// kernels take).
+SgmPathShape sgm_path_shape(int nd);
+inline int64_t sgm_path_chains(int cls, int w, int h) { return cls == 0 ? h : (cls == 1 ? w : w + h - 1); }
+
+// Device buffers of a wave (bytes, 256-byte aligned pieces).
+struct SgmPathBuffers {
+  size_t cost, sum, info, rkeys, total;
+};
+SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys);
+
+// A wave on the device: all jobs (device pointer), and per shape the range
+// of jobs with its chain-block counts.
+struct SgmPathSegment {
+  SgmPathShape shape;
+  int first, count;
+  int64_t blocks[kPathClasses];
+};
+struct SgmPathWave {
+  const SgmPathJob* jobs;
+  int njobs;
+  const SgmPathSegment* segs;  // host array
+  int nsegs;
+  int64_t cells, pixels, keys;
+  unsigned char* buffer;  // sgm_path_buffers(cells, pixels, keys).total bytes
+};
+
+// Costs, the 8 passes and the acceptance rules of one wave, on stream s.
+void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, cudaStream_t s);
+
+// Whether full-range tiles go to the path kernels (default) or to the
+// one-CTA-per-tile wavefront kernel (R3DGPU_FULL_KERNEL=wavefront).
+bool sgm_path_enabled();
+
+}  // namespace r3dgpu

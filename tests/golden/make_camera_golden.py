@@ -7,7 +7,7 @@ reads that file as text (nothing of the reference is compiled or run) and
 keeps the cameras and the vectors as JSON, so that the tests run without the
 reference tree.
 
-Usage: python tests/golden/make_camera_golden.py [path/to/reference]
+Usage: python tests/golden/make_camera_golden.py path/to/reference
 """
 
 from __future__ import annotations
@@ -50,7 +50,9 @@ def parse(text: str) -> dict:
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_camera_golden.py <root of a checkout of rhiestan/Regard3D_MVS>")
+    ref = sys.argv[1]
     with open(os.path.join(ref, "tests", "test_camera_model.cpp")) as f:
         data = parse(f.read())
     assert len(data["vectors"]) == 24 and len(data["cameras"]) == 4, (len(data["vectors"]), data["cameras"])

@@ -23,6 +23,9 @@ SUBPIXEL_TOL = 1e-4  # px; disparities are compared exactly, the bound is stated
 
 def _assert_same_map(a, b):
     assert same_disparities(a.disparity, b.disparity), mismatch_report(a.disparity, b.disparity)
+    # Confidence 1 - best / second of every accepted pixel, 0 elsewhere
+    # (stereo_matcher.cpp:517-520): float ops in the reference's order, exact.
+    assert np.array_equal(a.confidence, b.confidence), mismatch_report(a.confidence, b.confidence)
     assert a.cells == b.cells
     assert a.levels == b.levels
     assert a.num_disparities == b.num_disparities
@@ -292,3 +295,60 @@ def test_errors(gpu_matcher):
     # The context stays usable after errors.
     r = gpu_matcher.match_stereo(img, img, None, None, 0, 16, StereoOptions(levels=0))
     assert r.disparity.shape == (16, 32)
+
+
+def _bench_pair(spec):
+    """A pair of the benchmark lists from the seeded generator (compiled into
+    the oracle library from the same source as the CUDA library's), 8-bit
+    lifted x257 as the reference's image reader does (io/image_io.hpp:25)."""
+    from oracle import oracle
+
+    L, R = oracle.synth_pair(spec["w"], spec["h"], spec["nd"], spec["seed"], spec["textureless"], spec["occluded"])
+    return L.astype(np.uint16) * np.uint16(257), R.astype(np.uint16) * np.uint16(257)
+
+
+def _bench_options(spec):
+    return StereoOptions(levels=spec["levels"], range_radius=spec["radius"], range_margin=spec["margin"])
+
+
+def test_config1_pair_3072x2048_256_four_levels(gpu_matcher, oracle):
+    """3072x2048, labels 0..255, 15 % textureless patches, 10 % occluded right
+    pixels, 4-level hierarchy with +-8 labels around the upsampled coarser
+    disparity (range_radius 0, range_margin 8)."""
+    import bench
+
+    spec = bench.workload_pairs("pair3072", 1, 0)[0]
+    left, right = _bench_pair(spec)
+    o = _bench_options(spec)
+    oracle.set_threads(oracle.max_threads())
+    got = gpu_matcher.match_stereo(left, right, None, None, 0, spec["nd"], o)
+    ref = oracle.match_stereo(left, right, None, None, 0, spec["nd"], o)
+    assert got.levels == 3
+    _assert_same_map(got, ref)
+
+
+# Pairs of the 64-pair batch: the widest pair (5624 px, hierarchical, 256
+# labels), the widest single-level pair (5605 px, 192 labels), a 384-label
+# single-level pair and a 5524 px 384-label hierarchical pair.
+BATCH64_SAMPLE = (55, 38, 10, 31)
+
+
+def test_config2_pairs_batched(gpu_matcher, oracle):
+    """Config-2 pairs matched together in one batch call, each against the
+    oracle matching it alone."""
+    import bench
+
+    specs = bench.workload_pairs("batch64", 64, 0)
+    chosen = [specs[i] for i in BATCH64_SAMPLE]
+    assert max(s["w"] for s in chosen) == max(s["w"] for s in specs)
+    assert any(s["nd"] == 384 and s["levels"] == 0 for s in chosen)
+    assert any(s["nd"] == 384 and s["levels"] == 3 for s in chosen)
+    pairs = []
+    for s in chosen:
+        left, right = _bench_pair(s)
+        pairs.append(dict(left=left, right=right, disparity_min=0, num_disparities=s["nd"], options=_bench_options(s)))
+    batch = gpu_matcher.match_stereo_batch(pairs)
+    oracle.set_threads(oracle.max_threads())
+    for p, got in zip(pairs, batch):
+        ref = oracle.match_stereo(p["left"], p["right"], None, None, 0, p["num_disparities"], p["options"])
+        _assert_same_map(got, ref)

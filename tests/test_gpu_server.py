@@ -43,7 +43,7 @@ def _same(a, b):
     assert (a.cells, a.levels, a.num_disparities) == (b.cells, b.levels, b.num_disparities)
 
 
-def test_server_mix_equals_alone(pairs, alone):
+def test_server_mix_equals_alone(pairs, alone, oracle):
     got, times = {}, {}
     lock = threading.Lock()
     with Server(workers=2, max_batch=3, hbm_budget=16 << 30, scratch_budget=8 << 30) as srv:
@@ -62,6 +62,10 @@ def test_server_mix_equals_alone(pairs, alone):
     for i, a in enumerate(alone):
         _same(got[i], a)
     assert {t["worker"] for t in times.values()} <= {0, 1}
+    # The served maps are the reference's maps too.
+    oracle.set_threads(oracle.max_threads())
+    for i, p in enumerate(pairs):
+        _same(got[i], oracle.match_stereo(p["left"], p["right"], None, None, 0, p["num_disparities"], p["options"]))
 
 
 def test_server_tight_budget(pairs, alone):

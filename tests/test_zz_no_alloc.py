@@ -70,6 +70,19 @@ def test_no_alloc_rejects_maps_above_the_static_maximum(gpu_matcher):
     assert 2049 * 2048 > MAX_PIXELS
 
 
+@pytest.mark.gpu
+def test_no_alloc_rejects_memory_of_no_device(gpu_matcher):
+    """The map must be device memory of the thread's device: a host array is
+    rejected before any launch, and an empty call (the set-up alone) is fine."""
+    lib = gpu_matcher.lib
+    st = lib.r3dgpu_remove_speckles_no_alloc(None, 0, 0, 10, 1.0, None)
+    assert st == 0, _status_name(lib, st)
+    host = np.zeros((4, 4), np.float32)
+    st = lib.r3dgpu_remove_speckles_no_alloc(host.ctypes.data_as(ctypes.c_void_p), 4, 4, 10, 1.0, None)
+    assert st == 1, _status_name(lib, st)  # R3DGPU_EINVAL
+    assert "not" in lib.r3dgpu_last_error().decode() and "memory" in lib.r3dgpu_last_error().decode()
+
+
 def test_no_alloc_on_the_emulator(simt_matcher, oracle):
     """The same entry point on the CPU SIMT emulator, where device memory is
     host memory, against the oracle."""
