@@ -347,6 +347,7 @@ struct Match {
   std::vector<uint64_t> tile_cells;  // host copy (ranged: counted on the device)
   std::vector<int> tile_maxnum;
   std::vector<int> tile_width;  // ranged: label width of the kernel shape chosen for the tile
+  std::vector<int> tile_over32;  // ranged: pixels with more than 32 labels
   bool ranged = false;
   // device outputs of the SGM stage
   float* tile_disp = nullptr;
@@ -603,12 +604,14 @@ bool finalize_layout(Match& M, int W, int H_, int partner_w, const r3dgpu_stereo
   M.tile_cells.resize(n);
   M.tile_maxnum.resize(n);
   M.tile_width.assign(n, 0);
+  M.tile_over32.assign(n, 0);
   for (size_t i = 0; i < n; ++i) {
     const Tile& t = M.layout.tiles[i];
     if (M.ranged) {
       const int* st = M.h_stats + i * kTileStats;
       M.tile_cells[i] = M.h_count[i];
       M.tile_maxnum[i] = st[0];
+      M.tile_over32[i] = st[1];
       M.tile_width[i] = sgm_ranged_width_for(st, static_cast<int64_t>(t.w) * t.h);
     } else {
       M.tile_cells[i] = static_cast<uint64_t>(t.w) * static_cast<uint64_t>(t.h) * static_cast<uint64_t>(M.m.nd);
@@ -711,19 +714,25 @@ void finish_level(PairRun& P, Arena& A, Pinned& H, cudaStream_t s) {
   }
 }
 
-// Waves of the full-range tiles of a round for the chain passes: tiles in
-// order of kernel shape, a new wave whenever the next tile would take the
-// wave's buffers past `cap_bytes` (a tile larger than that gets a wave of its
-// own). The job tables are copied to the device on s; `max_bytes` receives
-// the largest wave's buffer size.
-void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::vector<Match*>& matches,
-                     size_t cap_bytes, Arena& A, Pinned& H, cudaStream_t s, std::vector<SgmPathWave>& waves,
-                     std::vector<std::vector<SgmPathSegment>>& segs, size_t& max_bytes, uint64_t& cells_sum,
-                     uint64_t& px_sum) {
+// Waves of the tiles of a round for the chain passes (full-range tiles, or
+// with `ranged` the tiles with per-pixel ranges): tiles in order of kernel
+// shape, a new wave whenever the next tile would take the wave's buffers past
+// `cap_bytes` (a tile larger than that gets a wave of its own). The job
+// tables are copied to the device on s; `max_bytes` receives the largest
+// wave's buffer size.
+void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::vector<Match*>& matches, bool ranged,
+                     size_t cap_bytes, int sms, Arena& A, Pinned& H, cudaStream_t s,
+                     std::vector<SgmPathRangedWave>& waves, std::vector<std::vector<SgmPathSegment>>& segs,
+                     size_t& max_bytes, uint64_t& cells_sum, uint64_t& px_sum) {
   struct Entry {
     int i, t;
     SgmPathShape sh;
-    int64_t cells, px, keys;
+    int64_t cells, px, keys, rows;
+    int maxnum;
+  };
+  auto bytes = [&](int64_t cells, int64_t px, int64_t keys, int64_t rows, int maxnum) -> size_t {
+    return ranged ? sgm_path_ranged_buffers(cells, px, keys, rows, maxnum, sms).total
+                  : sgm_path_buffers(cells, px, keys).total;
   };
   std::vector<Entry> es;
   es.reserve(tiles.size());
@@ -731,8 +740,10 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     const Match& M = *matches[mt.first];
     const Tile& T = M.layout.tiles[mt.second];
     const int64_t px = static_cast<int64_t>(T.w) * T.h;
-    es.push_back(Entry{mt.first, mt.second, sgm_path_shape(M.m.nd), px * M.m.nd, px,
-                       M.m.diagonal_lr ? static_cast<int64_t>(T.h) * (T.w + M.m.nd) : 0});
+    const SgmPathShape sh = ranged ? sgm_path_ranged_shape(M.tile_over32[mt.second], px) : sgm_path_shape(M.m.nd);
+    es.push_back(Entry{mt.first, mt.second, sh, static_cast<int64_t>(M.tile_cells[mt.second]), px,
+                       M.m.diagonal_lr ? static_cast<int64_t>(T.h) * (T.w + M.m.nd) : 0, T.h,
+                       M.tile_maxnum[mt.second]});
   }
   std::stable_sort(es.begin(), es.end(),
                    [](const Entry& a, const Entry& b) { return a.sh.g_ * a.sh.k_ < b.sh.g_ * b.sh.k_; });
@@ -743,20 +754,25 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
   segs.clear();
   size_t begin = 0;
   while (begin < es.size()) {
-    int64_t cells = 0, px = 0, keys = 0;
+    int64_t cells = 0, px = 0, keys = 0, rows = 0;
+    int maxnum = 16;
     size_t end = begin;
     while (end < es.size()) {
       const Entry& e = es[end];
-      if (end > begin && sgm_path_buffers(cells + e.cells, px + e.px, keys + e.keys).total > cap_bytes) break;
+      if (end > begin &&
+          bytes(cells + e.cells, px + e.px, keys + e.keys, rows + e.rows, std::max(maxnum, e.maxnum)) > cap_bytes)
+        break;
       cells += e.cells;
       px += e.px;
       keys += e.keys;
+      rows += e.rows;
+      maxnum = std::max(maxnum, e.maxnum);
       ++end;
     }
     const int n = static_cast<int>(end - begin);
     SgmPathJob* hj = H.alloc<SgmPathJob>(n);
     std::vector<SgmPathSegment> sg;
-    int64_t co = 0, po = 0, ko = 0;
+    int64_t co = 0, po = 0, ko = 0, ro = 0;
     for (int q = 0; q < n; ++q) {
       const Entry& e = es[begin + q];
       if (sg.empty() || sg.back().shape.g_ != e.sh.g_ || sg.back().shape.k_ != e.sh.k_)
@@ -774,6 +790,7 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
       J.cell_off = co;
       J.px_off = po;
       J.rk_off = ko;
+      J.row_off = ro;
       const int cpw = 32 / e.sh.g_;
       for (int c = 0; c < kPathClasses; ++c) {
         J.blk[c] = g.blocks[c];
@@ -787,18 +804,21 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
       co += e.cells;
       po += e.px;
       ko += e.keys;
+      ro += e.rows;
     }
     SgmPathJob* dj = A.alloc<SgmPathJob>(n);
     R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmPathJob) * n, cudaMemcpyHostToDevice, s));
-    SgmPathWave wv{};
+    SgmPathRangedWave wv{};
     wv.jobs = dj;
     wv.njobs = n;
     wv.cells = co;
     wv.pixels = po;
     wv.keys = ko;
+    wv.rows = ro;
+    wv.maxnum = maxnum;
     waves.push_back(wv);
     segs.push_back(std::move(sg));
-    max_bytes = std::max(max_bytes, sgm_path_buffers(co, po, ko).total);
+    max_bytes = std::max(max_bytes, bytes(co, po, ko, ro, maxnum));
     cells_sum += static_cast<uint64_t>(co);
     px_sum += static_cast<uint64_t>(po);
     begin = end;
@@ -885,7 +905,7 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch) * nm, cudaMemcpyHostToDevice, s));
     // Launch groups: full-range matches by label count; ranged tiles by the
     // kernel shape chosen for each tile (or all into the general kernel).
-    enum Kind { kFull, kRanged, kGeneral, kPath };
+    enum Kind { kFull, kRanged, kGeneral, kPath, kPathRanged };
     struct Group {
       Kind kind;
       SgmFullPlan plan;
@@ -916,6 +936,11 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
           continue;
         }
       }
+      if (M.ranged && sgm_path_ranged_enabled()) {
+        Group& g = group_for(kPathRanged, 0, SgmFullPlan{{0, 0}, 0});
+        for (int t = 0; t < nt; ++t) g.tiles.emplace_back(i, t);
+        continue;
+      }
       const int gw = general_width();
       for (int t = 0; t < nt; ++t) {
         if (M.ranged && !general_ranged_kernel() && M.tile_width[t] < gw)
@@ -935,8 +960,8 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
       size_t slot_bytes, scratch_off;
       uint64_t cells_sum, px_sum;
       double longest;
-      // kPath: the waves (one buffer of slot_bytes, reused wave after wave)
-      std::vector<SgmPathWave> waves;
+      // kPath, kPathRanged: the waves (one buffer of slot_bytes, reused wave after wave)
+      std::vector<SgmPathRangedWave> waves;
       std::vector<std::vector<SgmPathSegment>> segs;
     };
     std::vector<Launch> launches;
@@ -944,9 +969,9 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     for (const Group& g : groups) {
       Launch L{};
       L.g = &g;
-      if (g.kind == kPath) {
-        plan_path_waves(g.tiles, matches, round_budget / 2, A, H, s, L.waves, L.segs, L.slot_bytes, L.cells_sum,
-                        L.px_sum);
+      if (g.kind == kPath || g.kind == kPathRanged) {
+        plan_path_waves(g.tiles, matches, g.kind == kPathRanged, round_budget / 4, W.sms, A, H, s, L.waves, L.segs,
+                        L.slot_bytes, L.cells_sum, L.px_sum);
         L.njobs = static_cast<int>(g.tiles.size());
         L.grid = 1;
         L.longest = 1e300;  // first: the largest share of the round's work
@@ -1070,11 +1095,25 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
       }
       if (g.kind == kPath) {
         for (size_t k = 0; k < L.waves.size(); ++k) {
-          SgmPathWave w = L.waves[k];
+          const SgmPathRangedWave& rw = L.waves[k];
+          SgmPathWave w{};
+          w.jobs = rw.jobs;
+          w.njobs = rw.njobs;
+          w.segs = L.segs[k].data();
+          w.nsegs = static_cast<int>(L.segs[k].size());
+          w.cells = rw.cells;
+          w.pixels = rw.pixels;
+          w.keys = rw.keys;
+          w.buffer = scratch;
+          launch_sgm_path_wave(dm, w, W.sms, gs);
+        }
+      } else if (g.kind == kPathRanged) {
+        for (size_t k = 0; k < L.waves.size(); ++k) {
+          SgmPathRangedWave w = L.waves[k];
           w.segs = L.segs[k].data();
           w.nsegs = static_cast<int>(L.segs[k].size());
           w.buffer = scratch;
-          launch_sgm_path_wave(dm, w, W.sms, gs);
+          launch_sgm_path_ranged_wave(dm, w, W.sms, gs);
         }
       } else if (g.kind == kFull) {
         launch_sgm_full(g.plan.shape, g.nd, dm, L.dj, L.njobs, L.rows, L.grid, scratch, L.slot_bytes, counter, gs);
@@ -1088,10 +1127,11 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
         ev.cells = L.cells_sum;
         ev.pixels = L.px_sum;
         ev.tiles = static_cast<uint64_t>(L.njobs);
-        ev.kernel = g.kind == kPath   ? "sgm_path_kernel"
-                    : g.kind == kFull ? "sgm_full_kernel"
+        ev.kernel = g.kind == kPath         ? "sgm_path_kernel"
+                    : g.kind == kPathRanged ? "sgm_path_ranged_kernel"
+                    : g.kind == kFull       ? "sgm_full_kernel"
                                       : (g.kind == kRanged ? "sgm_ranged_kernel" : "sgm_tile_kernel");
-        ev.shape = g.kind == kPath ? "waves" + std::to_string(L.waves.size())
+        ev.shape = (g.kind == kPath || g.kind == kPathRanged) ? "waves" + std::to_string(L.waves.size())
                    : g.kind == kFull ? std::to_string(g.plan.shape.g_) + "x" + std::to_string(g.plan.shape.k_) + "/nd" +
                                          std::to_string(g.nd)
                    : g.kind == kRanged ? std::to_string(L.rplan.shape.g_) + "x" + std::to_string(L.rplan.shape.k_) +
@@ -1472,6 +1512,43 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
       W.scratch.reserve(sgm_path_buffers(wv.cells, px, 0).total);
       wv.buffer = W.scratch.get();
       launch_sgm_path_wave(dm, wv, W.sms, s);
+      R3D_CUDA(cudaMemcpyAsync(out, vol, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s));
+      R3D_CUDA(cudaStreamSynchronize(s));
+      return;
+    }
+    if (ranges_lo && ranges_num && sgm_path_ranged_enabled()) {
+      // The whole image as one ranged tile through the chain passes.
+      SgmMatch* dm = A.alloc<SgmMatch>(1);
+      R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch), cudaMemcpyHostToDevice, s));
+      const int64_t px = static_cast<int64_t>(wl) * h;
+      int over32 = 0;
+      for (int64_t i = 0; i < px; ++i) over32 += ranges_num[i] > 32 ? 1 : 0;
+      const SgmPathShape sh = sgm_path_ranged_shape(over32, px);
+      SgmPathJob* hj = W.pinned.alloc<SgmPathJob>(1);
+      *hj = SgmPathJob{};
+      hj->w = wl;
+      hj->h = h;
+      SgmPathSegment seg{sh, 0, 1, {0, 0, 0}};
+      for (int c = 0; c < kPathClasses; ++c) seg.blocks[c] = (sgm_path_chains(c, wl, h) + 32 / sh.g_ - 1) / (32 / sh.g_);
+      hj->disp = A.alloc<float>(static_cast<size_t>(px));
+      hj->cells = A.alloc<unsigned long long>(1);
+      uint16_t* vol = A.alloc<uint16_t>(cells);
+      hj->volume = vol;
+      SgmPathJob* dj = A.alloc<SgmPathJob>(1);
+      R3D_CUDA(cudaMemcpyAsync(dj, hj, sizeof(SgmPathJob), cudaMemcpyHostToDevice, s));
+      SgmPathRangedWave wv{};
+      wv.jobs = dj;
+      wv.njobs = 1;
+      wv.segs = &seg;
+      wv.nsegs = 1;
+      wv.cells = static_cast<int64_t>(cells);
+      wv.pixels = px;
+      wv.keys = 0;
+      wv.rows = h;
+      wv.maxnum = max_num;
+      W.scratch.reserve(sgm_path_ranged_buffers(wv.cells, px, 0, h, max_num, W.sms).total);
+      wv.buffer = W.scratch.get();
+      launch_sgm_path_ranged_wave(dm, wv, W.sms, s);
       R3D_CUDA(cudaMemcpyAsync(out, vol, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s));
       R3D_CUDA(cudaStreamSynchronize(s));
       return;

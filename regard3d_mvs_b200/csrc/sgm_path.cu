@@ -87,41 +87,42 @@ R3D_DEVICE void chain_geometry(int cls, int dx, int dy, int w, int h, int64_t c,
 }
 
 // ---------------------------------------------------------------- costs
-// C(p, a) of stereo_matcher.cpp:305-353 for 8 labels per item, u8.
+// C(p, a) of stereo_matcher.cpp:305-353, u8, 16 labels per thread (nd is a
+// multiple of 16): one left Census code and 16 right codes, L1-shared with
+// the neighbouring threads of the same pixel and row.
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     sgm_path_cost_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
                          int64_t items, uint8_t* R3D_RESTRICT cost) {
   const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < items; i += stride) {
-    const int64_t cell = 8 * i;
+    const int64_t cell = 16 * i;
     const int j = find_job(jobs, njobs, cell, [](const SgmPathJob& q) { return q.cell_off; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
     const int nd = m.nd;
-    const int64_t local = cell - job.cell_off;
-    const int p = static_cast<int>(local / nd);
-    const int b = static_cast<int>(local - static_cast<int64_t>(p) * nd) >> 3;
-    const int y = p / job.w, x = p - (p / job.w) * job.w;
+    const int local = static_cast<int>(cell - job.cell_off);  // a tile has fewer than 2^31 cells
+    const int p = local / nd;
+    const int b = (local - p * nd) >> 4;
+    const int y = p / job.w, x = p - y * job.w;
     const int bx = job.x0 + x, by = job.y0 + y;
     const RowInterval lv = m.bv[by], rv = m.pv[by];
-    uint32_t lo4 = 0, hi4 = 0;
+    uint32_t q[4] = {0, 0, 0, 0};
     if (bx >= lv.first && bx <= lv.last) {
       const uint64_t cl = m.cbase[static_cast<int64_t>(by) * m.cb_stride + bx];
       const uint64_t* crow = m.cpart + static_cast<int64_t>(by) * m.cp_stride;
-      const int xr0 = bx - m.dmin - 8 * b;
+      const int xr0 = bx - m.dmin - 16 * b;
       const int safe = rv.first > 0 ? rv.first : 0;
-      uint32_t c[8];
+      const uint32_t inv = static_cast<uint32_t>(m.invalid_cost);
 #pragma unroll
-      for (int k = 0; k < 8; ++k) {
+      for (int k = 0; k < 16; ++k) {
         const int xr = xr0 - k;
         const bool ok = xr >= rv.first && xr <= rv.last;
         const uint64_t cr = crow[ok ? xr : safe];
-        c[k] = ok ? static_cast<uint32_t>(r3dsimt::popc64(cl ^ cr)) : static_cast<uint32_t>(m.invalid_cost);
+        const uint32_t c = ok ? static_cast<uint32_t>(r3dsimt::popc64(cl ^ cr)) : inv;
+        q[k >> 2] |= c << (8 * (k & 3));
       }
-      lo4 = c[0] | (c[1] << 8) | (c[2] << 16) | (c[3] << 24);
-      hi4 = c[4] | (c[5] << 8) | (c[6] << 16) | (c[7] << 24);
     }
-    *reinterpret_cast<uint2*>(cost + cell) = make_uint2(lo4, hi4);
+    *reinterpret_cast<uint4*>(cost + cell) = make_uint4(q[0], q[1], q[2], q[3]);
   }
 }
 
@@ -131,6 +132,17 @@ enum PassMode { kFirst = 0, kAccumulate = 1, kLast = 2 };
 // Per-halfword a + b modulo 2^16.
 R3D_DEVICE uint32_t add2(uint32_t a, uint32_t b, bool no_carry) { return no_carry ? a + b : r3dsimt::vadd2(a, b); }
 
+// Per-warp shared-memory ring of the pass kernels: kPathStages stages, each
+// with the costs (ND bytes) and sums (2 ND bytes) of one pixel per chain.
+constexpr int kPathStages = 4;
+template <int G, int K>
+struct PathRing {
+  static constexpr int ND = 2 * G * K;
+  static constexpr int kStageBytes = (32 / G) * 3 * ND;
+  static constexpr int kWarpBytes = kPathStages * kStageBytes;
+  static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
+};
+
 template <int G, int K, int MODE>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
@@ -138,6 +150,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
                     int4* R3D_RESTRICT info, uint32_t* rkeys) {
   constexpr int CPW = 32 / G;  // chains per warp
   constexpr int U = K / 4;     // units of 8 labels per lane
+  R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u);
   const int gi = lane / G, t = lane % G;
   const int e0 = 2 * t * K;  // first label of the lane
@@ -163,31 +176,41 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     uint16_t* sbase = sum + job.cell_off + e0;
     const uint16_t* img = m.base + static_cast<int64_t>(job.y0) * m.base_stride + job.x0;
 
-    // Data of the current and the next pixel of the chain.
-    uint2 craw[U], cnext[U];
-    uint4 sraw[U], snext[U];
-    int icur = 0, inext = 0;
-    auto load = [&](int i, uint2 (&cr)[U], uint4 (&sr)[U], int& iv) {
-      if (i >= len) return;
-      const int x = sx + i * dx, y = sy + i * dy;
-      const int64_t cell = static_cast<int64_t>(y * w + x) * nd;
+    // Costs and sums of the next kPathStages - 1 pixels stream into the
+    // warp's shared-memory ring with cp.async (each lane copies and later
+    // reads only its own labels); intensities wait in a register queue.
+    unsigned char* ring = smem + static_cast<size_t>(threadIdx.x >> 5) * PathRing<G, K>::kWarpBytes;
+    auto stage_cost = [&](int st) -> unsigned char* {
+      return ring + st * PathRing<G, K>::kStageBytes + gi * PathRing<G, K>::ND + e0;
+    };
+    auto stage_sum = [&](int st) -> unsigned char* {
+      return ring + st * PathRing<G, K>::kStageBytes + CPW * PathRing<G, K>::ND + gi * 2 * PathRing<G, K>::ND + 2 * e0;
+    };
+    auto issue = [&](int i) {
+      if (i < len) {
+        const int x = sx + i * dx, y = sy + i * dy;
+        const int64_t cell = static_cast<int64_t>(y * w + x) * nd;
+        const int st = i & (kPathStages - 1);
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        if (uvalid[u]) {
-          cr[u] = *reinterpret_cast<const uint2*>(cbase + cell + 8 * u);
-          if constexpr (MODE != kFirst) sr[u] = r3dsimt::ld_stream(reinterpret_cast<const uint4*>(sbase + cell + 8 * u));
+        for (int u = 0; u < U; ++u) {
+          if (uvalid[u]) {
+            r3dsimt::cp_async8(stage_cost(st) + 8 * u, cbase + cell + 8 * u);
+            if constexpr (MODE != kFirst) r3dsimt::cp_async16(stage_sum(st) + 16 * u, sbase + cell + 8 * u);
+          }
         }
       }
-      iv = img[static_cast<int64_t>(y) * m.base_stride + x];
+      r3dsimt::cp_async_commit();
     };
+    auto intensity = [&](int i) -> int {
+      if (i >= len) return 0;
+      return img[static_cast<int64_t>(sy + i * dy) * m.base_stride + sx + i * dx];
+    };
+    int iq[kPathStages];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      craw[u] = make_uint2(0, 0);
-      cnext[u] = make_uint2(0, 0);
-      sraw[u] = make_uint4(0, 0, 0, 0);
-      snext[u] = make_uint4(0, 0, 0, 0);
+    for (int k = 0; k < kPathStages - 1; ++k) {
+      issue(k);
+      iq[k] = intensity(k);
     }
-    load(0, craw, sraw, icur);
     uint32_t prev[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) prev[k] = kSent2;
@@ -195,7 +218,23 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     int iprev = 0;
     for (int i = 0; i < maxlen; ++i) {
       const bool on = i < len;
-      load(i + 1, cnext, snext, inext);
+      issue(i + kPathStages - 1);
+      iq[kPathStages - 1] = intensity(i + kPathStages - 1);
+      r3dsimt::cp_async_wait<kPathStages - 1>();
+      const int icur = iq[0];
+      uint2 craw[U];
+      uint4 sraw[U];
+      {
+        const int st = i & (kPathStages - 1);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          craw[u] = uvalid[u] ? *reinterpret_cast<const uint2*>(stage_cost(st) + 8 * u) : make_uint2(0, 0);
+          if constexpr (MODE != kFirst)
+            sraw[u] = uvalid[u] ? *reinterpret_cast<const uint4*>(stage_sum(st) + 16 * u) : make_uint4(0, 0, 0, 0);
+          else
+            sraw[u] = make_uint4(0, 0, 0, 0);
+        }
+      }
       uint32_t c2[K];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
@@ -338,13 +377,10 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 #pragma unroll
       for (int k = 0; k < K; ++k) prev[k] = out[k];
       iprev = icur;
-      icur = inext;
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        craw[u] = cnext[u];
-        sraw[u] = snext[u];
-      }
+      for (int k = 0; k + 1 < kPathStages; ++k) iq[k] = iq[k + 1];
     }
+    r3dsimt::cp_async_wait<0>();
   }
 }
 
@@ -399,6 +435,444 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
   }
 }
 
+// ================================================================ ranged tiles
+// Per-pixel label ranges (lo, num; num a multiple of 16): the same passes on
+// costs and sums packed per tile (pixel after pixel, num labels each).
+
+// Per wave row: the in-row exclusive prefix of num (the pixel's cell offset
+// before its row start is added), the range and the base intensity of every
+// pixel as one 16-byte record {offset, lo | num << 16, intensity, 0}; the
+// row's label total and its right-WTA shift max(lo + num - 1 - x).
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+    sgm_path_ranged_rows_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
+                                int64_t rows, int4* R3D_RESTRICT rec, int* R3D_RESTRICT rowsum,
+                                int* R3D_RESTRICT rowshift) {
+  const int lane = static_cast<int>(threadIdx.x & 31u);
+  const int wpb = static_cast<int>(blockDim.x) >> 5;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * wpb + (threadIdx.x >> 5); r < rows; r += nwarps) {
+    const int j = find_job(jobs, njobs, r, [](const SgmPathJob& q) { return q.row_off; });
+    const SgmPathJob& job = jobs[j];
+    const SgmMatch& m = matches[job.match];
+    const int y = static_cast<int>(r - job.row_off), by = job.y0 + y, w = job.w;
+    int run = 0, shift = -0x7FFFFFFF;
+    for (int xb = 0; xb < w; xb += 32) {
+      const int x = xb + lane;
+      int lo = 0, num = 0, iv = 0;
+      if (x < w) {
+        const int64_t ri = static_cast<int64_t>(by) * m.r_stride + job.x0 + x;
+        lo = m.rlo[ri];
+        num = m.rnum[ri];
+        iv = m.base[static_cast<int64_t>(by) * m.base_stride + job.x0 + x];
+        shift = r3dsimt::imax(shift, lo + num - 1 - x);
+      }
+      int incl = num;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(incl), lane >= o ? lane - o : lane));
+        if (lane >= o) incl += v;
+      }
+      if (x < w)
+        rec[job.px_off + static_cast<int64_t>(y) * w + x] =
+            make_int4(run + incl - num, lo | (num << 16), iv, 0);
+      run += static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(incl), 31));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+      shift = r3dsimt::imax(shift, static_cast<int>(r3dsimt::shfl_xor(static_cast<uint32_t>(shift), o)));
+    if (lane == 0) {
+      rowsum[r] = run;
+      rowshift[r] = shift;
+    }
+  }
+}
+
+// Per tile: exclusive prefix of the row totals (the cell offset of each row).
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+    sgm_path_ranged_rowstart_kernel(const SgmPathJob* R3D_RESTRICT jobs, int njobs, const int* R3D_RESTRICT rowsum,
+                                    int* R3D_RESTRICT rowstart) {
+  const int lane = static_cast<int>(threadIdx.x & 31u);
+  const int wpb = static_cast<int>(blockDim.x) >> 5;
+  for (int j = static_cast<int>(blockIdx.x) * wpb + static_cast<int>(threadIdx.x >> 5); j < njobs;
+       j += static_cast<int>(gridDim.x) * wpb) {
+    const SgmPathJob& job = jobs[j];
+    int carry = 0;
+    for (int yb = 0; yb < job.h; yb += 32) {
+      const int y = yb + lane;
+      const int v = y < job.h ? rowsum[job.row_off + y] : 0;
+      int incl = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(incl), lane >= o ? lane - o : lane));
+        if (lane >= o) incl += u;
+      }
+      if (y < job.h) rowstart[job.row_off + y] = carry + incl - v;
+      carry += static_cast<int>(r3dsimt::shfl(static_cast<uint32_t>(incl), 31));
+    }
+    if (lane == 0) *job.cells = static_cast<unsigned long long>(carry);
+  }
+}
+
+// Per pixel: the final cell offset (row start added) and the u8 costs of its
+// num labels, C(p, lo + j) of stereo_matcher.cpp:305-353.
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+    sgm_path_ranged_cost_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
+                                int64_t pixels, int4* R3D_RESTRICT rec, const int* R3D_RESTRICT rowstart,
+                                uint8_t* R3D_RESTRICT cost) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < pixels; i += stride) {
+    const int j = find_job(jobs, njobs, i, [](const SgmPathJob& q) { return q.px_off; });
+    const SgmPathJob& job = jobs[j];
+    const SgmMatch& m = matches[job.match];
+    const int p = static_cast<int>(i - job.px_off);
+    const int y = p / job.w, x = p - y * job.w;
+    int4 rc = rec[i];
+    rc.x += rowstart[job.row_off + y];
+    rec[i] = rc;
+    const int lo = rc.y & 0xFFFF, num = static_cast<int>(static_cast<uint32_t>(rc.y) >> 16);
+    const int bx = job.x0 + x, by = job.y0 + y;
+    const RowInterval lv = m.bv[by], rv = m.pv[by];
+    const bool inside = bx >= lv.first && bx <= lv.last;
+    const uint64_t cl = inside ? m.cbase[static_cast<int64_t>(by) * m.cb_stride + bx] : 0;
+    const uint64_t* crow = m.cpart + static_cast<int64_t>(by) * m.cp_stride;
+    const int safe = rv.first > 0 ? rv.first : 0;
+    const uint32_t inv = static_cast<uint32_t>(m.invalid_cost);
+    uint8_t* out = cost + job.cell_off + rc.x;
+    for (int c = 0; c < num; c += 16) {
+      uint32_t q[4] = {0, 0, 0, 0};
+      if (inside) {
+        const int xr0 = bx - m.dmin - lo - c;
+#pragma unroll
+        for (int k = 0; k < 16; ++k) {
+          const int xr = xr0 - k;
+          const bool ok = xr >= rv.first && xr <= rv.last;
+          const uint64_t cr = crow[ok ? xr : safe];
+          const uint32_t v = ok ? static_cast<uint32_t>(r3dsimt::popc64(cl ^ cr)) : inv;
+          q[k >> 2] |= v << (8 * (k & 3));
+        }
+      }
+      *reinterpret_cast<uint4*>(out + c) = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+  }
+}
+
+// Labels of a chain's predecessor vector kept in shared memory (u32 words of
+// two labels); wider vectors continue in the chain's global overflow.
+constexpr int kRangedSmemWords = 32;
+
+template <int G, int K>
+struct RangedRing {
+  static constexpr int CH = 2 * G * K;  // labels per chunk
+  static constexpr int CPW = 32 / G;
+  static constexpr int kDataStage = CPW * 3 * CH;
+  static constexpr int kData = kPathStages * kDataStage;
+  static constexpr int kRec = 2 * kPathStages * 32 * 16;  // one record slot per lane and stage
+  static constexpr int kPrev = CPW * 2 * kRangedSmemWords * 4;
+  static constexpr int kWarpBytes = kData + kRec + kPrev;
+  static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
+};
+
+template <int G, int K, int MODE>
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+    sgm_path_ranged_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
+                           int cls, int dx, int dy, int64_t total_blocks, const int4* R3D_RESTRICT rec,
+                           const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words) {
+  using R = RangedRing<G, K>;
+  constexpr int CPW = R::CPW, U = K / 4, CH = R::CH, D = kPathStages;
+  R3D_DYNAMIC_SMEM(smem);
+  const int lane = static_cast<int>(threadIdx.x & 31u), warp = static_cast<int>(threadIdx.x >> 5);
+  const int gi = lane / G, t = lane % G;
+  const int e0 = 2 * t * K;  // first label of the lane within a chunk
+  const int wpb = static_cast<int>(blockDim.x) >> 5;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
+  unsigned char* wb = smem + static_cast<size_t>(warp) * R::kWarpBytes;
+  int4* recs = reinterpret_cast<int4*>(wb + R::kData);
+  uint32_t* prevw = reinterpret_cast<uint32_t*>(wb + R::kData + R::kRec) + gi * 2 * kRangedSmemWords;
+  uint32_t* ovfc = ovf + (static_cast<int64_t>(blockIdx.x) * wpb * CPW + warp * CPW + gi) * 2 * ovf_words;
+  auto stage_cost = [&](int st) -> unsigned char* { return wb + st * R::kDataStage + gi * CH + e0; };
+  auto stage_sum = [&](int st) -> unsigned char* {
+    return wb + st * R::kDataStage + CPW * CH + gi * 2 * CH + 2 * e0;
+  };
+  // Word idx (labels 2 idx, 2 idx + 1) of buffer b of the predecessor vector
+  // (nw words long): two sentinels outside it.
+  auto qword = [&](int b, int idx, int nw) -> uint32_t {
+    if (idx < 0 || idx >= nw) return kSent2;
+    return idx < kRangedSmemWords ? prevw[b * kRangedSmemWords + idx]
+                                  : ovfc[b * ovf_words + (idx - kRangedSmemWords)];
+  };
+  auto put_word = [&](int b, int idx, uint32_t v) {
+    if (idx < kRangedSmemWords) prevw[b * kRangedSmemWords + idx] = v;
+    else ovfc[b * ovf_words + (idx - kRangedSmemWords)] = v;
+  };
+  for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + warp; blk < total_blocks; blk += nwarps) {
+    const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
+    const SgmPathJob& job = jobs[j];
+    const SgmMatch& m = matches[job.match];
+    const int w = job.w;
+    const uint32_t p1x2 = static_cast<uint32_t>(m.p1) * 0x10001u;
+    const bool no_carry = m.sum_no_carry != 0;
+    int sx, sy, len;
+    chain_geometry(cls, dx, dy, w, job.h, (blk - job.blk[cls]) * CPW + gi, sx, sy, len);
+    int maxlen = len;
+#pragma unroll
+    for (int o = G; o < 32; o <<= 1) maxlen = r3dsimt::imax(maxlen, static_cast<int>(r3dsimt::shfl_xor(maxlen, o)));
+    const uint8_t* cbase = cost + job.cell_off;
+    uint16_t* sbase = sum + job.cell_off;
+    const int4* rbase = rec + job.px_off;
+    auto pix = [&](int i) -> int { return (sy + i * dy) * w + sx + i * dx; };
+    auto issue_rec = [&](int i) {
+      if (i < len) r3dsimt::cp_async16(&recs[(i & (2 * D - 1)) * 32 + lane], rbase + pix(i));
+    };
+    auto issue_data = [&](int i, int4 r) {
+      if (i >= len) return;
+      const int off = r.x, num = static_cast<int>(static_cast<uint32_t>(r.y) >> 16);
+      const int st = i & (D - 1);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (e0 + 8 * u < num) {
+          r3dsimt::cp_async8(stage_cost(st) + 8 * u, cbase + off + e0 + 8 * u);
+          if constexpr (MODE != kFirst) r3dsimt::cp_async16(stage_sum(st) + 16 * u, sbase + off + e0 + 8 * u);
+        }
+      }
+    };
+    // Records of the first 2 D - 1 pixels now, the first D - 1 pixels' data in flight.
+#pragma unroll
+    for (int k = 0; k < 2 * D - 1; ++k)
+      if (k < len) recs[k * 32 + lane] = rbase[pix(k)];
+#pragma unroll
+    for (int k = 0; k < D - 1; ++k) {
+      issue_data(k, recs[k * 32 + lane]);
+      r3dsimt::cp_async_commit();
+    }
+    uint32_t pmin = 0;
+    int lo_q = 0, num_q = 0, iprev = 0;
+    for (int i = 0; i < maxlen; ++i) {
+      const bool on = i < len;
+      r3dsimt::cp_async_wait<D - 1>();
+      const int4 rn = recs[((i + D - 1) & (2 * D - 1)) * 32 + lane];
+      issue_rec(i + 2 * D - 1);
+      issue_data(i + D - 1, rn);
+      r3dsimt::cp_async_commit();
+      r3dsimt::cp_async_wait<D - 1>();
+      const int4 rc = recs[(i & (2 * D - 1)) * 32 + lane];
+      const int off = rc.x, lo = rc.y & 0xFFFF, icur = rc.z;
+      const int num = on ? static_cast<int>(static_cast<uint32_t>(rc.y) >> 16) : 0;
+      int nchw = (num + CH - 1) / CH;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) nchw = r3dsimt::imax(nchw, static_cast<int>(r3dsimt::shfl_xor(nchw, o)));
+      const int sh = lo - lo_q, nwq = num_q >> 1;
+      const int cur = i & 1, prv = cur ^ 1;
+      uint32_t pen2 = 0, negmp = 0;
+      if (i > 0) {
+        const int dI = icur - iprev;
+        const uint32_t pen = pmin + m.lut[(dI < 0 ? -dI : dI) >> 8];
+        pen2 = pen | (pen << 16);
+        negmp = 0u - (pmin | (pmin << 16));
+      }
+      uint32_t pm = kSent2;
+      for (int c = 0; c < nchw; ++c) {
+        const int j0 = c * CH + e0;
+        bool uv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) uv[u] = j0 + 8 * u < num;
+        uint2 craw[U];
+        uint4 sraw[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          craw[u] = make_uint2(0, 0);
+          sraw[u] = make_uint4(0, 0, 0, 0);
+          if (uv[u]) {
+            if (c == 0) {
+              const int st = i & (D - 1);
+              craw[u] = *reinterpret_cast<const uint2*>(stage_cost(st) + 8 * u);
+              if constexpr (MODE != kFirst) sraw[u] = *reinterpret_cast<const uint4*>(stage_sum(st) + 16 * u);
+            } else {
+              craw[u] = *reinterpret_cast<const uint2*>(cbase + off + j0 + 8 * u);
+              if constexpr (MODE != kFirst)
+                sraw[u] = r3dsimt::ld_stream(reinterpret_cast<const uint4*>(sbase + off + j0 + 8 * u));
+            }
+          }
+        }
+        uint32_t c2[K];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          c2[4 * u + 0] = r3dsimt::perm(craw[u].x, 0u, 0x4140u);
+          c2[4 * u + 1] = r3dsimt::perm(craw[u].x, 0u, 0x4342u);
+          c2[4 * u + 2] = r3dsimt::perm(craw[u].y, 0u, 0x4140u);
+          c2[4 * u + 3] = r3dsimt::perm(craw[u].y, 0u, 0x4342u);
+        }
+        uint32_t out[K];
+        if (i == 0) {
+#pragma unroll
+          for (int k = 0; k < K; ++k) out[k] = c2[k];
+        } else {
+          // Predecessor labels j0 + sh - 2 .. j0 + sh + 2 K + 1 (its own
+          // indexing), sentinels outside its range, realigned by one label
+          // when the shift is odd.
+          const int b = j0 + sh - 2;
+          const int f = b >> 1;
+          uint32_t qw[K + 3];
+#pragma unroll
+          for (int k = 0; k < K + 3; ++k) qw[k] = qword(prv, f + k, nwq);
+          uint32_t wv[K + 2];
+          if (b & 1) {
+#pragma unroll
+            for (int k = 0; k < K + 2; ++k) wv[k] = r3dsimt::perm(qw[k], qw[k + 1], 0x5432u);
+          } else {
+#pragma unroll
+            for (int k = 0; k < K + 2; ++k) wv[k] = qw[k];
+          }
+          uint32_t mprev = r3dsimt::perm(wv[0], wv[1], 0x5432u);
+#pragma unroll
+          for (int k = 0; k < K; ++k) {
+            const uint32_t mnext = r3dsimt::perm(wv[k + 1], wv[k + 2], 0x5432u);
+            const uint32_t nb = r3dsimt::vmin2(mprev, mnext);
+            const uint32_t best = r3dsimt::vmin2(wv[k + 1], r3dsimt::vaddmin2(nb, p1x2, pen2));
+            out[k] = best + c2[k] + negmp;
+            mprev = mnext;
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          if (!uv[k / 4]) out[k] = kSent2;
+          pm = r3dsimt::vmin2(pm, out[k]);
+          if (uv[k / 4]) put_word(cur, (j0 >> 1) + k, out[k]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          if (!uv[u]) continue;
+          uint4 v;
+          if constexpr (MODE == kFirst) {
+            v = make_uint4(out[4 * u], out[4 * u + 1], out[4 * u + 2], out[4 * u + 3]);
+          } else {
+            v = make_uint4(add2(sraw[u].x, out[4 * u], no_carry), add2(sraw[u].y, out[4 * u + 1], no_carry),
+                           add2(sraw[u].z, out[4 * u + 2], no_carry), add2(sraw[u].w, out[4 * u + 3], no_carry));
+          }
+          r3dsimt::st_stream(reinterpret_cast<uint4*>(sbase + off + j0 + 8 * u), v);
+        }
+      }
+      pmin = group_umin<G>(r3dsimt::umin(pm & 0xFFFFu, pm >> 16));
+      r3dsimt::syncwarp();
+      if (on) {
+        lo_q = lo;
+        num_q = num;
+        iprev = icur;
+      }
+    }
+    r3dsimt::cp_async_wait<0>();
+    r3dsimt::syncwarp();
+  }
+}
+
+// Per pixel: winner-takes-all over the total sums (sgm_kernels.cpp:332-358;
+// first minimum, second best outside +-1, S at kb -+ 1 within the range),
+// the optional volume copy and the right-view keys of the diagonal check.
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+    sgm_path_ranged_wta_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
+                               int64_t pixels, const int4* R3D_RESTRICT rec, const uint16_t* R3D_RESTRICT sum,
+                               const int* R3D_RESTRICT rowshift, int4* R3D_RESTRICT info, uint32_t* rkeys) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < pixels; i += stride) {
+    const int j = find_job(jobs, njobs, i, [](const SgmPathJob& q) { return q.px_off; });
+    const SgmPathJob& job = jobs[j];
+    const SgmMatch& m = matches[job.match];
+    const int p = static_cast<int>(i - job.px_off);
+    const int y = p / job.w, x = p - y * job.w;
+    const int4 rc = rec[i];
+    const int lo = rc.y & 0xFFFF, num = static_cast<int>(static_cast<uint32_t>(rc.y) >> 16);
+    const uint16_t* sp16 = sum + job.cell_off + rc.x;
+    uint32_t kmin = 0xFFFFFFFFu;
+    for (int c = 0; c < num; c += 8) {
+      const uint4 v = *reinterpret_cast<const uint4*>(sp16 + c);
+      const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t e = static_cast<uint32_t>(c + 2 * k);
+        kmin = r3dsimt::umin(kmin, r3dsimt::umin(((wv[k] & 0xFFFFu) << 16) | e, (wv[k] & 0xFFFF0000u) | (e + 1)));
+      }
+      if (job.volume != nullptr) *reinterpret_cast<uint4*>(job.volume + rc.x + c) = v;
+    }
+    const int kb = static_cast<int>(kmin & 0xFFFFu);
+    const uint32_t bcost = kmin >> 16;
+    uint32_t sec = 0xFFFFu;
+    for (int e = 0; e < num; ++e)
+      if (e + 1 < kb || e > kb + 1) sec = r3dsimt::umin(sec, sp16[e]);
+    const int km = kb > 0 ? kb - 1 : 0;
+    const int kp = kb + 1 < num ? kb + 1 : (num > 0 ? num - 1 : 0);
+    const uint32_t sm = sp16[km], spv = sp16[kp];
+    info[i] = make_int4(static_cast<int>(static_cast<uint32_t>(lo + kb) | (bcost << 16)),
+                        static_cast<int>(sec | (sm << 16)), static_cast<int>(spv), 0);
+    if (m.diagonal_lr) {
+      const RowInterval lv = m.bv[job.y0 + y];
+      const int bx = job.x0 + x;
+      if (bx >= lv.first && bx <= lv.last) {
+        uint32_t* keys = rkeys + job.rk_off + static_cast<int64_t>(y) * (job.w + m.nd);
+        const int base = x - lo + rowshift[job.row_off + y];
+        for (int e = 0; e < num; ++e)
+          atomicMin(keys + (base - e), (static_cast<uint32_t>(sp16[e]) << 16) | static_cast<uint32_t>(x));
+      }
+    }
+  }
+}
+
+// Acceptance rules with per-pixel ranges (stereo_matcher.cpp:474-523): as
+// the full-range kernel's, plus the rejection of a minimum on the edge of a
+// reduced range (:501-503).
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+    sgm_path_ranged_accept_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs,
+                                  int njobs, int64_t pixels, const int4* R3D_RESTRICT rec,
+                                  const int4* R3D_RESTRICT info, const uint32_t* R3D_RESTRICT rkeys,
+                                  const int* R3D_RESTRICT rowshift) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < pixels; i += stride) {
+    const int j = find_job(jobs, njobs, i, [](const SgmPathJob& q) { return q.px_off; });
+    const SgmPathJob& job = jobs[j];
+    const SgmMatch& m = matches[job.match];
+    const int w = job.w;
+    const int p = static_cast<int>(i - job.px_off);
+    const int y = p / w, x = p - y * w;
+    const int bx = job.x0 + x, by = job.y0 + y;
+    const RowInterval lv = m.bv[by];
+    float d = kInfF, cf = 0.0F;
+    if (bx >= lv.first && bx <= lv.last) {
+      const int4 in = info[i];
+      const int4 rc = rec[i];
+      const int lo = rc.y & 0xFFFF, num = static_cast<int>(static_cast<uint32_t>(rc.y) >> 16);
+      const int best = in.x & 0xFFFF;
+      const uint32_t bcost = static_cast<uint32_t>(in.x) >> 16;
+      const uint32_t sec = static_cast<uint32_t>(in.y) & 0xFFFFu;
+      const uint32_t sm = static_cast<uint32_t>(in.y) >> 16;
+      const uint32_t sp = static_cast<uint32_t>(in.z);
+      const int jb = best - lo;
+      const RowInterval rv = m.pv[by];
+      const int xr = bx - m.dmin - best;
+      bool ok = xr >= rv.first && xr <= rv.last;
+      if ((jb == 0 && lo > 0) || (jb == num - 1 && lo + num < m.nd)) ok = false;
+      if (ok && m.diagonal_lr) {
+        const uint32_t key =
+            rkeys[job.rk_off + static_cast<int64_t>(y) * (w + m.nd) + (x - best + rowshift[job.row_off + y])];
+        const int rb = key == 0xFFFFFFFFu ? 0xFFFF : static_cast<int>(key & 0xFFFFu) - x + best;
+        const int diff = rb - best;
+        if ((diff < 0 ? -diff : diff) > m.lr_max_diff) ok = false;
+      }
+      const float best_cost = static_cast<float>(bcost);
+      if (ok && m.uniqueness > 0.0F && sec != 0xFFFFu &&
+          best_cost > __fmul_rn(__fsub_rn(1.0F, m.uniqueness), static_cast<float>(sec)))
+        ok = false;
+      if (ok) {
+        float delta = 0.0F;
+        if (jb > 0 && jb < num - 1)
+          delta = sgm_simd::subpixel_delta(m.subpixel, static_cast<float>(sm), best_cost, static_cast<float>(sp));
+        d = __fadd_rn(static_cast<float>(m.dmin + best), delta);
+        if (m.confidence)
+          cf = (sec != 0xFFFFu && sec > 0u) ? __fsub_rn(1.0F, __fdiv_rn(best_cost, static_cast<float>(sec))) : 0.0F;
+      }
+    }
+    job.disp[p] = d;
+    if (job.conf != nullptr) job.conf[p] = cf;
+  }
+}
+
 // ---------------------------------------------------------------- launches
 // Pass order: the first pass writes the sums, the last takes the WTA.
 struct Pass {
@@ -408,12 +882,29 @@ constexpr Pass kPasses[8] = {{0, 1, 0},  {1, 0, 1},   {2, 1, 1},  {2, -1, 1},
                              {1, 0, -1}, {2, -1, -1}, {2, 1, -1}, {0, -1, 0}};
 
 template <class Kernel>
-int resident_grid(Kernel kernel, int sms, int64_t work_items, int per_block) {
+int resident_grid(Kernel kernel, int sms, int64_t work_items, int per_block, size_t smem = 0) {
   int per_sm = 1;
-  R3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPathThreads, 0));
+  R3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPathThreads, smem));
   const int64_t need = (work_items + per_block - 1) / per_block;
   const int64_t resident = static_cast<int64_t>(sms) * (per_sm > 0 ? per_sm : 1);
   return static_cast<int>(need < resident ? (need > 0 ? need : 1) : resident);
+}
+
+template <int G, int K, int MODE>
+void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
+                 const uint8_t* cost, uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s) {
+  auto* k = sgm_path_kernel<G, K, MODE>;
+  constexpr size_t smem = PathRing<G, K>::kBlockBytes;
+  static thread_local int configured[64] = {};
+  int dev = 0;
+  R3D_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    R3D_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    configured[dev] = 1;
+  }
+  R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32, smem)), dim3(kPathThreads), smem, s, dm, jobs,
+             njobs, ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys);
+  launched("sgm_path_kernel");
 }
 
 template <int G, int K>
@@ -423,20 +914,12 @@ void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, int njobs, const 
     const Pass ps = kPasses[q];
     const int64_t nb = blocks[ps.cls];
     if (nb <= 0) continue;
-    if (q == 0) {
-      auto* k = sgm_path_kernel<G, K, kFirst>;
-      R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32)), dim3(kPathThreads), 0, s, dm, jobs, njobs,
-                 ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys);
-    } else if (q < 7) {
-      auto* k = sgm_path_kernel<G, K, kAccumulate>;
-      R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32)), dim3(kPathThreads), 0, s, dm, jobs, njobs,
-                 ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys);
-    } else {
-      auto* k = sgm_path_kernel<G, K, kLast>;
-      R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32)), dim3(kPathThreads), 0, s, dm, jobs, njobs,
-                 ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys);
-    }
-    launched("sgm_path_kernel");
+    if (q == 0)
+      launch_pass<G, K, kFirst>(ps, dm, jobs, njobs, nb, cost, sum, info, rkeys, sms, s);
+    else if (q < 7)
+      launch_pass<G, K, kAccumulate>(ps, dm, jobs, njobs, nb, cost, sum, info, rkeys, sms, s);
+    else
+      launch_pass<G, K, kLast>(ps, dm, jobs, njobs, nb, cost, sum, info, rkeys, sms, s);
   }
 }
 
@@ -498,7 +981,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
   uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
   if (wave.keys > 0) R3D_CUDA(cudaMemsetAsync(rkeys, 0xFF, static_cast<size_t>(wave.keys) * 4, s));
   {
-    const int64_t items = wave.cells / 8;
+    const int64_t items = wave.cells / 16;
     R3D_LAUNCH(sgm_path_cost_kernel, dim3(resident_grid(sgm_path_cost_kernel, sms, items, kPathThreads)),
                dim3(kPathThreads), 0, s, dm, wave.jobs, wave.njobs, items, cost);
     launched("sgm_path_cost_kernel");
@@ -519,6 +1002,126 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
   R3D_LAUNCH(sgm_path_accept_kernel, dim3(resident_grid(sgm_path_accept_kernel, sms, wave.pixels, kPathThreads)),
              dim3(kPathThreads), 0, s, dm, wave.jobs, wave.njobs, wave.pixels, info, rkeys);
   launched("sgm_path_accept_kernel");
+}
+
+// ---------------------------------------------------------------- ranged launches
+namespace {
+
+// Largest number of resident CTAs per SM any ranged pass kernel is launched
+// with (the overflow has one slot per resident chain).
+constexpr int kRangedMaxPerSm = 4;
+
+template <int G, int K, int MODE>
+void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
+                        const int4* rec, const uint8_t* cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words,
+                        int sms, cudaStream_t s) {
+  auto* k = sgm_path_ranged_kernel<G, K, MODE>;
+  constexpr size_t smem = RangedRing<G, K>::kBlockBytes;
+  static thread_local int configured[64] = {};
+  int dev = 0;
+  R3D_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !configured[dev]) {
+    R3D_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    configured[dev] = 1;
+  }
+  int grid = resident_grid(k, sms, nb, kPathThreads / 32, smem);
+  grid = grid < sms * kRangedMaxPerSm ? grid : sms * kRangedMaxPerSm;
+  R3D_LAUNCH(k, dim3(grid), dim3(kPathThreads), smem, s, dm, jobs, njobs, ps.cls, ps.dx, ps.dy, nb, rec, cost, sum,
+             ovf, ovf_words);
+  launched("sgm_path_ranged_kernel");
+}
+
+template <int G, int K>
+void launch_ranged_passes(const SgmMatch* dm, const SgmPathJob* jobs, int njobs,
+                          const int64_t (&blocks)[kPathClasses], const int4* rec, const uint8_t* cost, uint16_t* sum,
+                          uint32_t* ovf, int64_t ovf_words, int sms, cudaStream_t s) {
+  for (int q = 0; q < 8; ++q) {
+    const Pass ps = kPasses[q];
+    const int64_t nb = blocks[ps.cls];
+    if (nb <= 0) continue;
+    if (q == 0)
+      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, njobs, nb, rec, cost, sum, ovf, ovf_words, sms, s);
+    else
+      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, njobs, nb, rec, cost, sum, ovf, ovf_words, sms, s);
+  }
+}
+
+}  // namespace
+
+bool sgm_path_ranged_enabled() {
+  const char* e = std::getenv("R3DGPU_RANGED_KERNEL");
+  return e == nullptr || std::strcmp(e, "path") == 0;
+}
+
+SgmPathShape sgm_path_ranged_shape(int over32, int64_t pixels) {
+  // 32-label chunks unless more than a tenth of the tile's pixels need two.
+  return static_cast<int64_t>(over32) * 10 > pixels ? SgmPathShape{4, 8} : SgmPathShape{2, 8};
+}
+
+SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
+                                       int sms) {
+  SgmPathBuffers b = sgm_path_buffers(cells, pixels, keys);
+  size_t o = b.total;
+  b.rec = o;
+  o += align256(static_cast<size_t>(pixels) * 16);
+  b.rowsum = o;
+  o += align256(static_cast<size_t>(rows) * 4);
+  b.rowstart = o;
+  o += align256(static_cast<size_t>(rows) * 4);
+  b.rowshift = o;
+  o += align256(static_cast<size_t>(rows) * 4);
+  b.overflow_words = maxnum > 2 * kRangedSmemWords ? (maxnum - 2 * kRangedSmemWords + 1) / 2 : 0;
+  b.overflow = o;
+  // One slot (two buffers) per resident chain: at most 16 chains per warp.
+  const int64_t slots = static_cast<int64_t>(sms) * kRangedMaxPerSm * (kPathThreads / 32) * 16;
+  o += align256(static_cast<size_t>(slots) * 2 * static_cast<size_t>(b.overflow_words) * 4);
+  b.total = o;
+  return b;
+}
+
+void launch_sgm_path_ranged_wave(const SgmMatch* dm, const SgmPathRangedWave& wave, int sms, cudaStream_t s) {
+  if (wave.njobs <= 0 || wave.pixels <= 0) return;
+  const SgmPathBuffers B = sgm_path_ranged_buffers(wave.cells, wave.pixels, wave.keys, wave.rows, wave.maxnum, sms);
+  uint8_t* cost = wave.buffer + B.cost;
+  uint16_t* sum = reinterpret_cast<uint16_t*>(wave.buffer + B.sum);
+  int4* info = reinterpret_cast<int4*>(wave.buffer + B.info);
+  uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
+  int4* rec = reinterpret_cast<int4*>(wave.buffer + B.rec);
+  int* rowsum = reinterpret_cast<int*>(wave.buffer + B.rowsum);
+  int* rowstart = reinterpret_cast<int*>(wave.buffer + B.rowstart);
+  int* rowshift = reinterpret_cast<int*>(wave.buffer + B.rowshift);
+  uint32_t* ovf = reinterpret_cast<uint32_t*>(wave.buffer + B.overflow);
+  if (wave.keys > 0) R3D_CUDA(cudaMemsetAsync(rkeys, 0xFF, static_cast<size_t>(wave.keys) * 4, s));
+  R3D_LAUNCH(sgm_path_ranged_rows_kernel,
+             dim3(resident_grid(sgm_path_ranged_rows_kernel, sms, wave.rows, kPathThreads / 32)), dim3(kPathThreads),
+             0, s, dm, wave.jobs, wave.njobs, wave.rows, rec, rowsum, rowshift);
+  launched("sgm_path_ranged_rows_kernel");
+  R3D_LAUNCH(sgm_path_ranged_rowstart_kernel,
+             dim3(resident_grid(sgm_path_ranged_rowstart_kernel, sms, wave.njobs, kPathThreads / 32)),
+             dim3(kPathThreads), 0, s, wave.jobs, wave.njobs, rowsum, rowstart);
+  launched("sgm_path_ranged_rowstart_kernel");
+  R3D_LAUNCH(sgm_path_ranged_cost_kernel,
+             dim3(resident_grid(sgm_path_ranged_cost_kernel, sms, wave.pixels, kPathThreads)), dim3(kPathThreads), 0,
+             s, dm, wave.jobs, wave.njobs, wave.pixels, rec, rowstart, cost);
+  launched("sgm_path_ranged_cost_kernel");
+  for (int q = 0; q < wave.nsegs; ++q) {
+    const SgmPathSegment& g = wave.segs[q];
+    const SgmPathJob* jobs = wave.jobs + g.first;
+    if (g.shape.g_ == 2 && g.shape.k_ == 8)
+      launch_ranged_passes<2, 8>(dm, jobs, g.count, g.blocks, rec, cost, sum, ovf, B.overflow_words, sms, s);
+    else if (g.shape.g_ == 4 && g.shape.k_ == 8)
+      launch_ranged_passes<4, 8>(dm, jobs, g.count, g.blocks, rec, cost, sum, ovf, B.overflow_words, sms, s);
+    else
+      fail(R3DGPU_EINVAL, "stereo: bad ranged path kernel shape");
+  }
+  R3D_LAUNCH(sgm_path_ranged_wta_kernel,
+             dim3(resident_grid(sgm_path_ranged_wta_kernel, sms, wave.pixels, kPathThreads)), dim3(kPathThreads), 0,
+             s, dm, wave.jobs, wave.njobs, wave.pixels, rec, sum, rowshift, info, rkeys);
+  launched("sgm_path_ranged_wta_kernel");
+  R3D_LAUNCH(sgm_path_ranged_accept_kernel,
+             dim3(resident_grid(sgm_path_ranged_accept_kernel, sms, wave.pixels, kPathThreads)), dim3(kPathThreads),
+             0, s, dm, wave.jobs, wave.njobs, wave.pixels, rec, info, rkeys, rowshift);
+  launched("sgm_path_ranged_accept_kernel");
 }
 
 }  // namespace r3dgpu

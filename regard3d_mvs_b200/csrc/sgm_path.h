@@ -27,6 +27,7 @@ struct SgmPathJob {
   int64_t px_off;             // first pixel of the tile in the wave's WTA records
   int64_t rk_off;             // first right-WTA key of the tile (diagonal LR only)
   int64_t blk[kPathClasses];  // first chain block (32 / G chains) of the tile, per chain class
+  int64_t row_off;            // ranged waves: first row of the tile in the wave's per-row arrays
   float* disp;
   float* conf;
   unsigned long long* cells;
@@ -47,6 +48,8 @@ inline int64_t sgm_path_chains(int cls, int w, int h) { return cls == 0 ? h : (c
 // Device buffers of a wave (bytes, 256-byte aligned pieces).
 struct SgmPathBuffers {
   size_t cost, sum, info, rkeys, total;
+  size_t rec, rowsum, rowstart, rowshift, overflow;  // ranged waves only
+  int64_t overflow_words;                            // per chain buffer
 };
 SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys);
 
@@ -72,5 +75,25 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
 // Whether full-range tiles go to the path kernels (default) or to the
 // one-CTA-per-tile wavefront kernel (R3DGPU_FULL_KERNEL=wavefront).
 bool sgm_path_enabled();
+
+// ---- Ranged tiles (per-pixel label ranges lo, num) through the chain passes.
+// Sums and costs are packed per tile (each pixel's num labels, row-major);
+// chunk 0 of a chain's predecessor vector (64 labels) stays in shared memory,
+// labels beyond it of the rare wide pixels in a per-chain overflow in global
+// memory. Shapes: (2, 8) = 32 labels per chunk, (4, 8) = 64.
+SgmPathShape sgm_path_ranged_shape(int over32, int64_t pixels);
+struct SgmPathRangedWave {
+  const SgmPathJob* jobs;
+  int njobs;
+  const SgmPathSegment* segs;
+  int nsegs;
+  int64_t cells, pixels, keys, rows;
+  int maxnum;  // largest label count of a pixel of the wave
+  unsigned char* buffer;
+};
+SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
+                                       int sms);
+void launch_sgm_path_ranged_wave(const SgmMatch* dm, const SgmPathRangedWave& wave, int sms, cudaStream_t s);
+bool sgm_path_ranged_enabled();
 
 }  // namespace r3dgpu

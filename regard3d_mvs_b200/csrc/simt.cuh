@@ -61,6 +61,12 @@ R3D_DEVICE void cp_async16(void* smem_dst, const void* gmem_src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
+// 8-byte asynchronous global -> shared copy (through L1). Both addresses
+// must be 8-byte aligned.
+R3D_DEVICE void cp_async8(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
 R3D_DEVICE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 R3D_DEVICE void cp_async_wait() {
@@ -169,6 +175,7 @@ inline int popc64(uint64_t v) { return __builtin_popcountll(v); }
 inline uint4 ld_stream(const uint4* p) { return *p; }
 inline void st_stream(uint4* p, uint4 v) { *p = v; }
 void cp_async16(void* smem_dst, const void* gmem_src);
+void cp_async8(void* smem_dst, const void* gmem_src);
 void cp_async_commit();
 void cp_async_wait_n(int n);
 template <int N>

@@ -33,6 +33,7 @@ enum class State { runnable, block_wait, warp_wait, done };
 struct Copy {
   unsigned char* dst;
   unsigned char bytes[16];
+  int size;
 };
 
 struct Fiber {
@@ -78,7 +79,7 @@ void switch_to_sched() {
 }
 
 void apply_group(std::vector<Copy>& g) {
-  for (Copy& c : g) std::memcpy(c.dst, c.bytes, 16);
+  for (Copy& c : g) std::memcpy(c.dst, c.bytes, static_cast<size_t>(c.size));
 }
 
 void fiber_entry() {
@@ -189,7 +190,20 @@ void cp_async16(void* dst, const void* src) {
   if (d < t_smem.get() || d + 16 > t_smem.get() + t_smem_size) throw std::runtime_error("simt: cp.async outside shared memory");
   Copy c;
   c.dst = d;
+  c.size = 16;
   std::memcpy(c.bytes, src, 16);
+  t_cur->pending.push_back(c);
+}
+
+void cp_async8(void* dst, const void* src) {
+  if ((reinterpret_cast<uintptr_t>(dst) & 7u) || (reinterpret_cast<uintptr_t>(src) & 7u))
+    throw std::runtime_error("simt: misaligned cp.async");
+  unsigned char* d = static_cast<unsigned char*>(dst);
+  if (d < t_smem.get() || d + 8 > t_smem.get() + t_smem_size) throw std::runtime_error("simt: cp.async outside shared memory");
+  Copy c;
+  c.dst = d;
+  c.size = 8;
+  std::memcpy(c.bytes, src, 8);
   t_cur->pending.push_back(c);
 }
 
