@@ -231,7 +231,13 @@ struct Workspace {
   std::vector<cudaStream_t> side;
   std::vector<cudaEvent_t> side_done;
   cudaEvent_t fork = nullptr;
+  // Stream and events of a second track of a batch (slot 1 workspaces).
+  cudaStream_t track = nullptr;
+  cudaEvent_t track_start = nullptr, track_done = nullptr;
   ~Workspace() {
+    if (track != nullptr) cudaStreamDestroy(track);
+    if (track_start != nullptr) cudaEventDestroy(track_start);
+    if (track_done != nullptr) cudaEventDestroy(track_done);
     for (cudaStream_t st : side) cudaStreamDestroy(st);
     for (cudaEvent_t ev : side_done) cudaEventDestroy(ev);
     if (fork != nullptr) cudaEventDestroy(fork);
@@ -249,13 +255,17 @@ struct Workspace {
   }
 };
 
-thread_local std::vector<std::unique_ptr<Workspace>> t_workspaces;  // per device, this thread's
+// This thread's workspaces: per device, slot 0 (every entry point) and slot
+// 1 (the single-level track of a batch that also has hierarchical pairs).
+constexpr int kWorkspaceSlots = 2;
+thread_local std::vector<std::unique_ptr<Workspace>> t_workspaces;
 
-Workspace& workspace() {
+Workspace& workspace(int slot = 0) {
   std::vector<std::unique_ptr<Workspace>>& per_device = t_workspaces;
-  int dev = t_device;
-  if (static_cast<int>(per_device.size()) <= dev) per_device.resize(dev + 1);
-  if (!per_device[dev]) {
+  const int dev = t_device;
+  const int idx = dev * kWorkspaceSlots + slot;
+  if (static_cast<int>(per_device.size()) <= idx) per_device.resize(idx + 1);
+  if (!per_device[idx]) {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count <= dev) {
       (void)cudaGetLastError();
@@ -274,10 +284,10 @@ Workspace& workspace() {
     ws->sms = prop.multiProcessorCount;
     ws->smem_optin = static_cast<int>(prop.sharedMemPerBlockOptin);
     ws->counter.reset(64);
-    per_device[dev] = std::move(ws);
+    per_device[idx] = std::move(ws);
   }
   R3D_CUDA(cudaSetDevice(dev));
-  return *per_device[dev];
+  return *per_device[idx];
 }
 
 // ------------------------------------------------------------------ views
@@ -825,14 +835,26 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
   }
 }
 
-// Runs a batch of pairs to completion on stream s.
-void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
-  Workspace& W = workspace();
+// A batch whose work is enqueued: what finish_batch completes once the
+// stream has run it.
+struct BatchRun {
+  Workspace* W = nullptr;
+  std::vector<PairRun> runs;
+};
+
+// Enqueues the whole matching of a batch of pairs on stream s, using the
+// workspace `slot` of this thread. Host synchronisations happen only where
+// ranged tiles need their label statistics.
+BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) {
+  BatchRun B;
+  Workspace& W = workspace(slot);
+  B.W = &W;
   W.arena.reset();
   W.pinned.reset();
   Arena& A = W.arena;
   Pinned& H = W.pinned;
-  std::vector<PairRun> runs(count);
+  std::vector<PairRun>& runs = B.runs;
+  runs.resize(count);
   int max_levels = 0;
   for (int i = 0; i < count; ++i) {
     validate_pair(pairs[i]);
@@ -1175,10 +1197,13 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
       P.h_cell_arrays.push_back(hc);
     }
   }
-  R3D_CUDA(cudaStreamSynchronize(s));
-  H.release_retired();
-  profile_collect();
-  for (auto& P : runs) {
+  return B;
+}
+
+// After the stream ran an enqueued batch: cell counts and output metadata.
+void finish_batch(BatchRun& B) {
+  B.W->pinned.release_retired();
+  for (auto& P : B.runs) {
     uint64_t cells = 0;
     for (size_t k = 0; k < P.h_cell_arrays.size(); ++k)
       for (int t = 0; t < P.cell_counts[k]; ++t) cells += P.h_cell_arrays[k][t];
@@ -1188,6 +1213,57 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     out.levels = P.levels;
     out.cells = cells;
   }
+}
+
+// Whether a batch that mixes single-level and hierarchical pairs runs them
+// as two concurrent tracks (default; R3DGPU_BATCH_TRACKS=1 runs one).
+bool batch_tracks_enabled() {
+  const char* e = std::getenv("R3DGPU_BATCH_TRACKS");
+  return e == nullptr || std::atoi(e) != 1;
+}
+
+// Runs a batch of pairs to completion on stream s. The levels of a batch run
+// in rounds (every pair's coarsest level first); when single-level pairs
+// share the batch with hierarchical ones, the single-level pairs form a
+// second track on their own stream and workspace, so that their matching
+// overlaps the hierarchy's rounds instead of waiting for its last one.
+void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
+  std::vector<int> flat, hier;
+  for (int i = 0; i < count; ++i) {
+    validate_pair(pairs[i]);
+    const int lv = pairs[i].options.levels >= 0
+                       ? pairs[i].options.levels
+                       : automatic_levels(pairs[i].left.width, pairs[i].left.height, pairs[i].num_disparities);
+    (lv == 0 ? flat : hier).push_back(i);
+  }
+  if (flat.empty() || hier.empty() || !batch_tracks_enabled()) {
+    BatchRun B = enqueue_batch(pairs, count, s, 0);
+    R3D_CUDA(cudaStreamSynchronize(s));
+    profile_collect();
+    finish_batch(B);
+    return;
+  }
+  std::vector<r3dgpu_pair> fp, hp;
+  for (int i : flat) fp.push_back(pairs[i]);
+  for (int i : hier) hp.push_back(pairs[i]);
+  Workspace& W1 = workspace(1);
+  if (W1.track == nullptr) {
+    R3D_CUDA(cudaStreamCreateWithFlags(&W1.track, cudaStreamNonBlocking));
+    R3D_CUDA(cudaEventCreateWithFlags(&W1.track_start, cudaEventDisableTiming));
+    R3D_CUDA(cudaEventCreateWithFlags(&W1.track_done, cudaEventDisableTiming));
+  }
+  R3D_CUDA(cudaEventRecord(W1.track_start, s));
+  R3D_CUDA(cudaStreamWaitEvent(W1.track, W1.track_start, 0));
+  BatchRun a = enqueue_batch(fp.data(), static_cast<int>(fp.size()), W1.track, 1);
+  R3D_CUDA(cudaEventRecord(W1.track_done, W1.track));
+  BatchRun b = enqueue_batch(hp.data(), static_cast<int>(hp.size()), s, 0);
+  R3D_CUDA(cudaStreamWaitEvent(s, W1.track_done, 0));
+  R3D_CUDA(cudaStreamSynchronize(s));
+  profile_collect();
+  finish_batch(a);
+  finish_batch(b);
+  for (size_t k = 0; k < flat.size(); ++k) pairs[flat[k]].out = fp[k].out;
+  for (size_t k = 0; k < hier.size(); ++k) pairs[hier[k]].out = hp[k].out;
 }
 
 template <class F>
@@ -1266,10 +1342,13 @@ r3dgpu_status r3dgpu_set_device(int32_t device) {
 
 r3dgpu_status r3dgpu_release_workspace(void) {
   return guarded([&] {
-    if (t_device < static_cast<int>(t_workspaces.size()) && t_workspaces[t_device]) {
-      R3D_CUDA(cudaSetDevice(t_device));
-      R3D_CUDA(cudaDeviceSynchronize());
-      t_workspaces[t_device].reset();
+    for (int slot = 0; slot < kWorkspaceSlots; ++slot) {
+      const int idx = t_device * kWorkspaceSlots + slot;
+      if (idx < static_cast<int>(t_workspaces.size()) && t_workspaces[idx]) {
+        R3D_CUDA(cudaSetDevice(t_device));
+        R3D_CUDA(cudaDeviceSynchronize());
+        t_workspaces[idx].reset();
+      }
     }
   });
 }

@@ -55,6 +55,7 @@ cudaError_t cudaGetDeviceCount(int* n);
 cudaError_t cudaGetDeviceProperties(cudaDeviceProp* p, int d);
 cudaError_t cudaDeviceGetAttribute(int* v, cudaDeviceAttr a, int d);
 cudaError_t cudaEventCreate(cudaEvent_t* e);
+cudaError_t cudaEventCreateWithFlags(cudaEvent_t* e, unsigned flags);
 cudaError_t cudaEventDestroy(cudaEvent_t e);
 cudaError_t cudaEventRecord(cudaEvent_t e, cudaStream_t st = nullptr);
 cudaError_t cudaEventSynchronize(cudaEvent_t e);
@@ -78,3 +79,4 @@ cudaError_t cudaOccupancyMaxActiveBlocksPerMultiprocessor(int* n, F, int, size_t
 }
 
 #define cudaStreamNonBlocking 1u
+#define cudaEventDisableTiming 2u

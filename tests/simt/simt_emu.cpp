@@ -375,6 +375,8 @@ cudaError_t cudaEventDestroy(cudaEvent_t e) {
   delete e;
   return ok();
 }
+cudaError_t cudaEventCreateWithFlags(cudaEvent_t* e, unsigned) { return cudaEventCreate(e); }
+
 cudaError_t cudaEventRecord(cudaEvent_t e, cudaStream_t) {
   e->t = std::chrono::steady_clock::now();
   return ok();

@@ -239,11 +239,13 @@ def _smooth_ranges(w, h, nd, seed, wide_frac=0.05):
 
 @pytest.mark.parametrize("kernel,shape,rows", [("ranged", "4,4", 32), ("ranged", "8,4", 16), ("ranged", "4,4", 8),
                                                ("ranged", "8,4", 64), ("ranged", "8,8", 12), ("ranged", "16,12", 6),
-                                               ("ranged", "32,8", 5), ("ranged", "", 0), ("general", "", 0)])
+                                               ("ranged", "32,8", 5), ("ranged", "", 0), ("general", "", 0),
+                                               ("path", "", 0)])
 def test_ranged_volume_kernels(gpu_matcher, oracle, monkeypatch, kernel, shape, rows):
-    """Per-pixel ranges through the ranged kernel (both shapes, several band
-    heights: aligned, shifted and bounds-checked predecessor reads, wide
-    pixels, seams) and through the general kernel, against the textbook volume."""
+    """Per-pixel ranges through the one-CTA-per-tile ranged kernel (both
+    shapes, several band heights: aligned, shifted and bounds-checked
+    predecessor reads, wide pixels, seams), the general kernel and the chain
+    passes (the default), against the textbook volume."""
     monkeypatch.setenv("R3DGPU_RANGED_KERNEL", kernel)
     if shape:
         monkeypatch.setenv("R3DGPU_RANGED_SHAPE", shape)

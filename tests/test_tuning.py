@@ -28,7 +28,21 @@ def _launches(m, run):
     return out, [e for e in json.loads(buf.value.decode() or "[]") if e["kernel"] != "sgm_round"]
 
 
+def test_default_kernels_are_the_chain_passes(simt_matcher):
+    """Full-range and ranged tiles go to the chain-pass kernels by default."""
+    tex = Texture(61)
+    left, right, _ = render_pair(tex, 40, 30, lambda x, y: 6.0 + 0.1 * x)
+    pairs = [dict(left=left, right=right, disparity_min=0, num_disparities=32, options=StereoOptions(levels=0)),
+             dict(left=left, right=right, disparity_min=0, num_disparities=32, options=StereoOptions(levels=1))]
+    _, launches = _launches(simt_matcher, lambda: simt_matcher.match_stereo_batch(pairs))
+    kinds = {e["kernel"] for e in launches}
+    assert kinds == {"sgm_path_kernel", "sgm_path_ranged_kernel"}, kinds
+
+
 def test_table_from_environment(simt_matcher, monkeypatch):
+    """The table drives the one-CTA-per-tile kernels (selected by the environment)."""
+    monkeypatch.setenv("R3DGPU_FULL_KERNEL", "wavefront")
+    monkeypatch.setenv("R3DGPU_RANGED_KERNEL", "ranged")
     tex = Texture(61)
     left, right, _ = render_pair(tex, 40, 30, lambda x, y: 6.0 + 0.1 * x)
     pairs = [dict(left=left, right=right, disparity_min=0, num_disparities=32, options=StereoOptions(levels=0))]
