@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--pairs", type=int, default=64)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-per-pair", action="store_true")
+    ap.add_argument("--no-plain", dest="plain", action="store_false",
+                    help="skip the one-pair-per-call run with the one-CTA-per-tile kernels")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve", action="store_true",
                     help="also run the serving sweep (config 3) in a fresh process and add its results")
@@ -174,14 +176,45 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def sgm_traffic_per_cell():
-    """DRAM bytes per aggregated cell of the SGM kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "sgm_traffic.json")
+def pass_traffic_per_cell():
+    """DRAM bytes per cell of one accumulate pass of the chain kernels, from
+    the committed ncu summary (profiles/sgm_path_traffic.json), if any."""
+    path = os.path.join(ROOT, "profiles", "sgm_path_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
             d = json.load(f)
-        return float(d["dram_bytes_per_cell"]), float(d.get("dram_bytes_per_pixel", 0.0))
-    return None, None
+        return float(d["accumulate_pass_dram_bytes_per_cell"])
+    return None
+
+
+def pass_roofline(launch_log, peak, peak_kind):
+    """Roofline of the dominant kernel, the chain pass (sgm_path_kernel):
+    algorithmic bytes of its launches (costs read, sums read and written) over
+    their CUDA-event durations on the launching stream."""
+    passes = [e for e in launch_log if e.get("pass") and e["kernel"] == "sgm_path_kernel"]
+    rpasses = [e for e in launch_log if e.get("pass") and e["kernel"] == "sgm_path_ranged_kernel"]
+    if not passes:
+        return None
+    ms = sum(e["ms"] for e in passes)
+    nbytes = sum(e["bytes"] for e in passes)
+    cells = sum(e["cells"] for e in passes)
+    achieved = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+    tpc = pass_traffic_per_cell()
+    acc = [e for e in passes if e["shape"].endswith("mode1")]
+    out = {"bound": "hbm", "kernel": "sgm_path_kernel (one chain pass of full-range tiles)", "achieved": achieved,
+           "peak": peak, "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": achieved / peak,
+           "traffic": (tpc * sum(e["cells"] for e in acc) / len(acc)) if (tpc and acc) else None,
+           "launches": len(passes), "avg_launch_ms": ms / len(passes), "alg_bytes_per_launch": nbytes / len(passes),
+           "alg_bytes_per_cell": {"first pass": 3, "accumulate pass": 5, "last pass": "3 + 16 per pixel"},
+           "cells_per_launch": cells / len(passes)}
+    if rpasses:
+        rms = sum(e["ms"] for e in rpasses)
+        rb = sum(e["bytes"] for e in rpasses)
+        out["ranged_pass"] = {"kernel": "sgm_path_ranged_kernel", "achieved": rb / (rms * 1e-3) / 1e9 if rms else 0.0,
+                              "frac": (rb / (rms * 1e-3) / 1e9) / peak if rms else 0.0, "launches": len(rpasses),
+                              "avg_launch_ms": rms / len(rpasses),
+                              "alg_bytes_per_cell": "3 (first) or 5, + 16 per pixel (range record)"}
+    return out
 
 
 def oracle_images(spec):
@@ -1002,7 +1035,35 @@ def main():
         lats = sorted(a.elapsed_time(b) for a, b in lat)
         per_pair = {"value": world * cells_full / (pp_ms * 1e-3) / 1e9, "unit": "Gcells/s", "ms_per_batch": pp_ms,
                     "latency_ms": {"p50": float(np.percentile(lats, 50)), "p99": float(np.percentile(lats, 99)),
-                                   "max": lats[-1]}}
+                                   "max": lats[-1]},
+                    "kernels": "chain passes (the library's default), one call per pair"}
+
+    # The plain one-pair-per-launch matcher: one CTA per tile (the wavefront
+    # kernels, selected by the environment), one call per pair.
+    per_pair_plain = None
+    if not args.no_per_pair and args.plain:
+        os.environ["R3DGPU_FULL_KERNEL"] = "wavefront"
+        os.environ["R3DGPU_RANGED_KERNEL"] = "ranged"
+        try:
+            barrier()
+            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            for i in range(n):
+                st = lib.r3dgpu_match_stereo(ctypes.byref(pairs[i].left), ctypes.byref(pairs[i].right),
+                                             ctypes.byref(pairs[i].left_valid), ctypes.byref(pairs[i].right_valid),
+                                             pairs[i].disparity_min, pairs[i].num_disparities,
+                                             ctypes.byref(pairs[i].options), ctypes.byref(pairs[i].out), sptr)
+                if st != 0:
+                    raise RuntimeError(lib.r3dgpu_last_error().decode())
+            p1.record(stream)
+            barrier()
+            pl_ms = max_over_ranks(p0.elapsed_time(p1))
+        finally:
+            del os.environ["R3DGPU_FULL_KERNEL"]
+            del os.environ["R3DGPU_RANGED_KERNEL"]
+        per_pair_plain = {"value": world * cells_full / (pl_ms * 1e-3) / 1e9, "unit": "Gcells/s",
+                          "ms_per_batch": pl_ms,
+                          "kernels": "one CTA per tile (skewed-wavefront kernels), one call per pair"}
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -1013,10 +1074,6 @@ def main():
         sgm_ms = prof.sgm_ms / rounds
         alg_bytes = (ALG_BYTES_PER_CELL * prof.sgm_cells + ALG_BYTES_PER_PIXEL * prof.sgm_pixels) / rounds
         achieved = alg_bytes / (sgm_ms * 1e-3) / 1e9 if sgm_ms > 0 else 0.0
-        tpc, tpp = sgm_traffic_per_cell()
-        traffic = None
-        if tpc is not None:
-            traffic = (tpc * prof.sgm_cells + tpp * prof.sgm_pixels) / rounds
         sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
         clocks = clk.summary()
         int_peak = sm_count * 128 * (clocks.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
@@ -1031,21 +1088,23 @@ def main():
             "e2e": {"value": e2e_value, "unit": "Gcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "SGM stage: sgm_full_kernel + sgm_ranged_kernel launches of a round",
-                         "achieved": achieved, "peak": peak,
-                         "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "avg_stage_ms": sgm_ms, "stages": rounds,
-                         "launches": int(prof.sgm_launches), "alg_bytes_per_stage": alg_bytes,
-                         "stage_ms_of_first_step": [round(e["ms"], 2) for e in launch_log
-                                                    if e["kernel"] == "sgm_round"][:rounds // max(args.steps, 1)],
-                         "sgm_share_of_step": prof.sgm_ms / max(ms, 1e-9)},
+            "roofline": pass_roofline(launch_log, peak, peak_kind),
+            "stage_roofline": {"bound": "hbm", "kernel": "SGM stage of a round (fork to join of its chain-pass waves)",
+                               "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                               "alg_bytes_per_cell": ALG_BYTES_PER_CELL, "alg_bytes_per_pixel": ALG_BYTES_PER_PIXEL,
+                               "avg_stage_ms": sgm_ms, "stages": rounds, "alg_bytes_per_stage": alg_bytes,
+                               "stage_ms_of_first_step": [round(e["ms"], 2) for e in launch_log
+                                                          if e["kernel"] == "sgm_round"][:rounds // max(args.steps, 1)],
+                               "sgm_share_of_step": prof.sgm_ms / max(ms, 1e-9)},
             "int_roofline": {"ops_per_cell": INT_OPS_PER_CELL, "achieved_tops": int_achieved,
                              "nominal_int32_tops": int_peak, "frac": int_achieved / int_peak},
             "clocks": clocks,
         }
+        if line["roofline"] is None:
+            line["roofline"] = dict(line["stage_roofline"])
         breakdown = {}
         for e in launch_log:
-            if e["kernel"] == "sgm_round":
+            if e["kernel"] == "sgm_round" or e.get("pass"):
                 continue
             k = f"{e['kernel']}:{e['shape']}"
             b = breakdown.setdefault(k, {"launches": 0, "ms": 0.0, "cells": 0, "tiles": 0})
@@ -1059,6 +1118,9 @@ def main():
         if per_pair is not None:
             line["per_pair"] = per_pair
             line["batched_vs_per_pair"] = value / per_pair["value"]
+        if per_pair_plain is not None:
+            line["per_pair_plain"] = per_pair_plain
+            line["batched_vs_plain_per_pair"] = value / per_pair_plain["value"]
         if not args.no_cpu_baseline and world == 1:
             # The CPU baseline and the other stages' lines at N = 1 only.
             gpu_maps = {i: dD[i].cpu().numpy() for i in range(n)

@@ -60,6 +60,8 @@ struct ProfileState {
     std::string kernel, shape;
     int grid, rows;
     bool span;  // the SGM stage of a round (fork to join), not one launch
+    bool pass = false;  // one pass launch of the chain kernels (inside a group)
+    uint64_t bytes = 0;  // its algorithmic HBM bytes
   };
   std::vector<Pending> pending;
   std::string launches;       // JSON objects of the launches since the last take
@@ -74,6 +76,18 @@ void profile_collect() {
     (void)cudaGetLastError();
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);
+    if (p.pass) {
+      char line[256];
+      std::snprintf(line, sizeof(line),
+                    "{\"kernel\": \"%s\", \"pass\": true, \"shape\": \"%s\", \"cells\": %llu, \"pixels\": %llu, "
+                    "\"bytes\": %llu, \"ms\": %.4f}",
+                    p.kernel.c_str(), p.shape.c_str(), static_cast<unsigned long long>(p.cells),
+                    static_cast<unsigned long long>(p.pixels), static_cast<unsigned long long>(p.bytes),
+                    static_cast<double>(ms));
+      if (!t_prof.launches.empty()) t_prof.launches += ", ";
+      t_prof.launches += line;
+      continue;
+    }
     if (p.span) {
       // Launches of a round overlap: the stage time is the round's span.
       t_prof.acc.sgm_ms += ms;
@@ -144,6 +158,33 @@ void p2_lut(const r3dgpu_stereo_options& o, uint16_t* lut) {
     lut[di] = static_cast<uint16_t>(p2);
   }
 }
+
+}  // namespace
+
+bool profile_on() { return t_prof.on; }
+
+cudaEvent_t profile_mark(cudaStream_t s) {
+  cudaEvent_t e = nullptr;
+  R3D_CUDA(cudaEventCreate(&e));
+  R3D_CUDA(cudaEventRecord(e, s));
+  return e;
+}
+
+void profile_pass(cudaEvent_t a, cudaEvent_t b, const char* kernel, const char* shape, uint64_t cells,
+                  uint64_t pixels, uint64_t bytes) {
+  ProfileState::Pending p{};
+  p.a = a;
+  p.b = b;
+  p.kernel = kernel;
+  p.shape = shape;
+  p.cells = cells;
+  p.pixels = pixels;
+  p.pass = true;
+  p.bytes = bytes;
+  t_prof.pending.push_back(p);
+}
+
+namespace {
 
 // ------------------------------------------------------------------ memory
 // Bump allocator over grow-only device chunks; reset() rewinds it so that the
@@ -786,8 +827,10 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     for (int q = 0; q < n; ++q) {
       const Entry& e = es[begin + q];
       if (sg.empty() || sg.back().shape.g_ != e.sh.g_ || sg.back().shape.k_ != e.sh.k_)
-        sg.push_back(SgmPathSegment{e.sh, q, 0, {0, 0, 0}});
+        sg.push_back(SgmPathSegment{e.sh, q, 0, {0, 0, 0}, 0, 0});
       SgmPathSegment& g = sg.back();
+      g.cells += e.cells;
+      g.pixels += e.px;
       Match& M = *matches[e.i];
       const Tile& T = M.layout.tiles[e.t];
       SgmPathJob& J = hj[q];
@@ -946,7 +989,9 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
       const int nt = static_cast<int>(M.layout.tiles.size());
       if (!M.ranged) {
         // Full-range tiles of every label count: the chain passes, one group.
-        if (sgm_path_enabled() && sgm_path_shape(M.m.nd).g_ != 0) {
+        bool fits = true;
+        for (int t = 0; t < nt; ++t) fits = fits && sgm_path_fits(M.layout.tiles[t].w, M.m.nd);
+        if (sgm_path_enabled() && sgm_path_shape(M.m.nd).g_ != 0 && fits) {
           Group& g = group_for(kPath, 0, SgmFullPlan{{0, 0}, 0});
           for (int t = 0; t < nt; ++t) g.tiles.emplace_back(i, t);
           continue;
@@ -1126,6 +1171,7 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
           w.cells = rw.cells;
           w.pixels = rw.pixels;
           w.keys = rw.keys;
+          w.rows = rw.rows;
           w.buffer = scratch;
           launch_sgm_path_wave(dm, w, W.sms, gs);
         }
@@ -1562,7 +1608,7 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
     }
     SgmMatch* hm = W.pinned.alloc<SgmMatch>(1);
     fill_match(*hm, o, DView<uint16_t>{dl, wl, h, wl}, cl, cr, wr, il, ir, rlo, rnum, disparity_min, nd, false, false);
-    if (!(ranges_lo && ranges_num) && sgm_path_enabled() && sgm_path_shape(nd).g_ != 0) {
+    if (!(ranges_lo && ranges_num) && sgm_path_enabled() && sgm_path_shape(nd).g_ != 0 && sgm_path_fits(wl, nd)) {
       // The whole image as one full-range tile through the chain passes.
       SgmMatch* dm = A.alloc<SgmMatch>(1);
       R3D_CUDA(cudaMemcpyAsync(dm, hm, sizeof(SgmMatch), cudaMemcpyHostToDevice, s));
@@ -1572,7 +1618,7 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
       hj->w = wl;
       hj->h = h;
       const SgmPathShape sh = sgm_path_shape(nd);
-      SgmPathSegment seg{sh, 0, 1, {0, 0, 0}};
+      SgmPathSegment seg{sh, 0, 1, {0, 0, 0}, static_cast<int64_t>(cells), px};
       for (int c = 0; c < kPathClasses; ++c) seg.blocks[c] = (sgm_path_chains(c, wl, h) + 32 / sh.g_ - 1) / (32 / sh.g_);
       hj->disp = A.alloc<float>(static_cast<size_t>(px));
       hj->cells = A.alloc<unsigned long long>(1);
@@ -1588,6 +1634,7 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
       wv.cells = static_cast<int64_t>(cells);
       wv.pixels = px;
       wv.keys = 0;
+      wv.rows = h;
       W.scratch.reserve(sgm_path_buffers(wv.cells, px, 0).total);
       wv.buffer = W.scratch.get();
       launch_sgm_path_wave(dm, wv, W.sms, s);
@@ -1607,7 +1654,7 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
       *hj = SgmPathJob{};
       hj->w = wl;
       hj->h = h;
-      SgmPathSegment seg{sh, 0, 1, {0, 0, 0}};
+      SgmPathSegment seg{sh, 0, 1, {0, 0, 0}, static_cast<int64_t>(cells), px};
       for (int c = 0; c < kPathClasses; ++c) seg.blocks[c] = (sgm_path_chains(c, wl, h) + 32 / sh.g_ - 1) / (32 / sh.g_);
       hj->disp = A.alloc<float>(static_cast<size_t>(px));
       hj->cells = A.alloc<unsigned long long>(1);

@@ -24,6 +24,7 @@
 // as many SMs as it has chains, so one small pair fills the GPU as well as a
 // batch does. HBM traffic per aggregated cell: 1 B cost write, 8 x 1 B cost
 // reads, 2 B + 6 x 4 B + 2 B sum traffic.
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 
@@ -87,42 +88,68 @@ R3D_DEVICE void chain_geometry(int cls, int dx, int dy, int w, int h, int64_t c,
 }
 
 // ---------------------------------------------------------------- costs
-// C(p, a) of stereo_matcher.cpp:305-353, u8, 16 labels per thread (nd is a
-// multiple of 16): one left Census code and 16 right codes, L1-shared with
-// the neighbouring threads of the same pixel and row.
+// C(p, a) of stereo_matcher.cpp:305-353, u8. One warp per tile row: the
+// partner Census codes the row can reach (right columns x0 - dmin - nd + 1 ..
+// x0 + w - 1 - dmin) are staged in the warp's shared memory, then the lanes
+// take 32 consecutive pixels and write 32 labels (one sector) at a time.
+constexpr int kCostStage = 2048;  // staged partner codes per warp (sgm_path_fits: w + nd - 1 <= 2048)
+
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     sgm_path_cost_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
-                         int64_t items, uint8_t* R3D_RESTRICT cost) {
-  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < items; i += stride) {
-    const int64_t cell = 16 * i;
-    const int j = find_job(jobs, njobs, cell, [](const SgmPathJob& q) { return q.cell_off; });
+                         int64_t rows, uint8_t* R3D_RESTRICT cost) {
+  R3D_DYNAMIC_SMEM(smem);
+  const int lane = static_cast<int>(threadIdx.x & 31u), warp = static_cast<int>(threadIdx.x >> 5);
+  const int wpb = static_cast<int>(blockDim.x) >> 5;
+  uint64_t* stage = reinterpret_cast<uint64_t*>(smem) + static_cast<size_t>(warp) * kCostStage;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
+  for (int64_t r = static_cast<int64_t>(blockIdx.x) * wpb + warp; r < rows; r += nwarps) {
+    const int j = find_job(jobs, njobs, r, [](const SgmPathJob& q) { return q.row_off; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
-    const int nd = m.nd;
-    const int local = static_cast<int>(cell - job.cell_off);  // a tile has fewer than 2^31 cells
-    const int p = local / nd;
-    const int b = (local - p * nd) >> 4;
-    const int y = p / job.w, x = p - y * job.w;
-    const int bx = job.x0 + x, by = job.y0 + y;
+    const int nd = m.nd, w = job.w;
+    const int y = static_cast<int>(r - job.row_off), by = job.y0 + y;
     const RowInterval lv = m.bv[by], rv = m.pv[by];
-    uint32_t q[4] = {0, 0, 0, 0};
-    if (bx >= lv.first && bx <= lv.last) {
-      const uint64_t cl = m.cbase[static_cast<int64_t>(by) * m.cb_stride + bx];
-      const uint64_t* crow = m.cpart + static_cast<int64_t>(by) * m.cp_stride;
-      const int xr0 = bx - m.dmin - 16 * b;
-      const int safe = rv.first > 0 ? rv.first : 0;
-      const uint32_t inv = static_cast<uint32_t>(m.invalid_cost);
+    const uint64_t* crow = m.cpart + static_cast<int64_t>(by) * m.cp_stride;
+    const uint64_t* lrow = m.cbase + static_cast<int64_t>(by) * m.cb_stride;
+    // Staged right column xr is stage[xr - xr0]; columns outside the valid
+    // right interval are never read (their cost is invalid_cost).
+    const int xr0 = job.x0 - m.dmin - nd + 1;
+    const int span = w + nd - 1;
+    r3dsimt::syncwarp();
+    for (int k = lane; k < span; k += 32) {
+      const int xr = xr0 + k;
+      stage[k] = (xr >= rv.first && xr <= rv.last) ? crow[xr] : 0;
+    }
+    r3dsimt::syncwarp();
+    const uint32_t inv = static_cast<uint32_t>(m.invalid_cost);
+    uint8_t* row_out = cost + job.cell_off + static_cast<int64_t>(y) * w * nd;
+    for (int xb = 0; xb < w; xb += 32) {
+      const int x = xb + lane;
+      if (x >= w) continue;
+      const int bx = job.x0 + x;
+      const bool inside = bx >= lv.first && bx <= lv.last;
+      const uint64_t cl = inside ? lrow[bx] : 0;
+      uint8_t* out = row_out + static_cast<int64_t>(x) * nd;
+      for (int c = 0; c < nd; c += 32) {
+        const int nl = nd - c < 32 ? 16 : 32;  // nd is a multiple of 16
+        uint32_t q[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (inside) {
+          // Label a = c + k reads right column bx - dmin - a = xr0 + (x + nd - 1 - a).
+          const int base = x + nd - 1 - c;
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        const int xr = xr0 - k;
-        const bool ok = xr >= rv.first && xr <= rv.last;
-        const uint64_t cr = crow[ok ? xr : safe];
-        const uint32_t c = ok ? static_cast<uint32_t>(r3dsimt::popc64(cl ^ cr)) : inv;
-        q[k >> 2] |= c << (8 * (k & 3));
+          for (int k = 0; k < 32; ++k) {
+            if (k < nl) {
+              const int xr = bx - m.dmin - c - k;
+              const bool ok = xr >= rv.first && xr <= rv.last;
+              const uint32_t v = ok ? static_cast<uint32_t>(r3dsimt::popc64(cl ^ stage[base - k])) : inv;
+              q[k >> 2] |= v << (8 * (k & 3));
+            }
+          }
+        }
+        *reinterpret_cast<uint4*>(out + c) = make_uint4(q[0], q[1], q[2], q[3]);
+        if (nl == 32) *reinterpret_cast<uint4*>(out + c + 16) = make_uint4(q[4], q[5], q[6], q[7]);
       }
     }
-    *reinterpret_cast<uint4*>(cost + cell) = make_uint4(q[0], q[1], q[2], q[3]);
   }
 }
 
@@ -557,8 +584,11 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 }
 
 // Labels of a chain's predecessor vector kept in shared memory (u32 words of
-// two labels); wider vectors continue in the chain's global overflow.
+// two labels); wider vectors continue in the chain's global overflow. The
+// buffers of a warp's chains are kRangedSmemStride words apart (odd, so that
+// the chains of a warp start in different banks).
 constexpr int kRangedSmemWords = 32;
+constexpr int kRangedSmemStride = kRangedSmemWords + 1;
 
 template <int G, int K>
 struct RangedRing {
@@ -567,7 +597,7 @@ struct RangedRing {
   static constexpr int kDataStage = CPW * 3 * CH;
   static constexpr int kData = kPathStages * kDataStage;
   static constexpr int kRec = 2 * kPathStages * 32 * 16;  // one record slot per lane and stage
-  static constexpr int kPrev = CPW * 2 * kRangedSmemWords * 4;
+  static constexpr int kPrev = CPW * 2 * kRangedSmemStride * 4;
   static constexpr int kWarpBytes = kData + kRec + kPrev;
   static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
 };
@@ -587,7 +617,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
   unsigned char* wb = smem + static_cast<size_t>(warp) * R::kWarpBytes;
   int4* recs = reinterpret_cast<int4*>(wb + R::kData);
-  uint32_t* prevw = reinterpret_cast<uint32_t*>(wb + R::kData + R::kRec) + gi * 2 * kRangedSmemWords;
+  // Buffer b of this lane's chain: words (b * CPW + gi) * kRangedSmemStride onwards.
+  uint32_t* prevw = reinterpret_cast<uint32_t*>(wb + R::kData + R::kRec) + gi * kRangedSmemStride;
   uint32_t* ovfc = ovf + (static_cast<int64_t>(blockIdx.x) * wpb * CPW + warp * CPW + gi) * 2 * ovf_words;
   auto stage_cost = [&](int st) -> unsigned char* { return wb + st * R::kDataStage + gi * CH + e0; };
   auto stage_sum = [&](int st) -> unsigned char* {
@@ -595,13 +626,15 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
   };
   // Word idx (labels 2 idx, 2 idx + 1) of buffer b of the predecessor vector
   // (nw words long): two sentinels outside it.
+  // The shared-memory word is read unconditionally (at a wrapped, in-bounds
+  // index); only the rare words of wide vectors go to the overflow.
   auto qword = [&](int b, int idx, int nw) -> uint32_t {
-    if (idx < 0 || idx >= nw) return kSent2;
-    return idx < kRangedSmemWords ? prevw[b * kRangedSmemWords + idx]
-                                  : ovfc[b * ovf_words + (idx - kRangedSmemWords)];
+    uint32_t v = prevw[b * CPW * kRangedSmemStride + (idx & (kRangedSmemWords - 1))];
+    if (idx >= kRangedSmemWords && idx < nw) v = ovfc[b * ovf_words + (idx - kRangedSmemWords)];
+    return (idx < 0 || idx >= nw) ? kSent2 : v;
   };
   auto put_word = [&](int b, int idx, uint32_t v) {
-    if (idx < kRangedSmemWords) prevw[b * kRangedSmemWords + idx] = v;
+    if (idx < kRangedSmemWords) prevw[b * CPW * kRangedSmemStride + idx] = v;
     else ovfc[b * ovf_words + (idx - kRangedSmemWords)] = v;
   };
   for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + warp; blk < total_blocks; blk += nwarps) {
@@ -890,9 +923,21 @@ int resident_grid(Kernel kernel, int sms, int64_t work_items, int per_block, siz
   return static_cast<int>(need < resident ? (need > 0 ? need : 1) : resident);
 }
 
+// Algorithmic HBM bytes of one pass over `cells` cells of `pixels` pixels:
+// costs read, sums read (not by the first pass) and written (not by the
+// full-range last pass, which writes the WTA records instead).
+uint64_t pass_bytes(int mode, bool ranged, const SgmPathSegment& g) {
+  const uint64_t c = static_cast<uint64_t>(g.cells), px = static_cast<uint64_t>(g.pixels);
+  if (mode == kFirst) return 3 * c;
+  if (mode == kLast && !ranged) return 3 * c + 16 * px;
+  return 5 * c;
+}
+
 template <int G, int K, int MODE>
 void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
-                 const uint8_t* cost, uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s) {
+                 const uint8_t* cost, uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s,
+                 const SgmPathSegment& seg) {
+  const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_kernel<G, K, MODE>;
   constexpr size_t smem = PathRing<G, K>::kBlockBytes;
   static thread_local int configured[64] = {};
@@ -905,21 +950,27 @@ void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int
   R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32, smem)), dim3(kPathThreads), smem, s, dm, jobs,
              njobs, ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys);
   launched("sgm_path_kernel");
+  if (ev0 != nullptr) {
+    char shape[32];
+    std::snprintf(shape, sizeof(shape), "%dx%d/mode%d", G, K, MODE);
+    profile_pass(ev0, profile_mark(s), "sgm_path_kernel", shape, static_cast<uint64_t>(seg.cells),
+                 static_cast<uint64_t>(seg.pixels), pass_bytes(MODE, false, seg));
+  }
 }
 
 template <int G, int K>
-void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, int njobs, const int64_t (&blocks)[kPathClasses],
-                   const uint8_t* cost, uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s) {
+void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const uint8_t* cost,
+                   uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s) {
   for (int q = 0; q < 8; ++q) {
     const Pass ps = kPasses[q];
-    const int64_t nb = blocks[ps.cls];
+    const int64_t nb = g.blocks[ps.cls];
     if (nb <= 0) continue;
     if (q == 0)
-      launch_pass<G, K, kFirst>(ps, dm, jobs, njobs, nb, cost, sum, info, rkeys, sms, s);
+      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g);
     else if (q < 7)
-      launch_pass<G, K, kAccumulate>(ps, dm, jobs, njobs, nb, cost, sum, info, rkeys, sms, s);
+      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g);
     else
-      launch_pass<G, K, kLast>(ps, dm, jobs, njobs, nb, cost, sum, info, rkeys, sms, s);
+      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g);
   }
 }
 
@@ -981,9 +1032,18 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
   uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
   if (wave.keys > 0) R3D_CUDA(cudaMemsetAsync(rkeys, 0xFF, static_cast<size_t>(wave.keys) * 4, s));
   {
-    const int64_t items = wave.cells / 16;
-    R3D_LAUNCH(sgm_path_cost_kernel, dim3(resident_grid(sgm_path_cost_kernel, sms, items, kPathThreads)),
-               dim3(kPathThreads), 0, s, dm, wave.jobs, wave.njobs, items, cost);
+    constexpr size_t smem = static_cast<size_t>(kPathThreads / 32) * kCostStage * 8;
+    static thread_local int configured[64] = {};
+    int dev = 0;
+    R3D_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64 && !configured[dev]) {
+      R3D_CUDA(cudaFuncSetAttribute(sgm_path_cost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+      configured[dev] = 1;
+    }
+    R3D_LAUNCH(sgm_path_cost_kernel,
+               dim3(resident_grid(sgm_path_cost_kernel, sms, wave.rows, kPathThreads / 32, smem)),
+               dim3(kPathThreads), smem, s, dm, wave.jobs, wave.njobs, wave.rows, cost);
     launched("sgm_path_cost_kernel");
   }
   for (int q = 0; q < wave.nsegs; ++q) {
@@ -992,7 +1052,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
     bool done = false;
 #define R3D_SHAPE(gg, kk)                                                                                     \
   if (!done && g.shape.g_ == gg && g.shape.k_ == kk) {                                                        \
-    launch_passes<gg, kk>(dm, jobs, g.count, g.blocks, cost, sum, info, rkeys, sms, s);                       \
+    launch_passes<gg, kk>(dm, jobs, g, cost, sum, info, rkeys, sms, s);                                      \
     done = true;                                                                                              \
   }
     R3D_PATH_SHAPES(R3D_SHAPE)
@@ -1014,7 +1074,8 @@ constexpr int kRangedMaxPerSm = 4;
 template <int G, int K, int MODE>
 void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
                         const int4* rec, const uint8_t* cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words,
-                        int sms, cudaStream_t s) {
+                        int sms, cudaStream_t s, const SgmPathSegment& seg) {
+  const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_ranged_kernel<G, K, MODE>;
   constexpr size_t smem = RangedRing<G, K>::kBlockBytes;
   static thread_local int configured[64] = {};
@@ -1029,20 +1090,27 @@ void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jo
   R3D_LAUNCH(k, dim3(grid), dim3(kPathThreads), smem, s, dm, jobs, njobs, ps.cls, ps.dx, ps.dy, nb, rec, cost, sum,
              ovf, ovf_words);
   launched("sgm_path_ranged_kernel");
+  if (ev0 != nullptr) {
+    char shape[32];
+    std::snprintf(shape, sizeof(shape), "%dx%d/mode%d", G, K, MODE);
+    // Per pixel and pass also the 16-byte record (range and cell offset).
+    profile_pass(ev0, profile_mark(s), "sgm_path_ranged_kernel", shape, static_cast<uint64_t>(seg.cells),
+                 static_cast<uint64_t>(seg.pixels), pass_bytes(MODE, true, seg) + 16 * static_cast<uint64_t>(seg.pixels));
+  }
 }
 
 template <int G, int K>
-void launch_ranged_passes(const SgmMatch* dm, const SgmPathJob* jobs, int njobs,
-                          const int64_t (&blocks)[kPathClasses], const int4* rec, const uint8_t* cost, uint16_t* sum,
-                          uint32_t* ovf, int64_t ovf_words, int sms, cudaStream_t s) {
+void launch_ranged_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const int4* rec,
+                          const uint8_t* cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words, int sms,
+                          cudaStream_t s) {
   for (int q = 0; q < 8; ++q) {
     const Pass ps = kPasses[q];
-    const int64_t nb = blocks[ps.cls];
+    const int64_t nb = g.blocks[ps.cls];
     if (nb <= 0) continue;
     if (q == 0)
-      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, njobs, nb, rec, cost, sum, ovf, ovf_words, sms, s);
+      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g);
     else
-      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, njobs, nb, rec, cost, sum, ovf, ovf_words, sms, s);
+      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g);
   }
 }
 
@@ -1108,9 +1176,9 @@ void launch_sgm_path_ranged_wave(const SgmMatch* dm, const SgmPathRangedWave& wa
     const SgmPathSegment& g = wave.segs[q];
     const SgmPathJob* jobs = wave.jobs + g.first;
     if (g.shape.g_ == 2 && g.shape.k_ == 8)
-      launch_ranged_passes<2, 8>(dm, jobs, g.count, g.blocks, rec, cost, sum, ovf, B.overflow_words, sms, s);
+      launch_ranged_passes<2, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s);
     else if (g.shape.g_ == 4 && g.shape.k_ == 8)
-      launch_ranged_passes<4, 8>(dm, jobs, g.count, g.blocks, rec, cost, sum, ovf, B.overflow_words, sms, s);
+      launch_ranged_passes<4, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s);
     else
       fail(R3DGPU_EINVAL, "stereo: bad ranged path kernel shape");
   }

@@ -41,8 +41,11 @@ struct SgmPathShape {
 };
 
 // Narrowest compiled shape for nd labels ({0, 0}: more labels than the path
-// kernels take).
+// kernels take, or a tile too wide for the cost kernel's staged partner row:
+// tile width + nd - 1 must stay within 2048).
 SgmPathShape sgm_path_shape(int nd);
+// Whether a full-range tile of width w with nd labels fits the cost kernel.
+inline bool sgm_path_fits(int w, int nd) { return w + nd - 1 <= 2048; }
 inline int64_t sgm_path_chains(int cls, int w, int h) { return cls == 0 ? h : (cls == 1 ? w : w + h - 1); }
 
 // Device buffers of a wave (bytes, 256-byte aligned pieces).
@@ -59,13 +62,22 @@ struct SgmPathSegment {
   SgmPathShape shape;
   int first, count;
   int64_t blocks[kPathClasses];
+  int64_t cells, pixels;  // of the segment's tiles (per-launch profiling)
 };
+
+// Per-launch timing of the pass kernels while the library's profiling is on
+// (defined with the rest of the profiling in matcher.cpp): `bytes` is the
+// launch's algorithmic HBM traffic.
+bool profile_on();
+cudaEvent_t profile_mark(cudaStream_t s);
+void profile_pass(cudaEvent_t a, cudaEvent_t b, const char* kernel, const char* shape, uint64_t cells,
+                  uint64_t pixels, uint64_t bytes);
 struct SgmPathWave {
   const SgmPathJob* jobs;
   int njobs;
   const SgmPathSegment* segs;  // host array
   int nsegs;
-  int64_t cells, pixels, keys;
+  int64_t cells, pixels, keys, rows;
   unsigned char* buffer;  // sgm_path_buffers(cells, pixels, keys).total bytes
 };
 

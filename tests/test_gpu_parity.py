@@ -329,10 +329,12 @@ def test_config1_pair_3072x2048_256_four_levels(gpu_matcher, oracle):
     _assert_same_map(got, ref)
 
 
-# Pairs of the 64-pair batch: the widest pair (5624 px, hierarchical, 256
-# labels), the widest single-level pair (5605 px, 192 labels), a 384-label
-# single-level pair and a 5524 px 384-label hierarchical pair.
-BATCH64_SAMPLE = (55, 38, 10, 31)
+# Pairs of the 64-pair benchmark batch (bench.py's default seed): the widest
+# pair (5775 px, hierarchical, 192 labels), the widest single-level pair
+# (5365x4024, 192 labels), a 3194x2396 384-label single-level pair and a
+# 5048 px 384-label hierarchical pair.
+BATCH64_SEED = 2024
+BATCH64_SAMPLE = (63, 50, 48, 15)
 
 
 def test_config2_pairs_batched(gpu_matcher, oracle):
@@ -340,7 +342,7 @@ def test_config2_pairs_batched(gpu_matcher, oracle):
     oracle matching it alone."""
     import bench
 
-    specs = bench.workload_pairs("batch64", 64, 0)
+    specs = bench.workload_pairs("batch64", 64, BATCH64_SEED)
     chosen = [specs[i] for i in BATCH64_SAMPLE]
     assert max(s["w"] for s in chosen) == max(s["w"] for s in specs)
     assert any(s["nd"] == 384 and s["levels"] == 0 for s in chosen)
