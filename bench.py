@@ -60,7 +60,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "combine", "rectify", "depth", "view"),
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "pair2048", "combine", "rectify", "depth",
+                                           "view"),
                     default="batch64",
                     help="combine / rectify / depth: only the multi-view combination of one view / the "
                          "rectification resampling of one pair / the depth stage after the combination "
@@ -85,6 +86,9 @@ def workload_pairs(name: str, npairs: int, seed: int):
     out = []
     if name == "pair640":
         return [dict(w=640, h=480, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
+    if name == "pair2048":
+        # One full-range pair of a config-4 view's size (profiling case of the pass kernels).
+        return [dict(w=2048, h=1536, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
     if name == "pair3072":
         return [dict(w=3072, h=2048, nd=256, levels=3, radius=0, margin=8, textureless=0.15, occluded=0.10,
                      seed=seed)]

@@ -109,6 +109,27 @@ int32_t r3dgpu_automatic_levels(int32_t width, int32_t height, int32_t num_dispa
 /* Selects the CUDA device used by this thread's later calls (default 0). */
 r3dgpu_status r3dgpu_set_device(int32_t device);
 
+/* Cancellation token, the counterpart of the reference's per-thread
+ * CancelToken (src/r3d/core/cancel.hpp:36-55, polled before every tile chunk
+ * at src/r3d/core/thread_pool.cpp:53-55). A token is a flag in page-locked
+ * host memory mapped into the device's address space. r3dgpu_cancel sets it
+ * (from any thread); the matcher entry points of a thread that attached it
+ * with r3dgpu_set_cancel_token poll it on the host between hierarchy rounds
+ * and waves of tiles, and the SGM chain kernels read it once per chain block
+ * (a plain read, never a wait), so work already enqueued drains within one
+ * block. A call that sees the flag returns R3DGPU_ECANCELLED after its
+ * enqueued work has finished; its outputs are then unspecified, and the
+ * device and the library stay usable. r3dgpu_cancel_token_reset clears the
+ * flag for the next call. */
+typedef struct r3dgpu_cancel_token r3dgpu_cancel_token;
+r3dgpu_status r3dgpu_cancel_token_create(r3dgpu_cancel_token** out);
+void r3dgpu_cancel_token_destroy(r3dgpu_cancel_token* token);
+void r3dgpu_cancel(r3dgpu_cancel_token* token);
+void r3dgpu_cancel_token_reset(r3dgpu_cancel_token* token);
+int32_t r3dgpu_cancel_requested(const r3dgpu_cancel_token* token);
+/* Attaches a token to this thread's later calls (NULL detaches). */
+void r3dgpu_set_cancel_token(r3dgpu_cancel_token* token);
+
 /* Matches a rectified pair (host images, host outputs; copies inside).
  * Replaces r3d::match_stereo, src/r3d/stereo/stereo_matcher.hpp:82-85
  * (implementation src/r3d/stereo/stereo_matcher.cpp:1023-1095). */

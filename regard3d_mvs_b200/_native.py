@@ -32,6 +32,12 @@ EXPORTS = (
     "r3dgpu_default_options",
     "r3dgpu_automatic_levels",
     "r3dgpu_set_device",
+    "r3dgpu_cancel_token_create",
+    "r3dgpu_cancel_token_destroy",
+    "r3dgpu_cancel",
+    "r3dgpu_cancel_token_reset",
+    "r3dgpu_cancel_requested",
+    "r3dgpu_set_cancel_token",
     "r3dgpu_match_stereo_host",
     "r3dgpu_match_stereo",
     "r3dgpu_match_stereo_batch",
@@ -104,6 +110,14 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     L.r3dgpu_automatic_levels.restype = i32
     L.r3dgpu_set_device.argtypes = [i32]
     L.r3dgpu_set_device.restype = st
+    L.r3dgpu_cancel_token_create.argtypes = [ctypes.POINTER(P)]
+    L.r3dgpu_cancel_token_create.restype = st
+    for name in ("r3dgpu_cancel_token_destroy", "r3dgpu_cancel", "r3dgpu_cancel_token_reset",
+                 "r3dgpu_set_cancel_token"):
+        getattr(L, name).argtypes = [P]
+        getattr(L, name).restype = None
+    L.r3dgpu_cancel_requested.argtypes = [P]
+    L.r3dgpu_cancel_requested.restype = i32
     L.r3dgpu_match_stereo_host.argtypes = [ctypes.POINTER(CViewU16), ctypes.POINTER(CViewU16),
                                            ctypes.POINTER(CViewU8), ctypes.POINTER(CViewU8), i32, i32,
                                            ctypes.POINTER(COptions), ctypes.POINTER(CDisparityMap)]

@@ -48,6 +48,7 @@ int general_width() {
 
 thread_local std::string t_error;
 thread_local int t_device = 0;
+thread_local r3dgpu_cancel_token* t_cancel = nullptr;
 thread_local size_t t_scratch_budget = 0;  // 0: the default SGM scratch budget
 
 // Profiling of the SGM launches (r3dgpu_profile_*).
@@ -158,6 +159,28 @@ void p2_lut(const r3dgpu_stereo_options& o, uint16_t* lut) {
     lut[di] = static_cast<uint16_t>(p2);
   }
 }
+
+}  // namespace
+
+}  // namespace r3dgpu
+
+// A cancellation flag in page-locked host memory and its device view.
+struct r3dgpu_cancel_token {
+  int32_t* host = nullptr;
+  const int* dev = nullptr;
+};
+
+namespace r3dgpu {
+namespace {
+
+// Throws ECANCELLED when this thread's token is set (the reference's
+// CancelToken::check, src/r3d/core/cancel.hpp:36-55).
+void check_cancel() {
+  if (t_cancel != nullptr && *reinterpret_cast<volatile int32_t*>(t_cancel->host) != 0)
+    fail(R3DGPU_ECANCELLED, "stereo: cancelled");
+}
+
+const int* cancel_device_flag() { return t_cancel != nullptr ? t_cancel->dev : nullptr; }
 
 }  // namespace
 
@@ -913,6 +936,7 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
   for (auto& P : runs) build_levels(P, A, s);
 
   for (int round = 0; round <= max_levels; ++round) {
+    check_cancel();
     std::vector<PairRun*> active;
     // Round r runs level max_levels - r of every pair that has it, so that
     // all pairs reach level 0 (the largest) in the last round, where their
@@ -1162,8 +1186,10 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
       }
       if (g.kind == kPath) {
         for (size_t k = 0; k < L.waves.size(); ++k) {
+          check_cancel();
           const SgmPathRangedWave& rw = L.waves[k];
           SgmPathWave w{};
+          w.cancel = cancel_device_flag();
           w.jobs = rw.jobs;
           w.njobs = rw.njobs;
           w.segs = L.segs[k].data();
@@ -1177,7 +1203,9 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
         }
       } else if (g.kind == kPathRanged) {
         for (size_t k = 0; k < L.waves.size(); ++k) {
+          check_cancel();
           SgmPathRangedWave w = L.waves[k];
+          w.cancel = cancel_device_flag();
           w.segs = L.segs[k].data();
           w.nsegs = static_cast<int>(L.segs[k].size());
           w.buffer = scratch;
@@ -1282,10 +1310,25 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
                        : automatic_levels(pairs[i].left.width, pairs[i].left.height, pairs[i].num_disparities);
     (lv == 0 ? flat : hier).push_back(i);
   }
+  // On any error (a cancellation included) the work already enqueued ends
+  // before the call returns.
+  auto drain = [&](cudaStream_t other) {
+    (void)cudaStreamSynchronize(s);
+    if (other != nullptr) (void)cudaStreamSynchronize(other);
+    (void)cudaGetLastError();
+    profile_collect();
+  };
   if (flat.empty() || hier.empty() || !batch_tracks_enabled()) {
-    BatchRun B = enqueue_batch(pairs, count, s, 0);
+    BatchRun B;
+    try {
+      B = enqueue_batch(pairs, count, s, 0);
+    } catch (...) {
+      drain(nullptr);
+      throw;
+    }
     R3D_CUDA(cudaStreamSynchronize(s));
     profile_collect();
+    check_cancel();
     finish_batch(B);
     return;
   }
@@ -1300,12 +1343,19 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
   }
   R3D_CUDA(cudaEventRecord(W1.track_start, s));
   R3D_CUDA(cudaStreamWaitEvent(W1.track, W1.track_start, 0));
-  BatchRun a = enqueue_batch(fp.data(), static_cast<int>(fp.size()), W1.track, 1);
-  R3D_CUDA(cudaEventRecord(W1.track_done, W1.track));
-  BatchRun b = enqueue_batch(hp.data(), static_cast<int>(hp.size()), s, 0);
+  BatchRun a, b;
+  try {
+    a = enqueue_batch(fp.data(), static_cast<int>(fp.size()), W1.track, 1);
+    R3D_CUDA(cudaEventRecord(W1.track_done, W1.track));
+    b = enqueue_batch(hp.data(), static_cast<int>(hp.size()), s, 0);
+  } catch (...) {
+    drain(W1.track);
+    throw;
+  }
   R3D_CUDA(cudaStreamWaitEvent(s, W1.track_done, 0));
   R3D_CUDA(cudaStreamSynchronize(s));
   profile_collect();
+  check_cancel();
   finish_batch(a);
   finish_batch(b);
   for (size_t k = 0; k < flat.size(); ++k) pairs[flat[k]].out = fp[k].out;
@@ -1385,6 +1435,52 @@ r3dgpu_status r3dgpu_set_device(int32_t device) {
     (void)workspace();
   });
 }
+
+r3dgpu_status r3dgpu_cancel_token_create(r3dgpu_cancel_token** out) {
+  return guarded([&] {
+    if (out == nullptr) fail(R3DGPU_EINVAL, "cancel_token_create: null argument");
+    (void)workspace();  // the thread's device, current
+    auto* t = new r3dgpu_cancel_token();
+    void* h = nullptr;
+    void* d = nullptr;
+    const cudaError_t e = cudaHostAlloc(&h, sizeof(int32_t), cudaHostAllocMapped);
+    if (e != cudaSuccess) {
+      delete t;
+      cuda_check(e, "cancel_token_create: cudaHostAlloc");
+    }
+    *static_cast<int32_t*>(h) = 0;
+    const cudaError_t e2 = cudaHostGetDevicePointer(&d, h, 0);
+    if (e2 != cudaSuccess) {
+      cudaFreeHost(h);
+      delete t;
+      cuda_check(e2, "cancel_token_create: cudaHostGetDevicePointer");
+    }
+    t->host = static_cast<int32_t*>(h);
+    t->dev = static_cast<const int*>(d);
+    *out = t;
+  });
+}
+
+void r3dgpu_cancel_token_destroy(r3dgpu_cancel_token* token) {
+  if (token == nullptr) return;
+  if (t_cancel == token) t_cancel = nullptr;
+  cudaFreeHost(token->host);
+  delete token;
+}
+
+void r3dgpu_cancel(r3dgpu_cancel_token* token) {
+  if (token != nullptr) __atomic_store_n(token->host, 1, __ATOMIC_SEQ_CST);
+}
+
+void r3dgpu_cancel_token_reset(r3dgpu_cancel_token* token) {
+  if (token != nullptr) __atomic_store_n(token->host, 0, __ATOMIC_SEQ_CST);
+}
+
+int32_t r3dgpu_cancel_requested(const r3dgpu_cancel_token* token) {
+  return token != nullptr ? __atomic_load_n(token->host, __ATOMIC_SEQ_CST) : 0;
+}
+
+void r3dgpu_set_cancel_token(r3dgpu_cancel_token* token) { t_cancel = token; }
 
 r3dgpu_status r3dgpu_release_workspace(void) {
   return guarded([&] {

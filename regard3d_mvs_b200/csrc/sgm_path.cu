@@ -56,6 +56,14 @@ R3D_DEVICE int find_job(const SgmPathJob* jobs, int njobs, int64_t v, Key key) {
   return lo;
 }
 
+// Whether the caller's cancellation flag is set (read once per chain block,
+// by lane 0 for the whole warp; never a wait).
+R3D_DEVICE bool cancelled(const int* cancel) {
+  int c = 0;
+  if (cancel != nullptr) c = *reinterpret_cast<const volatile int*>(cancel);
+  return r3dsimt::shfl(static_cast<uint32_t>(c), 0) != 0;
+}
+
 // Start pixel and length of chain c of a direction (dx, dy) in a w x h tile;
 // length 0 for c past the class's last chain.
 R3D_DEVICE void chain_geometry(int cls, int dx, int dy, int w, int h, int64_t c, int& sx, int& sy, int& len) {
@@ -163,7 +171,7 @@ R3D_DEVICE uint32_t add2(uint32_t a, uint32_t b, bool no_carry) { return no_carr
 // with the costs (ND bytes) and sums (2 ND bytes) of one pixel per chain.
 constexpr int kPathStages = 4;
 template <int G, int K>
-struct PathRing {
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   static constexpr int ND = 2 * G * K;
   static constexpr int kStageBytes = (32 / G) * 3 * ND;
   static constexpr int kWarpBytes = kPathStages * kStageBytes;
@@ -171,10 +179,10 @@ struct PathRing {
 };
 
 template <int G, int K, int MODE>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, 3)
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
                     int dx, int dy, int64_t total_blocks, const uint8_t* R3D_RESTRICT cost, uint16_t* sum,
-                    int4* R3D_RESTRICT info, uint32_t* rkeys) {
+                    int4* R3D_RESTRICT info, uint32_t* rkeys, const int* cancel) {
   constexpr int CPW = 32 / G;  // chains per warp
   constexpr int U = K / 4;     // units of 8 labels per lane
   R3D_DYNAMIC_SMEM(smem);
@@ -185,6 +193,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
   const int wpb = static_cast<int>(blockDim.x) >> 5;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
   for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + (threadIdx.x >> 5); blk < total_blocks; blk += nwarps) {
+    if (cancelled(cancel)) break;
     const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
@@ -606,7 +615,8 @@ template <int G, int K, int MODE>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     sgm_path_ranged_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
                            int cls, int dx, int dy, int64_t total_blocks, const int4* R3D_RESTRICT rec,
-                           const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words) {
+                           const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words,
+                           const int* cancel) {
   using R = RangedRing<G, K>;
   constexpr int CPW = R::CPW, U = K / 4, CH = R::CH, D = kPathStages;
   R3D_DYNAMIC_SMEM(smem);
@@ -638,6 +648,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     else ovfc[b * ovf_words + (idx - kRangedSmemWords)] = v;
   };
   for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + warp; blk < total_blocks; blk += nwarps) {
+    if (cancelled(cancel)) break;
     const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
@@ -936,7 +947,7 @@ uint64_t pass_bytes(int mode, bool ranged, const SgmPathSegment& g) {
 template <int G, int K, int MODE>
 void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
                  const uint8_t* cost, uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s,
-                 const SgmPathSegment& seg) {
+                 const SgmPathSegment& seg, const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_kernel<G, K, MODE>;
   constexpr size_t smem = PathRing<G, K>::kBlockBytes;
@@ -948,7 +959,7 @@ void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int
     configured[dev] = 1;
   }
   R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32, smem)), dim3(kPathThreads), smem, s, dm, jobs,
-             njobs, ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys);
+             njobs, ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys, cancel);
   launched("sgm_path_kernel");
   if (ev0 != nullptr) {
     char shape[32];
@@ -960,17 +971,17 @@ void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int
 
 template <int G, int K>
 void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const uint8_t* cost,
-                   uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s) {
+                   uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s, const int* cancel) {
   for (int q = 0; q < 8; ++q) {
     const Pass ps = kPasses[q];
     const int64_t nb = g.blocks[ps.cls];
     if (nb <= 0) continue;
     if (q == 0)
-      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g);
+      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g, cancel);
     else if (q < 7)
-      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g);
+      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g, cancel);
     else
-      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g);
+      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g, cancel);
   }
 }
 
@@ -1052,7 +1063,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
     bool done = false;
 #define R3D_SHAPE(gg, kk)                                                                                     \
   if (!done && g.shape.g_ == gg && g.shape.k_ == kk) {                                                        \
-    launch_passes<gg, kk>(dm, jobs, g, cost, sum, info, rkeys, sms, s);                                      \
+    launch_passes<gg, kk>(dm, jobs, g, cost, sum, info, rkeys, sms, s, wave.cancel);                         \
     done = true;                                                                                              \
   }
     R3D_PATH_SHAPES(R3D_SHAPE)
@@ -1074,7 +1085,7 @@ constexpr int kRangedMaxPerSm = 4;
 template <int G, int K, int MODE>
 void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
                         const int4* rec, const uint8_t* cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words,
-                        int sms, cudaStream_t s, const SgmPathSegment& seg) {
+                        int sms, cudaStream_t s, const SgmPathSegment& seg, const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_ranged_kernel<G, K, MODE>;
   constexpr size_t smem = RangedRing<G, K>::kBlockBytes;
@@ -1088,7 +1099,7 @@ void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jo
   int grid = resident_grid(k, sms, nb, kPathThreads / 32, smem);
   grid = grid < sms * kRangedMaxPerSm ? grid : sms * kRangedMaxPerSm;
   R3D_LAUNCH(k, dim3(grid), dim3(kPathThreads), smem, s, dm, jobs, njobs, ps.cls, ps.dx, ps.dy, nb, rec, cost, sum,
-             ovf, ovf_words);
+             ovf, ovf_words, cancel);
   launched("sgm_path_ranged_kernel");
   if (ev0 != nullptr) {
     char shape[32];
@@ -1102,15 +1113,16 @@ void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jo
 template <int G, int K>
 void launch_ranged_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const int4* rec,
                           const uint8_t* cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words, int sms,
-                          cudaStream_t s) {
+                          cudaStream_t s, const int* cancel) {
   for (int q = 0; q < 8; ++q) {
     const Pass ps = kPasses[q];
     const int64_t nb = g.blocks[ps.cls];
     if (nb <= 0) continue;
     if (q == 0)
-      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g);
+      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g, cancel);
     else
-      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g);
+      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g,
+                                            cancel);
   }
 }
 
@@ -1176,9 +1188,9 @@ void launch_sgm_path_ranged_wave(const SgmMatch* dm, const SgmPathRangedWave& wa
     const SgmPathSegment& g = wave.segs[q];
     const SgmPathJob* jobs = wave.jobs + g.first;
     if (g.shape.g_ == 2 && g.shape.k_ == 8)
-      launch_ranged_passes<2, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s);
+      launch_ranged_passes<2, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s, wave.cancel);
     else if (g.shape.g_ == 4 && g.shape.k_ == 8)
-      launch_ranged_passes<4, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s);
+      launch_ranged_passes<4, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s, wave.cancel);
     else
       fail(R3DGPU_EINVAL, "stereo: bad ranged path kernel shape");
   }

@@ -79,6 +79,7 @@ struct SgmPathWave {
   int nsegs;
   int64_t cells, pixels, keys, rows;
   unsigned char* buffer;  // sgm_path_buffers(cells, pixels, keys).total bytes
+  const int* cancel;      // device view of the caller's cancellation flag, or null
 };
 
 // Costs, the 8 passes and the acceptance rules of one wave, on stream s.
@@ -102,6 +103,7 @@ struct SgmPathRangedWave {
   int64_t cells, pixels, keys, rows;
   int maxnum;  // largest label count of a pixel of the wave
   unsigned char* buffer;
+  const int* cancel;  // device view of the caller's cancellation flag, or null
 };
 SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
                                        int sms);

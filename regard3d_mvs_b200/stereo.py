@@ -524,6 +524,40 @@ class Matcher:
     def launch_count(self) -> int:
         return int(self.lib.r3dgpu_launch_count())
 
+    def cancel_token(self) -> "CancelToken":
+        """A new cancellation token (r3dgpu_cancel_token_create)."""
+        return CancelToken(self.lib)
+
+    def set_cancel_token(self, token: "CancelToken | None") -> None:
+        """Attaches `token` to this thread's later calls (None detaches);
+        a cancelled call raises StereoError with R3DGPU_ECANCELLED."""
+        self.lib.r3dgpu_set_cancel_token(token.handle if token is not None else None)
+
+
+class CancelToken:
+    """The r3dgpu_cancel_token of include/r3dgpu.h (r3d::CancelToken's
+    counterpart): cancel() from any thread, reset() before reuse."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        h = ctypes.c_void_p()
+        _native.check(lib, lib.r3dgpu_cancel_token_create(ctypes.byref(h)))
+        self.handle = h
+
+    def cancel(self) -> None:
+        self.lib.r3dgpu_cancel(self.handle)
+
+    def reset(self) -> None:
+        self.lib.r3dgpu_cancel_token_reset(self.handle)
+
+    def requested(self) -> bool:
+        return bool(self.lib.r3dgpu_cancel_requested(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            self.lib.r3dgpu_cancel_token_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
 
 _default: Matcher | None = None
 

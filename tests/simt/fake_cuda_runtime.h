@@ -38,6 +38,8 @@ cudaError_t cudaPeekAtLastError();
 cudaError_t cudaMalloc(void** p, size_t n);
 cudaError_t cudaFree(void* p);
 cudaError_t cudaMallocHost(void** p, size_t n);
+cudaError_t cudaHostAlloc(void** p, size_t n, unsigned flags);
+cudaError_t cudaHostGetDevicePointer(void** d, void* h, unsigned flags);
 cudaError_t cudaFreeHost(void* p);
 cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind k);
 cudaError_t cudaMemcpyAsync(void* d, const void* s, size_t n, cudaMemcpyKind k, cudaStream_t st = nullptr);
@@ -80,3 +82,4 @@ cudaError_t cudaOccupancyMaxActiveBlocksPerMultiprocessor(int* n, F, int, size_t
 
 #define cudaStreamNonBlocking 1u
 #define cudaEventDisableTiming 2u
+#define cudaHostAllocMapped 2u

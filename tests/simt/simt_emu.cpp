@@ -320,6 +320,11 @@ cudaError_t cudaFree(void* p) {
   return ok();
 }
 cudaError_t cudaMallocHost(void** p, size_t n) { return cudaMalloc(p, n); }
+cudaError_t cudaHostAlloc(void** p, size_t n, unsigned) { return cudaMalloc(p, n); }
+cudaError_t cudaHostGetDevicePointer(void** d, void* h, unsigned) {
+  *d = h;
+  return ok();
+}
 cudaError_t cudaFreeHost(void* p) { return cudaFree(p); }
 cudaError_t cudaMemcpy(void* d, const void* s, size_t n, cudaMemcpyKind) {
   if (n) std::memmove(d, s, n);
