@@ -171,15 +171,17 @@ R3D_DEVICE uint32_t add2(uint32_t a, uint32_t b, bool no_carry) { return no_carr
 // with the costs (ND bytes) and sums (2 ND bytes) of one pixel per chain.
 constexpr int kPathStages = 4;
 template <int G, int K>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
+struct PathRing {
   static constexpr int ND = 2 * G * K;
   static constexpr int kStageBytes = (32 / G) * 3 * ND;
   static constexpr int kWarpBytes = kPathStages * kStageBytes;
   static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
 };
 
+// Three CTAs per SM for the 8-word shapes (80 registers, no spills); the
+// 12-word shapes keep two.
 template <int G, int K, int MODE>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, 3)
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
                     int dx, int dy, int64_t total_blocks, const uint8_t* R3D_RESTRICT cost, uint16_t* sum,
                     int4* R3D_RESTRICT info, uint32_t* rkeys, const int* cancel) {
