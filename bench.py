@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "pair2048", "combine", "rectify", "depth",
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "pair1024", "pair2048", "combine", "rectify", "depth",
                                            "view"),
                     default="batch64",
                     help="combine / rectify / depth: only the multi-view combination of one view / the "
@@ -86,6 +86,10 @@ def workload_pairs(name: str, npairs: int, seed: int):
     out = []
     if name == "pair640":
         return [dict(w=640, h=480, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
+    if name == "pair1024":
+        # One full-range pair, 1024x768, 128 labels (ncu captures of the pass kernels: 0.2 G cells per pass,
+        # a working set of several times the L2 and under 2 GB of device memory).
+        return [dict(w=1024, h=768, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
     if name == "pair2048":
         # One full-range pair of a config-4 view's size (profiling case of the pass kernels).
         return [dict(w=2048, h=1536, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
@@ -180,21 +184,26 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+PASS_MODES = {0: "first pass (u16 sums)", 1: "accumulate pass (u16 sums)", 2: "last pass (u16 sums, WTA)",
+              3: "term pass (byte terms)", 4: "last pass (byte terms, WTA)"}
+
+
 def pass_traffic_per_cell():
-    """DRAM bytes per cell of one accumulate pass of the chain kernels, from
-    the committed ncu summary (profiles/sgm_path_traffic.json), if any."""
+    """DRAM bytes per cell of the chain-pass modes (mode number -> bytes),
+    from the committed ncu summaries (profiles/sgm_path_traffic.json)."""
     path = os.path.join(ROOT, "profiles", "sgm_path_traffic.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            d = json.load(f)
-        return float(d["accumulate_pass_dram_bytes_per_cell"])
-    return None
+    if not os.path.exists(path):
+        return {}
+    with open(path) as f:
+        d = json.load(f)
+    return {int(k): float(v) for k, v in d.get("dram_bytes_per_cell_by_mode", {}).items()}
 
 
 def pass_roofline(launch_log, peak, peak_kind):
     """Roofline of the dominant kernel, the chain pass (sgm_path_kernel):
-    algorithmic bytes of its launches (costs read, sums read and written) over
-    their CUDA-event durations on the launching stream."""
+    algorithmic bytes of its launches (costs read, sums or byte terms read and
+    written, WTA records) over their CUDA-event durations on the launching
+    stream; per pass mode as well."""
     passes = [e for e in launch_log if e.get("pass") and e["kernel"] == "sgm_path_kernel"]
     rpasses = [e for e in launch_log if e.get("pass") and e["kernel"] == "sgm_path_ranged_kernel"]
     if not passes:
@@ -204,13 +213,29 @@ def pass_roofline(launch_log, peak, peak_kind):
     cells = sum(e["cells"] for e in passes)
     achieved = nbytes / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
     tpc = pass_traffic_per_cell()
-    acc = [e for e in passes if e["shape"].endswith("mode1")]
+    by_mode = {}
+    for e in passes:
+        mode = int(e["shape"].rsplit("mode", 1)[1])
+        b = by_mode.setdefault(mode, {"what": PASS_MODES.get(mode, "?"), "launches": 0, "ms": 0.0, "bytes": 0,
+                                      "cells": 0})
+        b["launches"] += 1
+        b["ms"] += e["ms"]
+        b["bytes"] += e["bytes"]
+        b["cells"] += e["cells"]
+    for b in by_mode.values():
+        b["gbs"] = b["bytes"] / (b["ms"] * 1e-3) / 1e9 if b["ms"] > 0 else 0.0
+        b["frac"] = b["gbs"] / peak
+    traffic = None
+    if tpc and all(m in tpc for m in by_mode):
+        traffic = sum(tpc[m] * b["cells"] for m, b in by_mode.items()) / len(passes)
     out = {"bound": "hbm", "kernel": "sgm_path_kernel (one chain pass of full-range tiles)", "achieved": achieved,
            "peak": peak, "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": achieved / peak,
-           "traffic": (tpc * sum(e["cells"] for e in acc) / len(acc)) if (tpc and acc) else None,
+           "traffic": traffic, "traffic_source": "profiles/sgm_path_traffic.json (ncu DRAM bytes per cell by mode)",
            "launches": len(passes), "avg_launch_ms": ms / len(passes), "alg_bytes_per_launch": nbytes / len(passes),
-           "alg_bytes_per_cell": {"first pass": 3, "accumulate pass": 5, "last pass": "3 + 16 per pixel"},
-           "cells_per_launch": cells / len(passes)}
+           "alg_bytes_per_cell": {"first pass": 3, "accumulate pass": 5, "last pass": "3 + 16 per pixel",
+                                  "term pass": 2, "last pass (byte terms)": "8 + 16 per pixel"},
+           "cells_per_launch": cells / len(passes),
+           "by_mode": {str(k): v for k, v in sorted(by_mode.items())}}
     if rpasses:
         rms = sum(e["ms"] for e in rpasses)
         rb = sum(e["bytes"] for e in rpasses)

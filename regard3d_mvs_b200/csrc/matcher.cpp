@@ -568,6 +568,9 @@ void fill_match(SgmMatch& m, const r3dgpu_stereo_options& o, const DView<uint16_
   int max_p2 = 0;
   for (int i = 0; i < 256; ++i) max_p2 = std::max(max_p2, static_cast<int>(m.lut[i]));
   m.sum_no_carry = 8 * (max_p2 + std::max(o.invalid_cost, 62)) <= 65535 ? 1 : 0;
+  // L_r(p, d) - C(p, d) = min(L(q, d), L(q, d -+ 1) + P1, min L(q) + P2) - min L(q)
+  // lies in [0, P2]: with P2 <= 255 the chain passes keep it in one byte.
+  m.term_u8 = max_p2 <= 255 ? 1 : 0;
 }
 
 // Stage 1 of a level: mirrored inputs, Census images, row intervals, label
@@ -804,9 +807,13 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     int64_t cells, px, keys, rows;
     int maxnum;
   };
+  // Full-range waves keep byte terms when every match of the group allows
+  // them (all P2 <= 255); otherwise the u16 sum volume.
+  bool terms = !ranged;
+  for (const auto& mt : tiles) terms = terms && matches[mt.first]->m.term_u8 != 0;
   auto bytes = [&](int64_t cells, int64_t px, int64_t keys, int64_t rows, int maxnum) -> size_t {
     return ranged ? sgm_path_ranged_buffers(cells, px, keys, rows, maxnum, sms).total
-                  : sgm_path_buffers(cells, px, keys).total;
+                  : sgm_path_buffers(cells, px, keys, terms).total;
   };
   std::vector<Entry> es;
   es.reserve(tiles.size());
@@ -892,6 +899,7 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     wv.keys = ko;
     wv.rows = ro;
     wv.maxnum = maxnum;
+    wv.terms = terms ? 1 : 0;
     waves.push_back(wv);
     segs.push_back(std::move(sg));
     max_bytes = std::max(max_bytes, bytes(co, po, ko, ro, maxnum));
@@ -1199,6 +1207,7 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
           w.keys = rw.keys;
           w.rows = rw.rows;
           w.buffer = scratch;
+          w.terms = rw.terms;
           launch_sgm_path_wave(dm, w, W.sms, gs);
         }
       } else if (g.kind == kPathRanged) {
@@ -1731,7 +1740,8 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
       wv.pixels = px;
       wv.keys = 0;
       wv.rows = h;
-      W.scratch.reserve(sgm_path_buffers(wv.cells, px, 0).total);
+      wv.terms = hm->term_u8;
+      W.scratch.reserve(sgm_path_buffers(wv.cells, px, 0, wv.terms != 0).total);
       wv.buffer = W.scratch.get();
       launch_sgm_path_wave(dm, wv, W.sms, s);
       R3D_CUDA(cudaMemcpyAsync(out, vol, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s));

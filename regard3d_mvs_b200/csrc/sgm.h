@@ -36,6 +36,7 @@ struct SgmMatch {
   float uniqueness;
   int lr_max_diff, diagonal_lr, confidence;
   int sum_no_carry;   // 1 if 8 paths can never exceed 65535 (plain 32-bit adds of packed sums are exact)
+  int term_u8;        // 1 if every P2 of the LUT is <= 255: a path's term L - C fits one byte
   uint16_t lut[256];  // P2 by 8-bit intensity step
 };
 

@@ -162,19 +162,33 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 }
 
 // ---------------------------------------------------------------- passes
-enum PassMode { kFirst = 0, kAccumulate = 1, kLast = 2 };
+// Pass modes. With u16 sums (any penalties): the first pass writes the sum
+// volume, the next six add to it, the last adds its path and takes the
+// winner-takes-all. With byte terms (every P2 <= 255): passes 1..7 write
+// their path's term T_r = L_r - C (in [0, P2]) as one byte per cell, and the
+// last pass forms S = L_8 + 7 C + sum T_r (at most 8 (255 + 255) < 2^16, so
+// the sum modulo 2^16 is the plain sum) and takes the winner-takes-all.
+enum PassMode { kFirst = 0, kAccumulate = 1, kLast = 2, kTerm = 3, kLastTerm = 4 };
+constexpr int kTermArrays = 7;
+constexpr int kPathStages = 4;  // ring stages of the ranged passes
 
 // Per-halfword a + b modulo 2^16.
 R3D_DEVICE uint32_t add2(uint32_t a, uint32_t b, bool no_carry) { return no_carry ? a + b : r3dsimt::vadd2(a, b); }
 
-// Per-warp shared-memory ring of the pass kernels: kPathStages stages, each
-// with the costs (ND bytes) and sums (2 ND bytes) of one pixel per chain.
-constexpr int kPathStages = 4;
-template <int G, int K>
+// Per-warp shared-memory ring of the pass kernels: Stages stages, each with
+// one pixel per chain of the bytes the pass reads (Planes bytes per label:
+// the cost, plus the u16 sum or the seven byte terms).
+template <int MODE>
+struct PathMode {
+  static constexpr int kPlanes = MODE == kAccumulate || MODE == kLast ? 3 : (MODE == kLastTerm ? 1 + kTermArrays : 1);
+  static constexpr int kStages = MODE == kLastTerm ? 3 : 4;
+};
+template <int G, int K, int MODE>
 struct PathRing {
   static constexpr int ND = 2 * G * K;
-  static constexpr int kStageBytes = (32 / G) * 3 * ND;
-  static constexpr int kWarpBytes = kPathStages * kStageBytes;
+  static constexpr int kStages = PathMode<MODE>::kStages;
+  static constexpr int kStageBytes = (32 / G) * PathMode<MODE>::kPlanes * ND;
+  static constexpr int kWarpBytes = kStages * kStageBytes;
   static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
 };
 
@@ -184,9 +198,14 @@ template <int G, int K, int MODE>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
                     int dx, int dy, int64_t total_blocks, const uint8_t* R3D_RESTRICT cost, uint16_t* sum,
-                    int4* R3D_RESTRICT info, uint32_t* rkeys, const int* cancel) {
+                    uint8_t* terms, int64_t tstride, int tslot, int4* R3D_RESTRICT info, uint32_t* rkeys,
+                    const int* cancel) {
   constexpr int CPW = 32 / G;  // chains per warp
   constexpr int U = K / 4;     // units of 8 labels per lane
+  constexpr int NS = PathRing<G, K, MODE>::kStages;
+  constexpr bool kTerms = MODE == kTerm || MODE == kLastTerm;
+  constexpr bool kReadsSum = MODE == kAccumulate || MODE == kLast;
+  constexpr bool kWta = MODE == kLast || MODE == kLastTerm;
   R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u);
   const int gi = lane / G, t = lane % G;
@@ -212,28 +231,37 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     for (int u = 0; u < U; ++u) uvalid[u] = e0 + 8 * u < nd;
     const uint8_t* cbase = cost + job.cell_off + e0;
     uint16_t* sbase = sum + job.cell_off + e0;
+    uint8_t* tbase = terms + job.cell_off + e0;
     const uint16_t* img = m.base + static_cast<int64_t>(job.y0) * m.base_stride + job.x0;
 
-    // Costs and sums of the next kPathStages - 1 pixels stream into the
-    // warp's shared-memory ring with cp.async (each lane copies and later
-    // reads only its own labels); intensities wait in a register queue.
-    unsigned char* ring = smem + static_cast<size_t>(threadIdx.x >> 5) * PathRing<G, K>::kWarpBytes;
-    auto stage_cost = [&](int st) -> unsigned char* {
-      return ring + st * PathRing<G, K>::kStageBytes + gi * PathRing<G, K>::ND + e0;
-    };
+    // The bytes of the next NS - 1 pixels stream into the warp's
+    // shared-memory ring with cp.async (each lane copies and later reads only
+    // its own labels); intensities wait in a register queue.
+    using Ring = PathRing<G, K, MODE>;
+    unsigned char* ring = smem + static_cast<size_t>(threadIdx.x >> 5) * Ring::kWarpBytes;
+    auto stage_cost = [&](int st) -> unsigned char* { return ring + st * Ring::kStageBytes + gi * Ring::ND + e0; };
     auto stage_sum = [&](int st) -> unsigned char* {
-      return ring + st * PathRing<G, K>::kStageBytes + CPW * PathRing<G, K>::ND + gi * 2 * PathRing<G, K>::ND + 2 * e0;
+      return ring + st * Ring::kStageBytes + CPW * Ring::ND + gi * 2 * Ring::ND + 2 * e0;
     };
+    auto stage_term = [&](int st, int r) -> unsigned char* {
+      return ring + st * Ring::kStageBytes + (1 + r) * CPW * Ring::ND + gi * Ring::ND + e0;
+    };
+    auto slot = [](int i) { return NS == 4 ? (i & 3) : i % NS; };
     auto issue = [&](int i) {
       if (i < len) {
         const int x = sx + i * dx, y = sy + i * dy;
         const int64_t cell = static_cast<int64_t>(y * w + x) * nd;
-        const int st = i & (kPathStages - 1);
+        const int st = slot(i);
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (uvalid[u]) {
             r3dsimt::cp_async8(stage_cost(st) + 8 * u, cbase + cell + 8 * u);
-            if constexpr (MODE != kFirst) r3dsimt::cp_async16(stage_sum(st) + 16 * u, sbase + cell + 8 * u);
+            if constexpr (kReadsSum) r3dsimt::cp_async16(stage_sum(st) + 16 * u, sbase + cell + 8 * u);
+            if constexpr (MODE == kLastTerm) {
+#pragma unroll
+              for (int r = 0; r < kTermArrays; ++r)
+                r3dsimt::cp_async8(stage_term(st, r) + 8 * u, tbase + r * tstride + cell + 8 * u);
+            }
           }
         }
       }
@@ -243,9 +271,9 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       if (i >= len) return 0;
       return img[static_cast<int64_t>(sy + i * dy) * m.base_stride + sx + i * dx];
     };
-    int iq[kPathStages];
+    int iq[NS];
 #pragma unroll
-    for (int k = 0; k < kPathStages - 1; ++k) {
+    for (int k = 0; k < NS - 1; ++k) {
       issue(k);
       iq[k] = intensity(k);
     }
@@ -256,22 +284,20 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     int iprev = 0;
     for (int i = 0; i < maxlen; ++i) {
       const bool on = i < len;
-      issue(i + kPathStages - 1);
-      iq[kPathStages - 1] = intensity(i + kPathStages - 1);
-      r3dsimt::cp_async_wait<kPathStages - 1>();
+      issue(i + NS - 1);
+      iq[NS - 1] = intensity(i + NS - 1);
+      r3dsimt::cp_async_wait<NS - 1>();
       const int icur = iq[0];
+      const int st = slot(i);
       uint2 craw[U];
       uint4 sraw[U];
-      {
-        const int st = i & (kPathStages - 1);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-          craw[u] = uvalid[u] ? *reinterpret_cast<const uint2*>(stage_cost(st) + 8 * u) : make_uint2(0, 0);
-          if constexpr (MODE != kFirst)
-            sraw[u] = uvalid[u] ? *reinterpret_cast<const uint4*>(stage_sum(st) + 16 * u) : make_uint4(0, 0, 0, 0);
-          else
-            sraw[u] = make_uint4(0, 0, 0, 0);
-        }
+      for (int u = 0; u < U; ++u) {
+        craw[u] = uvalid[u] ? *reinterpret_cast<const uint2*>(stage_cost(st) + 8 * u) : make_uint2(0, 0);
+        if constexpr (kReadsSum)
+          sraw[u] = uvalid[u] ? *reinterpret_cast<const uint4*>(stage_sum(st) + 16 * u) : make_uint4(0, 0, 0, 0);
+        else
+          sraw[u] = make_uint4(0, 0, 0, 0);
       }
       uint32_t c2[K];
 #pragma unroll
@@ -281,11 +307,15 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         c2[4 * u + 2] = r3dsimt::perm(craw[u].y, 0u, 0x4140u);
         c2[4 * u + 3] = r3dsimt::perm(craw[u].y, 0u, 0x4342u);
       }
-      uint32_t out[K];
+      // out = L_r = C + T_r, with T_r = best - min L(q) (0 at the chain's first pixel).
+      uint32_t out[K], tr[K];
       if (i == 0) {
         // First pixel of the chain: no predecessor inside the tile, L = C.
 #pragma unroll
-        for (int k = 0; k < K; ++k) out[k] = c2[k];
+        for (int k = 0; k < K; ++k) {
+          tr[k] = 0;
+          out[k] = c2[k];
+        }
       } else {
         const int dI = icur - iprev;
         const uint32_t pen = pmin + m.lut[(dI < 0 ? -dI : dI) >> 8];
@@ -304,7 +334,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
           const uint32_t mnext = r3dsimt::perm(wv[k + 1], wv[k + 2], 0x5432u);
           const uint32_t nb = r3dsimt::vmin2(mprev, mnext);
           const uint32_t best = r3dsimt::vmin2(wv[k + 1], r3dsimt::vaddmin2(nb, p1x2, pen2));
-          out[k] = best + c2[k] + negmp;
+          tr[k] = best + negmp;
+          out[k] = tr[k] + c2[k];
           mprev = mnext;
         }
       }
@@ -317,6 +348,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       pmin = group_umin<G>(r3dsimt::umin(mk & 0xFFFFu, mk >> 16));
       const int x = sx + i * dx, y = sy + i * dy;
       const int64_t cell = static_cast<int64_t>(y * w + x) * nd;
+      uint32_t s[K];
       if constexpr (MODE == kFirst) {
         if (on) {
 #pragma unroll
@@ -325,8 +357,32 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
               r3dsimt::st_stream(reinterpret_cast<uint4*>(sbase + cell + 8 * u),
                                  make_uint4(out[4 * u], out[4 * u + 1], out[4 * u + 2], out[4 * u + 3]));
         }
+      } else if constexpr (MODE == kTerm) {
+        if (on) {
+          uint8_t* tout = tbase + tslot * tstride + cell;
+#pragma unroll
+          for (int u = 0; u < U; ++u)
+            if (uvalid[u])
+              r3dsimt::st_stream8(reinterpret_cast<uint2*>(tout + 8 * u),
+                                  make_uint2(r3dsimt::perm(tr[4 * u], tr[4 * u + 1], 0x6420u),
+                                             r3dsimt::perm(tr[4 * u + 2], tr[4 * u + 3], 0x6420u)));
+        }
+      } else if constexpr (MODE == kLastTerm) {
+        // S = L_8 + 7 C + sum of the seven byte terms (no halfword overflows).
+#pragma unroll
+        for (int k = 0; k < K; ++k) s[k] = out[k] + 7u * c2[k];
+#pragma unroll
+        for (int r = 0; r < kTermArrays; ++r) {
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const uint2 tw = uvalid[u] ? *reinterpret_cast<const uint2*>(stage_term(st, r) + 8 * u) : make_uint2(0, 0);
+            s[4 * u + 0] += r3dsimt::perm(tw.x, 0u, 0x4140u);
+            s[4 * u + 1] += r3dsimt::perm(tw.x, 0u, 0x4342u);
+            s[4 * u + 2] += r3dsimt::perm(tw.y, 0u, 0x4140u);
+            s[4 * u + 3] += r3dsimt::perm(tw.y, 0u, 0x4342u);
+          }
+        }
       } else {
-        uint32_t s[K];
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           s[4 * u + 0] = add2(sraw[u].x, out[4 * u + 0], no_carry);
@@ -342,81 +398,84 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
                 r3dsimt::st_stream(reinterpret_cast<uint4*>(sbase + cell + 8 * u),
                                    make_uint4(s[4 * u], s[4 * u + 1], s[4 * u + 2], s[4 * u + 3]));
           }
-        } else {
-          // Winner-takes-all over the total sums (sgm_kernels.cpp:332-358):
-          // the first minimum, the second best outside +-1, and S at kb -+ 1.
-          uint32_t kmin = 0xFFFFFFFFu;
+        }
+      }
+      if constexpr (kWta) {
+        // Winner-takes-all over the total sums (sgm_kernels.cpp:332-358):
+        // the first minimum, the second best outside +-1, and S at kb -+ 1.
+        uint32_t kmin = 0xFFFFFFFFu;
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            if (uvalid[k / 4]) {
-              const uint32_t e = static_cast<uint32_t>(e0 + 2 * k);
-              kmin = r3dsimt::umin(kmin, r3dsimt::umin(((s[k] & 0xFFFFu) << 16) | e, (s[k] & 0xFFFF0000u) | (e + 1)));
-            }
+        for (int k = 0; k < K; ++k) {
+          if (uvalid[k / 4]) {
+            const uint32_t e = static_cast<uint32_t>(e0 + 2 * k);
+            kmin = r3dsimt::umin(kmin, r3dsimt::umin(((s[k] & 0xFFFFu) << 16) | e, (s[k] & 0xFFFF0000u) | (e + 1)));
           }
-          kmin = group_umin<G>(kmin);
-          const int kb = static_cast<int>(kmin & 0xFFFFu);
-          const uint32_t bcost = kmin >> 16;
-          uint32_t sec = 0xFFFFu;
+        }
+        kmin = group_umin<G>(kmin);
+        const int kb = static_cast<int>(kmin & 0xFFFFu);
+        const uint32_t bcost = kmin >> 16;
+        uint32_t sec = 0xFFFFu;
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            if (uvalid[k / 4]) {
-              const int e = e0 + 2 * k;
-              if (e + 1 < kb || e > kb + 1) sec = r3dsimt::umin(sec, s[k] & 0xFFFFu);
-              if (e + 2 < kb || e + 1 > kb + 1) sec = r3dsimt::umin(sec, s[k] >> 16);
-            }
+        for (int k = 0; k < K; ++k) {
+          if (uvalid[k / 4]) {
+            const int e = e0 + 2 * k;
+            if (e + 1 < kb || e > kb + 1) sec = r3dsimt::umin(sec, s[k] & 0xFFFFu);
+            if (e + 2 < kb || e + 1 > kb + 1) sec = r3dsimt::umin(sec, s[k] >> 16);
           }
-          sec = group_umin<G>(sec);
-          const int km = kb > 0 ? kb - 1 : 0, kp = kb + 1 < nd ? kb + 1 : nd - 1;
-          const int jm = (km % (2 * K)) >> 1, jp = (kp % (2 * K)) >> 1;
-          uint32_t vm = 0, vp = 0;
+        }
+        sec = group_umin<G>(sec);
+        const int km = kb > 0 ? kb - 1 : 0, kp = kb + 1 < nd ? kb + 1 : nd - 1;
+        const int jm = (km % (2 * K)) >> 1, jp = (kp % (2 * K)) >> 1;
+        uint32_t vm = 0, vp = 0;
 #pragma unroll
-          for (int k = 0; k < K; ++k) {
-            if (k == jm) vm = s[k];
-            if (k == jp) vp = s[k];
+        for (int k = 0; k < K; ++k) {
+          if (k == jm) vm = s[k];
+          if (k == jp) vp = s[k];
+        }
+        const int base_lane = gi * G;
+        vm = r3dsimt::shfl(vm, (base_lane + km / (2 * K)) & 31);
+        vp = r3dsimt::shfl(vp, (base_lane + kp / (2 * K)) & 31);
+        const uint32_t sm = (km & 1) ? (vm >> 16) : (vm & 0xFFFFu);
+        const uint32_t sp = (kp & 1) ? (vp >> 16) : (vp & 0xFFFFu);
+        if (on) {
+          if (t == 0)
+            info[job.px_off + static_cast<int64_t>(y) * w + x] =
+                make_int4(static_cast<int>(static_cast<uint32_t>(kb) | (bcost << 16)),
+                          static_cast<int>(sec | (sm << 16)), static_cast<int>(sp), 0);
+          if (job.volume != nullptr) {
+            uint16_t* vb = job.volume + cell + e0;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              if (uvalid[u])
+                *reinterpret_cast<uint4*>(vb + 8 * u) = make_uint4(s[4 * u], s[4 * u + 1], s[4 * u + 2], s[4 * u + 3]);
           }
-          const int base_lane = gi * G;
-          vm = r3dsimt::shfl(vm, (base_lane + km / (2 * K)) & 31);
-          vp = r3dsimt::shfl(vp, (base_lane + kp / (2 * K)) & 31);
-          const uint32_t sm = (km & 1) ? (vm >> 16) : (vm & 0xFFFFu);
-          const uint32_t sp = (kp & 1) ? (vp >> 16) : (vp & 0xFFFFu);
-          if (on) {
-            if (t == 0)
-              info[job.px_off + static_cast<int64_t>(y) * w + x] =
-                  make_int4(static_cast<int>(static_cast<uint32_t>(kb) | (bcost << 16)),
-                            static_cast<int>(sec | (sm << 16)), static_cast<int>(sp), 0);
-            if (job.volume != nullptr) {
-              uint16_t* vb = job.volume + cell + e0;
+          if (m.diagonal_lr) {
+            // Right-view WTA along the diagonal (sgm_kernels.cpp:349-356): the
+            // smallest (S, x) key per right column.
+            const RowInterval lv = m.bv[job.y0 + y];
+            const int bx = job.x0 + x;
+            if (bx >= lv.first && bx <= lv.last) {
+              uint32_t* keys = rkeys + job.rk_off + static_cast<int64_t>(y) * (w + nd);
+              const int b0 = x + nd - 1;
 #pragma unroll
-              for (int u = 0; u < U; ++u)
-                if (uvalid[u])
-                  *reinterpret_cast<uint4*>(vb + 8 * u) = make_uint4(s[4 * u], s[4 * u + 1], s[4 * u + 2], s[4 * u + 3]);
-            }
-            if (m.diagonal_lr) {
-              // Right-view WTA along the diagonal (sgm_kernels.cpp:349-356): the
-              // smallest (S, x) key per right column.
-              const RowInterval lv = m.bv[job.y0 + y];
-              const int bx = job.x0 + x;
-              if (bx >= lv.first && bx <= lv.last) {
-                uint32_t* keys = rkeys + job.rk_off + static_cast<int64_t>(y) * (w + nd);
-                const int b0 = x + nd - 1;
-#pragma unroll
-                for (int k = 0; k < K; ++k) {
-                  if (uvalid[k / 4]) {
-                    const int e = e0 + 2 * k;
-                    atomicMin(keys + (b0 - e), ((s[k] & 0xFFFFu) << 16) | static_cast<uint32_t>(x));
-                    atomicMin(keys + (b0 - e - 1), (s[k] & 0xFFFF0000u) | static_cast<uint32_t>(x));
-                  }
+              for (int k = 0; k < K; ++k) {
+                if (uvalid[k / 4]) {
+                  const int e = e0 + 2 * k;
+                  atomicMin(keys + (b0 - e), ((s[k] & 0xFFFFu) << 16) | static_cast<uint32_t>(x));
+                  atomicMin(keys + (b0 - e - 1), (s[k] & 0xFFFF0000u) | static_cast<uint32_t>(x));
                 }
               }
             }
           }
         }
       }
+      (void)s;
+      (void)kTerms;
 #pragma unroll
       for (int k = 0; k < K; ++k) prev[k] = out[k];
       iprev = icur;
 #pragma unroll
-      for (int k = 0; k + 1 < kPathStages; ++k) iq[k] = iq[k + 1];
+      for (int k = 0; k + 1 < NS; ++k) iq[k] = iq[k + 1];
     }
     r3dsimt::cp_async_wait<0>();
   }
@@ -938,21 +997,24 @@ int resident_grid(Kernel kernel, int sms, int64_t work_items, int per_block, siz
 
 // Algorithmic HBM bytes of one pass over `cells` cells of `pixels` pixels:
 // costs read, sums read (not by the first pass) and written (not by the
-// full-range last pass, which writes the WTA records instead).
+// full-range last pass, which writes the WTA records instead); byte terms:
+// one written per cell by passes 1..7, seven read by the last pass.
 uint64_t pass_bytes(int mode, bool ranged, const SgmPathSegment& g) {
   const uint64_t c = static_cast<uint64_t>(g.cells), px = static_cast<uint64_t>(g.pixels);
   if (mode == kFirst) return 3 * c;
+  if (mode == kTerm) return 2 * c;
+  if (mode == kLastTerm) return (1 + kTermArrays) * c + 16 * px;
   if (mode == kLast && !ranged) return 3 * c + 16 * px;
   return 5 * c;
 }
 
 template <int G, int K, int MODE>
 void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
-                 const uint8_t* cost, uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s,
-                 const SgmPathSegment& seg, const int* cancel) {
+                 const uint8_t* cost, uint16_t* sum, uint8_t* terms, int64_t tstride, int tslot, int4* info,
+                 uint32_t* rkeys, int sms, cudaStream_t s, const SgmPathSegment& seg, const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_kernel<G, K, MODE>;
-  constexpr size_t smem = PathRing<G, K>::kBlockBytes;
+  constexpr size_t smem = PathRing<G, K, MODE>::kBlockBytes;
   static thread_local int configured[64] = {};
   int dev = 0;
   R3D_CUDA(cudaGetDevice(&dev));
@@ -961,7 +1023,7 @@ void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int
     configured[dev] = 1;
   }
   R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32, smem)), dim3(kPathThreads), smem, s, dm, jobs,
-             njobs, ps.cls, ps.dx, ps.dy, nb, cost, sum, info, rkeys, cancel);
+             njobs, ps.cls, ps.dx, ps.dy, nb, cost, sum, terms, tstride, tslot, info, rkeys, cancel);
   launched("sgm_path_kernel");
   if (ev0 != nullptr) {
     char shape[32];
@@ -973,17 +1035,31 @@ void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int
 
 template <int G, int K>
 void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const uint8_t* cost,
-                   uint16_t* sum, int4* info, uint32_t* rkeys, int sms, cudaStream_t s, const int* cancel) {
+                   uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, int sms,
+                   cudaStream_t s, const int* cancel) {
   for (int q = 0; q < 8; ++q) {
     const Pass ps = kPasses[q];
     const int64_t nb = g.blocks[ps.cls];
     if (nb <= 0) continue;
-    if (q == 0)
-      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g, cancel);
-    else if (q < 7)
-      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g, cancel);
-    else
-      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, nb, cost, sum, info, rkeys, sms, s, g, cancel);
+    if (terms != nullptr) {
+      // Every pass runs (a segment with pixels has chains of every class), so
+      // the last pass finds all seven term arrays written.
+      if (q < 7)
+        launch_pass<G, K, kTerm>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, q, info, rkeys, sms, s, g,
+                                 cancel);
+      else
+        launch_pass<G, K, kLastTerm>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s,
+                                     g, cancel);
+    } else if (q == 0) {
+      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s, g,
+                                cancel);
+    } else if (q < 7) {
+      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s, g,
+                                     cancel);
+    } else {
+      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s, g,
+                               cancel);
+    }
   }
 }
 
@@ -1021,13 +1097,15 @@ SgmPathShape sgm_path_shape(int nd) {
   return best;
 }
 
-SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys) {
+SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys, bool terms) {
   SgmPathBuffers b{};
   size_t o = 0;
   b.cost = o;
   o += align256(static_cast<size_t>(cells));
   b.sum = o;
-  o += align256(static_cast<size_t>(cells) * 2);
+  b.term_stride = terms ? static_cast<int64_t>(align256(static_cast<size_t>(cells))) : 0;
+  o += terms ? static_cast<size_t>(kTermArrays) * static_cast<size_t>(b.term_stride)
+             : align256(static_cast<size_t>(cells) * 2);
   b.info = o;
   o += align256(static_cast<size_t>(pixels) * 16);
   b.rkeys = o;
@@ -1038,9 +1116,10 @@ SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys) {
 
 void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, cudaStream_t s) {
   if (wave.njobs <= 0 || wave.cells <= 0) return;
-  const SgmPathBuffers B = sgm_path_buffers(wave.cells, wave.pixels, wave.keys);
+  const SgmPathBuffers B = sgm_path_buffers(wave.cells, wave.pixels, wave.keys, wave.terms != 0);
   uint8_t* cost = wave.buffer + B.cost;
   uint16_t* sum = reinterpret_cast<uint16_t*>(wave.buffer + B.sum);
+  uint8_t* terms = wave.terms != 0 ? wave.buffer + B.sum : nullptr;
   int4* info = reinterpret_cast<int4*>(wave.buffer + B.info);
   uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
   if (wave.keys > 0) R3D_CUDA(cudaMemsetAsync(rkeys, 0xFF, static_cast<size_t>(wave.keys) * 4, s));
@@ -1065,7 +1144,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
     bool done = false;
 #define R3D_SHAPE(gg, kk)                                                                                     \
   if (!done && g.shape.g_ == gg && g.shape.k_ == kk) {                                                        \
-    launch_passes<gg, kk>(dm, jobs, g, cost, sum, info, rkeys, sms, s, wave.cancel);                         \
+    launch_passes<gg, kk>(dm, jobs, g, cost, sum, terms, B.term_stride, info, rkeys, sms, s, wave.cancel);   \
     done = true;                                                                                              \
   }
     R3D_PATH_SHAPES(R3D_SHAPE)
@@ -1142,7 +1221,7 @@ SgmPathShape sgm_path_ranged_shape(int over32, int64_t pixels) {
 
 SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
                                        int sms) {
-  SgmPathBuffers b = sgm_path_buffers(cells, pixels, keys);
+  SgmPathBuffers b = sgm_path_buffers(cells, pixels, keys, false);
   size_t o = b.total;
   b.rec = o;
   o += align256(static_cast<size_t>(pixels) * 16);

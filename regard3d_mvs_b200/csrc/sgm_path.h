@@ -48,13 +48,16 @@ SgmPathShape sgm_path_shape(int nd);
 inline bool sgm_path_fits(int w, int nd) { return w + nd - 1 <= 2048; }
 inline int64_t sgm_path_chains(int cls, int w, int h) { return cls == 0 ? h : (cls == 1 ? w : w + h - 1); }
 
-// Device buffers of a wave (bytes, 256-byte aligned pieces).
+// Device buffers of a wave (bytes, 256-byte aligned pieces). With `terms`
+// the u16 sum volume is replaced by seven byte-term arrays of term_stride
+// bytes each (starting at `sum`).
 struct SgmPathBuffers {
   size_t cost, sum, info, rkeys, total;
+  int64_t term_stride;
   size_t rec, rowsum, rowstart, rowshift, overflow;  // ranged waves only
   int64_t overflow_words;                            // per chain buffer
 };
-SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys);
+SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys, bool terms);
 
 // A wave on the device: all jobs (device pointer), and per shape the range
 // of jobs with its chain-block counts.
@@ -78,8 +81,9 @@ struct SgmPathWave {
   const SgmPathSegment* segs;  // host array
   int nsegs;
   int64_t cells, pixels, keys, rows;
-  unsigned char* buffer;  // sgm_path_buffers(cells, pixels, keys).total bytes
+  unsigned char* buffer;  // sgm_path_buffers(cells, pixels, keys, terms).total bytes
   const int* cancel;      // device view of the caller's cancellation flag, or null
+  int terms;              // 1: byte terms (every match of the wave has term_u8)
 };
 
 // Costs, the 8 passes and the acceptance rules of one wave, on stream s.
@@ -104,6 +108,7 @@ struct SgmPathRangedWave {
   int maxnum;  // largest label count of a pixel of the wave
   unsigned char* buffer;
   const int* cancel;  // device view of the caller's cancellation flag, or null
+  int terms;          // full-range waves: byte terms (every match of the wave has term_u8)
 };
 SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
                                        int sms);

@@ -54,6 +54,7 @@ R3D_DEVICE int popc64(uint64_t v) { return __popcll(v); }
 // Streaming (evict-first) 16-byte load and store.
 R3D_DEVICE uint4 ld_stream(const uint4* p) { return __ldcs(p); }
 R3D_DEVICE void st_stream(uint4* p, uint4 v) { __stcs(p, v); }
+R3D_DEVICE void st_stream8(uint2* p, uint2 v) { __stcs(p, v); }
 
 // 16-byte asynchronous global -> shared copy (L2 only). Both addresses must
 // be 16-byte aligned.
@@ -174,6 +175,7 @@ inline uint32_t funnel_r(uint32_t lo, uint32_t hi, uint32_t s) {
 inline int popc64(uint64_t v) { return __builtin_popcountll(v); }
 inline uint4 ld_stream(const uint4* p) { return *p; }
 inline void st_stream(uint4* p, uint4 v) { *p = v; }
+inline void st_stream8(uint2* p, uint2 v) { *p = v; }
 void cp_async16(void* smem_dst, const void* gmem_src);
 void cp_async8(void* smem_dst, const void* gmem_src);
 void cp_async_commit();
