@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "pair1024", "pair2048", "combine", "rectify", "depth",
+    ap.add_argument("--workload", choices=("batch64", "pair3072", "pair640", "pair1024", "pair2048", "scene32", "combine", "rectify", "depth",
                                            "view"),
                     default="batch64",
                     help="combine / rectify / depth: only the multi-view combination of one view / the "
@@ -72,11 +72,11 @@ def parse():
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip the one-pair-per-call run with the one-CTA-per-tile kernels")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve", action="store_true",
-                    help="also run the serving sweep (config 3) in a fresh process and add its results")
+    ap.add_argument("--no-serve", dest="serve", action="store_false",
+                    help="skip the serving sweep (config 3), which runs in a fresh process after the batch")
     ap.add_argument("--serve-only", type=float, default=0.0, metavar="PAIRS_PER_S",
-                    help="run only the serving sweep against this saturated rate; print its JSON")
-    ap.add_argument("--serve-seconds", type=float, default=15.0, help="arrival window per load point")
+                    help="run only the serving sweep (its saturation run offers 3 x this batch rate); print its JSON")
+    ap.add_argument("--serve-seconds", type=float, default=8.0, help="arrival window per load point")
     return ap.parse_args()
 
 
@@ -110,7 +110,7 @@ def workload_pairs(name: str, npairs: int, seed: int):
 def make_images(lib, spec):
     from regard3d_mvs_b200.types import CSynthParams
 
-    p = CSynthParams(spec["w"], spec["h"], spec["nd"], spec["seed"] & 0xFFFFFFFF, 1.5, 2.0, 8,
+    p = CSynthParams(spec["w"], spec["h"], spec["nd"], spec["seed"] & 0xFFFFFFFF, 1.5, 2.0, spec.get("planes", 8),
                      spec["textureless"], spec["occluded"])
     L = np.empty((spec["h"], spec["w"]), np.uint8)
     R = np.empty_like(L)
@@ -800,89 +800,362 @@ def measure_view(lib, dev, stream, steps: int, warmup: int) -> dict:
                              "sample": "the same view once: rectify, match_stereo and combine_pairs of the oracle"}}
 
 
+# Config 4: the full depth stage of a 32-view scene (2048 x 1536 views on an
+# arc of radius 2 m around 20 textured planes, 4 nearest partners per view).
+SCENE_VIEWS, SCENE_W, SCENE_H, SCENE_SEED = 32, 2048, 1536, 11
+SCENE_CHECK_VIEW = 16  # compared with the oracle's chain (a central view)
+
+
+def _scene_env(plain: bool):
+    """Kernel selection of the plain GPU path: one CTA per SGM tile (the
+    skewed-wavefront kernels), single-track batches."""
+    keys = {"R3DGPU_FULL_KERNEL": "wavefront", "R3DGPU_RANGED_KERNEL": "ranged", "R3DGPU_BATCH_TRACKS": "1"}
+    if plain:
+        os.environ.update(keys)
+    else:
+        for k in keys:
+            os.environ.pop(k, None)
+
+
+def measure_scene(lib, dev, stream, steps: int, warmup: int) -> dict:
+    """Config 4 end to end on the device: per view compute_depth_map
+    (rectification of both images of its 4 pairs, one batch match,
+    combination), then the float refinement of every view against its
+    partners' refinement images and the consistency filter of the 32 maps;
+    the same through the host entry points (e2e), with the plain one-CTA-per-
+    tile kernels, one view's depth map against the oracle's chain, the float
+    refinement against the double oracle on a crop, and the oracle's time."""
+    import torch
+
+    from oracle import oracle as orc
+    from regard3d_mvs_b200.depth_maps import (CConsistencyStats, CDepthMap, ConsistencyOptions, CRefinementImage,
+                                              CRefinementStats, RefinementOptions, c_camera, neighbour_lists)
+    from regard3d_mvs_b200.multi_view import CViewPair, arc_scene, c_grid, pair_geometry
+    from regard3d_mvs_b200.stereo import Matcher
+    from regard3d_mvs_b200.types import (CViewU16, MultiStereoOptions, StereoOptions, camera_struct, pinhole_struct,
+                                         to_c_options)
+
+    scene = arc_scene(SCENE_VIEWS, SCENE_W, SCENE_H, seed=SCENE_SEED, device=dev)
+    views = scene["views"]
+    n, w, h = len(views), SCENE_W, SCENE_H
+    K = scene["K"]
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    cam = {"model": 0, "width": w, "height": h, "fx": K[0, 0], "fy": K[1, 1], "cx": K[0, 2], "cy": K[1, 2]}
+    cb = camera_struct(cam)
+    d_img = [torch.from_numpy(v["image"].view(np.int16)).to(dev) for v in views]
+    d_gray = [torch.from_numpy(v["image8"].astype(np.float32)).to(dev) for v in views]
+    d_color = [torch.from_numpy(np.repeat(v["image8"][..., None], 3, axis=2)).to(dev) for v in views]
+    pcams = [{"width": w, "height": h, "fx": K[0, 0], "fy": K[1, 1], "cx": K[0, 2], "cy": K[1, 2],
+              "rotation": v["camera"]["R"], "center": v["camera"]["C"]} for v in views]
+    ccams = [c_camera(c) for c in pcams]
+    grids = [c_grid(v["camera"]) for v in views]
+    vbs = [CViewU16(d_img[i].data_ptr(), w, h, w) for i in range(n)]
+    pair_arrs = []
+    for i, v in enumerate(views):
+        arr = (CViewPair * len(v["pairs"]))()
+        for k, p in enumerate(v["pairs"]):
+            q = arr[k]
+            q.partner = CViewU16(d_img[p["partner"]].data_ptr(), w, h, w)
+            q.partner_camera = camera_struct(cam)
+            q.base_from_rect[:] = [float(x) for x in (v["camera"]["R"] @ p["R_rect"].T).ravel()]
+            q.partner_from_rect[:] = [float(x) for x in (p["R_partner"] @ p["R_rect"].T).ravel()]
+            q.left, q.right = pinhole_struct(p["left"]), pinhole_struct(p["right"])
+            q.disparity_min, q.num_disparities = p["disparity_min"], p["num_disparities"]
+            q.geometry = pair_geometry(v["camera"], p)
+        pair_arrs.append(arr)
+    depth = [torch.empty((h, w), dtype=torch.float32, device=dev) for _ in views]
+    conf = [torch.empty_like(d) for d in depth]
+    mask = [torch.empty((h, w), dtype=torch.int16, device=dev) for _ in views]
+    support = [torch.zeros((h, w), dtype=torch.uint8, device=dev) for _ in views]
+    rimg_t = [torch.empty((h, w, 3), dtype=torch.float32, device=dev) for _ in views]
+    so, mo = to_c_options(StereoOptions()), MultiStereoOptions().c()
+    rimg = []
+    for i in range(n):
+        r = CRefinementImage()
+        r.camera, r.data, r.stride = ccams[i], rimg_t[i].data_ptr(), 3 * w
+        rimg.append(r)
+    partners = [v["partners"] for v in views]
+    partner_rimg = []
+    for i in range(n):
+        arr = (CRefinementImage * len(partners[i]))()
+        for k, j in enumerate(partners[i]):
+            arr[k] = rimg[j]
+        partner_rimg.append(arr)
+    maps = (CDepthMap * n)()
+    for i in range(n):
+        mp = maps[i]
+        mp.camera = ccams[i]
+        mp.depth, mp.confidence = depth[i].data_ptr(), conf[i].data_ptr()
+        mp.pair_mask, mp.support, mp.color = mask[i].data_ptr(), support[i].data_ptr(), d_color[i].data_ptr()
+        mp.stride, mp.color_stride, mp.width, mp.height = w, 3 * w, w, h
+        mp.view, mp.num_partners = i, len(partners[i])
+        for k, j in enumerate(partners[i]):
+            mp.partners[k] = j
+    off, idx = neighbour_lists(partners)
+    ropts = RefinementOptions(radius=3, step=1, fp32=True).c()
+    copts = ConsistencyOptions().c()
+    rstats, cstats = CRefinementStats(), CConsistencyStats()
+    cells = ctypes.c_uint64(0)
+    total_cells = [0]
+
+    def step():
+        total_cells[0] = 0
+        for i in range(n):
+            _native_check(lib, lib.r3dgpu_make_refinement_image(d_gray[i].data_ptr(), w, w, h, 0.0,
+                                                                rimg_t[i].data_ptr(), 3 * w, sptr))
+        for i in range(n):
+            _native_check(lib, lib.r3dgpu_compute_depth_map(ctypes.byref(vbs[i]), ctypes.byref(cb),
+                                                            ctypes.byref(grids[i]), pair_arrs[i], len(views[i]["pairs"]),
+                                                            ctypes.byref(so), ctypes.byref(mo), depth[i].data_ptr(),
+                                                            conf[i].data_ptr(), mask[i].data_ptr(), w,
+                                                            ctypes.byref(cells), sptr))
+            total_cells[0] += int(cells.value)
+        for i in range(n):
+            _native_check(lib, lib.r3dgpu_refine_depth_map(depth[i].data_ptr(), conf[i].data_ptr(), w,
+                                                           ctypes.byref(ccams[i]), w, h, ctypes.byref(rimg[i]),
+                                                           partner_rimg[i], len(partners[i]), ctypes.byref(ropts),
+                                                           ctypes.byref(rstats), sptr))
+        _native_check(lib, lib.r3dgpu_filter_depth_maps(maps, n, off.ctypes.data, idx.ctypes.data,
+                                                        ctypes.byref(copts), ctypes.byref(cstats), sptr))
+
+    def timed(k):
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = int(lib.r3dgpu_launch_count())
+        a.record(stream)
+        for _ in range(k):
+            step()
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        return a.elapsed_time(b) / k, (int(lib.r3dgpu_launch_count()) - l0) // k
+
+    for _ in range(warmup):
+        step()
+    ms, launches = timed(steps)
+    refine_stats, filter_stats = rstats.as_dict(), cstats.as_dict()
+    kept = float(sum(int((d > 0).sum().item()) for d in depth)) / (n * w * h)
+    full_cells = sum(w * h * p["num_disparities"] for v in views for p in v["pairs"])
+    # The plain GPU path: the same chain with one CTA per SGM tile.
+    _scene_env(True)
+    try:
+        step()
+        plain_ms, _ = timed(1)
+    finally:
+        _scene_env(False)
+
+    # End to end through the public host API: Matcher.compute_depth_map per
+    # view (host images in, maps out), then Matcher.depth_stage (host maps
+    # and refinement images in, refined and filtered maps out).
+    m = Matcher(device=dev.index or 0)
+    hrimg = [t.cpu().numpy() for t in rimg_t]
+
+    def e2e_step():
+        hmaps = []
+        for i, v in enumerate(views):
+            dm, _ = m.compute_depth_map(v["image"], v["camera"], v["pairs"])
+            hmaps.append({"camera": pcams[i], "depth": dm.depth, "confidence": dm.confidence,
+                          "pair_mask": dm.pair_mask, "color": np.repeat(v["image8"][..., None], 3, axis=2),
+                          "view": i, "partners": partners[i]})
+        m.depth_stage(hmaps, [{"camera": pcams[i], "data": hrimg[i]} for i in range(n)], partners,
+                      RefinementOptions(radius=3, step=1, fp32=True), ConsistencyOptions())
+        return hmaps
+
+    e2e_step()
+    t0 = time.perf_counter()
+    e2e_step()
+    e2e_s = time.perf_counter() - t0
+    h2d = n * (2 * w * h * 5 + 12 * w * h + 3 * w * h + 10 * w * h)
+    d2h = n * (10 * w * h + 9 * w * h)
+
+    # One view against the oracle's chain (rectify both images of every pair,
+    # match_stereo, combine_pairs), timed as the CPU baseline of that part.
+    c = SCENE_CHECK_VIEW
+    v = views[c]
+    got, _ = m.compute_depth_map(v["image"], v["camera"], v["pairs"])
+    t0 = time.perf_counter()
+    matched = []
+    for p in v["pairs"]:
+        left, lmask = orc.rectify_image(v["image"], cam, v["camera"]["R"] @ p["R_rect"].T, p["left"])
+        right, rmask = orc.rectify_image(p["image"], cam, p["R_partner"] @ p["R_rect"].T, p["right"])
+        mt = orc.match_stereo(left, right, lmask, rmask, p["disparity_min"], p["num_disparities"], StereoOptions())
+        matched.append(dict(p, disparity=mt.disparity, confidence=mt.confidence))
+    ref = orc.combine_pairs(v["camera"], matched, MultiStereoOptions())
+    chain_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ref.depth, got.depth) and np.array_equal(ref.pair_mask, got.pair_mask))
+    # Float refinement against the double oracle on a crop of that view (its
+    # combined depth map as the initial depths).
+    cw, ch = DEPTH_CROP
+    x0, y0 = (w - cw) // 2, (h - ch) // 2
+    cam_c = dict(pcams[c], width=cw, height=ch, cx=pcams[c]["cx"] - x0, cy=pcams[c]["cy"] - y0)
+    base = {"camera": cam_c, "data": np.ascontiguousarray(hrimg[c][y0:y0 + ch, x0:x0 + cw])}
+    pviews = [{"camera": pcams[j], "data": hrimg[j]} for j in partners[c]]
+    crop = {"camera": cam_c, "depth": np.ascontiguousarray(got.depth[y0:y0 + ch, x0:x0 + cw]),
+            "confidence": np.ascontiguousarray(got.confidence[y0:y0 + ch, x0:x0 + cw])}
+    g32 = {k: (x.copy() if isinstance(x, np.ndarray) else x) for k, x in crop.items()}
+    m.refine_depth_map(g32, base, pviews, RefinementOptions(radius=3, step=1, fp32=True))
+    o64 = {k: (x.copy() if isinstance(x, np.ndarray) else x) for k, x in crop.items()}
+    t0 = time.perf_counter()
+    orc.refine_depth_map(o64, base, pviews, RefinementOptions(radius=3, step=1))
+    refine_s = (time.perf_counter() - t0) * (w * h) / (cw * ch)
+    both = (g32["depth"] > 0) & (o64["depth"] > 0)
+    rel = np.abs(g32["depth"][both].astype(np.float64) - o64["depth"][both]) / o64["depth"][both]
+    flips = int(((g32["depth"] > 0) != (o64["depth"] > 0)).sum())
+    return {"workload": f"config 4: {n} views {w}x{h} on an arc of radius 2 m around 20 textured planes, 4 partners "
+                        "per view: rectify + match (reference defaults, one batch per view) + combine, FP32 7x7 "
+                        "refinement against the 4 partners, consistency over 4 neighbours",
+            "value": n / (ms * 1e-3), "unit": "depth maps/s", "ms_per_scene": ms, "gpu_launches": launches,
+            "full_range_cells": full_cells, "aggregated_cells": total_cells[0],
+            "label_ranges": sorted({p["num_disparities"] for vv in views for p in vv["pairs"]}),
+            "depth_fraction_kept": kept, "refinement": refine_stats, "consistency": filter_stats,
+            "plain_gpu_path": {"value": n / (plain_ms * 1e-3), "unit": "depth maps/s", "ms_per_scene": plain_ms,
+                               "kernels": "one CTA per SGM tile (skewed-wavefront kernels), single-track batches"},
+            "bit_exact_vs_oracle": {"view": c, "depth_and_pair_mask_equal": same},
+            "fp32_vs_f64_oracle": {"sample": f"{cw}x{ch} crop of view {c}", "pixels_compared": int(both.sum()),
+                                   "decision_flips": flips,
+                                   "rel_depth_error_p50": float(np.percentile(rel, 50)) if rel.size else 0.0,
+                                   "p99": float(np.percentile(rel, 99)) if rel.size else 0.0,
+                                   "max": float(rel.max()) if rel.size else 0.0, "target": 1e-5},
+            "e2e": {"value": n / e2e_s, "unit": "depth maps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "cpu_baseline": {"value": 1.0 / (chain_s + refine_s), "unit": "depth maps/s", "cores": orc.max_threads(),
+                             "kind": "port",
+                             "sample": f"view {c} once: the oracle's rectify, match_stereo and combine_pairs "
+                                       f"({chain_s:.1f} s), plus its double refinement of a {cw}x{ch} crop scaled "
+                                       f"to the view ({refine_s:.1f} s); consistency not included"}}
+
+
 SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
-SERVE_REQUEST_BUDGET = 118 << 30  # config 3's 150 GB: 118 GB for admitted requests + 2 x 16 GB worker scratch
+SERVE_REQUEST_BUDGET = 110 << 30  # config 3's 150 GB: 110 GB for admitted requests, 2 x 16 GB worker scratch, 8 GB cache
+SERVE_CACHE = 8 << 30
 SERVE_WORKERS = 2
+SERVE_SCENE_VIEWS = 200
+SERVE_POOL_VIEWS = 8
+SERVE_PARTNERS = 4
 
 
-def run_serving(args, sat_pairs_per_s: float) -> dict:
-    """Config 3: Poisson arrivals of the workload's pairs at fractions of the
-    saturated batch rate, through the serving loop (continuous batching,
-    admission by device-memory budget). Per load point: latency percentiles
-    of submit -> result on the host, achieved throughput, mean batch size."""
+def serving_views(lib, n: int, seed: int) -> list[dict]:
+    """Distinct views of the serving simulation: sizes, label ranges and
+    hierarchy as config 2 draws them per pair; each view's 4 partner pairs
+    share its left image (the generator's left image depends on the seed,
+    size and label count only) and differ in the disparity field (plane
+    count), so their right images differ."""
+    rng = np.random.default_rng(seed)
+    views = []
+    for v in range(n):
+        w = int(round(math.exp(rng.uniform(math.log(1024), math.log(6048)))))
+        h = int(round(w / (1.5 if rng.random() < 0.5 else 4.0 / 3.0)))
+        nd = int(ND_CHOICES[rng.integers(0, len(ND_CHOICES))])
+        hier = v % 2 == 1
+        spec = dict(w=w, h=h, nd=nd, levels=3 if hier else 0, radius=0 if hier else 3, margin=8 if hier else 4,
+                    textureless=0.0, occluded=0.0, seed=seed * 1000 + v)
+        rights, left = [], None
+        for k in range(SERVE_PARTNERS):
+            L, R = make_images(lib, dict(spec, planes=5 + k))
+            left = L if left is None else left
+            assert np.array_equal(left, L)
+            rights.append(R)
+        views.append(dict(spec, left=left, rights=rights))
+    return views
+
+
+def run_serving(args, rate_hint: float) -> dict:
+    """Config 3: a simulated 200-view scene, each view issuing its 4 partner
+    pair requests (Poisson arrivals of requests), through the serving loop
+    (continuous batching, admission by a device-memory budget, a view's left
+    image uploaded once and kept on the device across its partners by its
+    content key). The served saturation is measured first (offered load 3 x
+    the batch rate `rate_hint`), then latency percentiles and served
+    Gcells/s at fractions of that saturated rate."""
     import torch
 
     from regard3d_mvs_b200 import Server
     from regard3d_mvs_b200._native import load
 
     lib = load()
-    specs = workload_pairs("batch64", args.pairs, args.seed)
+    pool_views = serving_views(lib, SERVE_POOL_VIEWS, args.seed + 17)
 
     def pinned(a):
         t = torch.from_numpy(a.view(np.int16) if a.dtype == np.uint16 else a).pin_memory()
         return t.numpy().view(a.dtype)
 
-    # Page-locked inputs, and page-locked output maps from a pool per pair
-    # (a request takes a free map, its completion returns it).
-    host = [tuple(pinned(x) for x in make_images(lib, s)) for s in specs]
-    pool: list[list[np.ndarray]] = [[] for _ in specs]
-
-    def take(i):
-        return pool[i].pop() if pool[i] else pinned(np.empty((specs[i]["h"], specs[i]["w"]), np.float32))
-    cells = [s["w"] * s["h"] * ((s["nd"] + 15) // 16 * 16) for s in specs]
-    rng = np.random.default_rng(args.seed + 1)
-    points = []
+    for v in pool_views:
+        v["left"] = pinned(v["left"])
+        v["rights"] = [pinned(r) for r in v["rights"]]
+        v["outs"] = [[pinned(np.empty((v["h"], v["w"]), np.float32)) for _ in range(2)]
+                     for _ in range(SERVE_PARTNERS)]
+    # The scene's request sequence: view s uses the images of pool view
+    # s % POOL under its own content key (a new view: its left image is not
+    # on the device yet), partners in order.
+    seq = [(s, s % SERVE_POOL_VIEWS, k) for s in range(SERVE_SCENE_VIEWS) for k in range(SERVE_PARTNERS)]
+    cells = {vi: v["w"] * v["h"] * ((v["nd"] + 15) // 16 * 16) for vi, v in enumerate(pool_views)}
     free0, total = torch.cuda.mem_get_info(0)
-    peak_used = total - free0
-    # Enough page-locked output maps for the deepest queue, allocated before
-    # the arrivals start (page-locking during the sweep would slow it).
-    for i in range(len(specs)):
-        pool[i] += [take(i) for _ in range(3)]
+    peak_used = [total - free0]
+    rng = np.random.default_rng(args.seed + 1)
+    cursor = [0]
+    key_base = [1]
+
+    def submit(srv, s, vi, k):
+        v = pool_views[vi]
+        out = v["outs"][k].pop() if v["outs"][k] else pinned(np.empty((v["h"], v["w"]), np.float32))
+        t = srv.submit(v["left"], v["rights"][k], None, None, 0, v["nd"], options_for(v), out=(out, None),
+                       left_key=key_base[0] + s)
+        return (vi, k, out, t)
+
+    def run_point(srv, lam: float, seconds: float) -> dict:
+        nreq = int(min(max(16, round(lam * seconds)), len(seq)))
+        gaps = rng.exponential(1.0 / lam, nreq)
+        tickets = []
+        t0 = time.perf_counter()
+        arrival = t0
+        for q in range(nreq):
+            arrival += gaps[q]
+            delay = arrival - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            s, vi, k = seq[(cursor[0] + q) % len(seq)]
+            tickets.append(submit(srv, s, vi, k))
+            free, _ = torch.cuda.mem_get_info(0)
+            peak_used[0] = max(peak_used[0], total - free)
+        cursor[0] += nreq
+        key_base[0] += SERVE_SCENE_VIEWS  # keys of a point never match the previous point's
+        lat, batch, hits, up = [], [], 0, 0
+        for vi, k, out, t in tickets:
+            m, tm = srv.wait(t)
+            pool_views[vi]["outs"][k].append(out)
+            lat.append(tm["total_ms"])
+            batch.append(tm["batch_size"])
+            hits += tm["cache_hits"]
+            up += tm["uploaded_bytes"]
+        t1 = time.perf_counter()
+        lat = np.array(lat)
+        done_cells = sum(cells[vi] for vi, _, _, _ in tickets)
+        return {"offered_pairs_per_s": lam, "requests": nreq, "served_pairs_per_s": nreq / (t1 - t0),
+                "gcells_per_s": done_cells / (t1 - t0) / 1e9,
+                "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                               "p999": float(np.percentile(lat, 99.9)), "max": float(lat.max())},
+                "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
+                "mean_batch": float(np.mean(batch)), "left_image_cache_hits": hits / nreq,
+                "uploaded_mb_per_request": up / nreq / 1e6}
+
     with Server(device=0, workers=SERVE_WORKERS, max_batch=16, hbm_budget=SERVE_REQUEST_BUDGET,
-                scratch_budget=16 << 30) as srv:
-        # Warm-up: every worker compiles nothing, but allocates its buffers.
-        warm = [(i, srv.submit(host[i][0], host[i][1], None, None, 0, specs[i]["nd"], options_for(specs[i]),
-                               out=(take(i), None))) for i in range(min(4, len(specs)))]
-        for i, t in warm:
-            m, _ = srv.wait(t)
-            pool[i].append(m.disparity)
+                scratch_budget=16 << 30, cache_budget=SERVE_CACHE) as srv:
+        # Warm-up: the workers allocate their buffers.
+        run_point(srv, 4.0 * max(rate_hint, 1.0), 2.0)
+        sat = run_point(srv, 3.0 * max(rate_hint, 1.0), args.serve_seconds)
+        sat_rate = sat["served_pairs_per_s"]
+        points = []
         for frac in SERVE_FRACTIONS:
-            lam = frac * sat_pairs_per_s
-            nreq = int(min(max(16, round(lam * args.serve_seconds)), 192))
-            order = rng.integers(0, len(specs), nreq)
-            gaps = rng.exponential(1.0 / lam, nreq)
-            tickets = []
-            t0 = time.perf_counter()
-            arrival = t0
-            for k in range(nreq):
-                arrival += gaps[k]
-                delay = arrival - time.perf_counter()
-                if delay > 0:
-                    time.sleep(delay)
-                i = int(order[k])
-                tickets.append((i, srv.submit(host[i][0], host[i][1], None, None, 0, specs[i]["nd"],
-                                              options_for(specs[i]), out=(take(i), None))))
-                free, _ = torch.cuda.mem_get_info(0)
-                peak_used = max(peak_used, total - free)
-            lat, batch = [], []
-            for i, t in tickets:
-                m, tm = srv.wait(t)
-                pool[i].append(m.disparity)
-                lat.append(tm["total_ms"])
-                batch.append(tm["batch_size"])
-            t1 = time.perf_counter()
-            lat = np.array(lat)
-            done_cells = sum(cells[i] for i, _ in tickets)
-            points.append({"load": frac, "offered_pairs_per_s": lam, "requests": nreq,
-                           "gcells_per_s": done_cells / (t1 - t0) / 1e9,
-                           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
-                                          "p999": float(np.percentile(lat, 99.9)), "max": float(lat.max())},
-                           "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
-                           "mean_batch": float(np.mean(batch))})
-    return {"saturated_pairs_per_s": sat_pairs_per_s, "workers": SERVE_WORKERS, "max_batch": 16,
-            "host_buffers": "page-locked inputs and disparity maps; no confidence maps",
+            pt = run_point(srv, frac * sat_rate, args.serve_seconds)
+            pt["load"] = frac
+            points.append(pt)
+    return {"scene": f"{SERVE_SCENE_VIEWS} views x {SERVE_PARTNERS} partner pairs (images of {SERVE_POOL_VIEWS} "
+                     "distinct config-2 views; each view's pairs share its left image under the view's content key)",
+            "saturated_pairs_per_s": sat_rate, "saturation_run": sat,
+            "load_axis": "fraction of the served saturation measured above", "workers": SERVE_WORKERS,
+            "max_batch": 16, "host_buffers": "page-locked inputs and disparity maps; no confidence maps",
             "request_budget_bytes": SERVE_REQUEST_BUDGET, "worker_scratch_bytes": 16 << 30,
-            "device_used_peak_gb": peak_used / 1e9, "arrivals": "Poisson", "points": points}
+            "image_cache_bytes": SERVE_CACHE, "device_used_peak_gb": peak_used[0] / 1e9, "arrivals": "Poisson",
+            "points": points}
 
 
 def main():
@@ -925,6 +1198,13 @@ def main():
     if args.workload == "view":
         dev0 = torch.device(f"cuda:{local}")
         r = measure_view(lib, dev0, torch.cuda.current_stream(dev0), args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps(dict(r, metric="depth maps/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
+                                  higher_is_better=True, data="synthetic")), flush=True)
+        return
+    if args.workload == "scene32":
+        dev0 = torch.device(f"cuda:{local}")
+        r = measure_scene(lib, dev0, torch.cuda.current_stream(dev0), args.steps, args.warmup)
         if rank == 0:
             print(json.dumps(dict(r, metric="depth maps/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
                                   higher_is_better=True, data="synthetic")), flush=True)
@@ -1158,8 +1438,10 @@ def main():
             line["cpu_baseline"] = cpu_baseline(specs, gpu_maps)
             line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
             line["rectify"] = measure_rectify(lib, dev, stream, args.steps, args.warmup, peak)
-            line["depth_stage"] = measure_depth(lib, dev, stream, args.steps, args.warmup, peak)
-            line["view_depth_map"] = measure_view(lib, dev, stream, args.steps, args.warmup)
+            # Config 4 end to end (the depth stage of a 32-view scene); the
+            # separate depth-stage and one-view lines stay available as
+            # --workload depth / view.
+            line["scene32"] = measure_scene(lib, dev, stream, 2, 1)
         if args.serve and world == 1:
             # In a fresh process, with this one's device memory given back.
             del dL, dR, dD, dC

@@ -10,6 +10,13 @@
  * while batches are on the GPU are admitted by the next free worker, so
  * their work overlaps the running batches on the device. Results equal
  * r3dgpu_match_stereo_host per request, whatever the mix.
+ *
+ * Residency across requests: a request may name its images by content key
+ * (left_key, right_key; 0 = none). The server keeps device copies of keyed
+ * images in a cache of cache_budget bytes (least recently used first out,
+ * never while a running batch reads them) and uploads a keyed image only
+ * when its key is not cached, so the partner pairs of one view, which share
+ * the view's image, send it to the device once.
  */
 #ifndef R3DGPU_SERVER_H
 #define R3DGPU_SERVER_H
@@ -29,10 +36,14 @@ typedef struct r3dgpu_server_config {
   int32_t reserved;
   uint64_t hbm_budget;       /* bytes of device memory the admitted requests may hold together */
   uint64_t scratch_budget;   /* bytes of SGM scratch per worker (0: 16 GiB) */
+  uint64_t cache_budget;     /* bytes of device memory for keyed input images (0: no cache) */
 } r3dgpu_server_config;
 
 /* A request: host images and host outputs, kept alive by the caller until
- * r3dgpu_server_wait returns for its ticket. Fields as in r3dgpu_pair. */
+ * r3dgpu_server_wait returns for its ticket. Fields as in r3dgpu_pair, then
+ * the content keys: a nonzero key promises that every request carrying it
+ * has the same image (same size and pixels); the server may then use a
+ * cached device copy instead of this request's host image. */
 typedef struct r3dgpu_request {
   r3dgpu_view_u16 left;
   r3dgpu_view_u16 right;
@@ -42,6 +53,8 @@ typedef struct r3dgpu_request {
   int32_t num_disparities;
   r3dgpu_stereo_options options;
   r3dgpu_disparity_map out;
+  uint64_t left_key;
+  uint64_t right_key;
 } r3dgpu_request;
 
 /* What happened to a request (milliseconds on the host's steady clock). */
@@ -52,6 +65,9 @@ typedef struct r3dgpu_request_times {
   uint64_t device_bytes;  /* admission estimate of the request's device memory */
   int32_t batch_size;     /* requests in its batch */
   int32_t worker;
+  int32_t cache_hits;     /* images of the request served from the cache (0..2) */
+  int32_t reserved;
+  uint64_t uploaded_bytes; /* host -> device bytes of the request's images */
 } r3dgpu_request_times;
 
 /* Starts the workers. hbm_budget must hold the largest single request's

@@ -11,7 +11,7 @@ import ctypes
 import os
 
 from .types import (CCamera, CDepthGrid, CDisparityMap, CMultiStereoOptions, COptions, CPair, CPairGeometry, CPinhole, CProfile,
-                    CRequestTimes, CServerConfig, CSynthParams, CViewU8, CViewU16)
+                    CRequest, CRequestTimes, CServerConfig, CSynthParams, CViewU8, CViewU16)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libr3dgpu.so")
@@ -218,9 +218,9 @@ def _declare(L: ctypes.CDLL) -> ctypes.CDLL:
     # The request struct has the layout of r3dgpu_pair.
     L.r3dgpu_server_create.argtypes = [ctypes.POINTER(CServerConfig), ctypes.POINTER(P)]
     L.r3dgpu_server_create.restype = st
-    L.r3dgpu_server_submit.argtypes = [P, ctypes.POINTER(CPair), ctypes.POINTER(ctypes.c_uint64)]
+    L.r3dgpu_server_submit.argtypes = [P, ctypes.POINTER(CRequest), ctypes.POINTER(ctypes.c_uint64)]
     L.r3dgpu_server_submit.restype = st
-    L.r3dgpu_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(CPair),
+    L.r3dgpu_server_wait.argtypes = [P, ctypes.c_uint64, ctypes.c_double, ctypes.POINTER(CRequest),
                                      ctypes.POINTER(CRequestTimes)]
     L.r3dgpu_server_wait.restype = st
     L.r3dgpu_server_pending.argtypes = [P]

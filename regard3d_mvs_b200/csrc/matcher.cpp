@@ -807,12 +807,12 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     int64_t cells, px, keys, rows;
     int maxnum;
   };
-  // Full-range waves keep byte terms when every match of the group allows
-  // them (all P2 <= 255); otherwise the u16 sum volume.
-  bool terms = !ranged;
+  // Waves keep byte terms when every match of the group allows them (all
+  // P2 <= 255); otherwise u16 sums only.
+  bool terms = true;
   for (const auto& mt : tiles) terms = terms && matches[mt.first]->m.term_u8 != 0;
   auto bytes = [&](int64_t cells, int64_t px, int64_t keys, int64_t rows, int maxnum) -> size_t {
-    return ranged ? sgm_path_ranged_buffers(cells, px, keys, rows, maxnum, sms).total
+    return ranged ? sgm_path_ranged_buffers(cells, px, keys, rows, maxnum, sms, terms).total
                   : sgm_path_buffers(cells, px, keys, terms).total;
   };
   std::vector<Entry> es;
@@ -1778,7 +1778,8 @@ r3dgpu_status r3dgpu_sgm_cost_volume_host(const r3dgpu_view_u16* left, const r3d
       wv.keys = 0;
       wv.rows = h;
       wv.maxnum = max_num;
-      W.scratch.reserve(sgm_path_ranged_buffers(wv.cells, px, 0, h, max_num, W.sms).total);
+      wv.terms = hm->term_u8;
+      W.scratch.reserve(sgm_path_ranged_buffers(wv.cells, px, 0, h, max_num, W.sms, wv.terms != 0).total);
       wv.buffer = W.scratch.get();
       launch_sgm_path_ranged_wave(dm, wv, W.sms, s);
       R3D_CUDA(cudaMemcpyAsync(out, vol, sizeof(uint16_t) * cells, cudaMemcpyDeviceToHost, s));

@@ -7,10 +7,13 @@
 // copies the maps back; another worker can meanwhile admit the requests that
 // arrived later, so batches overlap on the device (continuous batching).
 // Requests are admitted in arrival order: a request that does not fit waits
-// until running ones complete, and later ones wait behind it.
+// until running ones complete, and later ones wait behind it. Images that a
+// request names by content key are kept on the device in an LRU cache and
+// uploaded once while they stay cached.
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <list>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -50,6 +53,18 @@ struct Request {
   bool finished = false;
   int batch_size = 0;
   int worker = -1;
+  int cache_hits = 0;
+  uint64_t uploaded = 0;
+};
+
+// A device copy of a keyed input image.
+struct CacheEntry {
+  uint16_t* data = nullptr;  // width x height, dense rows
+  int width = 0, height = 0;
+  size_t bytes = 0;
+  int users = 0;                // batches reading it now
+  cudaEvent_t ready = nullptr;  // recorded after its upload
+  std::list<uint64_t>::iterator lru;
 };
 
 using RequestPtr = std::shared_ptr<Request>;
@@ -86,6 +101,93 @@ struct r3dgpu_server {
   int running = 0;
   bool stop = false;
   std::vector<std::thread> threads;
+  // Keyed image cache (its own lock: workers stage while others admit).
+  std::mutex cache_mu;
+  std::unordered_map<uint64_t, CacheEntry> cache;
+  std::list<uint64_t> lru;  // least recently used first
+  uint64_t cache_bytes = 0;
+
+  // The device copy of a keyed image for a batch on stream st, uploaded on
+  // st if it is not cached; `hit` tells which. Null when the image is not
+  // cached and cannot be (no key, no cache, a key seen with another size, or
+  // no room beside the images in use): the caller stages it itself.
+  const uint16_t* cache_acquire(uint64_t key, const r3dgpu_view_u16& v, cudaStream_t st, bool& hit) {
+    hit = false;
+    if (key == 0 || cfg.cache_budget == 0) return nullptr;
+    std::lock_guard<std::mutex> lk(cache_mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      CacheEntry& e = it->second;
+      if (e.width != v.width || e.height != v.height) return nullptr;
+      if (cudaStreamWaitEvent(st, e.ready, 0) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return nullptr;
+      }
+      ++e.users;
+      lru.splice(lru.end(), lru, e.lru);
+      hit = true;
+      return e.data;
+    }
+    const size_t bytes = 2 * static_cast<size_t>(v.width) * static_cast<size_t>(v.height);
+    if (bytes > cfg.cache_budget) return nullptr;
+    for (auto li = lru.begin(); cache_bytes + bytes > cfg.cache_budget && li != lru.end();) {
+      auto ci = cache.find(*li);
+      if (ci->second.users == 0) {
+        // cudaFree waits for the device; entries in use are never freed.
+        (void)cudaFree(ci->second.data);
+        (void)cudaEventDestroy(ci->second.ready);
+        cache_bytes -= ci->second.bytes;
+        cache.erase(ci);
+        li = lru.erase(li);
+      } else {
+        ++li;
+      }
+    }
+    if (cache_bytes + bytes > cfg.cache_budget) return nullptr;
+    CacheEntry e;
+    if (cudaMalloc(reinterpret_cast<void**>(&e.data), bytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return nullptr;
+    }
+    if (cudaEventCreateWithFlags(&e.ready, cudaEventDisableTiming) != cudaSuccess ||
+        cudaMemcpy2DAsync(e.data, 2 * static_cast<size_t>(v.width), v.data, 2 * static_cast<size_t>(v.stride),
+                          2 * static_cast<size_t>(v.width), v.height, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaEventRecord(e.ready, st) != cudaSuccess) {
+      (void)cudaGetLastError();
+      (void)cudaStreamSynchronize(st);
+      (void)cudaFree(e.data);
+      if (e.ready != nullptr) (void)cudaEventDestroy(e.ready);
+      return nullptr;
+    }
+    e.width = v.width;
+    e.height = v.height;
+    e.bytes = bytes;
+    e.users = 1;
+    e.lru = lru.insert(lru.end(), key);
+    cache_bytes += bytes;
+    const uint16_t* data = e.data;
+    cache.emplace(key, e);
+    return data;
+  }
+
+  void cache_release(const std::vector<uint64_t>& keys) {
+    std::lock_guard<std::mutex> lk(cache_mu);
+    for (uint64_t k : keys) {
+      auto it = cache.find(k);
+      if (it != cache.end() && it->second.users > 0) --it->second.users;
+    }
+  }
+
+  void cache_clear() {
+    std::lock_guard<std::mutex> lk(cache_mu);
+    for (auto& kv : cache) {
+      (void)cudaFree(kv.second.data);
+      (void)cudaEventDestroy(kv.second.ready);
+    }
+    cache.clear();
+    lru.clear();
+    cache_bytes = 0;
+  }
 
   bool can_admit() const {
     return !queue.empty() && (inflight == 0 || inflight + queue.front()->bytes <= cfg.hbm_budget);
@@ -94,6 +196,12 @@ struct r3dgpu_server {
   // Stages the batch's inputs in `io`, matches, copies the maps back.
   // Returns the batch call's status; the message is on this thread.
   r3dgpu_status run(std::vector<RequestPtr>& batch, cudaStream_t st, DeviceBuffer<unsigned char>& io) {
+    std::vector<uint64_t> used;  // cache entries this batch reads, released once it ran
+    struct Release {
+      r3dgpu_server* s;
+      std::vector<uint64_t>& keys;
+      ~Release() { s->cache_release(keys); }
+    } release{this, used};
     size_t total = 0;
     auto room = [](size_t n) { return (n + 255) & ~static_cast<size_t>(255); };
     for (const RequestPtr& r : batch) {
@@ -121,12 +229,29 @@ struct r3dgpu_server {
       const int wl = q.left.width, wr = q.right.width, h = q.left.height;
       r3dgpu_pair& d = pairs[i];
       d = as_pair(q);
-      auto* dl = reinterpret_cast<uint16_t*>(take(2 * static_cast<size_t>(wl) * h));
-      auto* dr = reinterpret_cast<uint16_t*>(take(2 * static_cast<size_t>(wr) * h));
-      if (cudaMemcpy2DAsync(dl, 2 * wl, q.left.data, 2 * q.left.stride, 2 * wl, h, cudaMemcpyHostToDevice, st) !=
-              cudaSuccess ||
-          cudaMemcpy2DAsync(dr, 2 * wr, q.right.data, 2 * q.right.stride, 2 * wr, h, cudaMemcpyHostToDevice, st) !=
-              cudaSuccess) {
+      Request& rq = *batch[i];
+      rq.cache_hits = 0;
+      rq.uploaded = 0;
+      // Each image: the cached device copy of its key, or a staged copy.
+      auto image = [&](uint64_t key, const r3dgpu_view_u16& v) -> const uint16_t* {
+        bool hit = false;
+        const uint16_t* c = cache_acquire(key, v, st, hit);
+        if (c != nullptr) {
+          used.push_back(key);
+          if (hit) ++rq.cache_hits;
+          else rq.uploaded += 2 * static_cast<uint64_t>(v.width) * v.height;
+          return c;
+        }
+        auto* dv = reinterpret_cast<uint16_t*>(take(2 * static_cast<size_t>(v.width) * v.height));
+        if (cudaMemcpy2DAsync(dv, 2 * static_cast<size_t>(v.width), v.data, 2 * static_cast<size_t>(v.stride),
+                              2 * static_cast<size_t>(v.width), v.height, cudaMemcpyHostToDevice, st) != cudaSuccess)
+          return nullptr;
+        rq.uploaded += 2 * static_cast<uint64_t>(v.width) * v.height;
+        return dv;
+      };
+      const uint16_t* dl = image(q.left_key, q.left);
+      const uint16_t* dr = dl != nullptr ? image(q.right_key, q.right) : nullptr;
+      if (dl == nullptr || dr == nullptr) {
         set_thread_error(std::string("server: image upload: ") + cudaGetErrorString(cudaGetLastError()));
         return R3DGPU_EDEVICE;
       }
@@ -360,6 +485,9 @@ r3dgpu_status r3dgpu_server_wait(r3dgpu_server* server, uint64_t ticket, double 
     times->device_bytes = r->bytes;
     times->batch_size = r->batch_size;
     times->worker = r->worker;
+    times->cache_hits = r->cache_hits;
+    times->reserved = 0;
+    times->uploaded_bytes = r->uploaded;
   }
   set_thread_error(r->error);
   return r->status;
@@ -379,6 +507,7 @@ r3dgpu_status r3dgpu_server_destroy(r3dgpu_server* server) {
   }
   server->work_cv.notify_all();
   for (auto& t : server->threads) t.join();
+  if (server->cfg.cache_budget != 0 && r3dgpu_set_device(server->cfg.device) == R3DGPU_OK) server->cache_clear();
   delete server;
   set_thread_error("");
   return R3DGPU_OK;

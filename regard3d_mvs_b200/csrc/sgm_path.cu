@@ -194,6 +194,12 @@ struct PathRing {
 
 // Three CTAs per SM for the 8-word shapes (80 registers, no spills); the
 // 12-word shapes keep two.
+//
+// The step loop is unrolled by the ring depth NS so that ring slots and the
+// intensity queue are indexed statically; each chain keeps running pointers
+// (advanced by one pixel along the path per step) instead of recomputing
+// addresses. The first pixel needs no special case: with a zero predecessor
+// vector and a zero minimum, best = 0, so T = 0 and L = C there.
 template <int G, int K, int MODE>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
@@ -203,9 +209,11 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   constexpr int CPW = 32 / G;  // chains per warp
   constexpr int U = K / 4;     // units of 8 labels per lane
   constexpr int NS = PathRing<G, K, MODE>::kStages;
-  constexpr bool kTerms = MODE == kTerm || MODE == kLastTerm;
   constexpr bool kReadsSum = MODE == kAccumulate || MODE == kLast;
   constexpr bool kWta = MODE == kLast || MODE == kLastTerm;
+  // K = 8: a lane's 16 labels are one 16-byte aligned piece of every plane.
+  constexpr bool kVec = K == 8;
+  constexpr int kAhead = 8;  // intensities are prefetched into L2 this many pixels ahead
   R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u);
   const int gi = lane / G, t = lane % G;
@@ -213,6 +221,11 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   const int left_lane = (lane + 31) & 31, right_lane = (lane + 1) & 31;
   const int wpb = static_cast<int>(blockDim.x) >> 5;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
+  using Ring = PathRing<G, K, MODE>;
+  unsigned char* const ring = smem + static_cast<size_t>(threadIdx.x >> 5) * Ring::kWarpBytes;
+  unsigned char* const ring_cost = ring + gi * Ring::ND + e0;
+  unsigned char* const ring_sum = ring + CPW * Ring::ND + gi * 2 * Ring::ND + 2 * e0;
+  unsigned char* const ring_term = ring + CPW * Ring::ND + gi * Ring::ND + e0;  // + r * CPW * ND
   for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + (threadIdx.x >> 5); blk < total_blocks; blk += nwarps) {
     if (cancelled(cancel)) break;
     const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
@@ -229,75 +242,91 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     bool uvalid[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) uvalid[u] = e0 + 8 * u < nd;
-    const uint8_t* cbase = cost + job.cell_off + e0;
-    uint16_t* sbase = sum + job.cell_off + e0;
-    uint8_t* tbase = terms + job.cell_off + e0;
-    const uint16_t* img = m.base + static_cast<int64_t>(job.y0) * m.base_stride + job.x0;
+    // Running offsets (cells, pixels) of the pixel being issued (NS - 1
+    // ahead) and of the pixel being computed.
+    const int64_t dcell = (static_cast<int64_t>(dy) * w + dx) * nd;
+    const int64_t dimg = static_cast<int64_t>(dy) * m.base_stride + dx;
+    const int64_t cell0 = job.cell_off + e0 + (static_cast<int64_t>(sy) * w + sx) * nd;
+    const uint8_t* c_in = cost + cell0;
+    const uint16_t* s_in = sum + cell0;
+    const uint8_t* t_in = terms + cell0;
+    uint16_t* s_out = sum + cell0;
+    uint8_t* t_out = terms + cell0 + static_cast<int64_t>(tslot) * tstride;
+    int64_t px_out = job.px_off + static_cast<int64_t>(sy) * w + sx;
+    const int64_t dpx = static_cast<int64_t>(dy) * w + dx;
+    const uint16_t* i_in = m.base + (static_cast<int64_t>(job.y0) + sy) * m.base_stride + job.x0 + sx;
+    int x = sx, y = sy;
 
-    // The bytes of the next NS - 1 pixels stream into the warp's
-    // shared-memory ring with cp.async (each lane copies and later reads only
-    // its own labels); intensities wait in a register queue.
-    using Ring = PathRing<G, K, MODE>;
-    unsigned char* ring = smem + static_cast<size_t>(threadIdx.x >> 5) * Ring::kWarpBytes;
-    auto stage_cost = [&](int st) -> unsigned char* { return ring + st * Ring::kStageBytes + gi * Ring::ND + e0; };
-    auto stage_sum = [&](int st) -> unsigned char* {
-      return ring + st * Ring::kStageBytes + CPW * Ring::ND + gi * 2 * Ring::ND + 2 * e0;
-    };
-    auto stage_term = [&](int st, int r) -> unsigned char* {
-      return ring + st * Ring::kStageBytes + (1 + r) * CPW * Ring::ND + gi * Ring::ND + e0;
-    };
-    auto slot = [](int i) { return NS == 4 ? (i & 3) : i % NS; };
-    auto issue = [&](int i) {
+    auto issue = [&](int i, int st) {
       if (i < len) {
-        const int x = sx + i * dx, y = sy + i * dy;
-        const int64_t cell = static_cast<int64_t>(y * w + x) * nd;
-        const int st = slot(i);
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          if (uvalid[u]) {
-            r3dsimt::cp_async8(stage_cost(st) + 8 * u, cbase + cell + 8 * u);
-            if constexpr (kReadsSum) r3dsimt::cp_async16(stage_sum(st) + 16 * u, sbase + cell + 8 * u);
+        unsigned char* rc = ring_cost + st * Ring::kStageBytes;
+        if constexpr (kVec) {
+          if (uvalid[0]) {
+            r3dsimt::cp_async16(rc, c_in);
+            if constexpr (kReadsSum) {
+              r3dsimt::cp_async16(ring_sum + st * Ring::kStageBytes, s_in);
+              r3dsimt::cp_async16(ring_sum + st * Ring::kStageBytes + 16, s_in + 8);
+            }
             if constexpr (MODE == kLastTerm) {
 #pragma unroll
               for (int r = 0; r < kTermArrays; ++r)
-                r3dsimt::cp_async8(stage_term(st, r) + 8 * u, tbase + r * tstride + cell + 8 * u);
+                r3dsimt::cp_async16(ring_term + st * Ring::kStageBytes + r * CPW * Ring::ND, t_in + r * tstride);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            if (uvalid[u]) {
+              r3dsimt::cp_async8(rc + 8 * u, c_in + 8 * u);
+              if constexpr (kReadsSum) r3dsimt::cp_async16(ring_sum + st * Ring::kStageBytes + 16 * u, s_in + 8 * u);
+              if constexpr (MODE == kLastTerm) {
+#pragma unroll
+                for (int r = 0; r < kTermArrays; ++r)
+                  r3dsimt::cp_async8(ring_term + st * Ring::kStageBytes + r * CPW * Ring::ND + 8 * u,
+                                     t_in + r * tstride + 8 * u);
+              }
             }
           }
         }
       }
       r3dsimt::cp_async_commit();
-    };
-    auto intensity = [&](int i) -> int {
-      if (i >= len) return 0;
-      return img[static_cast<int64_t>(sy + i * dy) * m.base_stride + sx + i * dx];
+      c_in += dcell;
+      if constexpr (kReadsSum) s_in += dcell;
+      if constexpr (MODE == kLastTerm) t_in += dcell;
     };
     int iq[NS];
 #pragma unroll
     for (int k = 0; k < NS - 1; ++k) {
-      issue(k);
-      iq[k] = intensity(k);
+      issue(k, k);
+      iq[k] = k < len ? i_in[k * dimg] : 0;
+      if (kAhead + k < len) r3dsimt::prefetch_l2(i_in + (kAhead + k) * dimg);
     }
+    const uint16_t* i_next = i_in + (NS - 1) * dimg;
     uint32_t prev[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) prev[k] = kSent2;
+    for (int k = 0; k < K; ++k) prev[k] = 0;
     uint32_t pmin = 0;
     int iprev = 0;
-    for (int i = 0; i < maxlen; ++i) {
+
+    auto step = [&](const int i, const int q) {
       const bool on = i < len;
-      issue(i + NS - 1);
-      iq[NS - 1] = intensity(i + NS - 1);
+      constexpr int kNext = NS - 1;
+      issue(i + kNext, (q + kNext) % NS);
+      iq[(q + kNext) % NS] = i + kNext < len ? *i_next : 0;
+      if (i + kNext + kAhead < len) r3dsimt::prefetch_l2(i_next + kAhead * dimg);
+      i_next += dimg;
       r3dsimt::cp_async_wait<NS - 1>();
-      const int icur = iq[0];
-      const int st = slot(i);
+      const int icur = iq[q];
+      const unsigned char* sc = ring_cost + q * Ring::kStageBytes;
       uint2 craw[U];
-      uint4 sraw[U];
+      if constexpr (kVec) {
+        const uint4 v = uvalid[0] ? *reinterpret_cast<const uint4*>(sc) : make_uint4(0, 0, 0, 0);
+        craw[0] = make_uint2(v.x, v.y);
+        craw[1] = make_uint2(v.z, v.w);
+      } else {
 #pragma unroll
-      for (int u = 0; u < U; ++u) {
-        craw[u] = uvalid[u] ? *reinterpret_cast<const uint2*>(stage_cost(st) + 8 * u) : make_uint2(0, 0);
-        if constexpr (kReadsSum)
-          sraw[u] = uvalid[u] ? *reinterpret_cast<const uint4*>(stage_sum(st) + 16 * u) : make_uint4(0, 0, 0, 0);
-        else
-          sraw[u] = make_uint4(0, 0, 0, 0);
+        for (int u = 0; u < U; ++u)
+          craw[u] = uvalid[u] ? *reinterpret_cast<const uint2*>(sc + 8 * u) : make_uint2(0, 0);
       }
       uint32_t c2[K];
 #pragma unroll
@@ -307,95 +336,109 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         c2[4 * u + 2] = r3dsimt::perm(craw[u].y, 0u, 0x4140u);
         c2[4 * u + 3] = r3dsimt::perm(craw[u].y, 0u, 0x4342u);
       }
-      // out = L_r = C + T_r, with T_r = best - min L(q) (0 at the chain's first pixel).
+      // out = L_r = C + T_r with T_r = best - min L(q).
+      const int dI = icur - iprev;
+      const uint32_t pen = pmin + m.lut[(dI < 0 ? -dI : dI) >> 8];
+      const uint32_t pen2 = pen | (pen << 16);
+      const uint32_t negmp = 0u - (pmin | (pmin << 16));
+      const uint32_t hl = r3dsimt::shfl(prev[K - 1], left_lane);
+      const uint32_t hr = r3dsimt::shfl(prev[0], right_lane);
+      uint32_t wv[K + 2];
+      wv[0] = t > 0 ? hl : kSent2;
+#pragma unroll
+      for (int k = 0; k < K; ++k) wv[1 + k] = prev[k];
+      wv[K + 1] = t + 1 < G ? hr : kSent2;
       uint32_t out[K], tr[K];
-      if (i == 0) {
-        // First pixel of the chain: no predecessor inside the tile, L = C.
+      uint32_t mprev = r3dsimt::perm(wv[0], wv[1], 0x5432u);
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-          tr[k] = 0;
-          out[k] = c2[k];
-        }
-      } else {
-        const int dI = icur - iprev;
-        const uint32_t pen = pmin + m.lut[(dI < 0 ? -dI : dI) >> 8];
-        const uint32_t pen2 = pen | (pen << 16);
-        const uint32_t negmp = 0u - (pmin | (pmin << 16));
-        const uint32_t hl = r3dsimt::shfl(prev[K - 1], left_lane);
-        const uint32_t hr = r3dsimt::shfl(prev[0], right_lane);
-        uint32_t wv[K + 2];
-        wv[0] = t > 0 ? hl : kSent2;
-#pragma unroll
-        for (int k = 0; k < K; ++k) wv[1 + k] = prev[k];
-        wv[K + 1] = t + 1 < G ? hr : kSent2;
-        uint32_t mprev = r3dsimt::perm(wv[0], wv[1], 0x5432u);
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          const uint32_t mnext = r3dsimt::perm(wv[k + 1], wv[k + 2], 0x5432u);
-          const uint32_t nb = r3dsimt::vmin2(mprev, mnext);
-          const uint32_t best = r3dsimt::vmin2(wv[k + 1], r3dsimt::vaddmin2(nb, p1x2, pen2));
-          tr[k] = best + negmp;
-          out[k] = tr[k] + c2[k];
-          mprev = mnext;
-        }
+      for (int k = 0; k < K; ++k) {
+        const uint32_t mnext = r3dsimt::perm(wv[k + 1], wv[k + 2], 0x5432u);
+        const uint32_t nb = r3dsimt::vmin2(mprev, mnext);
+        const uint32_t best = r3dsimt::vmin2(wv[k + 1], r3dsimt::vaddmin2(nb, p1x2, pen2));
+        tr[k] = best + negmp;
+        out[k] = tr[k] + c2[k];
+        mprev = mnext;
       }
-      uint32_t mk = kSent2;
+      // Minimum over the lane's labels (a tree), then over the chain's lanes.
+      uint32_t mm[K];
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         if (!uvalid[k / 4]) out[k] = kSent2;
-        mk = r3dsimt::vmin2(mk, out[k]);
+        mm[k] = out[k];
       }
-      pmin = group_umin<G>(r3dsimt::umin(mk & 0xFFFFu, mk >> 16));
-      const int x = sx + i * dx, y = sy + i * dy;
-      const int64_t cell = static_cast<int64_t>(y * w + x) * nd;
+#pragma unroll
+      for (int s = 1; s < K; s <<= 1) {
+#pragma unroll
+        for (int k = 0; k + s < K; k += 2 * s) mm[k] = r3dsimt::vmin2(mm[k], mm[k + s]);
+      }
+      pmin = group_umin<G>(r3dsimt::umin(mm[0] & 0xFFFFu, mm[0] >> 16));
       uint32_t s[K];
       if constexpr (MODE == kFirst) {
         if (on) {
 #pragma unroll
           for (int u = 0; u < U; ++u)
             if (uvalid[u])
-              r3dsimt::st_stream(reinterpret_cast<uint4*>(sbase + cell + 8 * u),
+              r3dsimt::st_stream(reinterpret_cast<uint4*>(s_out + 8 * u),
                                  make_uint4(out[4 * u], out[4 * u + 1], out[4 * u + 2], out[4 * u + 3]));
         }
       } else if constexpr (MODE == kTerm) {
         if (on) {
-          uint8_t* tout = tbase + tslot * tstride + cell;
+          if constexpr (kVec) {
+            if (uvalid[0])
+              r3dsimt::st_stream(reinterpret_cast<uint4*>(t_out),
+                                 make_uint4(r3dsimt::perm(tr[0], tr[1], 0x6420u), r3dsimt::perm(tr[2], tr[3], 0x6420u),
+                                            r3dsimt::perm(tr[4], tr[5], 0x6420u), r3dsimt::perm(tr[6], tr[7], 0x6420u)));
+          } else {
 #pragma unroll
-          for (int u = 0; u < U; ++u)
-            if (uvalid[u])
-              r3dsimt::st_stream8(reinterpret_cast<uint2*>(tout + 8 * u),
-                                  make_uint2(r3dsimt::perm(tr[4 * u], tr[4 * u + 1], 0x6420u),
-                                             r3dsimt::perm(tr[4 * u + 2], tr[4 * u + 3], 0x6420u)));
+            for (int u = 0; u < U; ++u)
+              if (uvalid[u])
+                r3dsimt::st_stream8(reinterpret_cast<uint2*>(t_out + 8 * u),
+                                    make_uint2(r3dsimt::perm(tr[4 * u], tr[4 * u + 1], 0x6420u),
+                                               r3dsimt::perm(tr[4 * u + 2], tr[4 * u + 3], 0x6420u)));
+          }
         }
       } else if constexpr (MODE == kLastTerm) {
         // S = L_8 + 7 C + sum of the seven byte terms (no halfword overflows).
 #pragma unroll
         for (int k = 0; k < K; ++k) s[k] = out[k] + 7u * c2[k];
+        const unsigned char* stt = ring_term + q * Ring::kStageBytes;
 #pragma unroll
         for (int r = 0; r < kTermArrays; ++r) {
+          uint2 tw[U];
+          if constexpr (kVec) {
+            const uint4 v = uvalid[0] ? *reinterpret_cast<const uint4*>(stt + r * CPW * Ring::ND)
+                                      : make_uint4(0, 0, 0, 0);
+            tw[0] = make_uint2(v.x, v.y);
+            tw[1] = make_uint2(v.z, v.w);
+          } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              tw[u] = uvalid[u] ? *reinterpret_cast<const uint2*>(stt + r * CPW * Ring::ND + 8 * u) : make_uint2(0, 0);
+          }
 #pragma unroll
           for (int u = 0; u < U; ++u) {
-            const uint2 tw = uvalid[u] ? *reinterpret_cast<const uint2*>(stage_term(st, r) + 8 * u) : make_uint2(0, 0);
-            s[4 * u + 0] += r3dsimt::perm(tw.x, 0u, 0x4140u);
-            s[4 * u + 1] += r3dsimt::perm(tw.x, 0u, 0x4342u);
-            s[4 * u + 2] += r3dsimt::perm(tw.y, 0u, 0x4140u);
-            s[4 * u + 3] += r3dsimt::perm(tw.y, 0u, 0x4342u);
+            s[4 * u + 0] += r3dsimt::perm(tw[u].x, 0u, 0x4140u);
+            s[4 * u + 1] += r3dsimt::perm(tw[u].x, 0u, 0x4342u);
+            s[4 * u + 2] += r3dsimt::perm(tw[u].y, 0u, 0x4140u);
+            s[4 * u + 3] += r3dsimt::perm(tw[u].y, 0u, 0x4342u);
           }
         }
       } else {
+        const unsigned char* ss = ring_sum + q * Ring::kStageBytes;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          s[4 * u + 0] = add2(sraw[u].x, out[4 * u + 0], no_carry);
-          s[4 * u + 1] = add2(sraw[u].y, out[4 * u + 1], no_carry);
-          s[4 * u + 2] = add2(sraw[u].z, out[4 * u + 2], no_carry);
-          s[4 * u + 3] = add2(sraw[u].w, out[4 * u + 3], no_carry);
+          const uint4 sraw = uvalid[u] ? *reinterpret_cast<const uint4*>(ss + 16 * u) : make_uint4(0, 0, 0, 0);
+          s[4 * u + 0] = add2(sraw.x, out[4 * u + 0], no_carry);
+          s[4 * u + 1] = add2(sraw.y, out[4 * u + 1], no_carry);
+          s[4 * u + 2] = add2(sraw.z, out[4 * u + 2], no_carry);
+          s[4 * u + 3] = add2(sraw.w, out[4 * u + 3], no_carry);
         }
         if constexpr (MODE == kAccumulate) {
           if (on) {
 #pragma unroll
             for (int u = 0; u < U; ++u)
               if (uvalid[u])
-                r3dsimt::st_stream(reinterpret_cast<uint4*>(sbase + cell + 8 * u),
+                r3dsimt::st_stream(reinterpret_cast<uint4*>(s_out + 8 * u),
                                    make_uint4(s[4 * u], s[4 * u + 1], s[4 * u + 2], s[4 * u + 3]));
           }
         }
@@ -439,11 +482,10 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         const uint32_t sp = (kp & 1) ? (vp >> 16) : (vp & 0xFFFFu);
         if (on) {
           if (t == 0)
-            info[job.px_off + static_cast<int64_t>(y) * w + x] =
-                make_int4(static_cast<int>(static_cast<uint32_t>(kb) | (bcost << 16)),
-                          static_cast<int>(sec | (sm << 16)), static_cast<int>(sp), 0);
+            info[px_out] = make_int4(static_cast<int>(static_cast<uint32_t>(kb) | (bcost << 16)),
+                                     static_cast<int>(sec | (sm << 16)), static_cast<int>(sp), 0);
           if (job.volume != nullptr) {
-            uint16_t* vb = job.volume + cell + e0;
+            uint16_t* vb = job.volume + (static_cast<int64_t>(y) * w + x) * nd + e0;
 #pragma unroll
             for (int u = 0; u < U; ++u)
               if (uvalid[u])
@@ -470,12 +512,21 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         }
       }
       (void)s;
-      (void)kTerms;
 #pragma unroll
       for (int k = 0; k < K; ++k) prev[k] = out[k];
       iprev = icur;
+      if constexpr (MODE == kFirst || MODE == kAccumulate) s_out += dcell;
+      if constexpr (MODE == kTerm) t_out += dcell;
+      if constexpr (kWta) {
+        px_out += dpx;
+        x += dx;
+        y += dy;
+      }
+    };
+    for (int i0 = 0; i0 < maxlen; i0 += NS) {
 #pragma unroll
-      for (int k = 0; k + 1 < NS; ++k) iq[k] = iq[k + 1];
+      for (int q = 0; q < NS; ++q)
+        if (i0 + q < maxlen) step(i0 + q, q);
     }
     r3dsimt::cp_async_wait<0>();
   }
@@ -660,13 +711,17 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 constexpr int kRangedSmemWords = 32;
 constexpr int kRangedSmemStride = kRangedSmemWords + 1;
 
-template <int G, int K>
+// Ring of the ranged passes: D stages of chunk 0's bytes (kPlanes bytes per
+// label: cost, plus the u16 sum or the seven byte terms) and 2 D record slots.
+template <int G, int K, int MODE>
 struct RangedRing {
   static constexpr int CH = 2 * G * K;  // labels per chunk
   static constexpr int CPW = 32 / G;
-  static constexpr int kDataStage = CPW * 3 * CH;
-  static constexpr int kData = kPathStages * kDataStage;
-  static constexpr int kRec = 2 * kPathStages * 32 * 16;  // one record slot per lane and stage
+  static constexpr int D = MODE == kLastTerm ? 2 : kPathStages;
+  static constexpr int kPlanes = MODE == kAccumulate ? 3 : (MODE == kLastTerm ? 1 + kTermArrays : 1);
+  static constexpr int kDataStage = CPW * kPlanes * CH;
+  static constexpr int kData = D * kDataStage;
+  static constexpr int kRec = 2 * D * 32 * 16;  // one record slot per lane and stage
   static constexpr int kPrev = CPW * 2 * kRangedSmemStride * 4;
   static constexpr int kWarpBytes = kData + kRec + kPrev;
   static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
@@ -676,10 +731,14 @@ template <int G, int K, int MODE>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     sgm_path_ranged_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
                            int cls, int dx, int dy, int64_t total_blocks, const int4* R3D_RESTRICT rec,
-                           const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words,
-                           const int* cancel) {
-  using R = RangedRing<G, K>;
-  constexpr int CPW = R::CPW, U = K / 4, CH = R::CH, D = kPathStages;
+                           const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint8_t* terms, int64_t tstride,
+                           int tslot, uint32_t* ovf, int64_t ovf_words, const int* cancel) {
+  // Modes: kFirst / kAccumulate write or add u16 sums; kTerm writes the
+  // pass's byte terms; kLastTerm writes S = L_8 + 7 C + sum of the seven
+  // terms as the u16 sum (read by the per-pixel winner-takes-all).
+  using R = RangedRing<G, K, MODE>;
+  constexpr int CPW = R::CPW, U = K / 4, CH = R::CH, D = R::D;
+  constexpr bool kReadsSum = MODE == kAccumulate;
   R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u), warp = static_cast<int>(threadIdx.x >> 5);
   const int gi = lane / G, t = lane % G;
@@ -694,6 +753,9 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
   auto stage_cost = [&](int st) -> unsigned char* { return wb + st * R::kDataStage + gi * CH + e0; };
   auto stage_sum = [&](int st) -> unsigned char* {
     return wb + st * R::kDataStage + CPW * CH + gi * 2 * CH + 2 * e0;
+  };
+  auto stage_term = [&](int st, int r) -> unsigned char* {
+    return wb + st * R::kDataStage + (1 + r) * CPW * CH + gi * CH + e0;
   };
   // Word idx (labels 2 idx, 2 idx + 1) of buffer b of the predecessor vector
   // (nw words long): two sentinels outside it.
@@ -723,6 +785,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     for (int o = G; o < 32; o <<= 1) maxlen = r3dsimt::imax(maxlen, static_cast<int>(r3dsimt::shfl_xor(maxlen, o)));
     const uint8_t* cbase = cost + job.cell_off;
     uint16_t* sbase = sum + job.cell_off;
+    uint8_t* tbase = terms + job.cell_off;
     const int4* rbase = rec + job.px_off;
     auto pix = [&](int i) -> int { return (sy + i * dy) * w + sx + i * dx; };
     auto issue_rec = [&](int i) {
@@ -736,7 +799,12 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
       for (int u = 0; u < U; ++u) {
         if (e0 + 8 * u < num) {
           r3dsimt::cp_async8(stage_cost(st) + 8 * u, cbase + off + e0 + 8 * u);
-          if constexpr (MODE != kFirst) r3dsimt::cp_async16(stage_sum(st) + 16 * u, sbase + off + e0 + 8 * u);
+          if constexpr (kReadsSum) r3dsimt::cp_async16(stage_sum(st) + 16 * u, sbase + off + e0 + 8 * u);
+          if constexpr (MODE == kLastTerm) {
+#pragma unroll
+            for (int r = 0; r < kTermArrays; ++r)
+              r3dsimt::cp_async8(stage_term(st, r) + 8 * u, tbase + r * tstride + off + e0 + 8 * u);
+          }
         }
       }
     };
@@ -782,6 +850,9 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
         for (int u = 0; u < U; ++u) uv[u] = j0 + 8 * u < num;
         uint2 craw[U];
         uint4 sraw[U];
+        uint32_t tsum[K];  // kLastTerm: sum of the seven byte terms per label pair
+#pragma unroll
+        for (int k = 0; k < K; ++k) tsum[k] = 0;
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           craw[u] = make_uint2(0, 0);
@@ -790,11 +861,22 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
             if (c == 0) {
               const int st = i & (D - 1);
               craw[u] = *reinterpret_cast<const uint2*>(stage_cost(st) + 8 * u);
-              if constexpr (MODE != kFirst) sraw[u] = *reinterpret_cast<const uint4*>(stage_sum(st) + 16 * u);
+              if constexpr (kReadsSum) sraw[u] = *reinterpret_cast<const uint4*>(stage_sum(st) + 16 * u);
             } else {
               craw[u] = *reinterpret_cast<const uint2*>(cbase + off + j0 + 8 * u);
-              if constexpr (MODE != kFirst)
+              if constexpr (kReadsSum)
                 sraw[u] = r3dsimt::ld_stream(reinterpret_cast<const uint4*>(sbase + off + j0 + 8 * u));
+            }
+            if constexpr (MODE == kLastTerm) {
+#pragma unroll
+              for (int r = 0; r < kTermArrays; ++r) {
+                const uint2 tw = c == 0 ? *reinterpret_cast<const uint2*>(stage_term(i & (D - 1), r) + 8 * u)
+                                        : *reinterpret_cast<const uint2*>(tbase + r * tstride + off + j0 + 8 * u);
+                tsum[4 * u + 0] += r3dsimt::perm(tw.x, 0u, 0x4140u);
+                tsum[4 * u + 1] += r3dsimt::perm(tw.x, 0u, 0x4342u);
+                tsum[4 * u + 2] += r3dsimt::perm(tw.y, 0u, 0x4140u);
+                tsum[4 * u + 3] += r3dsimt::perm(tw.y, 0u, 0x4342u);
+              }
             }
           }
         }
@@ -806,10 +888,13 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
           c2[4 * u + 2] = r3dsimt::perm(craw[u].y, 0u, 0x4140u);
           c2[4 * u + 3] = r3dsimt::perm(craw[u].y, 0u, 0x4342u);
         }
-        uint32_t out[K];
+        uint32_t out[K], tr[K];
         if (i == 0) {
 #pragma unroll
-          for (int k = 0; k < K; ++k) out[k] = c2[k];
+          for (int k = 0; k < K; ++k) {
+            tr[k] = 0;
+            out[k] = c2[k];
+          }
         } else {
           // Predecessor labels j0 + sh - 2 .. j0 + sh + 2 K + 1 (its own
           // indexing), sentinels outside its range, realigned by one label
@@ -833,7 +918,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
             const uint32_t mnext = r3dsimt::perm(wv[k + 1], wv[k + 2], 0x5432u);
             const uint32_t nb = r3dsimt::vmin2(mprev, mnext);
             const uint32_t best = r3dsimt::vmin2(wv[k + 1], r3dsimt::vaddmin2(nb, p1x2, pen2));
-            out[k] = best + c2[k] + negmp;
+            tr[k] = best + negmp;
+            out[k] = tr[k] + c2[k];
             mprev = mnext;
           }
         }
@@ -846,9 +932,20 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (!uv[u]) continue;
+          if constexpr (MODE == kTerm) {
+            r3dsimt::st_stream8(reinterpret_cast<uint2*>(tbase + tslot * tstride + off + j0 + 8 * u),
+                                make_uint2(r3dsimt::perm(tr[4 * u], tr[4 * u + 1], 0x6420u),
+                                           r3dsimt::perm(tr[4 * u + 2], tr[4 * u + 3], 0x6420u)));
+            continue;
+          }
           uint4 v;
           if constexpr (MODE == kFirst) {
             v = make_uint4(out[4 * u], out[4 * u + 1], out[4 * u + 2], out[4 * u + 3]);
+          } else if constexpr (MODE == kLastTerm) {
+            v = make_uint4(out[4 * u] + 7u * c2[4 * u] + tsum[4 * u],
+                           out[4 * u + 1] + 7u * c2[4 * u + 1] + tsum[4 * u + 1],
+                           out[4 * u + 2] + 7u * c2[4 * u + 2] + tsum[4 * u + 2],
+                           out[4 * u + 3] + 7u * c2[4 * u + 3] + tsum[4 * u + 3]);
           } else {
             v = make_uint4(add2(sraw[u].x, out[4 * u], no_carry), add2(sraw[u].y, out[4 * u + 1], no_carry),
                            add2(sraw[u].z, out[4 * u + 2], no_carry), add2(sraw[u].w, out[4 * u + 3], no_carry));
@@ -1104,6 +1201,7 @@ SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys, boo
   o += align256(static_cast<size_t>(cells));
   b.sum = o;
   b.term_stride = terms ? static_cast<int64_t>(align256(static_cast<size_t>(cells))) : 0;
+  b.terms = b.sum;
   o += terms ? static_cast<size_t>(kTermArrays) * static_cast<size_t>(b.term_stride)
              : align256(static_cast<size_t>(cells) * 2);
   b.info = o;
@@ -1119,7 +1217,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
   const SgmPathBuffers B = sgm_path_buffers(wave.cells, wave.pixels, wave.keys, wave.terms != 0);
   uint8_t* cost = wave.buffer + B.cost;
   uint16_t* sum = reinterpret_cast<uint16_t*>(wave.buffer + B.sum);
-  uint8_t* terms = wave.terms != 0 ? wave.buffer + B.sum : nullptr;
+  uint8_t* terms = wave.terms != 0 ? wave.buffer + B.terms : nullptr;
   int4* info = reinterpret_cast<int4*>(wave.buffer + B.info);
   uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
   if (wave.keys > 0) R3D_CUDA(cudaMemsetAsync(rkeys, 0xFF, static_cast<size_t>(wave.keys) * 4, s));
@@ -1165,11 +1263,12 @@ constexpr int kRangedMaxPerSm = 4;
 
 template <int G, int K, int MODE>
 void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
-                        const int4* rec, const uint8_t* cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words,
-                        int sms, cudaStream_t s, const SgmPathSegment& seg, const int* cancel) {
+                        const int4* rec, const uint8_t* cost, uint16_t* sum, uint8_t* terms, int64_t tstride,
+                        int tslot, uint32_t* ovf, int64_t ovf_words, int sms, cudaStream_t s, const SgmPathSegment& seg,
+                        const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_ranged_kernel<G, K, MODE>;
-  constexpr size_t smem = RangedRing<G, K>::kBlockBytes;
+  constexpr size_t smem = RangedRing<G, K, MODE>::kBlockBytes;
   static thread_local int configured[64] = {};
   int dev = 0;
   R3D_CUDA(cudaGetDevice(&dev));
@@ -1180,30 +1279,42 @@ void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jo
   int grid = resident_grid(k, sms, nb, kPathThreads / 32, smem);
   grid = grid < sms * kRangedMaxPerSm ? grid : sms * kRangedMaxPerSm;
   R3D_LAUNCH(k, dim3(grid), dim3(kPathThreads), smem, s, dm, jobs, njobs, ps.cls, ps.dx, ps.dy, nb, rec, cost, sum,
-             ovf, ovf_words, cancel);
+             terms, tstride, tslot, ovf, ovf_words, cancel);
   launched("sgm_path_ranged_kernel");
   if (ev0 != nullptr) {
     char shape[32];
     std::snprintf(shape, sizeof(shape), "%dx%d/mode%d", G, K, MODE);
     // Per pixel and pass also the 16-byte record (range and cell offset).
+    const uint64_t alg = MODE == kLastTerm ? (1 + kTermArrays + 2) * static_cast<uint64_t>(seg.cells)
+                                           : pass_bytes(MODE, true, seg);
     profile_pass(ev0, profile_mark(s), "sgm_path_ranged_kernel", shape, static_cast<uint64_t>(seg.cells),
-                 static_cast<uint64_t>(seg.pixels), pass_bytes(MODE, true, seg) + 16 * static_cast<uint64_t>(seg.pixels));
+                 static_cast<uint64_t>(seg.pixels), alg + 16 * static_cast<uint64_t>(seg.pixels));
   }
 }
 
 template <int G, int K>
 void launch_ranged_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const int4* rec,
-                          const uint8_t* cost, uint16_t* sum, uint32_t* ovf, int64_t ovf_words, int sms,
-                          cudaStream_t s, const int* cancel) {
+                          const uint8_t* cost, uint16_t* sum, uint8_t* terms, int64_t tstride, uint32_t* ovf,
+                          int64_t ovf_words, int sms, cudaStream_t s, const int* cancel) {
   for (int q = 0; q < 8; ++q) {
     const Pass ps = kPasses[q];
     const int64_t nb = g.blocks[ps.cls];
     if (nb <= 0) continue;
-    if (q == 0)
-      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g, cancel);
-    else
-      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, rec, cost, sum, ovf, ovf_words, sms, s, g,
-                                            cancel);
+    if (terms != nullptr) {
+      // Byte terms: passes 1..7 write T_r, the last writes the total sum.
+      if (q < 7)
+        launch_ranged_pass<G, K, kTerm>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, q, ovf, ovf_words,
+                                        sms, s, g, cancel);
+      else
+        launch_ranged_pass<G, K, kLastTerm>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, 0, ovf,
+                                            ovf_words, sms, s, g, cancel);
+    } else if (q == 0) {
+      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, 0, ovf, ovf_words,
+                                       sms, s, g, cancel);
+    } else {
+      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, 0, ovf,
+                                            ovf_words, sms, s, g, cancel);
+    }
   }
 }
 
@@ -1220,9 +1331,14 @@ SgmPathShape sgm_path_ranged_shape(int over32, int64_t pixels) {
 }
 
 SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
-                                       int sms) {
+                                       int sms, bool terms) {
   SgmPathBuffers b = sgm_path_buffers(cells, pixels, keys, false);
   size_t o = b.total;
+  // Byte terms of the ranged passes come in addition to the u16 sum (which
+  // the last pass writes for the per-pixel winner-takes-all).
+  b.terms = o;
+  b.term_stride = terms ? static_cast<int64_t>(align256(static_cast<size_t>(cells))) : 0;
+  o += static_cast<size_t>(kTermArrays) * static_cast<size_t>(b.term_stride);
   b.rec = o;
   o += align256(static_cast<size_t>(pixels) * 16);
   b.rowsum = o;
@@ -1242,9 +1358,11 @@ SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t ke
 
 void launch_sgm_path_ranged_wave(const SgmMatch* dm, const SgmPathRangedWave& wave, int sms, cudaStream_t s) {
   if (wave.njobs <= 0 || wave.pixels <= 0) return;
-  const SgmPathBuffers B = sgm_path_ranged_buffers(wave.cells, wave.pixels, wave.keys, wave.rows, wave.maxnum, sms);
+  const SgmPathBuffers B =
+      sgm_path_ranged_buffers(wave.cells, wave.pixels, wave.keys, wave.rows, wave.maxnum, sms, wave.terms != 0);
   uint8_t* cost = wave.buffer + B.cost;
   uint16_t* sum = reinterpret_cast<uint16_t*>(wave.buffer + B.sum);
+  uint8_t* terms = wave.terms != 0 ? wave.buffer + B.terms : nullptr;
   int4* info = reinterpret_cast<int4*>(wave.buffer + B.info);
   uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
   int4* rec = reinterpret_cast<int4*>(wave.buffer + B.rec);
@@ -1269,9 +1387,11 @@ void launch_sgm_path_ranged_wave(const SgmMatch* dm, const SgmPathRangedWave& wa
     const SgmPathSegment& g = wave.segs[q];
     const SgmPathJob* jobs = wave.jobs + g.first;
     if (g.shape.g_ == 2 && g.shape.k_ == 8)
-      launch_ranged_passes<2, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s, wave.cancel);
+      launch_ranged_passes<2, 8>(dm, jobs, g, rec, cost, sum, terms, B.term_stride, ovf, B.overflow_words, sms, s,
+                                 wave.cancel);
     else if (g.shape.g_ == 4 && g.shape.k_ == 8)
-      launch_ranged_passes<4, 8>(dm, jobs, g, rec, cost, sum, ovf, B.overflow_words, sms, s, wave.cancel);
+      launch_ranged_passes<4, 8>(dm, jobs, g, rec, cost, sum, terms, B.term_stride, ovf, B.overflow_words, sms, s,
+                                 wave.cancel);
     else
       fail(R3DGPU_EINVAL, "stereo: bad ranged path kernel shape");
   }

@@ -48,11 +48,11 @@ SgmPathShape sgm_path_shape(int nd);
 inline bool sgm_path_fits(int w, int nd) { return w + nd - 1 <= 2048; }
 inline int64_t sgm_path_chains(int cls, int w, int h) { return cls == 0 ? h : (cls == 1 ? w : w + h - 1); }
 
-// Device buffers of a wave (bytes, 256-byte aligned pieces). With `terms`
-// the u16 sum volume is replaced by seven byte-term arrays of term_stride
-// bytes each (starting at `sum`).
+// Device buffers of a wave (bytes, 256-byte aligned pieces). Byte terms:
+// seven arrays of term_stride bytes from `terms` on (full-range waves keep
+// them in place of the u16 sum volume, ranged waves beside it).
 struct SgmPathBuffers {
-  size_t cost, sum, info, rkeys, total;
+  size_t cost, sum, terms, info, rkeys, total;
   int64_t term_stride;
   size_t rec, rowsum, rowstart, rowshift, overflow;  // ranged waves only
   int64_t overflow_words;                            // per chain buffer
@@ -108,10 +108,10 @@ struct SgmPathRangedWave {
   int maxnum;  // largest label count of a pixel of the wave
   unsigned char* buffer;
   const int* cancel;  // device view of the caller's cancellation flag, or null
-  int terms;          // full-range waves: byte terms (every match of the wave has term_u8)
+  int terms;          // byte terms (every match of the wave has term_u8)
 };
 SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
-                                       int sms);
+                                       int sms, bool terms);
 void launch_sgm_path_ranged_wave(const SgmMatch* dm, const SgmPathRangedWave& wave, int sms, cudaStream_t s);
 bool sgm_path_ranged_enabled();
 

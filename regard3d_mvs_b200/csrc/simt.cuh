@@ -68,6 +68,8 @@ R3D_DEVICE void cp_async8(void* smem_dst, const void* gmem_src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
+// Hint: bring the line holding p into L2 (no register, no wait).
+R3D_DEVICE void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 R3D_DEVICE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 R3D_DEVICE void cp_async_wait() {
@@ -180,6 +182,7 @@ void cp_async16(void* smem_dst, const void* gmem_src);
 void cp_async8(void* smem_dst, const void* gmem_src);
 void cp_async_commit();
 void cp_async_wait_n(int n);
+inline void prefetch_l2(const void*) {}
 template <int N>
 inline void cp_async_wait() {
   cp_async_wait_n(N);

@@ -255,3 +255,169 @@ def pipeline_scene(w: int, h: int, f: float, partners, seed: int = 0, plane=None
                           right={"width": w, "height": h, "fx": K[0, 0], "fy": K[1, 1], "cx": rp["cx_right"],
                                  "cy": K[1, 2]}))
     return rig, base, pairs
+
+
+# ---------------------------------------------------------------- an arc of views around textured planes
+# A multi-view scene of the full depth stage: n pinhole views on a circular
+# arc of radius `radius_m` (2 m) spanning `arc_deg` (neighbours about 3 degrees
+# apart for 32 views, so the 4 nearest partners see a pixel under 3 to 7
+# degrees, around the combination's minimum triangulation angle) looking at
+# the scene centre,
+# and `planes` textured rectangles: a back wall behind the centre (so every
+# ray meets a surface) and random rectangles in front of it. Every rectangle
+# carries its own texture made like the matcher's synthetic pairs: uniform
+# noise, Gaussian-blurred with sigma 1.5 texels and stretched to 0..255,
+# sampled bilinearly (wrapping) at `texel_m` per texel (by default about
+# one texel per pixel at the centre's distance, 1.1 mm for 2048 pixels). Each view gets its
+# image (u8, Gaussian noise sigma 2 added), its true depth, and its
+# `partners` nearest views on the arc with the pair rectification, disparity
+# range and combination geometry that compute_depth_map takes ("image" is
+# the 8-bit image lifted to 16 bits, v * 257, as the matcher reads 8-bit
+# files; "image8" the 8-bit one). Rendering
+# runs in torch on `device` (CPU or CUDA); numbers other than the images are
+# float64 numpy.
+
+
+def _noise_texture(rng, size: int) -> np.ndarray:
+    t = rng.random((size, size))
+    r = np.arange(-5, 6)
+    k = np.exp(-0.5 * (r / 1.5) ** 2)
+    k /= k.sum()
+    for axis in (0, 1):
+        t = np.apply_along_axis(lambda v: np.convolve(np.concatenate([v[-5:], v, v[:5]]), k, mode="valid"), axis, t)
+    t = (t - t.min()) / max(t.max() - t.min(), 1e-12) * 255.0
+    return t.astype(np.float32)
+
+
+def _look_at(c, target, up=(0.0, 1.0, 0.0)):
+    z = np.asarray(target, np.float64) - c
+    z /= np.linalg.norm(z)
+    x = np.cross(np.asarray(up, np.float64), z)
+    x /= np.linalg.norm(x)
+    return np.stack([x, np.cross(z, x), z])
+
+
+def arc_scene(n_views: int = 32, width: int = 2048, height: int = 1536, planes: int = 20, partners: int = 4,
+              seed: int = 0, arc_deg: float = 100.0, radius_m: float = 2.0, texel_m: float | None = None, device=None,
+              label_margin: int = 8) -> dict:
+    import torch
+
+    dev = torch.device(device or "cpu")
+    rng = np.random.default_rng(seed)
+    f = 0.9 * width
+    if texel_m is None:
+        texel_m = radius_m / f  # about one texel per pixel at the scene centre's distance
+    K = np.array([[f, 0.0, (width - 1) / 2.0], [0.0, f, (height - 1) / 2.0], [0.0, 0.0, 1.0]])
+    centre = np.zeros(3)
+    # Rectangles: centre p, in-plane axes e1, e2 (unit), half sizes.
+    rects = [(np.array([0.0, 0.0, 1.2]), np.array([1.0, 0.0, 0.0]), np.array([0.0, 1.0, 0.0]), 12.0, 9.0)]
+    while len(rects) < planes:
+        p = rng.uniform([-0.6, -0.45, -0.6], [0.6, 0.45, 0.6])
+        n = np.array([rng.uniform(-0.6, 0.6), rng.uniform(-0.5, 0.5), -1.0])
+        n /= np.linalg.norm(n)
+        a = rng.uniform(0.0, np.pi)
+        e1 = np.cross(n, [0.0, 1.0, 0.0])
+        e1 /= np.linalg.norm(e1)
+        e2 = np.cross(n, e1)
+        e1, e2 = np.cos(a) * e1 + np.sin(a) * e2, -np.sin(a) * e1 + np.cos(a) * e2
+        rects.append((p, e1, e2, rng.uniform(0.1, 0.35), rng.uniform(0.1, 0.35)))
+    tex_size = 512
+    textures = torch.from_numpy(np.stack([_noise_texture(rng, tex_size) for _ in rects])).to(dev)
+    span = np.deg2rad(arc_deg)
+    cams = []
+    for i in range(n_views):
+        a = -span / 2 + span * i / max(1, n_views - 1)
+        c = np.array([radius_m * np.sin(a), 0.03 * radius_m * np.sin(5.0 * a + 0.3), -radius_m * np.cos(a)])
+        cams.append({"K": K, "R": _look_at(c, centre), "C": c, "width": width, "height": height})
+
+    ys, xs = torch.meshgrid(torch.arange(height, device=dev, dtype=torch.float64),
+                            torch.arange(width, device=dev, dtype=torch.float64), indexing="ij")
+    pix = torch.stack([xs, ys, torch.ones_like(xs)], -1)
+    noise_rng = torch.Generator(device="cpu").manual_seed(seed + 1)
+
+    def render(cam):
+        m = torch.from_numpy(cam["R"].T @ np.linalg.inv(K)).to(dev)
+        d = pix @ m.T  # world directions, unit depth along the optical axis
+        C = torch.from_numpy(cam["C"]).to(dev)
+        best_t = torch.full((height, width), float("inf"), dtype=torch.float64, device=dev)
+        best_i = torch.full((height, width), -1, dtype=torch.int64, device=dev)
+        best_u = torch.zeros_like(best_t)
+        best_v = torch.zeros_like(best_t)
+        for k, (p, e1, e2, hw, hh) in enumerate(rects):
+            n = np.cross(e1, e2)
+            nt = torch.from_numpy(n).to(dev)
+            den = d @ nt
+            t = (float(n @ p) - float(n @ cam["C"])) / den
+            pts = C + t[..., None] * d - torch.from_numpy(p).to(dev)
+            u = pts @ torch.from_numpy(e1).to(dev)
+            v = pts @ torch.from_numpy(e2).to(dev)
+            hit = (t > 0) & (u.abs() <= hw) & (v.abs() <= hh) & (t < best_t)
+            best_t = torch.where(hit, t, best_t)
+            best_i = torch.where(hit, torch.full_like(best_i, k), best_i)
+            best_u = torch.where(hit, u, best_u)
+            best_v = torch.where(hit, v, best_v)
+        # Bilinear texture sample with wrap-around.
+        tu = (best_u / texel_m) % tex_size
+        tv = (best_v / texel_m) % tex_size
+        u0, v0 = torch.floor(tu).long(), torch.floor(tv).long()
+        fu, fv = (tu - u0).float(), (tv - v0).float()
+        u1, v1 = (u0 + 1) % tex_size, (v0 + 1) % tex_size
+        ti = best_i.clamp(min=0)
+        flat = textures.reshape(len(rects), -1)
+
+        def tap(vv, uu):
+            return flat[ti, vv * tex_size + uu]
+
+        val = ((1 - fu) * (1 - fv) * tap(v0, u0) + fu * (1 - fv) * tap(v0, u1) + (1 - fu) * fv * tap(v1, u0) +
+               fu * fv * tap(v1, u1))
+        noise = torch.randn((height, width), generator=noise_rng).to(dev) * 2.0
+        img = torch.clamp(torch.round(val + noise), 0, 255).to(torch.uint8)
+        img = torch.where(best_i >= 0, img, torch.zeros_like(img))
+        # Depth along the optical axis (d has unit depth).
+        return img.cpu().numpy(), best_t.float().cpu().numpy()
+
+    views = []
+    for cam in cams:
+        img, depth = render(cam)
+        views.append({"camera": cam, "image8": img, "image": img.astype(np.uint16) * np.uint16(257), "depth": depth})
+    ys_np, xs_np = np.mgrid[0:height, 0:width].astype(np.float64)
+    sub = (slice(None, None, 8), slice(None, None, 8))
+    for i, v in enumerate(views):
+        order = sorted((j for j in range(n_views) if j != i), key=lambda j: (abs(j - i), j))[:partners]
+        base = v["camera"]
+        # 3-D points of a sub-grid of the view (true depths) for the disparity ranges.
+        dirs = np.stack([xs_np[sub], ys_np[sub], np.ones_like(xs_np[sub])], -1) @ (base["R"].T @ np.linalg.inv(K)).T
+        pts = base["C"] + v["depth"][sub].astype(np.float64)[..., None] * dirs
+        pairs = []
+        for j in order:
+            other = views[j]["camera"]
+            b = other["C"] - base["C"]
+            x = b / np.linalg.norm(b)
+            z_mean = base["R"][2] + other["R"][2]
+            z_mean /= np.linalg.norm(z_mean)
+            y = np.cross(z_mean, x)
+            y /= np.linalg.norm(y)
+            R_rect = np.stack([x, y, np.cross(x, y)])
+            K_rect = K.copy()
+            q = (pts - base["C"]) @ R_rect.T
+            xl = f * q[..., 0] / q[..., 2] + K_rect[0, 2]
+            d_true = f * np.linalg.norm(b) / q[..., 2]
+            inside = (q[..., 2] > 0) & (xl >= 0) & (xl < width)
+            d_true = d_true[inside]
+            # The right camera's principal point moves the disparities to start near label_margin.
+            cx_right = K_rect[0, 2] - (label_margin - float(np.percentile(d_true, 0.5)))
+            offset = K_rect[0, 2] - cx_right
+            lo, hi = np.percentile(d_true, 0.5) + offset, np.percentile(d_true, 99.5) + offset
+            dmin = int(np.floor(lo)) - label_margin
+            nd = (int(np.ceil(hi)) + label_margin - dmin + 1 + 15) // 16 * 16
+            pairs.append({"K_rect": K_rect, "R_rect": R_rect, "baseline": float(np.linalg.norm(b)),
+                          "cx_right": cx_right, "centre": other["C"], "partner": j,
+                          "image": views[j]["image"], "R_partner": other["R"], "disparity_min": dmin,
+                          "num_disparities": nd,
+                          "left": {"width": width, "height": height, "fx": f, "fy": f, "cx": K_rect[0, 2],
+                                   "cy": K_rect[1, 2]},
+                          "right": {"width": width, "height": height, "fx": f, "fy": f, "cx": cx_right,
+                                    "cy": K_rect[1, 2]}})
+        v["pairs"] = pairs
+        v["partners"] = order
+    return {"views": views, "K": K}

@@ -20,7 +20,7 @@ from typing import Iterable, Sequence
 import numpy as np
 
 from . import _native
-from .types import (CDisparityMap, COptions, CPair, CRequestTimes, CServerConfig, CViewU8, CViewU16, DisparityMap,
+from .types import (CDisparityMap, COptions, CPair, CRequest, CRequestTimes, CServerConfig, CViewU8, CViewU16, DisparityMap,
                     LabelRanges, StereoOptions, to_c_options)
 
 
@@ -569,23 +569,27 @@ class Server:
     Requests run in continuous batches on `workers` CUDA streams; the
     estimated device memory of the admitted requests stays within
     `hbm_budget` bytes. Each result equals Matcher.match_stereo on the same
-    pair, whatever else ran beside it.
+    pair, whatever else ran beside it. With `cache_budget` > 0, images
+    submitted with a content key (left_key / right_key) stay on the device
+    and are uploaded once while cached.
     """
 
     def __init__(self, lib_path: str | None = None, device: int = 0, workers: int = 2, max_batch: int = 16,
-                 hbm_budget: int = 64 << 30, scratch_budget: int = 0):
+                 hbm_budget: int = 64 << 30, scratch_budget: int = 0, cache_budget: int = 0):
         self.lib = _native.load(lib_path)
-        cfg = CServerConfig(device, workers, max_batch, 0, hbm_budget, scratch_budget)
+        cfg = CServerConfig(device, workers, max_batch, 0, hbm_budget, scratch_budget, cache_budget)
         h = ctypes.c_void_p()
         _native.check(self.lib, self.lib.r3dgpu_server_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self._live: dict[int, tuple] = {}  # ticket -> (request, host arrays it points into)
 
     def submit(self, left, right, left_valid=None, right_valid=None, disparity_min: int = 0,
-               num_disparities: int = 64, options: StereoOptions | None = None, out=None) -> int:
+               num_disparities: int = 64, options: StereoOptions | None = None, out=None, left_key: int = 0,
+               right_key: int = 0) -> int:
         """Queues a pair. `out` = (disparity, confidence or None): caller-owned
         float32 arrays of the left image's shape (page-locked memory makes the
-        copies asynchronous); by default both are allocated here."""
+        copies asynchronous); by default both are allocated here. A nonzero
+        key promises that every request with that key has the same image."""
         L, R = _u16(left), _u16(right)
         lv = None if left_valid is None else np.ascontiguousarray(left_valid, dtype=np.uint8)
         rv = None if right_valid is None else np.ascontiguousarray(right_valid, dtype=np.uint8)
@@ -597,7 +601,8 @@ class Server:
             for a in (disp, conf):
                 if a is not None and (a.shape != (h, w) or a.dtype != np.float32 or not a.flags.c_contiguous):
                     raise _native.StereoError(1, "server: output arrays must be contiguous float32 of the image shape")
-        req = CPair()
+        req = CRequest()
+        req.left_key, req.right_key = int(left_key), int(right_key)
         req.left, req.right = _view16(L), _view16(R)
         req.left_valid, req.right_valid = _view8(lv), _view8(rv)
         req.disparity_min, req.num_disparities = int(disparity_min), int(num_disparities)
@@ -618,7 +623,8 @@ class Server:
         _native.check(self.lib, st)
         disp, conf = arrays[4], arrays[5]
         times = {"queued_ms": t.queued_ms, "run_ms": t.run_ms, "total_ms": t.total_ms,
-                 "device_bytes": int(t.device_bytes), "batch_size": t.batch_size, "worker": t.worker}
+                 "device_bytes": int(t.device_bytes), "batch_size": t.batch_size, "worker": t.worker,
+                 "cache_hits": t.cache_hits, "uploaded_bytes": int(t.uploaded_bytes)}
         return DisparityMap(disp, conf, req.out.disparity_min, req.out.num_disparities, req.out.levels,
                             int(req.out.cells)), times
 

@@ -250,7 +250,14 @@ class CServerConfig(ctypes.Structure):
         ("reserved", ctypes.c_int32),
         ("hbm_budget", ctypes.c_uint64),
         ("scratch_budget", ctypes.c_uint64),
+        ("cache_budget", ctypes.c_uint64),
     ]
+
+
+class CRequest(ctypes.Structure):
+    """r3dgpu_request: the fields of r3dgpu_pair, then the images' content keys."""
+
+    _fields_ = CPair._fields_ + [("left_key", ctypes.c_uint64), ("right_key", ctypes.c_uint64)]
 
 
 class CRequestTimes(ctypes.Structure):
@@ -261,6 +268,9 @@ class CRequestTimes(ctypes.Structure):
         ("device_bytes", ctypes.c_uint64),
         ("batch_size", ctypes.c_int32),
         ("worker", ctypes.c_int32),
+        ("cache_hits", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("uploaded_bytes", ctypes.c_uint64),
     ]
 
 

@@ -99,3 +99,29 @@ def test_destroy_finishes_queued_requests(pairs, alone):
     srv.close()
     for a, d in zip(alone, outs):
         assert same_disparities(d, a.disparity)
+
+
+def test_keyed_images_are_uploaded_once(pairs, alone):
+    """Requests that share a keyed left image (a view's partner pairs): the
+    image goes to the device once and stays cached; every result equals the
+    pair matched alone, and a cache too small for an image falls back to
+    staging it."""
+    p = pairs[0]
+    shifted = [dict(p, right=np.roll(p["right"], s, axis=1)) for s in (0, 1, 2)]
+    ref = [alone[0]] + [None, None]
+    with Server(SIMT_LIB, workers=2, max_batch=1, hbm_budget=1 << 30, cache_budget=1 << 20) as srv:
+        first = srv.wait(srv.submit(**shifted[0], left_key=7))
+        rest = [srv.wait(srv.submit(**q, left_key=7)) for q in shifted[1:]]
+    _same(first[0], ref[0])
+    assert first[1]["cache_hits"] == 0
+    assert all(t["cache_hits"] == 1 for _, t in rest)
+    nbytes = p["left"].size * 2
+    assert all(t["uploaded_bytes"] == nbytes for _, t in rest)  # the right image only
+    with Server(SIMT_LIB, workers=1, max_batch=1, hbm_budget=1 << 30) as srv:
+        plain = [srv.wait(srv.submit(**q)) for q in shifted[1:]]
+    for (a, _), (b, _) in zip(rest, plain):
+        _same(a, b)
+    with Server(SIMT_LIB, workers=1, max_batch=1, hbm_budget=1 << 30, cache_budget=16) as srv:
+        m, t = srv.wait(srv.submit(**shifted[0], left_key=7))
+    _same(m, ref[0])
+    assert t["cache_hits"] == 0 and t["uploaded_bytes"] == 2 * nbytes
