@@ -274,6 +274,9 @@ class Pinned {
     for (unsigned char* p : retired_) cudaFreeHost(p);
     retired_.clear();
   }
+  // Hands the replaced blocks to a caller that still needs them (a captured
+  // graph copies from them on every replay); it frees them with cudaFreeHost.
+  std::vector<unsigned char*> take_retired() { return std::move(retired_); }
 
  private:
   unsigned char* p_ = nullptr;
@@ -1305,6 +1308,106 @@ bool batch_tracks_enabled() {
   return e == nullptr || std::atoi(e) != 1;
 }
 
+#ifndef R3DGPU_SIMT_EMULATION
+// The single-level track of a two-track batch as a CUDA graph. The track
+// enqueues without any host synchronisation (its layouts depend on sizes and
+// options only), so its whole enqueue -- job tables copied from pinned host
+// memory, every launch on the track and side streams, the cell counts copied
+// back -- is captured once per batch description and replayed while the same
+// description comes again: the same pairs (buffers, sizes, options; not
+// their output fields), device, cancellation flag, scratch budget and kernel
+// selection. Between replays nothing else uses the track's workspace (slot
+// 1), so the captured pinned tables and device buffers stay as captured.
+// R3DGPU_GRAPH=0 enqueues the track on every call.
+struct TrackGraph {
+  std::string key;
+  cudaGraphExec_t exec = nullptr;
+  BatchRun run;
+  uint64_t launches = 0;
+  std::vector<unsigned char*> pinned;  // pinned blocks the graph copies from, replaced during its capture
+  void clear() {
+    if (exec != nullptr) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    for (unsigned char* p : pinned) cudaFreeHost(p);
+    pinned.clear();
+    key.clear();
+  }
+  ~TrackGraph() { clear(); }
+};
+thread_local std::vector<std::unique_ptr<TrackGraph>> t_track_graphs;
+
+bool track_graph_enabled() {
+  const char* e = std::getenv("R3DGPU_GRAPH");
+  return !t_prof.on && (e == nullptr || std::atoi(e) != 0);
+}
+
+std::string track_key(const std::vector<r3dgpu_pair>& fp) {
+  std::string k;
+  for (r3dgpu_pair p : fp) {
+    p.out.disparity_min = 0;
+    p.out.num_disparities = 0;
+    p.out.levels = 0;
+    p.out.reserved = 0;
+    p.out.cells = 0;
+    k.append(reinterpret_cast<const char*>(&p), sizeof(p));
+  }
+  const int* c = cancel_device_flag();
+  k.append(reinterpret_cast<const char*>(&c), sizeof(c));
+  k.append(reinterpret_cast<const char*>(&t_device), sizeof(t_device));
+  k.append(reinterpret_cast<const char*>(&t_scratch_budget), sizeof(t_scratch_budget));
+  for (const char* name : {"R3DGPU_FULL_KERNEL", "R3DGPU_RANGED_KERNEL", "R3DGPU_RANGED_GENERAL_WIDTH"}) {
+    const char* v = std::getenv(name);
+    k += v != nullptr ? v : "";
+    k += '\n';
+  }
+  return k;
+}
+
+TrackGraph& track_graph() {
+  const int idx = t_device;
+  if (static_cast<int>(t_track_graphs.size()) <= idx) t_track_graphs.resize(idx + 1);
+  if (!t_track_graphs[idx]) t_track_graphs[idx] = std::make_unique<TrackGraph>();
+  return *t_track_graphs[idx];
+}
+
+// Enqueues the single-level track on `track`: the captured graph of the same
+// description, or a fresh capture of enqueue_batch.
+BatchRun enqueue_track(std::vector<r3dgpu_pair>& fp, cudaStream_t track) {
+  TrackGraph& g = track_graph();
+  std::string key = track_key(fp);
+  if (g.exec == nullptr || g.key != key) {
+    R3D_CUDA(cudaStreamSynchronize(track));  // a previous replay may still read the blocks freed here
+    g.clear();
+    const uint64_t l0 = launch_counter().load();
+    R3D_CUDA(cudaStreamBeginCapture(track, cudaStreamCaptureModeRelaxed));
+    BatchRun run;
+    cudaGraph_t graph = nullptr;
+    try {
+      run = enqueue_batch(fp.data(), static_cast<int>(fp.size()), track, 1);
+    } catch (...) {
+      (void)cudaStreamEndCapture(track, &graph);
+      if (graph != nullptr) (void)cudaGraphDestroy(graph);
+      (void)cudaGetLastError();
+      throw;
+    }
+    R3D_CUDA(cudaStreamEndCapture(track, &graph));
+    g.pinned = run.W->pinned.take_retired();
+    const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    (void)cudaGraphDestroy(graph);
+    R3D_CUDA(e);
+    g.launches = launch_counter().load() - l0;
+    g.run = run;
+    g.key = std::move(key);
+  } else {
+    launch_counter().fetch_add(g.launches, std::memory_order_relaxed);
+  }
+  R3D_CUDA(cudaGraphLaunch(g.exec, track));
+  BatchRun run = g.run;
+  for (size_t i = 0; i < run.runs.size(); ++i) run.runs[i].req = &fp[i];
+  return run;
+}
+#endif
+
 // Runs a batch of pairs to completion on stream s. The levels of a batch run
 // in rounds (every pair's coarsest level first); when single-level pairs
 // share the batch with hierarchical ones, the single-level pairs form a
@@ -1354,7 +1457,12 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
   R3D_CUDA(cudaStreamWaitEvent(W1.track, W1.track_start, 0));
   BatchRun a, b;
   try {
-    a = enqueue_batch(fp.data(), static_cast<int>(fp.size()), W1.track, 1);
+#ifndef R3DGPU_SIMT_EMULATION
+    if (track_graph_enabled())
+      a = enqueue_track(fp, W1.track);
+    else
+#endif
+      a = enqueue_batch(fp.data(), static_cast<int>(fp.size()), W1.track, 1);
     R3D_CUDA(cudaEventRecord(W1.track_done, W1.track));
     b = enqueue_batch(hp.data(), static_cast<int>(hp.size()), s, 0);
   } catch (...) {
@@ -1493,6 +1601,9 @@ void r3dgpu_set_cancel_token(r3dgpu_cancel_token* token) { t_cancel = token; }
 
 r3dgpu_status r3dgpu_release_workspace(void) {
   return guarded([&] {
+#ifndef R3DGPU_SIMT_EMULATION
+    if (t_device < static_cast<int>(t_track_graphs.size())) t_track_graphs[t_device].reset();
+#endif
     for (int slot = 0; slot < kWorkspaceSlots; ++slot) {
       const int idx = t_device * kWorkspaceSlots + slot;
       if (idx < static_cast<int>(t_workspaces.size()) && t_workspaces[idx]) {

@@ -830,9 +830,9 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
       const int4 rc = recs[(i & (2 * D - 1)) * 32 + lane];
       const int off = rc.x, lo = rc.y & 0xFFFF, icur = rc.z;
       const int num = on ? static_cast<int>(static_cast<uint32_t>(rc.y) >> 16) : 0;
-      int nchw = (num + CH - 1) / CH;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) nchw = r3dsimt::imax(nchw, static_cast<int>(r3dsimt::shfl_xor(nchw, o)));
+      // Chunks of this pixel's range: the same for the chain's G lanes (one
+      // pixel), and the chunk loop holds no warp-wide operation.
+      const int nchw = (num + CH - 1) / CH;
       const int sh = lo - lo_q, nwq = num_q >> 1;
       const int cur = i & 1, prv = cur ^ 1;
       uint32_t pen2 = 0, negmp = 0;

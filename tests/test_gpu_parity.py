@@ -356,3 +356,59 @@ def test_config2_pairs_batched(gpu_matcher, oracle):
     for p, got in zip(pairs, batch):
         ref = oracle.match_stereo(p["left"], p["right"], None, None, 0, p["num_disparities"], p["options"])
         _assert_same_map(got, ref)
+
+
+def _device_batch(gpu_matcher, specs):
+    """The r3dgpu_pair array of `specs` over device-resident torch buffers
+    (stable pointers from call to call), and a reader of the maps."""
+    import ctypes
+
+    import torch
+
+    from regard3d_mvs_b200.types import CDisparityMap, CPair, CViewU8, CViewU16, to_c_options
+
+    keep, pairs = [], (CPair * len(specs))()
+    for i, (left, right, nd, opts) in enumerate(specs):
+        h, w = left.shape
+        dl = torch.from_numpy(left.view(np.int16)).cuda()
+        dr = torch.from_numpy(right.view(np.int16)).cuda()
+        dd = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        dc = torch.empty_like(dd)
+        keep += [dl, dr, dd, dc]
+        p = pairs[i]
+        p.left, p.right = CViewU16(dl.data_ptr(), w, h, w), CViewU16(dr.data_ptr(), w, h, w)
+        p.left_valid, p.right_valid = CViewU8(), CViewU8()
+        p.disparity_min, p.num_disparities = 0, nd
+        p.options = to_c_options(opts)
+        p.out = CDisparityMap(dd.data_ptr(), dc.data_ptr(), w, 0, 0, 0, 0, 0)
+
+    def run():
+        st = gpu_matcher.lib.r3dgpu_match_stereo_batch(pairs, len(specs), ctypes.c_void_p(0))
+        assert st == 0, gpu_matcher.lib.r3dgpu_last_error().decode()
+        torch.cuda.synchronize()
+        return [(keep[4 * i + 2].cpu().numpy().copy(), keep[4 * i + 3].cpu().numpy().copy(), int(pairs[i].out.cells))
+                for i in range(len(specs))]
+
+    return run, keep
+
+
+def test_single_level_track_graph_replays(gpu_matcher, monkeypatch):
+    """A batch mixing single-level and hierarchical pairs: its single-level
+    track is captured as a CUDA graph on the first call and replayed on the
+    next ones; every call's maps and cell counts equal those of the track
+    enqueued directly (R3DGPU_GRAPH=0)."""
+    specs = []
+    for i, (w, h, nd, lv) in enumerate(((320, 240, 64, 0), (256, 200, 128, 2), (400, 300, 96, 0), (96, 64, 32, 0))):
+        left, right = _synthetic_pair(w, h, nd, 30 + i)
+        specs.append((left, right, nd, StereoOptions(levels=lv)))
+    run, _ = _device_batch(gpu_matcher, specs)
+    monkeypatch.setenv("R3DGPU_GRAPH", "0")
+    want = run()
+    monkeypatch.delenv("R3DGPU_GRAPH")
+    before = gpu_matcher.launch_count()
+    got = [run() for _ in range(3)]  # capture, then two replays
+    assert gpu_matcher.launch_count() > before
+    for g in got:
+        for (d0, c0, n0), (d1, c1, n1) in zip(want, g):
+            assert np.array_equal(d0.view(np.uint32), d1.view(np.uint32))
+            assert np.array_equal(c0, c1) and n0 == n1
