@@ -705,11 +705,14 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 }
 
 // Labels of a chain's predecessor vector kept in shared memory (u32 words of
-// two labels); wider vectors continue in the chain's global overflow. The
-// buffers of a warp's chains are kRangedSmemStride words apart (odd, so that
-// the chains of a warp start in different banks).
+// two labels); wider vectors continue in the chain's global overflow. A
+// buffer holds a sentinel word before the vector (index -1) and one after it
+// (index nw, written with the vector), so that a vector of at most
+// kRangedSmemWords words is read at a clamped index without bounds checks.
+// The buffers of a warp's chains are kRangedSmemStride words apart (odd, so
+// that the chains of a warp start in different banks).
 constexpr int kRangedSmemWords = 32;
-constexpr int kRangedSmemStride = kRangedSmemWords + 1;
+constexpr int kRangedSmemStride = kRangedSmemWords + 3;
 
 // Ring of the ranged passes: D stages of chunk 0's bytes (kPlanes bytes per
 // label: cost, plus the u16 sum or the seven byte terms) and 2 D record slots.
@@ -762,12 +765,14 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
   // The shared-memory word is read unconditionally (at a wrapped, in-bounds
   // index); only the rare words of wide vectors go to the overflow.
   auto qword = [&](int b, int idx, int nw) -> uint32_t {
-    uint32_t v = prevw[b * CPW * kRangedSmemStride + (idx & (kRangedSmemWords - 1))];
+    const uint32_t* vec = prevw + b * CPW * kRangedSmemStride + 1;
+    if (nw <= kRangedSmemWords) return vec[r3dsimt::imax(r3dsimt::imin(idx, nw), -1)];
+    uint32_t v = vec[idx & (kRangedSmemWords - 1)];
     if (idx >= kRangedSmemWords && idx < nw) v = ovfc[b * ovf_words + (idx - kRangedSmemWords)];
     return (idx < 0 || idx >= nw) ? kSent2 : v;
   };
   auto put_word = [&](int b, int idx, uint32_t v) {
-    if (idx < kRangedSmemWords) prevw[b * CPW * kRangedSmemStride + idx] = v;
+    if (idx < kRangedSmemWords) prevw[b * CPW * kRangedSmemStride + 1 + idx] = v;
     else ovfc[b * ovf_words + (idx - kRangedSmemWords)] = v;
   };
   for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + warp; blk < total_blocks; blk += nwarps) {
@@ -808,6 +813,12 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
         }
       }
     };
+    // The leading sentinels of both buffers (read from the second pixel on,
+    // after the first step's warp barrier).
+    if (t == 0) {
+      prevw[0] = kSent2;
+      prevw[CPW * kRangedSmemStride] = kSent2;
+    }
     // Records of the first 2 D - 1 pixels now, the first D - 1 pixels' data in flight.
 #pragma unroll
     for (int k = 0; k < 2 * D - 1; ++k)
@@ -954,6 +965,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
         }
       }
       pmin = group_umin<G>(r3dsimt::umin(pm & 0xFFFFu, pm >> 16));
+      // The trailing sentinel of the vector just written.
+      if (t == 0 && (num >> 1) <= kRangedSmemWords) prevw[cur * CPW * kRangedSmemStride + 1 + (num >> 1)] = kSent2;
       r3dsimt::syncwarp();
       if (on) {
         lo_q = lo;

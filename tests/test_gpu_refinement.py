@@ -59,7 +59,13 @@ def test_float_path_close_to_oracle(gpu_matcher, oracle, scene):
     assert abs(ia["refined"] - ib["refined"]) <= max(3, ib["input"] // 1000)
     flips, rel = agreement(a, b, ia, ib)
     assert flips <= 1e-3
-    assert np.percentile(rel, 99) <= 1e-6 and rel.max() <= 1e-4, (np.percentile(rel, 99), rel.max())
+    # The target relative depth error of the FP32 refinement is 1e-5; it holds
+    # for 999 pixels in 1000. The rest are pixels whose last step's gain lies
+    # within float rounding of the acceptance threshold, where the two paths
+    # take one step more or less (bounded by the step size, below 1e-4).
+    assert np.percentile(rel, 99) <= 1e-6 and np.percentile(rel, 99.9) <= 1e-5, \
+        (np.percentile(rel, 99), np.percentile(rel, 99.9))
+    assert rel.max() <= 1e-4, rel.max()
 
 
 def test_unrelated_views(gpu_matcher, oracle, scene):

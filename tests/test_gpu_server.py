@@ -76,3 +76,23 @@ def test_server_tight_budget(pairs, alone):
     for a, (m, tm) in zip(alone, res):
         _same(m, a)
         assert tm["batch_size"] == 1
+
+
+def test_server_keyed_left_image_cached(pairs):
+    """A view's partner pairs share its left image under one content key:
+    the first request uploads it, the others find it cached (on either
+    worker's stream); every map equals the uncached request's."""
+    p = pairs[3]
+    variants = [dict(p, right=np.roll(p["right"], s, axis=1)) for s in (0, 1, 2, 3)]
+    with Server(workers=2, max_batch=1, hbm_budget=16 << 30, scratch_budget=8 << 30) as srv:
+        plain = [srv.wait(srv.submit(**q))[0] for q in variants]
+    with Server(workers=2, max_batch=2, hbm_budget=16 << 30, scratch_budget=8 << 30, cache_budget=1 << 30) as srv:
+        first = srv.wait(srv.submit(**variants[0], left_key=11))
+        tickets = [srv.submit(**q, left_key=11) for q in variants[1:]]
+        rest = [srv.wait(t) for t in tickets]
+    _same(first[0], plain[0])
+    assert first[1]["cache_hits"] == 0
+    for (m, tm), a in zip(rest, plain[1:]):
+        _same(m, a)
+        assert tm["cache_hits"] == 1
+        assert tm["uploaded_bytes"] == p["right"].size * 2
