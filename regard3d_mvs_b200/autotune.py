@@ -5,15 +5,16 @@ The objective is the SGM stage time (fork to join of every round, from the
 library's CUDA-event profile) of a mixed batch drawn like the batched
 workload: pairs of uneven size (width log-uniform in 1024..6048), label
 counts from {64, 128, 192, 256, 384}, half of them hierarchical. The search
-is coordinate-wise: the full-range kernel's (lanes per row G, label pairs per
-lane K, band rows; shapes up to 1.5x the label count) for each label count,
-largest share first, then the ranged
-kernel's band rows per label width and the share of wide pixels a tile may
-keep; a candidate replaces the current entry when it shortens the stage by
-more than 1 %. The table is written only where it beats the built-in
-defaults on the same batch.
+is coordinate-wise, largest label count first: the chain passes' shape
+(lanes per chain G, label pairs per lane K; rows of up to 1.5x the label
+count) for each label count; with --plain also the one-CTA-per-tile kernels'
+shapes and band rows, the ranged kernel's band rows per label width and the
+share of wide pixels a tile may keep. A candidate replaces the current entry
+when it shortens the stage by more than 1 %; the table is written only where
+it beats the built-in defaults on the same batch, and entries of the kinds
+not searched are kept from the existing table.
 
-    python -m regard3d_mvs_b200.autotune [--out regard3d_mvs_b200/tuning_b200.txt] [--pairs 24]
+    python -m regard3d_mvs_b200.autotune [--out regard3d_mvs_b200/tuning_b200.txt] [--pairs 24] [--plain]
 """
 
 from __future__ import annotations
@@ -32,6 +33,8 @@ from .types import CDisparityMap, CPair, CProfile, CSynthParams, CViewU8, CViewU
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 FULL_SHAPES = ((8, 4), (8, 8), (16, 4), (8, 12), (16, 6), (16, 8), (8, 16), (16, 12), (32, 8), (32, 12))
+PATH_SHAPES = ((2, 16), (4, 8), (4, 12), (4, 16), (8, 8), (8, 12), (8, 16), (16, 8), (16, 12), (16, 16), (32, 8),
+               (32, 12))
 FULL_ND = (384, 256, 192, 128, 64)
 ROWS = (64, 48, 32, 24, 16)
 ND_CHOICES = (64, 128, 192, 256, 384)
@@ -98,55 +101,70 @@ def main():
     ap.add_argument("--out", default=os.path.join(HERE, "tuning_b200.txt"))
     ap.add_argument("--pairs", type=int, default=24)
     ap.add_argument("--seed", type=int, default=77)
+    ap.add_argument("--plain", action="store_true", help="also tune the one-CTA-per-tile kernels")
     args = ap.parse_args()
     import torch
 
     t0 = time.time()
+    searched = {"path"} | ({"full", "ranged", "ranged_wide_frac"} if args.plain else set())
+    kept = []
+    if os.path.exists(args.out):
+        with open(args.out) as f:
+            for ln in f:
+                body = ln.split("#", 1)[0].strip()
+                if body and body.split()[0] not in searched:
+                    kept.append(body)
     bench = Bench(mixed_specs(args.pairs, args.seed), seed=args.seed)
-    bench.stage_ms([], reps=1)  # allocations
-    base = bench.stage_ms([], reps=3)
+    bench.stage_ms(kept, reps=1)  # allocations
+    base = bench.stage_ms(kept, reps=3)
     print(f"defaults: {base:.1f} ms", flush=True)
-    full: dict[int, str] = {}
-    ranged: dict[str, str] = {}
+    entries: dict[str, str] = {}
 
-    def table(extra_full=None, extra_ranged=None):
-        f = {**full, **(extra_full or {})}
-        r = {**ranged, **(extra_ranged or {})}
-        return list(f.values()) + list(r.values())
+    def table(extra=None):
+        return kept + list({**entries, **(extra or {})}.values())
 
     best = base
     for nd in FULL_ND:
-        for g, k in (s for s in FULL_SHAPES if nd <= 2 * s[0] * s[1] <= 1.5 * nd):
-            for rows in ROWS:
-                entry = f"full {nd} {g} {k} {rows}"
-                ms = bench.stage_ms(table({nd: entry}))
-                print(f"{entry}: {ms:.1f} ms", flush=True)
-                if ms < best * 0.99:
-                    best, full[nd] = ms, entry
-    for width in (32, 64, 128):
-        for rows in ROWS:
-            entry = f"ranged {width} {rows}"
-            ms = bench.stage_ms(table(extra_ranged={f"r{width}": entry}))
+        for g, k in (s for s in PATH_SHAPES if nd <= 2 * s[0] * s[1] <= 1.5 * nd):
+            entry = f"path {nd} {g} {k}"
+            ms = bench.stage_ms(table({f"p{nd}": entry}))
             print(f"{entry}: {ms:.1f} ms", flush=True)
             if ms < best * 0.99:
-                best, ranged[f"r{width}"] = ms, entry
-    for frac in (0.0005, 0.001, 0.004, 0.008):
-        entry = f"ranged_wide_frac {frac}"
-        ms = bench.stage_ms(table(extra_ranged={"frac": entry}))
-        print(f"{entry}: {ms:.1f} ms", flush=True)
-        if ms < best * 0.99:
-            best, ranged["frac"] = ms, entry
+                best, entries[f"p{nd}"] = ms, entry
+    if args.plain:
+        for nd in FULL_ND:
+            for g, k in (s for s in FULL_SHAPES if nd <= 2 * s[0] * s[1] <= 1.5 * nd):
+                for rows in ROWS:
+                    entry = f"full {nd} {g} {k} {rows}"
+                    ms = bench.stage_ms(table({f"f{nd}": entry}))
+                    print(f"{entry}: {ms:.1f} ms", flush=True)
+                    if ms < best * 0.99:
+                        best, entries[f"f{nd}"] = ms, entry
+        for width in (32, 64, 128):
+            for rows in ROWS:
+                entry = f"ranged {width} {rows}"
+                ms = bench.stage_ms(table({f"r{width}": entry}))
+                print(f"{entry}: {ms:.1f} ms", flush=True)
+                if ms < best * 0.99:
+                    best, entries[f"r{width}"] = ms, entry
+        for frac in (0.0005, 0.001, 0.004, 0.008):
+            entry = f"ranged_wide_frac {frac}"
+            ms = bench.stage_ms(table({"frac": entry}))
+            print(f"{entry}: {ms:.1f} ms", flush=True)
+            if ms < best * 0.99:
+                best, entries["frac"] = ms, entry
     final = table()
-    check_tuned, check_base = bench.stage_ms(final, reps=3), bench.stage_ms([], reps=3)
-    keep = final if final and check_tuned < check_base else []
-    verdict = ("" if keep else " (no candidate beat the defaults by more than 1 %: defaults kept)" if not final
-               else " (not better: defaults kept)")
+    check_tuned, check_base = bench.stage_ms(final, reps=3), bench.stage_ms(kept, reps=3)
+    keep = final if entries and check_tuned < check_base else kept
+    verdict = ("" if keep is final else " (no candidate beat the defaults by more than 1 %: defaults kept)"
+               if not entries else " (not better: defaults kept)")
     name = torch.cuda.get_device_name(0)
     with open(args.out, "w") as f:
         f.write(f"# SGM launch shapes chosen by regard3d_mvs_b200/autotune.py on {name} ({time.time() - t0:.0f} s):\n")
         f.write(f"# SGM stage of a {args.pairs}-pair mixed batch: defaults {check_base:.1f} ms, "
                 f"this table {check_tuned:.1f} ms{verdict}\n")
-        f.write("# fields: full <nd> <G> <K> <rows> | ranged <width> <rows> | ranged_wide_frac <f>\n")
+        f.write("# fields: path <nd> <G> <K> | full <nd> <G> <K> <rows> | ranged <width> <rows> | "
+                "ranged_wide_frac <f> | ranged_general_width <w>\n")
         for ln in keep:
             f.write(ln + "\n")
     print(f"wrote {args.out}: defaults {check_base:.1f} ms, tuned {check_tuned:.1f} ms", flush=True)

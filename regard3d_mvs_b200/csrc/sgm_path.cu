@@ -31,6 +31,7 @@
 #include "common.cuh"
 #include "sgm_path.h"
 #include "sgm_simd.cuh"
+#include "tuning.h"
 
 namespace r3dgpu {
 
@@ -193,7 +194,7 @@ struct PathRing {
 };
 
 // Three CTAs per SM for the 8-word shapes (80 registers, no spills); the
-// 12-word shapes keep two.
+// 12- and 16-word shapes keep two.
 //
 // The step loop is unrolled by the ring depth NS so that ring slots and the
 // intensity queue are indexed statically; each chain keeps running pointers
@@ -211,8 +212,11 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   constexpr int NS = PathRing<G, K, MODE>::kStages;
   constexpr bool kReadsSum = MODE == kAccumulate || MODE == kLast;
   constexpr bool kWta = MODE == kLast || MODE == kLastTerm;
-  // K = 8: a lane's 16 labels are one 16-byte aligned piece of every plane.
-  constexpr bool kVec = K == 8;
+  // K a multiple of 8: a lane's 2 K labels are NV 16-byte aligned pieces of
+  // every byte plane (piece v = units 2 v, 2 v + 1, valid together since
+  // label counts are multiples of 16).
+  constexpr bool kVec = K % 8 == 0;
+  constexpr int NV = K / 8;
   constexpr int kAhead = 8;  // intensities are prefetched into L2 this many pixels ahead
   R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u);
@@ -261,16 +265,20 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       if (i < len) {
         unsigned char* rc = ring_cost + st * Ring::kStageBytes;
         if constexpr (kVec) {
-          if (uvalid[0]) {
-            r3dsimt::cp_async16(rc, c_in);
-            if constexpr (kReadsSum) {
-              r3dsimt::cp_async16(ring_sum + st * Ring::kStageBytes, s_in);
-              r3dsimt::cp_async16(ring_sum + st * Ring::kStageBytes + 16, s_in + 8);
-            }
-            if constexpr (MODE == kLastTerm) {
 #pragma unroll
-              for (int r = 0; r < kTermArrays; ++r)
-                r3dsimt::cp_async16(ring_term + st * Ring::kStageBytes + r * CPW * Ring::ND, t_in + r * tstride);
+          for (int v = 0; v < NV; ++v) {
+            if (uvalid[2 * v]) {
+              r3dsimt::cp_async16(rc + 16 * v, c_in + 16 * v);
+              if constexpr (kReadsSum) {
+                r3dsimt::cp_async16(ring_sum + st * Ring::kStageBytes + 32 * v, s_in + 16 * v);
+                r3dsimt::cp_async16(ring_sum + st * Ring::kStageBytes + 32 * v + 16, s_in + 16 * v + 8);
+              }
+              if constexpr (MODE == kLastTerm) {
+#pragma unroll
+                for (int r = 0; r < kTermArrays; ++r)
+                  r3dsimt::cp_async16(ring_term + st * Ring::kStageBytes + r * CPW * Ring::ND + 16 * v,
+                                      t_in + r * tstride + 16 * v);
+              }
             }
           }
         } else {
@@ -320,9 +328,12 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       const unsigned char* sc = ring_cost + q * Ring::kStageBytes;
       uint2 craw[U];
       if constexpr (kVec) {
-        const uint4 v = uvalid[0] ? *reinterpret_cast<const uint4*>(sc) : make_uint4(0, 0, 0, 0);
-        craw[0] = make_uint2(v.x, v.y);
-        craw[1] = make_uint2(v.z, v.w);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          const uint4 w4 = uvalid[2 * v] ? *reinterpret_cast<const uint4*>(sc + 16 * v) : make_uint4(0, 0, 0, 0);
+          craw[2 * v] = make_uint2(w4.x, w4.y);
+          craw[2 * v + 1] = make_uint2(w4.z, w4.w);
+        }
       } else {
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -384,10 +395,14 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       } else if constexpr (MODE == kTerm) {
         if (on) {
           if constexpr (kVec) {
-            if (uvalid[0])
-              r3dsimt::st_stream(reinterpret_cast<uint4*>(t_out),
-                                 make_uint4(r3dsimt::perm(tr[0], tr[1], 0x6420u), r3dsimt::perm(tr[2], tr[3], 0x6420u),
-                                            r3dsimt::perm(tr[4], tr[5], 0x6420u), r3dsimt::perm(tr[6], tr[7], 0x6420u)));
+#pragma unroll
+            for (int v = 0; v < NV; ++v)
+              if (uvalid[2 * v])
+                r3dsimt::st_stream(reinterpret_cast<uint4*>(t_out + 16 * v),
+                                   make_uint4(r3dsimt::perm(tr[8 * v], tr[8 * v + 1], 0x6420u),
+                                              r3dsimt::perm(tr[8 * v + 2], tr[8 * v + 3], 0x6420u),
+                                              r3dsimt::perm(tr[8 * v + 4], tr[8 * v + 5], 0x6420u),
+                                              r3dsimt::perm(tr[8 * v + 6], tr[8 * v + 7], 0x6420u)));
           } else {
 #pragma unroll
             for (int u = 0; u < U; ++u)
@@ -406,10 +421,13 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         for (int r = 0; r < kTermArrays; ++r) {
           uint2 tw[U];
           if constexpr (kVec) {
-            const uint4 v = uvalid[0] ? *reinterpret_cast<const uint4*>(stt + r * CPW * Ring::ND)
-                                      : make_uint4(0, 0, 0, 0);
-            tw[0] = make_uint2(v.x, v.y);
-            tw[1] = make_uint2(v.z, v.w);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              const uint4 w4 = uvalid[2 * v] ? *reinterpret_cast<const uint4*>(stt + r * CPW * Ring::ND + 16 * v)
+                                             : make_uint4(0, 0, 0, 0);
+              tw[2 * v] = make_uint2(w4.x, w4.y);
+              tw[2 * v + 1] = make_uint2(w4.z, w4.w);
+            }
           } else {
 #pragma unroll
             for (int u = 0; u < U; ++u)
@@ -1178,12 +1196,16 @@ void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegm
   X(1, 8)                  \
   X(2, 8)                  \
   X(2, 12)                 \
+  X(2, 16)                 \
   X(4, 8)                  \
   X(4, 12)                 \
+  X(4, 16)                 \
   X(8, 8)                  \
   X(8, 12)                 \
+  X(8, 16)                 \
   X(16, 8)                 \
   X(16, 12)                \
+  X(16, 16)                \
   X(32, 8)                 \
   X(32, 12)
 
@@ -1194,13 +1216,35 @@ bool sgm_path_enabled() {
   return !(e != nullptr && std::strcmp(e, "wavefront") == 0);
 }
 
+namespace {
+bool path_shape_compiled(int g, int k) {
+  bool found = false;
+#define R3D_SHAPE(gg, kk) found = found || (g == gg && k == kk);
+  R3D_PATH_SHAPES(R3D_SHAPE)
+#undef R3D_SHAPE
+  return found;
+}
+}  // namespace
+
 SgmPathShape sgm_path_shape(int nd) {
+  // A compiled shape from R3DGPU_PATH_SHAPE ("G,K": any label count it
+  // covers) or the tuning table (an entry for exactly this label count),
+  // else the narrowest row of 8 or 12 label pairs per lane, ties to fewer
+  // lanes per chain.
+  if (const char* e = std::getenv("R3DGPU_PATH_SHAPE")) {
+    int g = 0, k = 0;
+    if (std::sscanf(e, "%d,%d", &g, &k) == 2 && path_shape_compiled(g, k) && 2 * g * k >= nd) return {g, k};
+  }
+  const auto it = tuning().path.find(nd);
+  if (it != tuning().path.end() && path_shape_compiled(it->second.g, it->second.k) &&
+      2 * it->second.g * it->second.k >= nd)
+    return {it->second.g, it->second.k};
   SgmPathShape best{0, 0};
   int best_nd = 1 << 30;
-#define R3D_SHAPE(g, k)                           \
-  if (2 * g * k >= nd && 2 * g * k < best_nd) { \
-    best = SgmPathShape{g, k};                    \
-    best_nd = 2 * g * k;                          \
+#define R3D_SHAPE(g, k)                                       \
+  if (k != 16 && 2 * g * k >= nd && 2 * g * k < best_nd) { \
+    best = SgmPathShape{g, k};                                \
+    best_nd = 2 * g * k;                                      \
   }
   R3D_PATH_SHAPES(R3D_SHAPE)
 #undef R3D_SHAPE

@@ -42,6 +42,9 @@ Tuning parse(std::istream& in) {
     } else if (kind == "ranged_wide_frac") {
       double f = -1.0;
       if (ss >> f && f >= 0.0) t.ranged_wide_frac = f;
+    } else if (kind == "path") {
+      int nd = 0, g = 0, k = 0;
+      if (ss >> nd >> g >> k && nd > 0 && g > 0 && k > 0) t.path[nd] = TunedPath{g, k};
     } else if (kind == "ranged_general_width") {
       int w = 0;
       if (ss >> w && w > 0) t.ranged_general_width = w;

@@ -39,6 +39,20 @@ def test_volume(simt_matcher, oracle, dmin, nd, p2_adapt):
                           oracle.sgm_cost_volume(left, right, dmin, nd, o))
 
 
+@pytest.mark.parametrize("shape,nd", [("2,16", 48), ("4,16", 128), ("8,16", 208), ("8,8", 112), ("4,12", 96)])
+@pytest.mark.parametrize("p2", [120, 8000])
+def test_volume_chain_shapes(simt_matcher, oracle, monkeypatch, shape, nd, p2):
+    """Every chain-pass shape selectable by R3DGPU_PATH_SHAPE (lanes per
+    chain, label pairs per lane) against the textbook volume, with byte terms
+    (P2 <= 255) and with u16 sums (P2 = 8000: sums that wrap)."""
+    monkeypatch.setenv("R3DGPU_PATH_SHAPE", shape)
+    tex = Texture(19)
+    left, right, _ = render_pair(tex, 30, 17, lambda x, y: 7.0 + 0.2 * x)
+    o = StereoOptions(p1=20, p2=p2, p2_adapt=0 if p2 > 255 else 6, invalid_cost=40)
+    assert np.array_equal(simt_matcher.sgm_cost_volume(left, right, -1, nd, o),
+                          oracle.sgm_cost_volume(left, right, -1, nd, o))
+
+
 def test_volume_ranges_and_wrap(simt_matcher, oracle):
     tex = Texture(13)
     w, h, nd = 37, 19, 96

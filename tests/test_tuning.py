@@ -62,3 +62,27 @@ def test_table_from_environment(simt_matcher, monkeypatch):
     assert [(e["shape"], e["rows"]) for e in launches] == [("16x4/nd32", 2)]
     vol = simt_matcher.sgm_cost_volume(left, right, 0, 32, StereoOptions(), LabelRanges(lo, num))
     assert vol.size == 16 * 40 * 30
+
+
+def test_path_shape_from_table(simt_matcher, monkeypatch):
+    """A `path` entry sets the chain passes' shape for its label count (seen
+    in the per-pass profile), R3DGPU_PATH_SHAPE overrides it, and the maps
+    stay identical."""
+    tex = Texture(62)
+    left, right, _ = render_pair(tex, 40, 30, lambda x, y: 6.0 + 0.1 * x)
+    pairs = [dict(left=left, right=right, disparity_min=0, num_disparities=64, options=StereoOptions(levels=0))]
+
+    def shapes(launches):
+        return {e["shape"].split("/")[0] for e in launches if e.get("pass")}
+
+    monkeypatch.setenv("R3DGPU_TUNING", "#")
+    ref, launches = _launches(simt_matcher, lambda: simt_matcher.match_stereo_batch(pairs))
+    assert shapes(launches) == {"4x8"}
+    monkeypatch.setenv("R3DGPU_TUNING", "path 64 2 16")
+    got, launches = _launches(simt_matcher, lambda: simt_matcher.match_stereo_batch(pairs))
+    assert shapes(launches) == {"2x16"}
+    assert np.array_equal(np.nan_to_num(got[0].disparity, posinf=-1), np.nan_to_num(ref[0].disparity, posinf=-1))
+    monkeypatch.setenv("R3DGPU_PATH_SHAPE", "8,8")
+    got, launches = _launches(simt_matcher, lambda: simt_matcher.match_stereo_batch(pairs))
+    assert shapes(launches) == {"8x8"}
+    assert np.array_equal(np.nan_to_num(got[0].disparity, posinf=-1), np.nan_to_num(ref[0].disparity, posinf=-1))
