@@ -1463,8 +1463,14 @@ def main():
             out = subprocess.run([sys.executable, os.path.abspath(__file__), "--serve-only",
                                   str(n * args.steps / (ms * 1e-3)), "--pairs", str(args.pairs), "--seed",
                                   str(args.seed), "--serve-seconds", str(args.serve_seconds)],
-                                 capture_output=True, text=True, check=True)
-            line["serving"] = json.loads(out.stdout.strip().splitlines()[-1])
+                                 capture_output=True, text=True)
+            if out.returncode == 0:
+                line["serving"] = json.loads(out.stdout.strip().splitlines()[-1])
+            else:
+                # The batch's line stands; the sweep's failure is reported in it.
+                sys.stderr.write(out.stderr)
+                line["serving"] = {"error": f"serving sweep exited {out.returncode}",
+                                   "stderr_tail": out.stderr.strip().splitlines()[-6:]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

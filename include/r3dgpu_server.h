@@ -35,7 +35,7 @@ typedef struct r3dgpu_server_config {
   int32_t max_batch;         /* requests per batch, >= 1 */
   int32_t reserved;
   uint64_t hbm_budget;       /* bytes of device memory the admitted requests may hold together */
-  uint64_t scratch_budget;   /* bytes of SGM scratch per worker (0: 16 GiB) */
+  uint64_t scratch_budget;   /* bytes of SGM scratch per worker, both tracks of a batch together (0: 16 GiB) */
   uint64_t cache_budget;     /* bytes of device memory for keyed input images (0: no cache) */
 } r3dgpu_server_config;
 

@@ -1447,6 +1447,13 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
   std::vector<r3dgpu_pair> fp, hp;
   for (int i : flat) fp.push_back(pairs[i]);
   for (int i : hier) hp.push_back(pairs[i]);
+  // A scratch budget set for this thread (a server worker's) bounds both
+  // tracks together: each track gets half of it.
+  struct HalfBudget {
+    size_t saved;
+    HalfBudget() : saved(t_scratch_budget) { t_scratch_budget /= 2; }
+    ~HalfBudget() { t_scratch_budget = saved; }
+  } half_budget;
   Workspace& W1 = workspace(1);
   if (W1.track == nullptr) {
     R3D_CUDA(cudaStreamCreateWithFlags(&W1.track, cudaStreamNonBlocking));
