@@ -811,8 +811,11 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     int maxnum;
   };
   // Waves keep byte terms when every match of the group allows them (all
-  // P2 <= 255); otherwise u16 sums only.
-  bool terms = true;
+  // P2 <= 255); otherwise u16 sums only. Ranged waves use byte terms only
+  // with R3DGPU_RANGED_TERMS=1: their packed rows measured slower with the
+  // larger buffers (more waves) and the eight-plane ring of the last pass.
+  const char* rt = std::getenv("R3DGPU_RANGED_TERMS");
+  bool terms = !ranged || (rt != nullptr && std::atoi(rt) == 1);
   for (const auto& mt : tiles) terms = terms && matches[mt.first]->m.term_u8 != 0;
   auto bytes = [&](int64_t cells, int64_t px, int64_t keys, int64_t rows, int maxnum) -> size_t {
     return ranged ? sgm_path_ranged_buffers(cells, px, keys, rows, maxnum, sms, terms).total
@@ -1423,10 +1426,18 @@ void run_batch(r3dgpu_pair* pairs, int count, cudaStream_t s) {
     (lv == 0 ? flat : hier).push_back(i);
   }
   // On any error (a cancellation included) the work already enqueued ends
-  // before the call returns.
+  // before the call returns: the call's stream, the second track's, and the
+  // side streams of both workspaces (a round's SGM groups are forked onto
+  // them, and an error between the fork and the join leaves them running;
+  // the next call would reuse their buffers).
   auto drain = [&](cudaStream_t other) {
     (void)cudaStreamSynchronize(s);
     if (other != nullptr) (void)cudaStreamSynchronize(other);
+    for (int slot = 0; slot < kWorkspaceSlots; ++slot) {
+      const int idx = t_device * kWorkspaceSlots + slot;
+      if (idx < static_cast<int>(t_workspaces.size()) && t_workspaces[idx])
+        for (cudaStream_t side : t_workspaces[idx]->side) (void)cudaStreamSynchronize(side);
+    }
     (void)cudaGetLastError();
     profile_collect();
   };

@@ -312,9 +312,17 @@ struct r3dgpu_server {
         work_cv.wait(lk, [&] { return can_admit() || (stop && queue.empty()); });
         if (!can_admit()) break;  // stopping with an empty queue
         const auto now = Clock::now();
+        // A worker's level data live in its own grow-only workspace, which
+        // keeps the memory of the largest batch it ran; a batch is therefore
+        // also held to the worker's share of the budget, so that what all
+        // workers keep stays within it (a larger single request runs alone).
+        const uint64_t share = cfg.hbm_budget / static_cast<uint64_t>(cfg.workers);
+        uint64_t mine = 0;
         while (!queue.empty() && static_cast<int>(batch.size()) < cfg.max_batch) {
           const RequestPtr& r = queue.front();
           if ((inflight > 0 || !batch.empty()) && inflight + r->bytes > cfg.hbm_budget) break;
+          if (!batch.empty() && mine + r->bytes > share) break;
+          mine += r->bytes;
           inflight += r->bytes;
           r->admitted = now;
           r->worker = index;

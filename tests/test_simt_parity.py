@@ -53,6 +53,29 @@ def test_volume_chain_shapes(simt_matcher, oracle, monkeypatch, shape, nd, p2):
                           oracle.sgm_cost_volume(left, right, -1, nd, o))
 
 
+@pytest.mark.parametrize("terms", ["0", "1"])
+def test_ranged_term_modes(simt_matcher, oracle, monkeypatch, terms):
+    """Per-pixel ranges through the chain passes with u16 sums (the default)
+    and with byte terms (R3DGPU_RANGED_TERMS=1): volume and a hierarchical
+    match against the oracle."""
+    monkeypatch.setenv("R3DGPU_RANGED_TERMS", terms)
+    tex = Texture(29)
+    w, h, nd = 33, 21, 112
+    left, right, _ = render_pair(tex, w, h, lambda x, y: 25.0 + 0.4 * x - 0.2 * y)
+    r = Rng(37)
+    num = np.array([[16 * r.uniform_int(1, 5) for _ in range(w)] for _ in range(h)], np.uint16)
+    lo = np.array([[r.uniform_int(0, nd - int(n)) for n in row] for row in num], np.uint16)
+    o = StereoOptions(p2=140, p2_adapt=5)
+    assert np.array_equal(simt_matcher.sgm_cost_volume(left, right, 1, nd, o, LabelRanges(lo, num)),
+                          oracle.sgm_cost_volume(left, right, 1, nd, o, (lo, num)))
+    left, right, _ = render_pair(tex, 120, 64, lambda x, y: np.where(x < 50, 9.0, 21.0))
+    o = StereoOptions(levels=2, tile_size=48, tile_margin=8, tile_blend=8, range_radius=1)
+    a = simt_matcher.match_stereo(left, right, None, None, 0, 48, o)
+    b = oracle.match_stereo(left, right, None, None, 0, 48, o)
+    assert same_disparities(a.disparity, b.disparity), mismatch_report(a.disparity, b.disparity)
+    assert a.cells == b.cells
+
+
 def test_volume_ranges_and_wrap(simt_matcher, oracle):
     tex = Texture(13)
     w, h, nd = 37, 19, 96
