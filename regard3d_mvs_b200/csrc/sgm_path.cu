@@ -314,7 +314,9 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
 #pragma unroll
     for (int k = 0; k < K; ++k) prev[k] = 0;
     uint32_t pmin = 0;
-    int iprev = 0;
+    // P2 of the step's intensity change, loaded one step ahead (the value of
+    // the first step is unused: its predecessor vector is zero).
+    uint32_t lutv = 0;
 
     auto step = [&](const int i, const int q) {
       const bool on = i < len;
@@ -348,8 +350,12 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         c2[4 * u + 3] = r3dsimt::perm(craw[u].y, 0u, 0x4342u);
       }
       // out = L_r = C + T_r with T_r = best - min L(q).
-      const int dI = icur - iprev;
-      const uint32_t pen = pmin + m.lut[(dI < 0 ? -dI : dI) >> 8];
+      const uint32_t pen = pmin + lutv;
+      {
+        // The next step's P2: its intensity came in NS - 2 steps ago.
+        const int dn = iq[(q + 1) % NS] - icur;
+        lutv = m.lut[(dn < 0 ? -dn : dn) >> 8];
+      }
       const uint32_t pen2 = pen | (pen << 16);
       const uint32_t negmp = 0u - (pmin | (pmin << 16));
       const uint32_t hl = r3dsimt::shfl(prev[K - 1], left_lane);
@@ -532,7 +538,6 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       (void)s;
 #pragma unroll
       for (int k = 0; k < K; ++k) prev[k] = out[k];
-      iprev = icur;
       if constexpr (MODE == kFirst || MODE == kAccumulate) s_out += dcell;
       if constexpr (MODE == kTerm) t_out += dcell;
       if constexpr (kWta) {
