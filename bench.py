@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--serve-only", type=float, default=0.0, metavar="PAIRS_PER_S",
                     help="run only the serving sweep (its saturation run offers 3 x this batch rate); print its JSON")
     ap.add_argument("--serve-seconds", type=float, default=8.0, help="arrival window per load point")
+    ap.add_argument("--serve-workers", type=int, default=SERVE_WORKERS, help="serving loop workers (streams)")
+    ap.add_argument("--serve-batch", type=int, default=SERVE_MAX_BATCH, help="requests per batch at most")
     return ap.parse_args()
 
 
@@ -1028,6 +1030,7 @@ SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
 SERVE_REQUEST_BUDGET = 110 << 30  # config 3's 150 GB: 110 GB for admitted requests, 2 x 16 GB worker scratch, 8 GB cache
 SERVE_CACHE = 8 << 30
 SERVE_WORKERS = 2
+SERVE_MAX_BATCH = 16
 SERVE_SCENE_VIEWS = 200
 SERVE_POOL_VIEWS = 8
 SERVE_PARTNERS = 4
@@ -1137,8 +1140,9 @@ def run_serving(args, rate_hint: float) -> dict:
                 "mean_batch": float(np.mean(batch)), "left_image_cache_hits": hits / nreq,
                 "uploaded_mb_per_request": up / nreq / 1e6}
 
-    with Server(device=0, workers=SERVE_WORKERS, max_batch=16, hbm_budget=SERVE_REQUEST_BUDGET,
-                scratch_budget=16 << 30, cache_budget=SERVE_CACHE) as srv:
+    scratch = min(16 << 30, (32 << 30) // args.serve_workers)  # 32 GB of SGM scratch over the workers
+    with Server(device=0, workers=args.serve_workers, max_batch=args.serve_batch, hbm_budget=SERVE_REQUEST_BUDGET,
+                scratch_budget=scratch, cache_budget=SERVE_CACHE) as srv:
         # Warm-up: the workers allocate their buffers.
         run_point(srv, 4.0 * max(rate_hint, 1.0), 2.0)
         sat = run_point(srv, 3.0 * max(rate_hint, 1.0), args.serve_seconds)
@@ -1151,9 +1155,9 @@ def run_serving(args, rate_hint: float) -> dict:
     return {"scene": f"{SERVE_SCENE_VIEWS} views x {SERVE_PARTNERS} partner pairs (images of {SERVE_POOL_VIEWS} "
                      "distinct config-2 views; each view's pairs share its left image under the view's content key)",
             "saturated_pairs_per_s": sat_rate, "saturation_run": sat,
-            "load_axis": "fraction of the served saturation measured above", "workers": SERVE_WORKERS,
-            "max_batch": 16, "host_buffers": "page-locked inputs and disparity maps; no confidence maps",
-            "request_budget_bytes": SERVE_REQUEST_BUDGET, "worker_scratch_bytes": 16 << 30,
+            "load_axis": "fraction of the served saturation measured above", "workers": args.serve_workers,
+            "max_batch": args.serve_batch, "host_buffers": "page-locked inputs and disparity maps; no confidence maps",
+            "request_budget_bytes": SERVE_REQUEST_BUDGET, "worker_scratch_bytes": scratch,
             "image_cache_bytes": SERVE_CACHE, "device_used_peak_gb": peak_used[0] / 1e9, "arrivals": "Poisson",
             "points": points}
 
@@ -1462,7 +1466,8 @@ def main():
             torch.cuda.empty_cache()
             out = subprocess.run([sys.executable, os.path.abspath(__file__), "--serve-only",
                                   str(n * args.steps / (ms * 1e-3)), "--pairs", str(args.pairs), "--seed",
-                                  str(args.seed), "--serve-seconds", str(args.serve_seconds)],
+                                  str(args.seed), "--serve-seconds", str(args.serve_seconds), "--serve-workers",
+                                  str(args.serve_workers), "--serve-batch", str(args.serve_batch)],
                                  capture_output=True, text=True)
             if out.returncode == 0:
                 line["serving"] = json.loads(out.stdout.strip().splitlines()[-1])

@@ -470,27 +470,37 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       if constexpr (kWta) {
         // Winner-takes-all over the total sums (sgm_kernels.cpp:332-358):
         // the first minimum, the second best outside +-1, and S at kb -+ 1.
-        uint32_t kmin = 0xFFFFFFFFu;
+        // Labels of units past nd count as 0xFFFF (they follow every valid
+        // label, so they never come first among equal minima).
+        uint32_t sv[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) sv[k] = uvalid[k / 4] ? s[k] : 0xFFFFFFFFu;
+        // The minimum value, by packed halfword minima and the lane group.
+        uint32_t mv = sv[0];
+#pragma unroll
+        for (int k = 1; k < K; ++k) mv = r3dsimt::vmin2(mv, sv[k]);
+        const uint32_t bcost = group_umin<G>(r3dsimt::umin(mv & 0xFFFFu, mv >> 16));
+        // Its first label: a bit per label pair word (even labels in the low
+        // half, odd labels in the high half), then the lowest label of the group.
+        const uint32_t b2 = bcost | (bcost << 16);
+        uint32_t hit = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) hit |= (r3dsimt::vcmpeq2(sv[k], b2) & 0x00010001u) << k;
+        const uint32_t he = hit & 0xFFFFu, ho = hit >> 16;
+        const uint32_t fe = he != 0 ? static_cast<uint32_t>(2 * (r3dsimt::ffs(he) - 1)) : 0xFFFFu;
+        const uint32_t fo = ho != 0 ? static_cast<uint32_t>(2 * (r3dsimt::ffs(ho) - 1) + 1) : 0xFFFFu;
+        const uint32_t first = r3dsimt::umin(fe, fo);
+        const int kb = static_cast<int>(group_umin<G>(first == 0xFFFFu ? 0xFFFFu : first + static_cast<uint32_t>(e0)));
+        // The second best outside kb -+ 1: the three labels masked to 0xFFFF.
+        uint32_t sec2 = 0xFFFFFFFFu;
+        const int d0 = e0 - kb + 1;  // label e0 + 2k lies in kb -+ 1 iff d0 + 2k is in [0, 2]
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          if (uvalid[k / 4]) {
-            const uint32_t e = static_cast<uint32_t>(e0 + 2 * k);
-            kmin = r3dsimt::umin(kmin, r3dsimt::umin(((s[k] & 0xFFFFu) << 16) | e, (s[k] & 0xFFFF0000u) | (e + 1)));
-          }
+          const uint32_t d = static_cast<uint32_t>(d0 + 2 * k);
+          const uint32_t mask = (d <= 2u ? 0xFFFFu : 0u) | (d + 1u <= 2u ? 0xFFFF0000u : 0u);
+          sec2 = r3dsimt::vmin2(sec2, sv[k] | mask);
         }
-        kmin = group_umin<G>(kmin);
-        const int kb = static_cast<int>(kmin & 0xFFFFu);
-        const uint32_t bcost = kmin >> 16;
-        uint32_t sec = 0xFFFFu;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          if (uvalid[k / 4]) {
-            const int e = e0 + 2 * k;
-            if (e + 1 < kb || e > kb + 1) sec = r3dsimt::umin(sec, s[k] & 0xFFFFu);
-            if (e + 2 < kb || e + 1 > kb + 1) sec = r3dsimt::umin(sec, s[k] >> 16);
-          }
-        }
-        sec = group_umin<G>(sec);
+        const uint32_t sec = group_umin<G>(r3dsimt::umin(sec2 & 0xFFFFu, sec2 >> 16));
         const int km = kb > 0 ? kb - 1 : 0, kp = kb + 1 < nd ? kb + 1 : nd - 1;
         const int jm = (km % (2 * K)) >> 1, jp = (kp % (2 * K)) >> 1;
         uint32_t vm = 0, vp = 0;

@@ -43,6 +43,8 @@ R3D_DEVICE void syncwarp() { __syncwarp(); }
 R3D_DEVICE void syncthreads() { __syncthreads(); }
 R3D_DEVICE void fence() { __threadfence(); }
 R3D_DEVICE uint32_t vmin2(uint32_t a, uint32_t b) { return __vminu2(a, b); }
+// Per-halfword a == b ? 0xFFFF : 0.
+R3D_DEVICE uint32_t vcmpeq2(uint32_t a, uint32_t b) { return __vcmpeq2(a, b); }
 // Per-halfword min(a, b, c) and min(a + b, c) (DPX instructions on sm_90+).
 R3D_DEVICE uint32_t vmin3(uint32_t a, uint32_t b, uint32_t c) { return __vimin3_u16x2(a, b, c); }
 R3D_DEVICE uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) { return __viaddmin_u16x2(a, b, c); }
@@ -154,6 +156,9 @@ inline uint32_t vmin2(uint32_t a, uint32_t b) {
   return lo | (hi << 16);
 }
 inline uint32_t vmin3(uint32_t a, uint32_t b, uint32_t c) { return vmin2(vmin2(a, b), c); }
+inline uint32_t vcmpeq2(uint32_t a, uint32_t b) {
+  return (((a ^ b) & 0xFFFFu) == 0 ? 0xFFFFu : 0u) | (((a ^ b) >> 16) == 0 ? 0xFFFF0000u : 0u);
+}
 inline uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) {
   const uint32_t lo = std::min((a + b) & 0xFFFFu, c & 0xFFFFu);
   const uint32_t hi = std::min(((a >> 16) + (b >> 16)) & 0xFFFFu, c >> 16);
