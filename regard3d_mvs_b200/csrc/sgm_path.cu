@@ -861,8 +861,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
       issue_data(k, recs[k * 32 + lane]);
       r3dsimt::cp_async_commit();
     }
-    uint32_t pmin = 0;
-    int lo_q = 0, num_q = 0, iprev = 0;
+    uint32_t pmin = 0, lutv = 0;
+    int lo_q = 0, num_q = 0;
     for (int i = 0; i < maxlen; ++i) {
       const bool on = i < len;
       r3dsimt::cp_async_wait<D - 1>();
@@ -881,10 +881,18 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
       const int cur = i & 1, prv = cur ^ 1;
       uint32_t pen2 = 0, negmp = 0;
       if (i > 0) {
-        const int dI = icur - iprev;
-        const uint32_t pen = pmin + m.lut[(dI < 0 ? -dI : dI) >> 8];
+        const uint32_t pen = pmin + lutv;
         pen2 = pen | (pen << 16);
         negmp = 0u - (pmin | (pmin << 16));
+      }
+      {
+        // The next step's P2, loaded one step ahead from the next pixel's
+        // record (landed: it was issued 2 D - 1 steps ahead). Past the end of
+        // the chain that record slot holds an older or an unwritten record,
+        // so the table index is clamped to the table.
+        const int dn = recs[((i + 1) & (2 * D - 1)) * 32 + lane].z - icur;
+        const uint32_t di = static_cast<uint32_t>(dn < 0 ? -dn : dn) >> 8;
+        lutv = m.lut[di < 255u ? di : 255u];
       }
       uint32_t pm = kSent2;
       for (int c = 0; c < nchw; ++c) {
@@ -1004,7 +1012,6 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
       if (on) {
         lo_q = lo;
         num_q = num;
-        iprev = icur;
       }
     }
     r3dsimt::cp_async_wait<0>();
