@@ -193,8 +193,9 @@ struct PathRing {
   static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
 };
 
-// Three CTAs per SM for the 8-word shapes (80 registers, no spills); the
-// 12- and 16-word shapes keep two.
+// Four CTAs per SM for the 8-word term passes (64 registers, no spills),
+// three for the other 8-word passes (80 registers); the 12- and 16-word
+// shapes keep two.
 //
 // The step loop is unrolled by the ring depth NS so that ring slots and the
 // intensity queue are indexed statically; each chain keeps running pointers
@@ -202,7 +203,7 @@ struct PathRing {
 // addresses. The first pixel needs no special case: with a zero predecessor
 // vector and a zero minimum, best = 0, so T = 0 and L = C there.
 template <int G, int K, int MODE>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? (MODE == kTerm ? 4 : 3) : 2))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
                     int dx, int dy, int64_t total_blocks, const uint8_t* R3D_RESTRICT cost, uint16_t* sum,
                     uint8_t* terms, int64_t tstride, int tslot, int4* R3D_RESTRICT info, uint32_t* rkeys,
