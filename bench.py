@@ -1488,12 +1488,23 @@ def main():
                         if specs[i]["w"] * specs[i]["h"] * specs[i]["nd"] ==
                         min(q["w"] * q["h"] * q["nd"] for q in specs)}
             line["cpu_baseline"] = cpu_baseline(specs, gpu_maps)
-            line["multi_view"] = measure_combine(lib, dev, stream, args.steps, args.warmup, peak)
-            line["rectify"] = measure_rectify(lib, dev, stream, args.steps, args.warmup, peak)
+
+            def extra(fn, *a):
+                # A failing side measurement is reported in the line, which stands.
+                try:
+                    return fn(*a)
+                except Exception as e:  # noqa: BLE001
+                    import traceback
+
+                    traceback.print_exc()
+                    return {"error": f"{type(e).__name__}: {e}"}
+
+            line["multi_view"] = extra(measure_combine, lib, dev, stream, args.steps, args.warmup, peak)
+            line["rectify"] = extra(measure_rectify, lib, dev, stream, args.steps, args.warmup, peak)
             # Config 4 end to end (the depth stage of a 32-view scene); the
             # separate depth-stage and one-view lines stay available as
             # --workload depth / view.
-            line["scene32"] = measure_scene(lib, dev, stream, 2, 1)
+            line["scene32"] = extra(measure_scene, lib, dev, stream, 2, 1)
         if args.serve and world == 1:
             # In a fresh process, with this one's device memory given back.
             del dL, dR, dD, dC
