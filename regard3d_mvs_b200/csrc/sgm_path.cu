@@ -179,10 +179,12 @@ R3D_DEVICE uint32_t add2(uint32_t a, uint32_t b, bool no_carry) { return no_carr
 // Per-warp shared-memory ring of the pass kernels: Stages stages, each with
 // one pixel per chain of the bytes the pass reads (Planes bytes per label:
 // the cost, plus the u16 sum or the seven byte terms).
+// The term passes read one byte per label and keep 8 stages in flight (their
+// step is short, so 3 stages ahead left them waiting on DRAM).
 template <int MODE>
 struct PathMode {
   static constexpr int kPlanes = MODE == kAccumulate || MODE == kLast ? 3 : (MODE == kLastTerm ? 1 + kTermArrays : 1);
-  static constexpr int kStages = MODE == kLastTerm ? 3 : 4;
+  static constexpr int kStages = MODE == kLastTerm ? 3 : (MODE == kTerm ? 8 : 4);
 };
 template <int G, int K, int MODE>
 struct PathRing {
@@ -193,9 +195,8 @@ struct PathRing {
   static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
 };
 
-// Four CTAs per SM for the 8-word term passes (64 registers, no spills),
-// three for the other 8-word passes (80 registers); the 12- and 16-word
-// shapes keep two.
+// Three CTAs per SM for the 8-word shapes (up to 80 registers, no spills);
+// the 12- and 16-word shapes keep two.
 //
 // The step loop is unrolled by the ring depth NS so that ring slots and the
 // intensity queue are indexed statically; each chain keeps running pointers
@@ -203,7 +204,7 @@ struct PathRing {
 // addresses. The first pixel needs no special case: with a zero predecessor
 // vector and a zero minimum, best = 0, so T = 0 and L = C there.
 template <int G, int K, int MODE>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? (MODE == kTerm ? 4 : 3) : 2))
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
                     int dx, int dy, int64_t total_blocks, const uint8_t* R3D_RESTRICT cost, uint16_t* sum,
                     uint8_t* terms, int64_t tstride, int tslot, int4* R3D_RESTRICT info, uint32_t* rkeys,
