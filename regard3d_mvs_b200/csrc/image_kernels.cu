@@ -513,17 +513,23 @@ R3D_GLOBAL void tile_cells_kernel(const uint16_t* R3D_RESTRICT rnum, int64_t str
   R3D_DYNAMIC_SMEM(smem_raw);
   unsigned long long* ssum = reinterpret_cast<unsigned long long*>(smem_raw);
   int* sst = reinterpret_cast<int*>(smem_raw + 8 * 32);  // [warp][kTileStats]
+  // Block (tile, slice): the slice's rows of the tile, a warp per row, the
+  // lanes over its columns; the slices' results meet in atomics (the
+  // launcher zeroes the outputs).
   const int4 t = tiles[blockIdx.x];
   unsigned long long s = 0;
   int st[kTileStats] = {};
-  const int64_t n = static_cast<int64_t>(t.z) * t.w;
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
-    const int y = static_cast<int>(i / t.z), x = static_cast<int>(i % t.z);
-    const int v = rnum[static_cast<int64_t>(t.y + y) * stride + t.x + x];
-    s += static_cast<unsigned long long>(v);
-    st[0] = r3dsimt::imax(st[0], v);
+  const int nwarps = static_cast<int>(blockDim.x >> 5);
+  for (int y = static_cast<int>(blockIdx.y) * nwarps + static_cast<int>(threadIdx.x >> 5); y < t.w;
+       y += static_cast<int>(gridDim.y) * nwarps) {
+    const uint16_t* row = rnum + static_cast<int64_t>(t.y + y) * stride + t.x;
+    for (int x = static_cast<int>(threadIdx.x & 31u); x < t.z; x += 32) {
+      const int v = row[x];
+      s += static_cast<unsigned long long>(v);
+      st[0] = r3dsimt::imax(st[0], v);
 #pragma unroll
-    for (int k = 1; k < kTileStats; ++k) st[k] += v > tile_stat_width(k - 1) ? 1 : 0;
+      for (int k = 1; k < kTileStats; ++k) st[k] += v > tile_stat_width(k - 1) ? 1 : 0;
+    }
   }
   // Warp reduction (64-bit sum as two 32-bit halves), then across warps.
 #pragma unroll
@@ -550,8 +556,9 @@ R3D_GLOBAL void tile_cells_kernel(const uint16_t* R3D_RESTRICT rnum, int64_t str
       out[0] = r3dsimt::imax(out[0], sst[i * kTileStats]);
       for (int k = 1; k < kTileStats; ++k) out[k] += sst[i * kTileStats + k];
     }
-    cells[blockIdx.x] = tot;
-    for (int k = 0; k < kTileStats; ++k) stats[static_cast<int64_t>(blockIdx.x) * kTileStats + k] = out[k];
+    atomicAdd(cells + blockIdx.x, tot);
+    atomicMax(stats + static_cast<int64_t>(blockIdx.x) * kTileStats, out[0]);
+    for (int k = 1; k < kTileStats; ++k) atomicAdd(stats + static_cast<int64_t>(blockIdx.x) * kTileStats + k, out[k]);
   }
 }
 
@@ -731,8 +738,12 @@ void launch_blend(const BlendTile* tiles, int ntiles, int tiles_x, const int* /*
 void launch_tile_cells(const uint16_t* rnum, int64_t stride, const int4* tiles, int ntiles, unsigned long long* cells,
                        int* stats, cudaStream_t s) {
   if (ntiles <= 0) return;
-  R3D_LAUNCH(tile_cells_kernel, dim3(ntiles), dim3(256), 8 * 32 + 4 * kTileStats * 8, s, rnum, stride, tiles, cells,
-             stats);
+  R3D_CUDA(cudaMemsetAsync(cells, 0, sizeof(unsigned long long) * ntiles, s));
+  R3D_CUDA(cudaMemsetAsync(stats, 0, sizeof(int) * kTileStats * ntiles, s));
+  // Enough slices per tile for several blocks per SM over all tiles.
+  const int slices = ntiles >= 296 ? 1 : (592 + ntiles - 1) / ntiles;
+  R3D_LAUNCH(tile_cells_kernel, dim3(ntiles, slices > 32 ? 32 : slices), dim3(256), 8 * 32 + 4 * kTileStats * 8, s, rnum,
+             stride, tiles, cells, stats);
   launched("tile_cells_kernel");
 }
 

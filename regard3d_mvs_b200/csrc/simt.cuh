@@ -213,6 +213,7 @@ inline unsigned long long atomicAdd(unsigned long long* p, unsigned long long v)
   return o;
 }
 inline unsigned atomicMin(unsigned* p, unsigned v) { const unsigned o = *p; if (v < o) *p = v; return o; }
+inline int atomicMax(int* p, int v) { const int o = *p; if (v > o) *p = v; return o; }
 inline int atomicCAS(int* p, int cmp, int v) { const int o = *p; if (o == cmp) *p = v; return o; }
 template <class T>
 inline T __ldcg(const T* p) { return *p; }
