@@ -842,7 +842,7 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
   size_t begin = 0;
   while (begin < es.size()) {
     int64_t cells = 0, px = 0, keys = 0, rows = 0;
-    int maxnum = 16;
+    int maxnum = 16, span = 0;
     size_t end = begin;
     while (end < es.size()) {
       const Entry& e = es[end];
@@ -854,6 +854,7 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
       keys += e.keys;
       rows += e.rows;
       maxnum = std::max(maxnum, e.maxnum);
+      span = std::max(span, matches[e.i]->layout.tiles[e.t].w + matches[e.i]->m.nd - 1);
       ++end;
     }
     const int n = static_cast<int>(end - begin);
@@ -906,6 +907,7 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     wv.rows = ro;
     wv.maxnum = maxnum;
     wv.terms = terms ? 1 : 0;
+    wv.max_span = span;
     waves.push_back(wv);
     segs.push_back(std::move(sg));
     max_bytes = std::max(max_bytes, bytes(co, po, ko, ro, maxnum));
@@ -1217,6 +1219,7 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
           w.rows = rw.rows;
           w.buffer = scratch;
           w.terms = rw.terms;
+          w.max_span = rw.max_span;
           launch_sgm_path_wave(dm, w, W.sms, gs);
         }
       } else if (g.kind == kPathRanged) {

@@ -101,15 +101,17 @@ R3D_DEVICE void chain_geometry(int cls, int dx, int dy, int w, int h, int64_t c,
 // partner Census codes the row can reach (right columns x0 - dmin - nd + 1 ..
 // x0 + w - 1 - dmin) are staged in the warp's shared memory, then the lanes
 // take 32 consecutive pixels and write 32 labels (one sector) at a time.
-constexpr int kCostStage = 2048;  // staged partner codes per warp (sgm_path_fits: w + nd - 1 <= 2048)
+constexpr int kCostStage = 2048;  // staged partner codes per warp at most (sgm_path_fits: w + nd - 1 <= 2048)
 
+// `stage_words` (<= kCostStage): the widest staged row of the wave (tile
+// width + labels - 1), so that narrow waves run more CTAs per SM.
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     sgm_path_cost_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
-                         int64_t rows, uint8_t* R3D_RESTRICT cost) {
+                         int64_t rows, uint8_t* R3D_RESTRICT cost, int stage_words) {
   R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u), warp = static_cast<int>(threadIdx.x >> 5);
   const int wpb = static_cast<int>(blockDim.x) >> 5;
-  uint64_t* stage = reinterpret_cast<uint64_t*>(smem) + static_cast<size_t>(warp) * kCostStage;
+  uint64_t* stage = reinterpret_cast<uint64_t*>(smem) + static_cast<size_t>(warp) * stage_words;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
   for (int64_t r = static_cast<int64_t>(blockIdx.x) * wpb + warp; r < rows; r += nwarps) {
     const int j = find_job(jobs, njobs, r, [](const SgmPathJob& q) { return q.row_off; });
@@ -1303,18 +1305,20 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
   uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
   if (wave.keys > 0) R3D_CUDA(cudaMemsetAsync(rkeys, 0xFF, static_cast<size_t>(wave.keys) * 4, s));
   {
-    constexpr size_t smem = static_cast<size_t>(kPathThreads / 32) * kCostStage * 8;
+    constexpr size_t max_smem = static_cast<size_t>(kPathThreads / 32) * kCostStage * 8;
     static thread_local int configured[64] = {};
     int dev = 0;
     R3D_CUDA(cudaGetDevice(&dev));
     if (dev >= 0 && dev < 64 && !configured[dev]) {
       R3D_CUDA(cudaFuncSetAttribute(sgm_path_cost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(smem)));
+                                    static_cast<int>(max_smem)));
       configured[dev] = 1;
     }
+    const int words = wave.max_span > 0 && wave.max_span <= kCostStage ? (wave.max_span + 1) & ~1 : kCostStage;
+    const size_t smem = static_cast<size_t>(kPathThreads / 32) * words * 8;
     R3D_LAUNCH(sgm_path_cost_kernel,
                dim3(resident_grid(sgm_path_cost_kernel, sms, wave.rows, kPathThreads / 32, smem)),
-               dim3(kPathThreads), smem, s, dm, wave.jobs, wave.njobs, wave.rows, cost);
+               dim3(kPathThreads), smem, s, dm, wave.jobs, wave.njobs, wave.rows, cost, words);
     launched("sgm_path_cost_kernel");
   }
   for (int q = 0; q < wave.nsegs; ++q) {

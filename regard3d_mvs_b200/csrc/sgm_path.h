@@ -84,6 +84,7 @@ struct SgmPathWave {
   unsigned char* buffer;  // sgm_path_buffers(cells, pixels, keys, terms).total bytes
   const int* cancel;      // device view of the caller's cancellation flag, or null
   int terms;              // 1: byte terms (every match of the wave has term_u8)
+  int max_span;           // largest tile width + labels - 1 of the wave (0: unknown)
 };
 
 // Costs, the 8 passes and the acceptance rules of one wave, on stream s.
@@ -109,6 +110,7 @@ struct SgmPathRangedWave {
   unsigned char* buffer;
   const int* cancel;  // device view of the caller's cancellation flag, or null
   int terms;          // byte terms (every match of the wave has term_u8)
+  int max_span;       // largest tile width + labels - 1 of the wave (0: unknown)
 };
 SgmPathBuffers sgm_path_ranged_buffers(int64_t cells, int64_t pixels, int64_t keys, int64_t rows, int maxnum,
                                        int sms, bool terms);
