@@ -869,13 +869,16 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     int lo_q = 0, num_q = 0;
     for (int i = 0; i < maxlen; ++i) {
       const bool on = i < len;
-      r3dsimt::cp_async_wait<D - 1>();
+      // One wait per step: the group of step i - D + 1 (this pixel's data)
+      // and the older one holding record i + D - 1 are complete when at most
+      // the D - 2 most recent groups are still in flight. The slots refilled
+      // here (record and data of the previous pixel) are no longer read.
+      r3dsimt::cp_async_wait<D - 2>();
+      const int4 rc = recs[(i & (2 * D - 1)) * 32 + lane];
       const int4 rn = recs[((i + D - 1) & (2 * D - 1)) * 32 + lane];
       issue_rec(i + 2 * D - 1);
       issue_data(i + D - 1, rn);
       r3dsimt::cp_async_commit();
-      r3dsimt::cp_async_wait<D - 1>();
-      const int4 rc = recs[(i & (2 * D - 1)) * 32 + lane];
       const int off = rc.x, lo = rc.y & 0xFFFF, icur = rc.z;
       const int num = on ? static_cast<int>(static_cast<uint32_t>(rc.y) >> 16) : 0;
       // Chunks of this pixel's range: the same for the chain's G lanes (one
