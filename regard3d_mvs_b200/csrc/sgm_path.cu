@@ -194,7 +194,8 @@ struct PathRing {
   static constexpr int kStages = PathMode<MODE>::kStages;
   static constexpr int kStageBytes = (32 / G) * PathMode<MODE>::kPlanes * ND;
   static constexpr int kWarpBytes = kStages * kStageBytes;
-  static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
+  // Each warp's rings, then each warp's copy of its match's P2 table.
+  static constexpr int kBlockBytes = (kPathThreads / 32) * (kWarpBytes + 512);
 };
 
 // Three CTAs per SM for the 8-word shapes (up to 80 registers, no spills);
@@ -231,6 +232,11 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * wpb;
   using Ring = PathRing<G, K, MODE>;
   unsigned char* const ring = smem + static_cast<size_t>(threadIdx.x >> 5) * Ring::kWarpBytes;
+  // The warp's copy of the P2 table of the match it works on (256 u16),
+  // reloaded when a chain block belongs to another match.
+  uint16_t* const lut = reinterpret_cast<uint16_t*>(smem + static_cast<size_t>(wpb) * Ring::kWarpBytes +
+                                                    static_cast<size_t>(threadIdx.x >> 5) * 512);
+  int lut_match = -1;
   unsigned char* const ring_cost = ring + gi * Ring::ND + e0;
   unsigned char* const ring_sum = ring + CPW * Ring::ND + gi * 2 * Ring::ND + 2 * e0;
   unsigned char* const ring_term = ring + CPW * Ring::ND + gi * Ring::ND + e0;  // + r * CPW * ND
@@ -239,6 +245,13 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
+    if (job.match != lut_match) {  // the same for the whole warp (one chain block)
+      r3dsimt::syncwarp();
+      for (int k = lane; k < 128; k += 32)
+        reinterpret_cast<uint32_t*>(lut)[k] = reinterpret_cast<const uint32_t*>(m.lut)[k];
+      r3dsimt::syncwarp();
+      lut_match = job.match;
+    }
     const int w = job.w, nd = m.nd;
     const uint32_t p1x2 = static_cast<uint32_t>(m.p1) * 0x10001u;
     const bool no_carry = m.sum_no_carry != 0;
@@ -358,7 +371,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       {
         // The next step's P2: its intensity came in NS - 2 steps ago.
         const int dn = iq[(q + 1) % NS] - icur;
-        lutv = m.lut[(dn < 0 ? -dn : dn) >> 8];
+        lutv = lut[(dn < 0 ? -dn : dn) >> 8];
       }
       const uint32_t pen2 = pen | (pen << 16);
       const uint32_t negmp = 0u - (pmin | (pmin << 16));
