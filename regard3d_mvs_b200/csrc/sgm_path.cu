@@ -776,7 +776,8 @@ struct RangedRing {
   static constexpr int kData = D * kDataStage;
   static constexpr int kRec = 2 * D * 32 * 16;  // one record slot per lane and stage
   static constexpr int kPrev = CPW * 2 * kRangedSmemStride * 4;
-  static constexpr int kWarpBytes = kData + kRec + kPrev;
+  static constexpr int kLut = 512;  // the warp's copy of its match's P2 table
+  static constexpr int kWarpBytes = kData + kRec + kPrev + kLut;
   static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
 };
 
@@ -802,6 +803,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
   int4* recs = reinterpret_cast<int4*>(wb + R::kData);
   // Buffer b of this lane's chain: words (b * CPW + gi) * kRangedSmemStride onwards.
   uint32_t* prevw = reinterpret_cast<uint32_t*>(wb + R::kData + R::kRec) + gi * kRangedSmemStride;
+  uint16_t* const lut = reinterpret_cast<uint16_t*>(wb + R::kData + R::kRec + R::kPrev);
+  int lut_match = -1;
   uint32_t* ovfc = ovf + (static_cast<int64_t>(blockIdx.x) * wpb * CPW + warp * CPW + gi) * 2 * ovf_words;
   auto stage_cost = [&](int st) -> unsigned char* { return wb + st * R::kDataStage + gi * CH + e0; };
   auto stage_sum = [&](int st) -> unsigned char* {
@@ -830,6 +833,13 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
+    if (job.match != lut_match) {  // the same for the whole warp (one chain block)
+      r3dsimt::syncwarp();
+      for (int k = lane; k < 128; k += 32)
+        reinterpret_cast<uint32_t*>(lut)[k] = reinterpret_cast<const uint32_t*>(m.lut)[k];
+      r3dsimt::syncwarp();
+      lut_match = job.match;
+    }
     const int w = job.w;
     const uint32_t p1x2 = static_cast<uint32_t>(m.p1) * 0x10001u;
     const bool no_carry = m.sum_no_carry != 0;
@@ -912,7 +922,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
         // so the table index is clamped to the table.
         const int dn = recs[((i + 1) & (2 * D - 1)) * 32 + lane].z - icur;
         const uint32_t di = static_cast<uint32_t>(dn < 0 ? -dn : dn) >> 8;
-        lutv = m.lut[di < 255u ? di : 255u];
+        lutv = lut[di < 255u ? di : 255u];
       }
       uint32_t pm = kSent2;
       for (int c = 0; c < nchw; ++c) {
