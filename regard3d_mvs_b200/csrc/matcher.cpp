@@ -1077,10 +1077,9 @@ BatchRun enqueue_batch(r3dgpu_pair* pairs, int count, cudaStream_t s, int slot) 
       Launch L{};
       L.g = &g;
       if (g.kind == kPath || g.kind == kPathRanged) {
-        // Full-range waves up to half the budget (fewer, longer pass launches),
-        // ranged waves (beside them in the same round) up to a quarter.
-        plan_path_waves(g.tiles, matches, g.kind == kPathRanged,
-                        g.kind == kPathRanged ? round_budget / 4 : round_budget / 2, W.sms, A, H, s, L.waves, L.segs,
+        // Waves up to half the budget (fewer, longer pass launches with more
+        // chains in flight); a round has at most one group of each kind.
+        plan_path_waves(g.tiles, matches, g.kind == kPathRanged, round_budget / 2, W.sms, A, H, s, L.waves, L.segs,
                         L.slot_bytes, L.cells_sum, L.px_sum);
         L.njobs = static_cast<int>(g.tiles.size());
         L.grid = 1;

@@ -762,6 +762,9 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 // The buffers of a warp's chains are kRangedSmemStride words apart (odd, so
 // that the chains of a warp start in different banks).
 constexpr int kRangedSmemWords = 32;
+// Ranged pass CTAs have 4 warps: about 15 KB of shared memory per warp
+// (ring, records, predecessor buffers), so that three CTAs fit an SM.
+constexpr int kRangedThreads = 128;
 constexpr int kRangedSmemStride = kRangedSmemWords + 3;
 
 // Ring of the ranged passes: D stages of chunk 0's bytes (kPlanes bytes per
@@ -778,11 +781,11 @@ struct RangedRing {
   static constexpr int kPrev = CPW * 2 * kRangedSmemStride * 4;
   static constexpr int kLut = 512;  // the warp's copy of its match's P2 table
   static constexpr int kWarpBytes = kData + kRec + kPrev + kLut;
-  static constexpr int kBlockBytes = (kPathThreads / 32) * kWarpBytes;
+  static constexpr int kBlockBytes = (kRangedThreads / 32) * kWarpBytes;
 };
 
 template <int G, int K, int MODE>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kRangedThreads)
     sgm_path_ranged_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
                            int cls, int dx, int dy, int64_t total_blocks, const int4* R3D_RESTRICT rec,
                            const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint8_t* terms, int64_t tstride,
@@ -1167,9 +1170,10 @@ constexpr Pass kPasses[8] = {{0, 1, 0},  {1, 0, 1},   {2, 1, 1},  {2, -1, 1},
                              {1, 0, -1}, {2, -1, -1}, {2, 1, -1}, {0, -1, 0}};
 
 template <class Kernel>
-int resident_grid(Kernel kernel, int sms, int64_t work_items, int per_block, size_t smem = 0) {
+int resident_grid(Kernel kernel, int sms, int64_t work_items, int per_block, size_t smem = 0,
+                  int threads = kPathThreads) {
   int per_sm = 1;
-  R3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPathThreads, smem));
+  R3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
   const int64_t need = (work_items + per_block - 1) / per_block;
   const int64_t resident = static_cast<int64_t>(sms) * (per_sm > 0 ? per_sm : 1);
   return static_cast<int>(need < resident ? (need > 0 ? need : 1) : resident);
@@ -1387,9 +1391,9 @@ void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jo
     R3D_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     configured[dev] = 1;
   }
-  int grid = resident_grid(k, sms, nb, kPathThreads / 32, smem);
+  int grid = resident_grid(k, sms, nb, kRangedThreads / 32, smem, kRangedThreads);
   grid = grid < sms * kRangedMaxPerSm ? grid : sms * kRangedMaxPerSm;
-  R3D_LAUNCH(k, dim3(grid), dim3(kPathThreads), smem, s, dm, jobs, njobs, ps.cls, ps.dx, ps.dy, nb, rec, cost, sum,
+  R3D_LAUNCH(k, dim3(grid), dim3(kRangedThreads), smem, s, dm, jobs, njobs, ps.cls, ps.dx, ps.dy, nb, rec, cost, sum,
              terms, tstride, tslot, ovf, ovf_words, cancel);
   launched("sgm_path_ranged_kernel");
   if (ev0 != nullptr) {
