@@ -178,6 +178,27 @@ constexpr int kPathStages = 4;  // ring stages of the ranged passes
 // Per-halfword a + b modulo 2^16.
 R3D_DEVICE uint32_t add2(uint32_t a, uint32_t b, bool no_carry) { return no_carry ? a + b : r3dsimt::vadd2(a, b); }
 
+// v[j] for a runtime j in [0, K): a tree of K - 1 selects on the bits of j
+// (a register array cannot be indexed at run time without local memory).
+template <int N>
+R3D_DEVICE void pick_level(uint32_t* t, bool hi) {
+#pragma unroll
+  for (int k = 0; 2 * k < N; ++k) t[k] = (2 * k + 1 < N && hi) ? t[2 * k + 1] : t[2 * k];
+}
+template <int K>
+R3D_DEVICE uint32_t pick(const uint32_t (&v)[K], int j) {
+  static_assert(K >= 2 && K <= 16, "pick: 2..16 words");
+  constexpr int n1 = (K + 1) / 2, n2 = (n1 + 1) / 2, n3 = (n2 + 1) / 2;
+  uint32_t t[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) t[k] = v[k];
+  pick_level<K>(t, (j & 1) != 0);
+  if constexpr (n1 > 1) pick_level<n1>(t, (j & 2) != 0);
+  if constexpr (n2 > 1) pick_level<n2>(t, (j & 4) != 0);
+  if constexpr (n3 > 1) pick_level<n3>(t, (j & 8) != 0);
+  return t[0];
+}
+
 // Per-warp shared-memory ring of the pass kernels: Stages stages, each with
 // one pixel per chain of the bytes the pass reads (Planes bytes per label:
 // the cost, plus the u16 sum or the seven byte terms).
@@ -222,7 +243,6 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   // label counts are multiples of 16).
   constexpr bool kVec = K % 8 == 0;
   constexpr int NV = K / 8;
-  constexpr int kAhead = 8;  // intensities are prefetched into L2 this many pixels ahead
   R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u);
   const int gi = lane / G, t = lane % G;
@@ -324,7 +344,6 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     for (int k = 0; k < NS - 1; ++k) {
       issue(k, k);
       iq[k] = k < len ? i_in[k * dimg] : 0;
-      if (kAhead + k < len) r3dsimt::prefetch_l2(i_in + (kAhead + k) * dimg);
     }
     const uint16_t* i_next = i_in + (NS - 1) * dimg;
     uint32_t prev[K];
@@ -340,7 +359,6 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
       constexpr int kNext = NS - 1;
       issue(i + kNext, (q + kNext) % NS);
       iq[(q + kNext) % NS] = i + kNext < len ? *i_next : 0;
-      if (i + kNext + kAhead < len) r3dsimt::prefetch_l2(i_next + kAhead * dimg);
       i_next += dimg;
       r3dsimt::cp_async_wait<NS - 1>();
       const int icur = iq[q];
@@ -373,8 +391,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         const int dn = iq[(q + 1) % NS] - icur;
         lutv = lut[(dn < 0 ? -dn : dn) >> 8];
       }
-      const uint32_t pen2 = pen | (pen << 16);
-      const uint32_t negmp = 0u - (pmin | (pmin << 16));
+      const uint32_t pen2 = pen * 0x10001u;
+      const uint32_t negmp = pmin * 0xFFFEFFFFu;  // -(pmin in both halves) modulo 2^32
       const uint32_t hl = r3dsimt::shfl(prev[K - 1], left_lane);
       const uint32_t hr = r3dsimt::shfl(prev[0], right_lane);
       uint32_t wv[K + 2];
@@ -488,45 +506,51 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         // Winner-takes-all over the total sums (sgm_kernels.cpp:332-358):
         // the first minimum, the second best outside +-1, and S at kb -+ 1.
         // Labels of units past nd count as 0xFFFF (they follow every valid
-        // label, so they never come first among equal minima).
+        // label, so they never come first among equal minima); with byte
+        // terms their sum is the sentinel 0x7FFF, above every valid S (at
+        // most 8 (255 + 255)), which serves as well.
         uint32_t sv[K];
 #pragma unroll
-        for (int k = 0; k < K; ++k) sv[k] = uvalid[k / 4] ? s[k] : 0xFFFFFFFFu;
-        // The minimum value, by packed halfword minima and the lane group.
+        for (int k = 0; k < K; ++k) sv[k] = (MODE == kLastTerm || uvalid[k / 4]) ? s[k] : 0xFFFFFFFFu;
+        // The lane's minimum and its first label, as one key S << 16 | label
+        // whose minimum over the lane group is (bcost, kb).
         uint32_t mv = sv[0];
 #pragma unroll
         for (int k = 1; k < K; ++k) mv = r3dsimt::vmin2(mv, sv[k]);
-        const uint32_t bcost = group_umin<G>(r3dsimt::umin(mv & 0xFFFFu, mv >> 16));
-        // Its first label: a bit per label pair word (even labels in the low
-        // half, odd labels in the high half), then the lowest label of the group.
-        const uint32_t b2 = bcost | (bcost << 16);
-        uint32_t hit = 0;
+        const uint32_t lmin = r3dsimt::umin(mv & 0xFFFFu, mv >> 16);
+        // Per word min(S - lmin, 1) is 0 in the halves at the minimum (every
+        // half is >= lmin, so the subtraction borrows nothing).
+        const uint32_t l2 = lmin * 0x10001u;
+        uint32_t miss = 0;
 #pragma unroll
-        for (int k = 0; k < K; ++k) hit |= (r3dsimt::vcmpeq2(sv[k], b2) & 0x00010001u) << k;
+        for (int k = 0; k < K; ++k) miss |= r3dsimt::vmin2(sv[k] - l2, 0x00010001u) << k;
+        const uint32_t hit = ~miss & (((1u << K) - 1u) * 0x10001u);
         const uint32_t he = hit & 0xFFFFu, ho = hit >> 16;
         const uint32_t fe = he != 0 ? static_cast<uint32_t>(2 * (r3dsimt::ffs(he) - 1)) : 0xFFFFu;
         const uint32_t fo = ho != 0 ? static_cast<uint32_t>(2 * (r3dsimt::ffs(ho) - 1) + 1) : 0xFFFFu;
-        const uint32_t first = r3dsimt::umin(fe, fo);
-        const int kb = static_cast<int>(group_umin<G>(first == 0xFFFFu ? 0xFFFFu : first + static_cast<uint32_t>(e0)));
-        // The second best outside kb -+ 1: the three labels masked to 0xFFFF.
+        const uint32_t key = group_umin<G>((lmin << 16) | (r3dsimt::umin(fe, fo) + static_cast<uint32_t>(e0)));
+        const uint32_t bcost = key >> 16;
+        const int kb = static_cast<int>(key & 0xFFFFu);
+        // The second best outside kb -+ 1. Label kb - 1 lies in the lane's
+        // word wa = (kb - 1 - e0) >> 1 (arithmetic shift; out of [0, K) in
+        // other lanes): its high half only when kb - 1 - e0 is odd, then kb and
+        // kb + 1 fill word wa + 1; its both halves when even, then kb + 1 is the
+        // low half of word wa + 1.
+        const int wo = kb - 1 - e0;
+        const int wa = wo >> 1;
+        const uint32_t mask_a = (wo & 1) ? 0xFFFF0000u : 0xFFFFFFFFu;
+        const uint32_t mask_b = (wo & 1) ? 0xFFFFFFFFu : 0x0000FFFFu;
         uint32_t sec2 = 0xFFFFFFFFu;
-        const int d0 = e0 - kb + 1;  // label e0 + 2k lies in kb -+ 1 iff d0 + 2k is in [0, 2]
 #pragma unroll
         for (int k = 0; k < K; ++k) {
-          const uint32_t d = static_cast<uint32_t>(d0 + 2 * k);
-          const uint32_t mask = (d <= 2u ? 0xFFFFu : 0u) | (d + 1u <= 2u ? 0xFFFF0000u : 0u);
-          sec2 = r3dsimt::vmin2(sec2, sv[k] | mask);
+          const uint32_t m = (k == wa ? mask_a : 0u) | (k == wa + 1 ? mask_b : 0u);
+          sec2 = r3dsimt::vmin2(sec2, sv[k] | m);
         }
         const uint32_t sec = group_umin<G>(r3dsimt::umin(sec2 & 0xFFFFu, sec2 >> 16));
         const int km = kb > 0 ? kb - 1 : 0, kp = kb + 1 < nd ? kb + 1 : nd - 1;
-        const int jm = (km % (2 * K)) >> 1, jp = (kp % (2 * K)) >> 1;
-        uint32_t vm = 0, vp = 0;
-#pragma unroll
-        for (int k = 0; k < K; ++k) {
-          if (k == jm) vm = s[k];
-          if (k == jp) vp = s[k];
-        }
         const int base_lane = gi * G;
+        uint32_t vm = pick<K>(s, (km % (2 * K)) >> 1);
+        uint32_t vp = pick<K>(s, (kp % (2 * K)) >> 1);
         vm = r3dsimt::shfl(vm, (base_lane + km / (2 * K)) & 31);
         vp = r3dsimt::shfl(vp, (base_lane + kp / (2 * K)) & 31);
         const uint32_t sm = (km & 1) ? (vm >> 16) : (vm & 0xFFFFu);

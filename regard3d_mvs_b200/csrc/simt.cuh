@@ -42,13 +42,23 @@ R3D_DEVICE int ffs(uint32_t v) { return __ffs(static_cast<int>(v)); }  // 1 + in
 R3D_DEVICE void syncwarp() { __syncwarp(); }
 R3D_DEVICE void syncthreads() { __syncthreads(); }
 R3D_DEVICE void fence() { __threadfence(); }
-R3D_DEVICE uint32_t vmin2(uint32_t a, uint32_t b) { return __vminu2(a, b); }
+// Per-halfword unsigned minimum and sum modulo 2^16: the u16x2 instructions
+// of sm_90+, written as PTX so that no emulated SIMD-video form is chosen.
+R3D_DEVICE uint32_t vmin2(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("min.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
+R3D_DEVICE uint32_t vadd2(uint32_t a, uint32_t b) {
+  uint32_t r;
+  asm("add.u16x2 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(b));
+  return r;
+}
 // Per-halfword a == b ? 0xFFFF : 0.
 R3D_DEVICE uint32_t vcmpeq2(uint32_t a, uint32_t b) { return __vcmpeq2(a, b); }
 // Per-halfword min(a, b, c) and min(a + b, c) (DPX instructions on sm_90+).
-R3D_DEVICE uint32_t vmin3(uint32_t a, uint32_t b, uint32_t c) { return __vimin3_u16x2(a, b, c); }
-R3D_DEVICE uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) { return __viaddmin_u16x2(a, b, c); }
-R3D_DEVICE uint32_t vadd2(uint32_t a, uint32_t b) { return __vadd2(a, b); }
+R3D_DEVICE uint32_t vmin3(uint32_t a, uint32_t b, uint32_t c) { return vmin2(vmin2(a, b), c); }
+R3D_DEVICE uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) { return vmin2(vadd2(a, b), c); }
 R3D_DEVICE uint32_t perm(uint32_t a, uint32_t b, uint32_t s) { return __byte_perm(a, b, s); }
 // Low word of (hi:lo) >> s, s in [0, 31].
 R3D_DEVICE uint32_t funnel_r(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_r(lo, hi, s); }
