@@ -230,7 +230,7 @@ def pass_roofline(launch_log, peak, peak_kind):
     traffic = None
     if tpc and all(m in tpc for m in by_mode):
         traffic = sum(tpc[m] * b["cells"] for m, b in by_mode.items()) / len(passes)
-    out = {"bound": "hbm", "kernel": "sgm_path_kernel (one chain pass of full-range tiles)", "achieved": achieved,
+    out = {"bound": "hbm", "kernel": "sgm_path_kernel (chain passes of full-range tiles; a launch runs one pass, or the seven term passes of a tile group)", "achieved": achieved,
            "peak": peak, "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": achieved / peak,
            "traffic": traffic, "traffic_source": "profiles/sgm_path_traffic.json (ncu DRAM bytes per cell by mode)",
            "launches": len(passes), "avg_launch_ms": ms / len(passes), "alg_bytes_per_launch": nbytes / len(passes),

@@ -147,13 +147,33 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
         if (inside) {
           // Label a = c + k reads right column bx - dmin - a = xr0 + (x + nd - 1 - a).
           const int base = x + nd - 1 - c;
+          const int xr_first = bx - m.dmin - c;  // right column of label c; label c + k reads xr_first - k
+          if (xr_first <= rv.last && xr_first - (nl - 1) >= rv.first) {
+            // Every label of the run reads a valid right column: four costs a
+            // word, the two 32-bit popcounts of each Census XOR packed
+            // separately by multiply-adds (each byte at most 32, no carries).
 #pragma unroll
-          for (int k = 0; k < 32; ++k) {
-            if (k < nl) {
-              const int xr = bx - m.dmin - c - k;
-              const bool ok = xr >= rv.first && xr <= rv.last;
-              const uint32_t v = ok ? static_cast<uint32_t>(r3dsimt::popc64(cl ^ stage[base - k])) : inv;
-              q[k >> 2] |= v << (8 * (k & 3));
+            for (int w4 = 0; w4 < 8; ++w4) {
+              if (4 * w4 < nl) {
+                uint32_t lo = 0, hi = 0;
+#pragma unroll
+                for (int i = 3; i >= 0; --i) {
+                  const uint64_t d = cl ^ stage[base - 4 * w4 - i];
+                  lo = lo * 256u + static_cast<uint32_t>(r3dsimt::popc(static_cast<uint32_t>(d)));
+                  hi = hi * 256u + static_cast<uint32_t>(r3dsimt::popc(static_cast<uint32_t>(d >> 32)));
+                }
+                q[w4] = lo + hi;
+              }
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+              if (k < nl) {
+                const int xr = xr_first - k;
+                const bool ok = xr >= rv.first && xr <= rv.last;
+                const uint32_t v = ok ? static_cast<uint32_t>(r3dsimt::popc64(cl ^ stage[base - k])) : inv;
+                q[k >> 2] |= v << (8 * (k & 3));
+              }
             }
           }
         }
@@ -173,6 +193,13 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
 // the sum modulo 2^16 is the plain sum) and takes the winner-takes-all.
 enum PassMode { kFirst = 0, kAccumulate = 1, kLast = 2, kTerm = 3, kLastTerm = 4 };
 constexpr int kTermArrays = 7;
+// The passes of one launch: n directions, chain blocks of pass q numbered
+// from start[q] (start[n] = all blocks), slot = its term array.
+struct PassSet {
+  int n;
+  int cls[kTermArrays], dx[kTermArrays], dy[kTermArrays], slot[kTermArrays];
+  int64_t start[kTermArrays + 1];
+};
 constexpr int kPathStages = 4;  // ring stages of the ranged passes
 
 // Per-halfword a + b modulo 2^16.
@@ -227,12 +254,15 @@ struct PathRing {
 // (advanced by one pixel along the path per step) instead of recomputing
 // addresses. The first pixel needs no special case: with a zero predecessor
 // vector and a zero minimum, best = 0, so T = 0 and L = C there.
+//
+// One launch runs the passes of a PassSet: a single pass, or the seven term
+// passes of a segment at once (they only read the costs and each writes its
+// own term array, so their chain blocks can be taken in any order).
 template <int G, int K, int MODE>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
-    sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs, int cls,
-                    int dx, int dy, int64_t total_blocks, const uint8_t* R3D_RESTRICT cost, uint16_t* sum,
-                    uint8_t* terms, int64_t tstride, int tslot, int4* R3D_RESTRICT info, uint32_t* rkeys,
-                    const int* cancel) {
+    sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
+                    const PassSet ps, const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint8_t* terms,
+                    int64_t tstride, int4* R3D_RESTRICT info, uint32_t* rkeys, const int* cancel) {
   constexpr int CPW = 32 / G;  // chains per warp
   constexpr int U = K / 4;     // units of 8 labels per lane
   constexpr int NS = PathRing<G, K, MODE>::kStages;
@@ -260,8 +290,23 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   unsigned char* const ring_cost = ring + gi * Ring::ND + e0;
   unsigned char* const ring_sum = ring + CPW * Ring::ND + gi * 2 * Ring::ND + 2 * e0;
   unsigned char* const ring_term = ring + CPW * Ring::ND + gi * Ring::ND + e0;  // + r * CPW * ND
-  for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + (threadIdx.x >> 5); blk < total_blocks; blk += nwarps) {
+  const int64_t total_blocks = ps.start[ps.n];
+  for (int64_t gblk = static_cast<int64_t>(blockIdx.x) * wpb + (threadIdx.x >> 5); gblk < total_blocks;
+       gblk += nwarps) {
     if (cancelled(cancel)) break;
+    // The pass of the block (static indices only: no local copy of ps).
+    int cls = ps.cls[0], dx = ps.dx[0], dy = ps.dy[0], tslot = ps.slot[0];
+    int64_t blk = gblk;
+#pragma unroll
+    for (int q = 1; q < kTermArrays; ++q) {
+      if (q < ps.n && gblk >= ps.start[q]) {
+        cls = ps.cls[q];
+        dx = ps.dx[q];
+        dy = ps.dy[q];
+        tslot = ps.slot[q];
+        blk = gblk - ps.start[q];
+      }
+    }
     const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
@@ -1217,9 +1262,9 @@ uint64_t pass_bytes(int mode, bool ranged, const SgmPathSegment& g) {
 }
 
 template <int G, int K, int MODE>
-void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
-                 const uint8_t* cost, uint16_t* sum, uint8_t* terms, int64_t tstride, int tslot, int4* info,
-                 uint32_t* rkeys, int sms, cudaStream_t s, const SgmPathSegment& seg, const int* cancel) {
+void launch_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, const uint8_t* cost,
+                 uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, int sms, cudaStream_t s,
+                 const SgmPathSegment& seg, const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_kernel<G, K, MODE>;
   constexpr size_t smem = PathRing<G, K, MODE>::kBlockBytes;
@@ -1230,44 +1275,62 @@ void launch_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int
     R3D_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     configured[dev] = 1;
   }
+  const int64_t nb = ps.start[ps.n];
   R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32, smem)), dim3(kPathThreads), smem, s, dm, jobs,
-             njobs, ps.cls, ps.dx, ps.dy, nb, cost, sum, terms, tstride, tslot, info, rkeys, cancel);
+             njobs, ps, cost, sum, terms, tstride, info, rkeys, cancel);
   launched("sgm_path_kernel");
   if (ev0 != nullptr) {
     char shape[32];
     std::snprintf(shape, sizeof(shape), "%dx%d/mode%d", G, K, MODE);
-    profile_pass(ev0, profile_mark(s), "sgm_path_kernel", shape, static_cast<uint64_t>(seg.cells),
-                 static_cast<uint64_t>(seg.pixels), pass_bytes(MODE, false, seg));
+    const uint64_t n = static_cast<uint64_t>(ps.n);
+    profile_pass(ev0, profile_mark(s), "sgm_path_kernel", shape, n * static_cast<uint64_t>(seg.cells),
+                 n * static_cast<uint64_t>(seg.pixels), n * pass_bytes(MODE, false, seg));
   }
+}
+
+// Passes q of kPasses in `qs` (count n) as one PassSet.
+PassSet pass_set(const SgmPathSegment& g, const int* qs, int n) {
+  PassSet ps{};
+  int64_t start = 0;
+  for (int i = 0; i < n; ++i) {
+    const Pass& p = kPasses[qs[i]];
+    ps.cls[ps.n] = p.cls;
+    ps.dx[ps.n] = p.dx;
+    ps.dy[ps.n] = p.dy;
+    ps.slot[ps.n] = qs[i];
+    ps.start[ps.n] = start;
+    start += g.blocks[p.cls];
+    ++ps.n;
+  }
+  ps.start[ps.n] = start;
+  return ps;
 }
 
 template <int G, int K>
 void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const uint8_t* cost,
                    uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, int sms,
                    cudaStream_t s, const int* cancel) {
+  for (int q = 0; q < 8; ++q)
+    if (g.blocks[kPasses[q].cls] <= 0) return;  // no pixels: every class has chains otherwise
+  if (terms != nullptr) {
+    // The seven term passes in one launch, then the last pass, which finds
+    // all seven term arrays written.
+    const int qs[kTermArrays] = {0, 1, 2, 3, 4, 5, 6};
+    const int last = 7;
+    launch_pass<G, K, kTerm>(pass_set(g, qs, kTermArrays), dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys,
+                             sms, s, g, cancel);
+    launch_pass<G, K, kLastTerm>(pass_set(g, &last, 1), dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys,
+                                 sms, s, g, cancel);
+    return;
+  }
   for (int q = 0; q < 8; ++q) {
-    const Pass ps = kPasses[q];
-    const int64_t nb = g.blocks[ps.cls];
-    if (nb <= 0) continue;
-    if (terms != nullptr) {
-      // Every pass runs (a segment with pixels has chains of every class), so
-      // the last pass finds all seven term arrays written.
-      if (q < 7)
-        launch_pass<G, K, kTerm>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, q, info, rkeys, sms, s, g,
-                                 cancel);
-      else
-        launch_pass<G, K, kLastTerm>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s,
-                                     g, cancel);
-    } else if (q == 0) {
-      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s, g,
-                                cancel);
-    } else if (q < 7) {
-      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s, g,
-                                     cancel);
-    } else {
-      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, nb, cost, sum, terms, tstride, 0, info, rkeys, sms, s, g,
-                               cancel);
-    }
+    const PassSet ps = pass_set(g, &q, 1);
+    if (q == 0)
+      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, sms, s, g, cancel);
+    else if (q < 7)
+      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, sms, s, g, cancel);
+    else
+      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, sms, s, g, cancel);
   }
 }
 

@@ -62,6 +62,7 @@ R3D_DEVICE uint32_t vaddmin2(uint32_t a, uint32_t b, uint32_t c) { return vmin2(
 R3D_DEVICE uint32_t perm(uint32_t a, uint32_t b, uint32_t s) { return __byte_perm(a, b, s); }
 // Low word of (hi:lo) >> s, s in [0, 31].
 R3D_DEVICE uint32_t funnel_r(uint32_t lo, uint32_t hi, uint32_t s) { return __funnelshift_r(lo, hi, s); }
+R3D_DEVICE int popc(uint32_t v) { return __popc(v); }
 R3D_DEVICE int popc64(uint64_t v) { return __popcll(v); }
 // Streaming (evict-first) 16-byte load and store.
 R3D_DEVICE uint4 ld_stream(const uint4* p) { return __ldcs(p); }
@@ -189,6 +190,7 @@ inline uint32_t perm(uint32_t a, uint32_t b, uint32_t s) {
 inline uint32_t funnel_r(uint32_t lo, uint32_t hi, uint32_t s) {
   return static_cast<uint32_t>(((static_cast<uint64_t>(hi) << 32) | lo) >> (s & 31u));
 }
+inline int popc(uint32_t v) { return __builtin_popcount(v); }
 inline int popc64(uint64_t v) { return __builtin_popcountll(v); }
 inline uint4 ld_stream(const uint4* p) { return *p; }
 inline void st_stream(uint4* p, uint4 v) { *p = v; }
