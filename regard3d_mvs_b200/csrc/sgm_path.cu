@@ -107,7 +107,7 @@ constexpr int kCostStage = 2048;  // staged partner codes per warp at most (sgm_
 // width + labels - 1), so that narrow waves run more CTAs per SM.
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     sgm_path_cost_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
-                         int64_t rows, uint8_t* R3D_RESTRICT cost, int stage_words) {
+                         int64_t rows, uint8_t* R3D_RESTRICT cost, int stage_words, uint16_t* R3D_RESTRICT ints) {
   R3D_DYNAMIC_SMEM(smem);
   const int lane = static_cast<int>(threadIdx.x & 31u), warp = static_cast<int>(threadIdx.x >> 5);
   const int wpb = static_cast<int>(blockDim.x) >> 5;
@@ -130,6 +130,12 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kPathThreads)
     for (int k = lane; k < span; k += 32) {
       const int xr = xr0 + k;
       stage[k] = (xr >= rv.first && xr <= rv.last) ? crow[xr] : 0;
+    }
+    // The row's base intensities, for the pass kernels.
+    {
+      const uint16_t* irow = m.base + static_cast<int64_t>(by) * m.base_stride + job.x0;
+      uint16_t* iout = ints + job.px_off + static_cast<int64_t>(y) * w;
+      for (int x = lane; x < w; x += 32) iout[x] = irow[x];
     }
     r3dsimt::syncwarp();
     const uint32_t inv = static_cast<uint32_t>(m.invalid_cost);
@@ -236,18 +242,24 @@ struct PathMode {
   static constexpr int kPlanes = MODE == kAccumulate || MODE == kLast ? 3 : (MODE == kLastTerm ? 1 + kTermArrays : 1);
   static constexpr int kStages = MODE == kLastTerm ? 3 : (MODE == kTerm ? 8 : 4);
 };
+// A stage ends with one 4-byte word per lane: the aligned word of the
+// intensities that holds its chain's pixel (every lane copies its own, since
+// a cp.async wait covers only the waiting thread's copies).
 template <int G, int K, int MODE>
 struct PathRing {
   static constexpr int ND = 2 * G * K;
   static constexpr int kStages = PathMode<MODE>::kStages;
-  static constexpr int kStageBytes = (32 / G) * PathMode<MODE>::kPlanes * ND;
+  static constexpr int kPlaneBytes = (32 / G) * PathMode<MODE>::kPlanes * ND;
+  static constexpr int kIntBytes = 32 * 4;
+  static constexpr int kStageBytes = kPlaneBytes + kIntBytes;
   static constexpr int kWarpBytes = kStages * kStageBytes;
   // Each warp's rings, then each warp's copy of its match's P2 table.
   static constexpr int kBlockBytes = (kPathThreads / 32) * (kWarpBytes + 512);
 };
 
-// Three CTAs per SM for the 8-word shapes (up to 80 registers, no spills);
-// the 12- and 16-word shapes keep two.
+// CTAs per SM: four for the 8-word term passes (64 registers, no spills),
+// three for the other 8-word passes (up to 80), two for the 12- and 16-word
+// shapes.
 //
 // The step loop is unrolled by the ring depth NS so that ring slots and the
 // intensity queue are indexed statically; each chain keeps running pointers
@@ -259,10 +271,11 @@ struct PathRing {
 // passes of a segment at once (they only read the costs and each writes its
 // own term array, so their chain blocks can be taken in any order).
 template <int G, int K, int MODE>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? (MODE == kTerm ? 4 : 3) : 2))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
                     const PassSet ps, const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint8_t* terms,
-                    int64_t tstride, int4* R3D_RESTRICT info, uint32_t* rkeys, const int* cancel) {
+                    int64_t tstride, int4* R3D_RESTRICT info, uint32_t* rkeys, const uint16_t* R3D_RESTRICT ints,
+                    const int* cancel) {
   constexpr int CPW = 32 / G;  // chains per warp
   constexpr int U = K / 4;     // units of 8 labels per lane
   constexpr int NS = PathRing<G, K, MODE>::kStages;
@@ -290,6 +303,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
   unsigned char* const ring_cost = ring + gi * Ring::ND + e0;
   unsigned char* const ring_sum = ring + CPW * Ring::ND + gi * 2 * Ring::ND + 2 * e0;
   unsigned char* const ring_term = ring + CPW * Ring::ND + gi * Ring::ND + e0;  // + r * CPW * ND
+  unsigned char* const ring_int = ring + Ring::kPlaneBytes + lane * 4;
   const int64_t total_blocks = ps.start[ps.n];
   for (int64_t gblk = static_cast<int64_t>(blockIdx.x) * wpb + (threadIdx.x >> 5); gblk < total_blocks;
        gblk += nwarps) {
@@ -331,7 +345,6 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     // Running offsets (cells, pixels) of the pixel being issued (NS - 1
     // ahead) and of the pixel being computed.
     const int64_t dcell = (static_cast<int64_t>(dy) * w + dx) * nd;
-    const int64_t dimg = static_cast<int64_t>(dy) * m.base_stride + dx;
     const int64_t cell0 = job.cell_off + e0 + (static_cast<int64_t>(sy) * w + sx) * nd;
     const uint8_t* c_in = cost + cell0;
     const uint16_t* s_in = sum + cell0;
@@ -340,7 +353,13 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
     uint8_t* t_out = terms + cell0 + static_cast<int64_t>(tslot) * tstride;
     int64_t px_out = job.px_off + static_cast<int64_t>(sy) * w + sx;
     const int64_t dpx = static_cast<int64_t>(dy) * w + dx;
-    const uint16_t* i_in = m.base + (static_cast<int64_t>(job.y0) + sy) * m.base_stride + job.x0 + sx;
+    // Intensity of the pixel being issued (each lane copies the aligned
+    // 4-byte word holding it into the stage), and the parity of the
+    // chain's first pixel (which half of a staged word holds the intensity:
+    // pixel i's parity is par0 ^ (i & dpar)).
+    const uint16_t* i_iss = ints + job.px_off + static_cast<int64_t>(sy) * w + sx;
+    const uint32_t par0 = static_cast<uint32_t>(reinterpret_cast<uintptr_t>(i_iss) >> 1) & 1u;
+    const uint32_t dpar = static_cast<uint32_t>(dpx) & 1u;
     int x = sx, y = sy;
 
     auto issue = [&](int i, int st) {
@@ -378,35 +397,32 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
             }
           }
         }
+        r3dsimt::cp_async4(ring_int + st * Ring::kStageBytes,
+                           reinterpret_cast<const void*>(reinterpret_cast<uintptr_t>(i_iss) & ~uintptr_t{3}));
       }
       r3dsimt::cp_async_commit();
       c_in += dcell;
       if constexpr (kReadsSum) s_in += dcell;
       if constexpr (MODE == kLastTerm) t_in += dcell;
+      i_iss += dpx;
     };
-    int iq[NS];
 #pragma unroll
-    for (int k = 0; k < NS - 1; ++k) {
-      issue(k, k);
-      iq[k] = k < len ? i_in[k * dimg] : 0;
-    }
-    const uint16_t* i_next = i_in + (NS - 1) * dimg;
+    for (int k = 0; k < NS - 1; ++k) issue(k, k);
     uint32_t prev[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) prev[k] = 0;
     uint32_t pmin = 0;
-    // P2 of the step's intensity change, loaded one step ahead (the value of
-    // the first step is unused: its predecessor vector is zero).
-    uint32_t lutv = 0;
+    // The previous pixel's intensity (the first step's P2 is unused: its
+    // predecessor vector is zero).
+    int iprev = 0;
 
     auto step = [&](const int i, const int q) {
       const bool on = i < len;
       constexpr int kNext = NS - 1;
       issue(i + kNext, (q + kNext) % NS);
-      iq[(q + kNext) % NS] = i + kNext < len ? *i_next : 0;
-      i_next += dimg;
       r3dsimt::cp_async_wait<NS - 1>();
-      const int icur = iq[q];
+      const uint32_t iw = *reinterpret_cast<const uint32_t*>(ring_int + q * Ring::kStageBytes);
+      const int icur = static_cast<int>((iw >> (16u * ((par0 ^ (static_cast<uint32_t>(i) & dpar)) & 1u))) & 0xFFFFu);
       const unsigned char* sc = ring_cost + q * Ring::kStageBytes;
       uint2 craw[U];
       if constexpr (kVec) {
@@ -430,12 +446,9 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? 3 : 2))
         c2[4 * u + 3] = r3dsimt::perm(craw[u].y, 0u, 0x4342u);
       }
       // out = L_r = C + T_r with T_r = best - min L(q).
-      const uint32_t pen = pmin + lutv;
-      {
-        // The next step's P2: its intensity came in NS - 2 steps ago.
-        const int dn = iq[(q + 1) % NS] - icur;
-        lutv = lut[(dn < 0 ? -dn : dn) >> 8];
-      }
+      const int dn = icur - iprev;
+      iprev = icur;
+      const uint32_t pen = pmin + lut[(dn < 0 ? -dn : dn) >> 8];
       const uint32_t pen2 = pen * 0x10001u;
       const uint32_t negmp = pmin * 0xFFFEFFFFu;  // -(pmin in both halves) modulo 2^32
       const uint32_t hl = r3dsimt::shfl(prev[K - 1], left_lane);
@@ -1263,8 +1276,8 @@ uint64_t pass_bytes(int mode, bool ranged, const SgmPathSegment& g) {
 
 template <int G, int K, int MODE>
 void launch_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, const uint8_t* cost,
-                 uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, int sms, cudaStream_t s,
-                 const SgmPathSegment& seg, const int* cancel) {
+                 uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, const uint16_t* ints,
+                 int sms, cudaStream_t s, const SgmPathSegment& seg, const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_kernel<G, K, MODE>;
   constexpr size_t smem = PathRing<G, K, MODE>::kBlockBytes;
@@ -1277,7 +1290,7 @@ void launch_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, 
   }
   const int64_t nb = ps.start[ps.n];
   R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, kPathThreads / 32, smem)), dim3(kPathThreads), smem, s, dm, jobs,
-             njobs, ps, cost, sum, terms, tstride, info, rkeys, cancel);
+             njobs, ps, cost, sum, terms, tstride, info, rkeys, ints, cancel);
   launched("sgm_path_kernel");
   if (ev0 != nullptr) {
     char shape[32];
@@ -1308,8 +1321,8 @@ PassSet pass_set(const SgmPathSegment& g, const int* qs, int n) {
 
 template <int G, int K>
 void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const uint8_t* cost,
-                   uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, int sms,
-                   cudaStream_t s, const int* cancel) {
+                   uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, const uint16_t* ints,
+                   int sms, cudaStream_t s, const int* cancel) {
   for (int q = 0; q < 8; ++q)
     if (g.blocks[kPasses[q].cls] <= 0) return;  // no pixels: every class has chains otherwise
   if (terms != nullptr) {
@@ -1318,19 +1331,22 @@ void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegm
     const int qs[kTermArrays] = {0, 1, 2, 3, 4, 5, 6};
     const int last = 7;
     launch_pass<G, K, kTerm>(pass_set(g, qs, kTermArrays), dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys,
-                             sms, s, g, cancel);
+                             ints, sms, s, g, cancel);
     launch_pass<G, K, kLastTerm>(pass_set(g, &last, 1), dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys,
-                                 sms, s, g, cancel);
+                                 ints, sms, s, g, cancel);
     return;
   }
   for (int q = 0; q < 8; ++q) {
     const PassSet ps = pass_set(g, &q, 1);
     if (q == 0)
-      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, sms, s, g, cancel);
+      launch_pass<G, K, kFirst>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, ints, sms, s, g,
+                                cancel);
     else if (q < 7)
-      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, sms, s, g, cancel);
+      launch_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, ints, sms, s, g,
+                                     cancel);
     else
-      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, sms, s, g, cancel);
+      launch_pass<G, K, kLast>(ps, dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys, ints, sms, s, g,
+                               cancel);
   }
 }
 
@@ -1408,6 +1424,10 @@ SgmPathBuffers sgm_path_buffers(int64_t cells, int64_t pixels, int64_t keys, boo
   o += align256(static_cast<size_t>(pixels) * 16);
   b.rkeys = o;
   o += align256(static_cast<size_t>(keys) * 4);
+  // The tiles' base intensities, pixel after pixel, and 16 bytes more: the
+  // pass kernels copy the aligned 4-byte word holding a pixel's intensity.
+  b.ints = o;
+  o += align256(static_cast<size_t>(pixels) * 2 + 16);
   b.total = o;
   return b;
 }
@@ -1420,6 +1440,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
   uint8_t* terms = wave.terms != 0 ? wave.buffer + B.terms : nullptr;
   int4* info = reinterpret_cast<int4*>(wave.buffer + B.info);
   uint32_t* rkeys = reinterpret_cast<uint32_t*>(wave.buffer + B.rkeys);
+  uint16_t* ints = reinterpret_cast<uint16_t*>(wave.buffer + B.ints);
   if (wave.keys > 0) R3D_CUDA(cudaMemsetAsync(rkeys, 0xFF, static_cast<size_t>(wave.keys) * 4, s));
   {
     constexpr size_t max_smem = static_cast<size_t>(kPathThreads / 32) * kCostStage * 8;
@@ -1435,7 +1456,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
     const size_t smem = static_cast<size_t>(kPathThreads / 32) * words * 8;
     R3D_LAUNCH(sgm_path_cost_kernel,
                dim3(resident_grid(sgm_path_cost_kernel, sms, wave.rows, kPathThreads / 32, smem)),
-               dim3(kPathThreads), smem, s, dm, wave.jobs, wave.njobs, wave.rows, cost, words);
+               dim3(kPathThreads), smem, s, dm, wave.jobs, wave.njobs, wave.rows, cost, words, ints);
     launched("sgm_path_cost_kernel");
   }
   for (int q = 0; q < wave.nsegs; ++q) {
@@ -1444,7 +1465,7 @@ void launch_sgm_path_wave(const SgmMatch* dm, const SgmPathWave& wave, int sms, 
     bool done = false;
 #define R3D_SHAPE(gg, kk)                                                                                     \
   if (!done && g.shape.g_ == gg && g.shape.k_ == kk) {                                                        \
-    launch_passes<gg, kk>(dm, jobs, g, cost, sum, terms, B.term_stride, info, rkeys, sms, s, wave.cancel);   \
+    launch_passes<gg, kk>(dm, jobs, g, cost, sum, terms, B.term_stride, info, rkeys, ints, sms, s, wave.cancel); \
     done = true;                                                                                              \
   }
     R3D_PATH_SHAPES(R3D_SHAPE)

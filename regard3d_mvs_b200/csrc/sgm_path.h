@@ -52,7 +52,7 @@ inline int64_t sgm_path_chains(int cls, int w, int h) { return cls == 0 ? h : (c
 // seven arrays of term_stride bytes from `terms` on (full-range waves keep
 // them in place of the u16 sum volume, ranged waves beside it).
 struct SgmPathBuffers {
-  size_t cost, sum, terms, info, rkeys, total;
+  size_t cost, sum, terms, info, rkeys, ints, total;  // ints: full-range waves, the tiles' intensities
   int64_t term_stride;
   size_t rec, rowsum, rowstart, rowshift, overflow;  // ranged waves only
   int64_t overflow_words;                            // per chain buffer

@@ -81,6 +81,12 @@ R3D_DEVICE void cp_async8(void* smem_dst, const void* gmem_src) {
   const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem_src) : "memory");
 }
+// 4-byte asynchronous global -> shared copy (through L1). Both addresses
+// must be 4-byte aligned.
+R3D_DEVICE void cp_async4(void* smem_dst, const void* gmem_src) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem_dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
 // Hint: bring the line holding p into L2 (no register, no wait).
 R3D_DEVICE void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 R3D_DEVICE void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
@@ -197,6 +203,7 @@ inline void st_stream(uint4* p, uint4 v) { *p = v; }
 inline void st_stream8(uint2* p, uint2 v) { *p = v; }
 void cp_async16(void* smem_dst, const void* gmem_src);
 void cp_async8(void* smem_dst, const void* gmem_src);
+void cp_async4(void* smem_dst, const void* gmem_src);
 void cp_async_commit();
 void cp_async_wait_n(int n);
 inline void prefetch_l2(const void*) {}

@@ -207,6 +207,18 @@ void cp_async8(void* dst, const void* src) {
   t_cur->pending.push_back(c);
 }
 
+void cp_async4(void* dst, const void* src) {
+  if ((reinterpret_cast<uintptr_t>(dst) & 3u) || (reinterpret_cast<uintptr_t>(src) & 3u))
+    throw std::runtime_error("simt: misaligned cp.async");
+  unsigned char* d = static_cast<unsigned char*>(dst);
+  if (d < t_smem.get() || d + 4 > t_smem.get() + t_smem_size) throw std::runtime_error("simt: cp.async outside shared memory");
+  Copy c;
+  c.dst = d;
+  c.size = 4;
+  std::memcpy(c.bytes, src, 4);
+  t_cur->pending.push_back(c);
+}
+
 void cp_async_commit() {
   t_cur->groups.push_back(std::move(t_cur->pending));
   t_cur->pending.clear();
