@@ -869,9 +869,9 @@ struct RangedRing {
 template <int G, int K, int MODE>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kRangedThreads)
     sgm_path_ranged_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
-                           int cls, int dx, int dy, int64_t total_blocks, const int4* R3D_RESTRICT rec,
-                           const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint8_t* terms, int64_t tstride,
-                           int tslot, uint32_t* ovf, int64_t ovf_words, const int* cancel) {
+                           const PassSet ps, const int4* R3D_RESTRICT rec, const uint8_t* R3D_RESTRICT cost,
+                           uint16_t* sum, uint8_t* terms, int64_t tstride, uint32_t* ovf, int64_t ovf_words,
+                           const int* cancel) {
   // Modes: kFirst / kAccumulate write or add u16 sums; kTerm writes the
   // pass's byte terms; kLastTerm writes S = L_8 + 7 C + sum of the seven
   // terms as the u16 sum (read by the per-pixel winner-takes-all).
@@ -913,8 +913,22 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kRangedThreads)
     if (idx < kRangedSmemWords) prevw[b * CPW * kRangedSmemStride + 1 + idx] = v;
     else ovfc[b * ovf_words + (idx - kRangedSmemWords)] = v;
   };
-  for (int64_t blk = static_cast<int64_t>(blockIdx.x) * wpb + warp; blk < total_blocks; blk += nwarps) {
+  const int64_t total_blocks = ps.start[ps.n];
+  for (int64_t gblk = static_cast<int64_t>(blockIdx.x) * wpb + warp; gblk < total_blocks; gblk += nwarps) {
     if (cancelled(cancel)) break;
+    // The pass of the block (static indices only: no local copy of ps).
+    int cls = ps.cls[0], dx = ps.dx[0], dy = ps.dy[0], tslot = ps.slot[0];
+    int64_t blk = gblk;
+#pragma unroll
+    for (int q = 1; q < kTermArrays; ++q) {
+      if (q < ps.n && gblk >= ps.start[q]) {
+        cls = ps.cls[q];
+        dx = ps.dx[q];
+        dy = ps.dy[q];
+        tslot = ps.slot[q];
+        blk = gblk - ps.start[q];
+      }
+    }
     const int j = find_job(jobs, njobs, blk, [cls](const SgmPathJob& q) { return q.blk[cls]; });
     const SgmPathJob& job = jobs[j];
     const SgmMatch& m = matches[job.match];
@@ -1485,10 +1499,9 @@ namespace {
 constexpr int kRangedMaxPerSm = 4;
 
 template <int G, int K, int MODE>
-void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, int64_t nb,
-                        const int4* rec, const uint8_t* cost, uint16_t* sum, uint8_t* terms, int64_t tstride,
-                        int tslot, uint32_t* ovf, int64_t ovf_words, int sms, cudaStream_t s, const SgmPathSegment& seg,
-                        const int* cancel) {
+void launch_ranged_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, const int4* rec,
+                        const uint8_t* cost, uint16_t* sum, uint8_t* terms, int64_t tstride, uint32_t* ovf,
+                        int64_t ovf_words, int sms, cudaStream_t s, const SgmPathSegment& seg, const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
   auto* k = sgm_path_ranged_kernel<G, K, MODE>;
   constexpr size_t smem = RangedRing<G, K, MODE>::kBlockBytes;
@@ -1499,19 +1512,21 @@ void launch_ranged_pass(const Pass& ps, const SgmMatch* dm, const SgmPathJob* jo
     R3D_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     configured[dev] = 1;
   }
+  const int64_t nb = ps.start[ps.n];
   int grid = resident_grid(k, sms, nb, kRangedThreads / 32, smem, kRangedThreads);
   grid = grid < sms * kRangedMaxPerSm ? grid : sms * kRangedMaxPerSm;
-  R3D_LAUNCH(k, dim3(grid), dim3(kRangedThreads), smem, s, dm, jobs, njobs, ps.cls, ps.dx, ps.dy, nb, rec, cost, sum,
-             terms, tstride, tslot, ovf, ovf_words, cancel);
+  R3D_LAUNCH(k, dim3(grid), dim3(kRangedThreads), smem, s, dm, jobs, njobs, ps, rec, cost, sum, terms, tstride, ovf,
+             ovf_words, cancel);
   launched("sgm_path_ranged_kernel");
   if (ev0 != nullptr) {
     char shape[32];
     std::snprintf(shape, sizeof(shape), "%dx%d/mode%d", G, K, MODE);
     // Per pixel and pass also the 16-byte record (range and cell offset).
+    const uint64_t n = static_cast<uint64_t>(ps.n);
     const uint64_t alg = MODE == kLastTerm ? (1 + kTermArrays + 2) * static_cast<uint64_t>(seg.cells)
                                            : pass_bytes(MODE, true, seg);
-    profile_pass(ev0, profile_mark(s), "sgm_path_ranged_kernel", shape, static_cast<uint64_t>(seg.cells),
-                 static_cast<uint64_t>(seg.pixels), alg + 16 * static_cast<uint64_t>(seg.pixels));
+    profile_pass(ev0, profile_mark(s), "sgm_path_ranged_kernel", shape, n * static_cast<uint64_t>(seg.cells),
+                 n * static_cast<uint64_t>(seg.pixels), n * (alg + 16 * static_cast<uint64_t>(seg.pixels)));
   }
 }
 
@@ -1519,25 +1534,27 @@ template <int G, int K>
 void launch_ranged_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegment& g, const int4* rec,
                           const uint8_t* cost, uint16_t* sum, uint8_t* terms, int64_t tstride, uint32_t* ovf,
                           int64_t ovf_words, int sms, cudaStream_t s, const int* cancel) {
+  for (int q = 0; q < 8; ++q)
+    if (g.blocks[kPasses[q].cls] <= 0) return;  // no pixels: every class has chains otherwise
+  if (terms != nullptr) {
+    // Byte terms: the seven term passes in one launch, then the last pass
+    // (the total sum).
+    const int qs[kTermArrays] = {0, 1, 2, 3, 4, 5, 6};
+    const int last = 7;
+    launch_ranged_pass<G, K, kTerm>(pass_set(g, qs, kTermArrays), dm, jobs, g.count, rec, cost, sum, terms, tstride,
+                                    ovf, ovf_words, sms, s, g, cancel);
+    launch_ranged_pass<G, K, kLastTerm>(pass_set(g, &last, 1), dm, jobs, g.count, rec, cost, sum, terms, tstride, ovf,
+                                        ovf_words, sms, s, g, cancel);
+    return;
+  }
   for (int q = 0; q < 8; ++q) {
-    const Pass ps = kPasses[q];
-    const int64_t nb = g.blocks[ps.cls];
-    if (nb <= 0) continue;
-    if (terms != nullptr) {
-      // Byte terms: passes 1..7 write T_r, the last writes the total sum.
-      if (q < 7)
-        launch_ranged_pass<G, K, kTerm>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, q, ovf, ovf_words,
-                                        sms, s, g, cancel);
-      else
-        launch_ranged_pass<G, K, kLastTerm>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, 0, ovf,
-                                            ovf_words, sms, s, g, cancel);
-    } else if (q == 0) {
-      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, 0, ovf, ovf_words,
-                                       sms, s, g, cancel);
-    } else {
-      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, nb, rec, cost, sum, terms, tstride, 0, ovf,
-                                            ovf_words, sms, s, g, cancel);
-    }
+    const PassSet ps = pass_set(g, &q, 1);
+    if (q == 0)
+      launch_ranged_pass<G, K, kFirst>(ps, dm, jobs, g.count, rec, cost, sum, terms, tstride, ovf, ovf_words, sms, s,
+                                       g, cancel);
+    else
+      launch_ranged_pass<G, K, kAccumulate>(ps, dm, jobs, g.count, rec, cost, sum, terms, tstride, ovf, ovf_words, sms,
+                                            s, g, cancel);
   }
 }
 
