@@ -1,18 +1,20 @@
 """Autotuner for the SGM launch shapes: measures candidates on the GPU and
 writes the table that the library reads (regard3d_mvs_b200/csrc/tuning.h).
 
-The objective is the SGM stage time (fork to join of every round, from the
-library's CUDA-event profile) of a mixed batch drawn like the batched
-workload: pairs of uneven size (width log-uniform in 1024..6048), label
-counts from {64, 128, 192, 256, 384}, half of them hierarchical. The search
-is coordinate-wise, largest label count first: the chain passes' shape
-(lanes per chain G, label pairs per lane K; rows of up to 1.5x the label
-count) for each label count; with --plain also the one-CTA-per-tile kernels'
-shapes and band rows, the ranged kernel's band rows per label width and the
-share of wide pixels a tile may keep. A candidate replaces the current entry
-when it shortens the stage by more than 1 %; the table is written only where
-it beats the built-in defaults on the same batch, and entries of the kinds
-not searched are kept from the existing table.
+The chain passes' shape (lanes per chain G, label pairs per lane K; rows of
+up to 1.5x the label count) is chosen per label count in isolation: the SGM
+stage time (fork to join, from the library's CUDA-event profile) of a batch
+of four single-level pairs (1536..4096 wide, 4:3) of that label count, the
+minimum of three runs per candidate, the built-in default measured before and
+after the candidates; a candidate wins when it beats the default by more
+than 3 %. With --plain the one-CTA-per-tile kernels' shapes and band rows,
+the ranged kernel's band rows per label width and the share of wide pixels a
+tile may keep are searched coordinate-wise on a mixed batch drawn like the
+batched workload (pairs of uneven size, label counts from {64, 128, 192,
+256, 384}, half of them hierarchical), a candidate replacing the current
+entry when it shortens the stage by more than 1 %. The table is written only
+where it beats the built-in defaults, and entries of the kinds not searched
+are kept from the existing table.
 
     python -m regard3d_mvs_b200.autotune [--out regard3d_mvs_b200/tuning_b200.txt] [--pairs 24] [--plain]
 """
@@ -114,23 +116,32 @@ def main():
                 body = ln.split("#", 1)[0].strip()
                 if body and body.split()[0] not in searched:
                     kept.append(body)
-    bench = Bench(mixed_specs(args.pairs, args.seed), seed=args.seed)
-    bench.stage_ms(kept, reps=1)  # allocations
-    base = bench.stage_ms(kept, reps=3)
-    print(f"defaults: {base:.1f} ms", flush=True)
     entries: dict[str, str] = {}
 
     def table(extra=None):
         return kept + list({**entries, **(extra or {})}.values())
 
-    best = base
+    summary = []
     for nd in FULL_ND:
+        iso = Bench([(w, (w * 3) // 4, nd, StereoOptions(levels=0)) for w in (1536, 2048, 3072, 4096)],
+                    seed=args.seed + nd)
+        iso.stage_ms(kept, reps=1)  # allocations
+        base = iso.stage_ms(kept, reps=3)
+        best, pick = base, None
         for g, k in (s for s in PATH_SHAPES if nd <= 2 * s[0] * s[1] <= 1.5 * nd):
             entry = f"path {nd} {g} {k}"
-            ms = bench.stage_ms(table({f"p{nd}": entry}))
-            print(f"{entry}: {ms:.1f} ms", flush=True)
-            if ms < best * 0.99:
-                best, entries[f"p{nd}"] = ms, entry
+            ms = iso.stage_ms(kept + [entry], reps=3)
+            print(f"{entry}: {ms:.1f} ms (default {base:.1f} ms)", flush=True)
+            if ms < best:
+                best, pick = ms, entry
+        base = min(base, iso.stage_ms(kept, reps=3))
+        if pick is not None and best < 0.97 * base:
+            entries[f"p{nd}"] = pick
+        summary.append(f"{nd} labels: default {base:.1f} ms, {pick or '-'} {best:.1f} ms")
+        del iso
+    bench = Bench(mixed_specs(args.pairs, args.seed), seed=args.seed)
+    bench.stage_ms(kept, reps=1)  # allocations
+    best = bench.stage_ms(table(), reps=3)
     if args.plain:
         for nd in FULL_ND:
             for g, k in (s for s in FULL_SHAPES if nd <= 2 * s[0] * s[1] <= 1.5 * nd):
@@ -163,6 +174,8 @@ def main():
         f.write(f"# SGM launch shapes chosen by regard3d_mvs_b200/autotune.py on {name} ({time.time() - t0:.0f} s):\n")
         f.write(f"# SGM stage of a {args.pairs}-pair mixed batch: defaults {check_base:.1f} ms, "
                 f"this table {check_tuned:.1f} ms{verdict}\n")
+        for ln in summary:
+            f.write(f"# chain passes, 4 single-level pairs of {ln}\n")
         f.write("# fields: path <nd> <G> <K> | full <nd> <G> <K> <rows> | ranged <width> <rows> | "
                 "ranged_wide_frac <f> | ranged_general_width <w>\n")
         for ln in keep:

@@ -1363,7 +1363,12 @@ std::string track_key(const std::vector<r3dgpu_pair>& fp) {
   k.append(reinterpret_cast<const char*>(&c), sizeof(c));
   k.append(reinterpret_cast<const char*>(&t_device), sizeof(t_device));
   k.append(reinterpret_cast<const char*>(&t_scratch_budget), sizeof(t_scratch_budget));
-  for (const char* name : {"R3DGPU_FULL_KERNEL", "R3DGPU_RANGED_KERNEL", "R3DGPU_RANGED_GENERAL_WIDTH"}) {
+  // Every environment setting that selects kernels or launch shapes (a
+  // captured graph replays the launches it was captured with).
+  for (const char* name :
+       {"R3DGPU_FULL_KERNEL", "R3DGPU_RANGED_KERNEL", "R3DGPU_RANGED_GENERAL_WIDTH", "R3DGPU_TUNING",
+        "R3DGPU_TUNING_FILE", "R3DGPU_PATH_SHAPE", "R3DGPU_RANGED_TERMS", "R3DGPU_FULL_ROWS", "R3DGPU_FULL_SHAPE",
+        "R3DGPU_RANGED_ROWS", "R3DGPU_RANGED_SHAPE", "R3DGPU_RANGED_WIDE_FRAC"}) {
     const char* v = std::getenv(name);
     k += v != nullptr ? v : "";
     k += '\n';

@@ -31,6 +31,42 @@ def _assert_same_map(a, b):
     assert a.num_disparities == b.num_disparities
 
 
+@pytest.mark.parametrize("shape,nd", [("1,8", 16), ("2,8", 32), ("2,16", 48), ("4,8", 64), ("4,12", 96),
+                                      ("4,16", 128), ("8,8", 112), ("8,12", 192), ("8,16", 208), ("16,8", 256),
+                                      ("16,12", 384), ("16,16", 512), ("32,8", 512), ("32,12", 768)])
+@pytest.mark.parametrize("p2", [120, 8000])
+def test_volume_chain_shapes(gpu_matcher, oracle, monkeypatch, shape, nd, p2):
+    """Every compiled chain-pass shape (lanes per chain, label pairs per lane)
+    against the textbook volume, with byte terms (P2 <= 255, intensity-adapted
+    penalties) and with u16 sums (P2 = 8000: sums that wrap)."""
+    monkeypatch.setenv("R3DGPU_PATH_SHAPE", shape)
+    tex = Texture(19)
+    left, right, _ = render_pair(tex, 70, 37, lambda x, y: 7.0 + 0.2 * x)
+    o = StereoOptions(p1=20, p2=p2, p2_adapt=0 if p2 > 255 else 6, invalid_cost=40)
+    assert np.array_equal(gpu_matcher.sgm_cost_volume(left, right, -1, nd, o),
+                          oracle.sgm_cost_volume(left, right, -1, nd, o))
+
+
+@pytest.mark.parametrize("terms", ["0", "1"])
+def test_ranged_term_modes(gpu_matcher, oracle, monkeypatch, terms):
+    """Per-pixel ranges through the chain passes with u16 sums and with byte
+    terms (R3DGPU_RANGED_TERMS): a volume and a hierarchical match."""
+    monkeypatch.setenv("R3DGPU_RANGED_TERMS", terms)
+    tex = Texture(29)
+    w, h, nd = 67, 41, 112
+    left, right, _ = render_pair(tex, w, h, lambda x, y: 25.0 + 0.4 * x - 0.2 * y)
+    r = Rng(37)
+    num = np.array([[16 * r.uniform_int(1, 5) for _ in range(w)] for _ in range(h)], np.uint16)
+    lo = np.array([[r.uniform_int(0, nd - int(n)) for n in row] for row in num], np.uint16)
+    o = StereoOptions(p2=140, p2_adapt=5)
+    assert np.array_equal(gpu_matcher.sgm_cost_volume(left, right, 1, nd, o, LabelRanges(lo, num)),
+                          oracle.sgm_cost_volume(left, right, 1, nd, o, (lo, num)))
+    left, right, _ = render_pair(tex, 240, 128, lambda x, y: np.where(x < 100, 9.0, 21.0))
+    o = StereoOptions(levels=2, tile_size=96, tile_margin=8, tile_blend=8, range_radius=1)
+    _assert_same_map(gpu_matcher.match_stereo(left, right, None, None, 0, 48, o),
+                     oracle.match_stereo(left, right, None, None, 0, 48, o))
+
+
 def test_census(gpu_matcher, oracle):
     for w in (1, 5, 16, 31, 64, 77, 640):
         img = random_image(w, 13, w)
