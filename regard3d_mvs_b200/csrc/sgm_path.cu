@@ -203,6 +203,7 @@ constexpr int kTermArrays = 7;
 // from start[q] (start[n] = all blocks), slot = its term array.
 struct PassSet {
   int n;
+  uint32_t one;  // 1 (see fma_add)
   int cls[kTermArrays], dx[kTermArrays], dy[kTermArrays], slot[kTermArrays];
   int64_t start[kTermArrays + 1];
 };
@@ -210,6 +211,11 @@ constexpr int kPathStages = 4;  // ring stages of the ranged passes
 
 // Per-halfword a + b modulo 2^16.
 R3D_DEVICE uint32_t add2(uint32_t a, uint32_t b, bool no_carry) { return no_carry ? a + b : r3dsimt::vadd2(a, b); }
+
+// a * one + b with one = 1 at run time: an integer multiply-add, which the
+// FMA pipe executes, in place of an add on the ALU pipe (the pass kernels'
+// packed min, byte permutes and adds keep the ALU pipe the busier one).
+R3D_DEVICE uint32_t fma_add(uint32_t a, uint32_t one, uint32_t b) { return a * one + b; }
 
 // v[j] for a runtime j in [0, K): a tree of K - 1 selects on the bits of j
 // (a register array cannot be indexed at run time without local memory).
@@ -305,6 +311,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? (MODE == kTerm ? 4
   unsigned char* const ring_term = ring + CPW * Ring::ND + gi * Ring::ND + e0;  // + r * CPW * ND
   unsigned char* const ring_int = ring + Ring::kPlaneBytes + lane * 4;
   const int64_t total_blocks = ps.start[ps.n];
+  const uint32_t one = ps.one;
   for (int64_t gblk = static_cast<int64_t>(blockIdx.x) * wpb + (threadIdx.x >> 5); gblk < total_blocks;
        gblk += nwarps) {
     if (cancelled(cancel)) break;
@@ -465,8 +472,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? (MODE == kTerm ? 4
         const uint32_t mnext = r3dsimt::perm(wv[k + 1], wv[k + 2], 0x5432u);
         const uint32_t nb = r3dsimt::vmin2(mprev, mnext);
         const uint32_t best = r3dsimt::vmin2(wv[k + 1], r3dsimt::vaddmin2(nb, p1x2, pen2));
-        tr[k] = best + negmp;
-        out[k] = tr[k] + c2[k];
+        tr[k] = fma_add(best, one, negmp);
+        out[k] = fma_add(tr[k], one, c2[k]);
         mprev = mnext;
       }
       // Minimum over the lane's labels (a tree), then over the chain's lanes.
@@ -534,10 +541,10 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(kPathThreads, (K <= 8 ? (MODE == kTerm ? 4
           }
 #pragma unroll
           for (int u = 0; u < U; ++u) {
-            s[4 * u + 0] += r3dsimt::perm(tw[u].x, 0u, 0x4140u);
-            s[4 * u + 1] += r3dsimt::perm(tw[u].x, 0u, 0x4342u);
-            s[4 * u + 2] += r3dsimt::perm(tw[u].y, 0u, 0x4140u);
-            s[4 * u + 3] += r3dsimt::perm(tw[u].y, 0u, 0x4342u);
+            s[4 * u + 0] = fma_add(r3dsimt::perm(tw[u].x, 0u, 0x4140u), one, s[4 * u + 0]);
+            s[4 * u + 1] = fma_add(r3dsimt::perm(tw[u].x, 0u, 0x4342u), one, s[4 * u + 1]);
+            s[4 * u + 2] = fma_add(r3dsimt::perm(tw[u].y, 0u, 0x4140u), one, s[4 * u + 2]);
+            s[4 * u + 3] = fma_add(r3dsimt::perm(tw[u].y, 0u, 0x4342u), one, s[4 * u + 3]);
           }
         }
       } else {
@@ -914,6 +921,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kRangedThreads)
     else ovfc[b * ovf_words + (idx - kRangedSmemWords)] = v;
   };
   const int64_t total_blocks = ps.start[ps.n];
+  const uint32_t one = ps.one;
   for (int64_t gblk = static_cast<int64_t>(blockIdx.x) * wpb + warp; gblk < total_blocks; gblk += nwarps) {
     if (cancelled(cancel)) break;
     // The pass of the block (static indices only: no local copy of ps).
@@ -1053,10 +1061,10 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kRangedThreads)
               for (int r = 0; r < kTermArrays; ++r) {
                 const uint2 tw = c == 0 ? *reinterpret_cast<const uint2*>(stage_term(i & (D - 1), r) + 8 * u)
                                         : *reinterpret_cast<const uint2*>(tbase + r * tstride + off + j0 + 8 * u);
-                tsum[4 * u + 0] += r3dsimt::perm(tw.x, 0u, 0x4140u);
-                tsum[4 * u + 1] += r3dsimt::perm(tw.x, 0u, 0x4342u);
-                tsum[4 * u + 2] += r3dsimt::perm(tw.y, 0u, 0x4140u);
-                tsum[4 * u + 3] += r3dsimt::perm(tw.y, 0u, 0x4342u);
+                tsum[4 * u + 0] = fma_add(r3dsimt::perm(tw.x, 0u, 0x4140u), one, tsum[4 * u + 0]);
+                tsum[4 * u + 1] = fma_add(r3dsimt::perm(tw.x, 0u, 0x4342u), one, tsum[4 * u + 1]);
+                tsum[4 * u + 2] = fma_add(r3dsimt::perm(tw.y, 0u, 0x4140u), one, tsum[4 * u + 2]);
+                tsum[4 * u + 3] = fma_add(r3dsimt::perm(tw.y, 0u, 0x4342u), one, tsum[4 * u + 3]);
               }
             }
           }
@@ -1099,8 +1107,8 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS(kRangedThreads)
             const uint32_t mnext = r3dsimt::perm(wv[k + 1], wv[k + 2], 0x5432u);
             const uint32_t nb = r3dsimt::vmin2(mprev, mnext);
             const uint32_t best = r3dsimt::vmin2(wv[k + 1], r3dsimt::vaddmin2(nb, p1x2, pen2));
-            tr[k] = best + negmp;
-            out[k] = tr[k] + c2[k];
+            tr[k] = fma_add(best, one, negmp);
+            out[k] = fma_add(tr[k], one, c2[k]);
             mprev = mnext;
           }
         }
@@ -1318,6 +1326,7 @@ void launch_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, 
 // Passes q of kPasses in `qs` (count n) as one PassSet.
 PassSet pass_set(const SgmPathSegment& g, const int* qs, int n) {
   PassSet ps{};
+  ps.one = 1;
   int64_t start = 0;
   for (int i = 0; i < n; ++i) {
     const Pass& p = kPasses[qs[i]];
