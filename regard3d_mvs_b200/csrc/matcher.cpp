@@ -810,17 +810,6 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     int64_t cells, px, keys, rows;
     int maxnum;
   };
-  // Waves keep byte terms when every match of the group allows them (all
-  // P2 <= 255); otherwise u16 sums only. Ranged waves use byte terms only
-  // with R3DGPU_RANGED_TERMS=1: their packed rows measured slower with the
-  // larger buffers (more waves) and the eight-plane ring of the last pass.
-  const char* rt = std::getenv("R3DGPU_RANGED_TERMS");
-  bool terms = !ranged || (rt != nullptr && std::atoi(rt) == 1);
-  for (const auto& mt : tiles) terms = terms && matches[mt.first]->m.term_u8 != 0;
-  auto bytes = [&](int64_t cells, int64_t px, int64_t keys, int64_t rows, int maxnum) -> size_t {
-    return ranged ? sgm_path_ranged_buffers(cells, px, keys, rows, maxnum, sms, terms).total
-                  : sgm_path_buffers(cells, px, keys, terms).total;
-  };
   std::vector<Entry> es;
   es.reserve(tiles.size());
   for (const auto& mt : tiles) {
@@ -832,6 +821,35 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
                        M.m.diagonal_lr ? static_cast<int64_t>(T.h) * (T.w + M.m.nd) : 0, T.h,
                        M.tile_maxnum[mt.second]});
   }
+  // Waves keep byte terms when every match of the group allows them (all
+  // P2 <= 255); otherwise u16 sums only. Ranged groups take byte terms when
+  // all their tiles fit one wave with them (10 bytes per cell held against
+  // 3): a single hierarchical pair's level runs about twice as fast, while
+  // a large batch level split into more waves measured no faster beside the
+  // single-level track. R3DGPU_RANGED_TERMS=0 or 1 forces either.
+  bool terms = true;
+  for (const auto& mt : tiles) terms = terms && matches[mt.first]->m.term_u8 != 0;
+  if (ranged && terms) {
+    const char* rt = std::getenv("R3DGPU_RANGED_TERMS");
+    if (rt != nullptr && *rt != '\0') {
+      terms = std::atoi(rt) == 1;
+    } else {
+      int64_t c = 0, p = 0, k = 0, r = 0;
+      int mx = 16;
+      for (const Entry& e : es) {
+        c += e.cells;
+        p += e.px;
+        k += e.keys;
+        r += e.rows;
+        mx = std::max(mx, e.maxnum);
+      }
+      terms = sgm_path_ranged_buffers(c, p, k, r, mx, sms, true).total <= cap_bytes;
+    }
+  }
+  auto bytes = [&](int64_t cells, int64_t px, int64_t keys, int64_t rows, int maxnum) -> size_t {
+    return ranged ? sgm_path_ranged_buffers(cells, px, keys, rows, maxnum, sms, terms).total
+                  : sgm_path_buffers(cells, px, keys, terms).total;
+  };
   std::stable_sort(es.begin(), es.end(),
                    [](const Entry& a, const Entry& b) { return a.sh.g_ * a.sh.k_ < b.sh.g_ * b.sh.k_; });
   max_bytes = 0;
