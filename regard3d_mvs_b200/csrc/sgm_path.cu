@@ -244,19 +244,24 @@ R3D_DEVICE uint32_t pick(const uint32_t (&v)[K], int j) {
 // The term passes read one byte per label and keep 8 stages in flight (their
 // step is short, so 3 stages ahead left them waiting on DRAM).
 // The last pass with byte terms stages eight byte planes per pixel: two
-// stages (its step is long, one pixel ahead covers the DRAM latency) in
-// 4-warp CTAs, so that more warps fit an SM's shared memory.
+// stages (its step is long, one pixel ahead covers the DRAM latency).
 template <int MODE>
 struct PathMode {
   static constexpr int kPlanes = MODE == kAccumulate || MODE == kLast ? 3 : (MODE == kLastTerm ? 1 + kTermArrays : 1);
   static constexpr int kStages = MODE == kLastTerm ? 2 : (MODE == kTerm ? 8 : 4);
-  static constexpr int kThreads = MODE == kLastTerm ? 128 : kPathThreads;
 };
 // A stage ends with one 4-byte word per lane: the aligned word of the
 // intensities that holds its chain's pixel (every lane copies its own, since
 // a cp.async wait covers only the waiting thread's copies).
+// CTA size and resident CTAs per SM: 4-warp CTAs for the byte-term last
+// pass (its eight-plane ring) and the 12- and 16-word term passes (96
+// registers), so that CTAs pack an SM's registers and shared memory finely.
 template <int G, int K, int MODE>
 struct PathRing {
+  static constexpr int kThreads = (MODE == kLastTerm || (MODE == kTerm && K >= 12)) ? 128 : kPathThreads;
+  static constexpr int kMinBlocks = MODE == kLastTerm ? (K <= 8 ? 6 : 3)
+                                    : MODE == kTerm   ? (K <= 8 ? 4 : 5)
+                                                      : (K <= 8 ? 3 : 2);
   static constexpr int ND = 2 * G * K;
   static constexpr int kStages = PathMode<MODE>::kStages;
   static constexpr int kPlaneBytes = (32 / G) * PathMode<MODE>::kPlanes * ND;
@@ -264,12 +269,13 @@ struct PathRing {
   static constexpr int kStageBytes = kPlaneBytes + kIntBytes;
   static constexpr int kWarpBytes = kStages * kStageBytes;
   // Each warp's rings, then each warp's copy of its match's P2 table.
-  static constexpr int kBlockBytes = (PathMode<MODE>::kThreads / 32) * (kWarpBytes + 512);
+  static constexpr int kBlockBytes = (kThreads / 32) * (kWarpBytes + 512);
 };
 
-// CTAs per SM: four for the 8-word term passes (64 registers, no spills),
-// three for the other 8-word passes (up to 80), two for the 12- and 16-word
-// shapes; the last pass with byte terms runs 4-warp CTAs, six or three.
+// CTAs per SM (PathRing): four 8-warp CTAs for the 8-word term passes (64
+// registers, no spills), five 4-warp CTAs for the 12- and 16-word ones;
+// six or three 4-warp CTAs for the byte-term last pass; three or two 8-warp
+// CTAs for the u16-sum passes.
 //
 // The step loop is unrolled by the ring depth NS so that ring slots and the
 // intensity queue are indexed statically; each chain keeps running pointers
@@ -281,8 +287,7 @@ struct PathRing {
 // passes of a segment at once (they only read the costs and each writes its
 // own term array, so their chain blocks can be taken in any order).
 template <int G, int K, int MODE>
-R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN(PathMode<MODE>::kThreads,
-                                     (MODE == kLastTerm ? (K <= 8 ? 6 : 3) : (K <= 8 ? (MODE == kTerm ? 4 : 3) : 2)))
+R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN((PathRing<G, K, MODE>::kThreads), (PathRing<G, K, MODE>::kMinBlocks))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
                     const PassSet ps, const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint8_t* terms,
                     int64_t tstride, int4* R3D_RESTRICT info, uint32_t* rkeys, const uint16_t* R3D_RESTRICT ints,
@@ -1316,7 +1321,7 @@ void launch_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, 
     configured[dev] = 1;
   }
   const int64_t nb = ps.start[ps.n];
-  constexpr int threads = PathMode<MODE>::kThreads;
+  constexpr int threads = PathRing<G, K, MODE>::kThreads;
   R3D_LAUNCH(k, dim3(resident_grid(k, sms, nb, threads / 32, smem, threads)), dim3(threads), smem, s, dm, jobs, njobs,
              ps, cost, sum, terms, tstride, info, rkeys, ints, cancel);
   launched("sgm_path_kernel");
