@@ -872,7 +872,10 @@ template <int G, int K, int MODE>
 struct RangedRing {
   static constexpr int CH = 2 * G * K;  // labels per chunk
   static constexpr int CPW = 32 / G;
-  static constexpr int D = MODE == kLastTerm ? 2 : kPathStages;
+  // Two stages for the passes that stage several planes (the accumulate
+  // pass: cost and sum; the byte-term last pass: eight planes), four for
+  // the one-plane passes: less shared memory per warp, more warps per SM.
+  static constexpr int D = MODE == kLastTerm || MODE == kAccumulate ? 2 : kPathStages;
   static constexpr int kPlanes = MODE == kAccumulate ? 3 : (MODE == kLastTerm ? 1 + kTermArrays : 1);
   static constexpr int kDataStage = CPW * kPlanes * CH;
   static constexpr int kData = D * kDataStage;
@@ -1516,7 +1519,7 @@ namespace {
 
 // Largest number of resident CTAs per SM any ranged pass kernel is launched
 // with (the overflow has one slot per resident chain).
-constexpr int kRangedMaxPerSm = 4;
+constexpr int kRangedMaxPerSm = 6;
 
 template <int G, int K, int MODE>
 void launch_ranged_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, const int4* rec,
