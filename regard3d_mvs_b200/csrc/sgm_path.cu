@@ -254,13 +254,14 @@ struct PathMode {
 // intensities that holds its chain's pixel (every lane copies its own, since
 // a cp.async wait covers only the waiting thread's copies).
 // CTA size and resident CTAs per SM: 4-warp CTAs for the byte-term last
-// pass (its eight-plane ring) and the 12- and 16-word term passes (96
-// registers), so that CTAs pack an SM's registers and shared memory finely.
+// pass (its eight-plane ring) and the 16-word term passes (92 registers),
+// so that CTAs pack an SM's registers and shared memory finely (the 12-word
+// term passes measured 12-19 % slower that way than in two 8-warp CTAs).
 template <int G, int K, int MODE>
 struct PathRing {
-  static constexpr int kThreads = (MODE == kLastTerm || (MODE == kTerm && K >= 12)) ? 128 : kPathThreads;
+  static constexpr int kThreads = (MODE == kLastTerm || (MODE == kTerm && K >= 16)) ? 128 : kPathThreads;
   static constexpr int kMinBlocks = MODE == kLastTerm ? (K <= 8 ? 6 : 3)
-                                    : MODE == kTerm   ? (K <= 8 ? 4 : 5)
+                                    : MODE == kTerm   ? (K <= 8 ? 4 : (K >= 16 ? 5 : 2))
                                                       : (K <= 8 ? 3 : 2);
   static constexpr int ND = 2 * G * K;
   static constexpr int kStages = PathMode<MODE>::kStages;
@@ -273,9 +274,9 @@ struct PathRing {
 };
 
 // CTAs per SM (PathRing): four 8-warp CTAs for the 8-word term passes (64
-// registers, no spills), five 4-warp CTAs for the 12- and 16-word ones;
-// six or three 4-warp CTAs for the byte-term last pass; three or two 8-warp
-// CTAs for the u16-sum passes.
+// registers, no spills), two for the 12-word ones, five 4-warp CTAs for the
+// 16-word ones; six or three 4-warp CTAs for the byte-term last pass; three
+// or two 8-warp CTAs for the u16-sum passes.
 //
 // The step loop is unrolled by the ring depth NS so that ring slots and the
 // intensity queue are indexed statically; each chain keeps running pointers
