@@ -73,7 +73,7 @@ def parse():
                     help="skip the one-pair-per-call run with the one-CTA-per-tile kernels")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serve", dest="serve", action="store_false",
-                    help="skip the serving sweep (config 3), which runs in a fresh process after the batch")
+                    help="skip the serving sweep, which runs in a fresh process after the batch")
     ap.add_argument("--serve-only", type=float, default=0.0, metavar="PAIRS_PER_S",
                     help="run only the serving sweep (its saturation run offers 3 x this batch rate); print its JSON")
     ap.add_argument("--serve-seconds", type=float, default=8.0, help="arrival window per load point")
@@ -93,7 +93,7 @@ def workload_pairs(name: str, npairs: int, seed: int):
         # a working set of several times the L2 and under 2 GB of device memory).
         return [dict(w=1024, h=768, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
     if name == "pair2048":
-        # One full-range pair of a config-4 view's size (profiling case of the pass kernels).
+        # One full-range 2048x1536 pair, the size of a depth-stage view (profiling case of the pass kernels).
         return [dict(w=2048, h=1536, nd=128, levels=0, radius=3, margin=4, textureless=0.0, occluded=0.0, seed=seed)]
     if name == "pair3072":
         return [dict(w=3072, h=2048, nd=256, levels=3, radius=0, margin=8, textureless=0.15, occluded=0.10,
@@ -514,7 +514,7 @@ def measure_rectify(lib, dev, stream, steps: int, warmup: int, peak: float) -> d
                              "kind": "port", "sample": "one image of the pair, once"}}
 
 
-# Depth stage after the combination (config 4's refinement and consistency):
+# Depth stage after the combination (refinement and consistency):
 # 8 views of 2048 x 1536, each refined against its 4 nearest views with a
 # 7 x 7 window (radius 3, step 1), then one consistency filter of all 8 maps
 # (4 neighbours each). Algorithmic bytes per view: its refinement image and
@@ -802,7 +802,7 @@ def measure_view(lib, dev, stream, steps: int, warmup: int) -> dict:
                              "sample": "the same view once: rectify, match_stereo and combine_pairs of the oracle"}}
 
 
-# Config 4: the full depth stage of a 32-view scene (2048 x 1536 views on an
+# The full depth stage of a 32-view scene (2048 x 1536 views on an
 # arc of radius 2 m around 20 textured planes, 4 nearest partners per view).
 SCENE_VIEWS, SCENE_W, SCENE_H, SCENE_SEED = 32, 2048, 1536, 11
 SCENE_CHECK_VIEW = 16  # compared with the oracle's chain (a central view)
@@ -821,7 +821,7 @@ def _scene_env(plain: bool):
 
 
 def measure_scene(lib, dev, stream, steps: int, warmup: int) -> dict:
-    """Config 4 end to end on the device: per view compute_depth_map
+    """The 32-view depth stage end to end on the device: per view compute_depth_map
     (rectification of both images of its 4 pairs, one batch match,
     combination), then the float refinement of every view against its
     partners' refinement images and the consistency filter of the 32 maps;
@@ -1036,7 +1036,7 @@ def measure_scene(lib, dev, stream, steps: int, warmup: int) -> dict:
     both = (g32["depth"] > 0) & (o64["depth"] > 0)
     rel = np.abs(g32["depth"][both].astype(np.float64) - o64["depth"][both]) / o64["depth"][both]
     flips = int(((g32["depth"] > 0) != (o64["depth"] > 0)).sum())
-    return {"workload": f"config 4: {n} views {w}x{h} on an arc of radius 2 m around 20 textured planes, 4 partners "
+    return {"workload": f"depth stage: {n} views {w}x{h} on an arc of radius 2 m around 20 textured planes, 4 partners "
                         "per view: rectify + match (reference defaults, one batch per view) + combine, FP32 7x7 "
                         "refinement against the 4 partners, consistency over 4 neighbours; views on "
                         f"{SCENE_THREADS} host threads with a CUDA stream each",
@@ -1062,7 +1062,7 @@ def measure_scene(lib, dev, stream, steps: int, warmup: int) -> dict:
 
 
 SERVE_FRACTIONS = (0.1, 0.5, 0.8, 1.0, 1.2)
-SERVE_REQUEST_BUDGET = 110 << 30  # config 3's 150 GB: 110 GB for admitted requests, 2 x 16 GB worker scratch, 8 GB cache
+SERVE_REQUEST_BUDGET = 110 << 30  # of a 150 GB serving budget: 110 GB for admitted requests, 2 x 16 GB worker scratch, 8 GB cache
 SERVE_CACHE = 8 << 30
 SERVE_WORKERS = 2
 SERVE_MAX_BATCH = 16
@@ -1073,7 +1073,7 @@ SERVE_PARTNERS = 4
 
 def serving_views(lib, n: int, seed: int) -> list[dict]:
     """Distinct views of the serving simulation: sizes, label ranges and
-    hierarchy as config 2 draws them per pair; each view's 4 partner pairs
+    hierarchy as the 64-pair batch draws them per pair; each view's 4 partner pairs
     share its left image (the generator's left image depends on the seed,
     size and label count only) and differ in the disparity field (plane
     count), so their right images differ."""
@@ -1097,7 +1097,7 @@ def serving_views(lib, n: int, seed: int) -> list[dict]:
 
 
 def run_serving(args, rate_hint: float) -> dict:
-    """Config 3: a simulated 200-view scene, each view issuing its 4 partner
+    """Serving: a simulated 200-view scene, each view issuing its 4 partner
     pair requests (Poisson arrivals of requests), through the serving loop
     (continuous batching, admission by a device-memory budget, a view's left
     image uploaded once and kept on the device across its partners by its
@@ -1188,7 +1188,7 @@ def run_serving(args, rate_hint: float) -> dict:
             pt["load"] = frac
             points.append(pt)
     return {"scene": f"{SERVE_SCENE_VIEWS} views x {SERVE_PARTNERS} partner pairs (images of {SERVE_POOL_VIEWS} "
-                     "distinct config-2 views; each view's pairs share its left image under the view's content key)",
+                     "distinct views drawn like the 64-pair batch; each view's pairs share its left image under the view's content key)",
             "saturated_pairs_per_s": sat_rate, "saturation_run": sat,
             "load_axis": "fraction of the served saturation measured above", "workers": args.serve_workers,
             "max_batch": args.serve_batch, "host_buffers": "page-locked inputs and disparity maps; no confidence maps",
@@ -1501,7 +1501,7 @@ def main():
 
             line["multi_view"] = extra(measure_combine, lib, dev, stream, args.steps, args.warmup, peak)
             line["rectify"] = extra(measure_rectify, lib, dev, stream, args.steps, args.warmup, peak)
-            # Config 4 end to end (the depth stage of a 32-view scene); the
+            # The depth stage of a 32-view scene end to end; the
             # separate depth-stage and one-view lines stay available as
             # --workload depth / view.
             line["scene32"] = extra(measure_scene, lib, dev, stream, 2, 1)

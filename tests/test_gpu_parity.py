@@ -349,7 +349,7 @@ def _bench_options(spec):
     return StereoOptions(levels=spec["levels"], range_radius=spec["radius"], range_margin=spec["margin"])
 
 
-def test_config1_pair_3072x2048_256_four_levels(gpu_matcher, oracle):
+def test_pair_3072x2048_256_four_levels(gpu_matcher, oracle):
     """3072x2048, labels 0..255, 15 % textureless patches, 10 % occluded right
     pixels, 4-level hierarchy with +-8 labels around the upsampled coarser
     disparity (range_radius 0, range_margin 8)."""
@@ -373,8 +373,9 @@ BATCH64_SEED = 2024
 BATCH64_SAMPLE = (63, 50, 48, 15)
 
 
-def test_config2_pairs_batched(gpu_matcher, oracle):
-    """Config-2 pairs matched together in one batch call, each against the
+def test_batch64_pairs_batched(gpu_matcher, oracle):
+    """Pairs of the 64-pair batch workload (up to 6048 wide, 384 labels)
+    matched together in one batch call, each against the
     oracle matching it alone."""
     import bench
 
