@@ -882,11 +882,12 @@ void plan_path_waves(const std::vector<std::pair<int, int>>& tiles, const std::v
     for (int q = 0; q < n; ++q) {
       const Entry& e = es[begin + q];
       if (sg.empty() || sg.back().shape.g_ != e.sh.g_ || sg.back().shape.k_ != e.sh.k_)
-        sg.push_back(SgmPathSegment{e.sh, q, 0, {0, 0, 0}, 0, 0});
+        sg.push_back(SgmPathSegment{e.sh, q, 0, {0, 0, 0}, 0, 0, 1});
       SgmPathSegment& g = sg.back();
       g.cells += e.cells;
       g.pixels += e.px;
       Match& M = *matches[e.i];
+      g.full = g.full != 0 && !ranged && M.m.nd == 2 * e.sh.g_ * e.sh.k_ ? 1 : 0;
       const Tile& T = M.layout.tiles[e.t];
       SgmPathJob& J = hj[q];
       J = SgmPathJob{};

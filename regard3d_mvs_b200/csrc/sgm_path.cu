@@ -287,7 +287,7 @@ struct PathRing {
 // One launch runs the passes of a PassSet: a single pass, or the seven term
 // passes of a segment at once (they only read the costs and each writes its
 // own term array, so their chain blocks can be taken in any order).
-template <int G, int K, int MODE>
+template <int G, int K, int MODE, bool FULL>
 R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN((PathRing<G, K, MODE>::kThreads), (PathRing<G, K, MODE>::kMinBlocks))
     sgm_path_kernel(const SgmMatch* R3D_RESTRICT matches, const SgmPathJob* R3D_RESTRICT jobs, int njobs,
                     const PassSet ps, const uint8_t* R3D_RESTRICT cost, uint16_t* sum, uint8_t* terms,
@@ -359,7 +359,7 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN((PathRing<G, K, MODE>::kThreads), (PathRin
     for (int o = G; o < 32; o <<= 1) maxlen = r3dsimt::imax(maxlen, static_cast<int>(r3dsimt::shfl_xor(maxlen, o)));
     bool uvalid[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) uvalid[u] = e0 + 8 * u < nd;
+    for (int u = 0; u < U; ++u) uvalid[u] = FULL || e0 + 8 * u < nd;
     // Running offsets (cells, pixels) of the pixel being issued (NS - 1
     // ahead) and of the pixel being computed.
     const int64_t dcell = (static_cast<int64_t>(dy) * w + dx) * nd;
@@ -1310,12 +1310,12 @@ uint64_t pass_bytes(int mode, bool ranged, const SgmPathSegment& g) {
   return 5 * c;
 }
 
-template <int G, int K, int MODE>
+template <int G, int K, int MODE, bool FULL = false>
 void launch_pass(const PassSet& ps, const SgmMatch* dm, const SgmPathJob* jobs, int njobs, const uint8_t* cost,
                  uint16_t* sum, uint8_t* terms, int64_t tstride, int4* info, uint32_t* rkeys, const uint16_t* ints,
                  int sms, cudaStream_t s, const SgmPathSegment& seg, const int* cancel) {
   const cudaEvent_t ev0 = profile_on() ? profile_mark(s) : nullptr;
-  auto* k = sgm_path_kernel<G, K, MODE>;
+  auto* k = sgm_path_kernel<G, K, MODE, FULL>;
   constexpr size_t smem = PathRing<G, K, MODE>::kBlockBytes;
   static thread_local int configured[64] = {};
   int dev = 0;
@@ -1368,10 +1368,19 @@ void launch_passes(const SgmMatch* dm, const SgmPathJob* jobs, const SgmPathSegm
     // all seven term arrays written.
     const int qs[kTermArrays] = {0, 1, 2, 3, 4, 5, 6};
     const int last = 7;
-    launch_pass<G, K, kTerm>(pass_set(g, qs, kTermArrays), dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys,
-                             ints, sms, s, g, cancel);
-    launch_pass<G, K, kLastTerm>(pass_set(g, &last, 1), dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys,
-                                 ints, sms, s, g, cancel);
+    // Segments whose matches fill every label unit take the kernels without
+    // the per-unit validity selects.
+    if (g.full != 0) {
+      launch_pass<G, K, kTerm, true>(pass_set(g, qs, kTermArrays), dm, jobs, g.count, cost, sum, terms, tstride, info,
+                                     rkeys, ints, sms, s, g, cancel);
+      launch_pass<G, K, kLastTerm, true>(pass_set(g, &last, 1), dm, jobs, g.count, cost, sum, terms, tstride, info,
+                                         rkeys, ints, sms, s, g, cancel);
+    } else {
+      launch_pass<G, K, kTerm>(pass_set(g, qs, kTermArrays), dm, jobs, g.count, cost, sum, terms, tstride, info,
+                               rkeys, ints, sms, s, g, cancel);
+      launch_pass<G, K, kLastTerm>(pass_set(g, &last, 1), dm, jobs, g.count, cost, sum, terms, tstride, info, rkeys,
+                                   ints, sms, s, g, cancel);
+    }
     return;
   }
   for (int q = 0; q < 8; ++q) {

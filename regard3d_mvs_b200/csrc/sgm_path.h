@@ -66,6 +66,7 @@ struct SgmPathSegment {
   int first, count;
   int64_t blocks[kPathClasses];
   int64_t cells, pixels;  // of the segment's tiles (per-launch profiling)
+  int full = 0;           // every match of the segment has exactly 2 G K labels (no unit past nd)
 };
 
 // Per-launch timing of the pass kernels while the library's profiling is on
