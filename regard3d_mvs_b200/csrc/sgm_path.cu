@@ -430,17 +430,45 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN((PathRing<G, K, MODE>::kThreads), (PathRin
 #pragma unroll
     for (int k = 0; k < K; ++k) prev[k] = 0;
     uint32_t pmin = 0;
-    // The previous pixel's intensity (the first step's P2 is unused: its
-    // predecessor vector is zero).
+    // Intensities and P2. With four stages or more, the next pixel's stage
+    // has landed when this pixel is computed, so the P2 of the step into the
+    // next pixel is looked up one step ahead, off the step's critical path
+    // (iprev is then this pixel's intensity); with two stages the P2 of the
+    // step into this pixel is looked up in its step (iprev is the previous
+    // pixel's intensity). The first step's P2 is unused: its predecessor
+    // vector is zero.
+    constexpr bool kAheadP2 = NS >= 4;
     int iprev = 0;
+    uint32_t p2next = 0;
+    if constexpr (kAheadP2) {
+      r3dsimt::cp_async_wait<NS - 2>();  // the first of the NS - 1 stages in flight
+      const uint32_t iw0 = *reinterpret_cast<const uint32_t*>(ring_int);
+      iprev = static_cast<int>((iw0 >> (16u * par0)) & 0xFFFFu);
+    }
 
     auto step = [&](const int i, const int q) {
       const bool on = i < len;
       constexpr int kNext = NS - 1;
       issue(i + kNext, (q + kNext) % NS);
-      r3dsimt::cp_async_wait<NS - 1>();
-      const uint32_t iw = *reinterpret_cast<const uint32_t*>(ring_int + q * Ring::kStageBytes);
-      const int icur = static_cast<int>((iw >> (16u * ((par0 ^ (static_cast<uint32_t>(i) & dpar)) & 1u))) & 0xFFFFu);
+      uint32_t pen;
+      if constexpr (kAheadP2) {
+        r3dsimt::cp_async_wait<NS - 2>();  // this pixel's stage and the next one's
+        const uint32_t iw = *reinterpret_cast<const uint32_t*>(ring_int + ((q + 1) % NS) * Ring::kStageBytes);
+        const int inext =
+            static_cast<int>((iw >> (16u * ((par0 ^ (static_cast<uint32_t>(i + 1) & dpar)) & 1u))) & 0xFFFFu);
+        pen = pmin + p2next;
+        const int dn = inext - iprev;
+        p2next = lut[(dn < 0 ? -dn : dn) >> 8];
+        iprev = inext;
+      } else {
+        r3dsimt::cp_async_wait<NS - 1>();
+        const uint32_t iw = *reinterpret_cast<const uint32_t*>(ring_int + q * Ring::kStageBytes);
+        const int icur =
+            static_cast<int>((iw >> (16u * ((par0 ^ (static_cast<uint32_t>(i) & dpar)) & 1u))) & 0xFFFFu);
+        const int dn = icur - iprev;
+        iprev = icur;
+        pen = pmin + lut[(dn < 0 ? -dn : dn) >> 8];
+      }
       const unsigned char* sc = ring_cost + q * Ring::kStageBytes;
       uint2 craw[U];
       if constexpr (kVec) {
@@ -464,9 +492,6 @@ R3D_GLOBAL void R3D_LAUNCH_BOUNDS_MIN((PathRing<G, K, MODE>::kThreads), (PathRin
         c2[4 * u + 3] = r3dsimt::perm(craw[u].y, 0u, 0x4342u);
       }
       // out = L_r = C + T_r with T_r = best - min L(q).
-      const int dn = icur - iprev;
-      iprev = icur;
-      const uint32_t pen = pmin + lut[(dn < 0 ? -dn : dn) >> 8];
       const uint32_t pen2 = pen * 0x10001u;
       const uint32_t negmp = pmin * 0xFFFEFFFFu;  // -(pmin in both halves) modulo 2^32
       const uint32_t hl = r3dsimt::shfl(prev[K - 1], left_lane);
